@@ -1,0 +1,321 @@
+#!/usr/bin/env python
+"""Benchmark of the Yee/CPML/ADE/TF-SF hot path on B200.
+
+Default workload: the large dispersive configuration -- 512^3 cells on a
+graded 1-3 mm mesh plus 12 CPML layers per face (536^3 swept cells), 30 % of
+the volume in 2-pair pole-residue blocks, a soft Ez dipole at the centre --
+built from seeded synthetic inputs.  A step is one whole leapfrog step (E
+half: curl + CPML + ADE + sources; H half: curl + CPML + sources; probe
+gather).  Metric: Gcell-updates/s = swept cells x steps / s.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun (N > 1) every rank runs an independent replica on its own GPU
+(the hot path is single-rank; "replicas only"), time is the max over ranks and
+value is the sum of the replicas' cell updates over that time.
+
+--impl reference times the reference algorithm's CPU implementation (the
+C++ restatement in oracle/, OpenMP over all host cores) on a bounded sample of
+the same workload; the Fortran reference itself cannot be built here.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Gcell-upd/s"
+CONFIGS = {
+    # name: (generator, kwargs, workload label)
+    "dispersive_large": ("dispersive_large", {}, "512^3 graded 1-3 mm, CPML 12 (536^3 swept), 30% 2-pair pole-residue, soft Ez dipole"),
+    "plain_mid": ("plain_mid", {}, "256^3 dx 5 mm, CPML 12, lossy sphere + 20 PEC/dielectric blocks, TF/SF plane wave"),
+    "plain_small": ("plain_small", {}, "64^3 dx 1 cm, CPML 10, TF/SF plane wave"),
+}
+CPU_SAMPLE_N = 160  # the reference arm and cpu_baseline run this scaled sample
+
+
+def env_rank():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+def make_case(config: str, n: int | None, steps_needed: int):
+    from semba_fdtd_b200 import casegen, read_case
+    gen, kw, label = CONFIGS[config]
+    kw = dict(kw)
+    if n is not None:
+        kw["n"] = n
+        if config == "dispersive_large":
+            kw["edge"] = (max(4, n // 16), max(8, n // 4))
+    d = Path(tempfile.mkdtemp(prefix="semba_bench_"))
+    path = getattr(casegen, gen)(d, **kw)
+    pb = read_case(path)
+    pb.nsteps = max(pb.nsteps, steps_needed)
+    return pb, label
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "100"], stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in Path(self.out.name).read_text().splitlines() if r.strip()]
+        except Exception:
+            rows = []
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[q] for r in rows for q in range(4) if len(r) > 5 + q and r[5 + q].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_hbm_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary."""
+    p = ROOT / "profiles" / "ncu_traffic.json"
+    try:
+        t = json.loads(p.read_text())
+        return t.get(kernel)
+    except Exception:
+        return None
+
+
+def cpu_oracle_rate(steps: int, threads: int | None = None, budget_s: float = 20.0):
+    """Gcell-upd/s of the oracle on a bounded sample (scaled dispersive case)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    pb, _ = make_case("dispersive_large", CPU_SAMPLE_N, steps + 2)
+    threads = threads or os.cpu_count() or 1
+    o = oracle.Oracle(pb, threads=threads)
+    o.step(1)  # warm-up step
+    t0 = time.perf_counter()
+    done = 0
+    while done < steps:
+        o.step(1)
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    rate = pb.swept_cells * done / dt / 1e9
+    o.close()
+    sample = f"dispersive case scaled to {CPU_SAMPLE_N}^3 (+CPML: {pb.swept_cells} swept cells), {done} steps, FP32 oracle"
+    return rate, threads, sample
+
+
+def run_reference(args):
+    rank, _, world = env_rank()
+    if rank != 0:
+        return
+    warm = max(0, args.warmup)
+    rate, cores, sample = cpu_oracle_rate(max(1, args.steps), budget_s=max(30.0, 5.0 * args.steps))
+    line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": "Gcell-upd/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": warm, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": CONFIGS["dispersive_large"][2], "sample_n": CPU_SAMPLE_N},
+            "cpu_baseline": {"value": rate, "unit": "Gcell-upd/s", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": rate, "unit": "Gcell-upd/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    rank, local, world = env_rank()
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from semba_fdtd_b200 import Solver, _lib
+    lib = _lib.load("exact")
+    if lib.sgpu_select_device(local) != 0:
+        raise SystemExit("cannot select CUDA device")
+    K, W = args.steps, max(3, args.warmup)
+    pb, label = make_case(args.config, args.n, K + W + 8)
+    cells = pb.swept_cells
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def allmax(x):
+        if not dist:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def allsum(x):
+        if not dist:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    # ---- device-resident throughput ------------------------------------
+    s = Solver(pb, probe_capacity=max(1024, K + W + 8))
+    s.step(W)
+    s.synchronize()
+    ms = C.c_float()
+    barrier()
+    with ClockSampler(local) as clk:
+        rc = lib.sgpu_elapsed_steps(s.handle, s.n, K, C.byref(ms))
+    if rc:
+        raise SystemExit(f"sgpu_elapsed_steps failed: {lib.sgpu_last_error(s.handle).decode()}")
+    s.n += K
+    t_ms = allmax(ms.value)
+    barrier()
+    per_step = C.c_int()
+    lib.sgpu_kernels_per_step(s.handle, C.byref(per_step))
+    launches = per_step.value * K + (K + 31) // 32 + 1
+    # ---- per-phase device times and algorithmic bytes (roofline) -------
+    phases = (C.c_float * 6)()
+    s._drain()
+    rc = lib.sgpu_profile_steps(s.handle, s.n, K, phases)
+    if rc:
+        raise SystemExit(f"sgpu_profile_steps failed: {lib.sgpu_last_error(s.handle).decode()}")
+    s.n += K
+    bytes6 = (C.c_double * 6)()
+    lib.sgpu_algorithmic_bytes(s.handle, bytes6)
+    names = ["efield_curl_cpml", "edispersive_ade", "sources_e", "hfield_curl_cpml", "sources_h", "probes"]
+    kern = ["k_efield", "k_edisp", "k_sources", "k_hfield", "k_sources", "k_probes"]
+    avg_ms = [phases[q] / K for q in range(6)]
+    dom = int(np.argmax(avg_ms))
+    peak, peak_kind = measured_hbm_peak()
+    achieved = bytes6[dom] / (avg_ms[dom] * 1e-3) / 1e9 if avg_ms[dom] > 0 else None
+    finite = s.check_finite()
+    s.close()
+
+    # ---- end to end through the C ABI with host buffers -----------------
+    e2e = None if args.quick else run_e2e(pb, K, lib)
+
+    value = allsum(cells * K) / (t_ms * 1e-3) / 1e9
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    step_bytes = sum(bytes6[q] for q in range(6))
+    line = {"metric": METRIC, "value": value, "unit": "Gcell-upd/s", "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": t_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": label, "swept_cells": cells, "parallelism": f"replicas{world}",
+                       "l2": "inputs larger than L2 (fields alone %.1f GB)" % (cells * 24 / 1e9),
+                       "build": "-fmad=false (bit-exact)"},
+            "hbm_frac_step": (step_bytes / (t_ms / K * 1e-3) / 1e9) / peak,
+            "roofline": {"bound": "hbm", "kernel": kern[dom], "phase": names[dom], "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                         "traffic": ncu_traffic(kern[dom]), "algorithmic_bytes": bytes6[dom],
+                         "avg_ms": avg_ms[dom],
+                         "phases_ms": dict(zip(names, avg_ms)), "phases_bytes": dict(zip(names, list(bytes6)))},
+            "clocks": clk.summary(), "gpu_launches": launches, "finite": finite, "e2e": e2e}
+    try:
+        if args.quick:
+            raise RuntimeError("skipped (--quick)")
+        rate, cores, sample = cpu_oracle_rate(3, budget_s=20.0)
+        line["cpu_baseline"] = {"value": rate, "unit": "Gcell-upd/s", "cores": cores, "kind": "port", "sample": sample}
+    except Exception as ex:  # the baseline is reported, not the target
+        line["cpu_baseline"] = {"value": None, "unit": "Gcell-upd/s", "cores": os.cpu_count(), "kind": "port",
+                                "sample": f"failed: {ex}"}
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def run_e2e(pb, K, lib):
+    """Host problem -> device (set-up, media and initial fields from host
+    buffers) -> K steps -> probe traces and final fields back to host."""
+    from semba_fdtd_b200 import Solver
+    t0 = time.perf_counter()
+    s = Solver(pb, probe_capacity=max(1024, K + 8))
+    h2d = 0
+    for c in range(6):
+        xi, xe, yi, ye, zi, ze = s.alloc[c]
+        n = (xe - xi + 1) * (ye - yi + 1) * (ze - zi + 1)
+        h2d += n * 2  # media matrices uploaded by sgpu_host_create
+    zeros = None
+    for c in range(6):
+        xi, xe, yi, ye, zi, ze = s.alloc[c]
+        n = (xe - xi + 1) * (ye - yi + 1) * (ze - zi + 1)
+        if zeros is None or zeros.size < n:
+            zeros = np.zeros(n, np.float32)
+        rc = lib.sgpu_upload_field(s.handle, c, zeros.ctypes.data_as(C.POINTER(C.c_float)))
+        if rc:
+            raise SystemExit("upload failed")
+        h2d += n * 4
+    s.step(K)
+    tr = s.probes()
+    d2h = tr.nbytes
+    for c in range(6):
+        d2h += s.field(c).nbytes
+    t = time.perf_counter() - t0
+    s.close()
+    return {"value": pb.swept_cells * K / t / 1e9, "unit": "Gcell-upd/s", "h2d_bytes_per_step": h2d / K,
+            "d2h_bytes_per_step": d2h / K, "seconds": t,
+            "includes": "host set-up, media + initial-field upload, K graph steps, probe and final-field download"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="dispersive_large", choices=list(CONFIGS))
+    ap.add_argument("--n", type=int, default=None, help="scale the configuration (cells per axis)")
+    ap.add_argument("--quick", action="store_true", help="skip the end-to-end and CPU-baseline legs (profiling runs)")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

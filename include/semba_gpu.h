@@ -1,0 +1,299 @@
+/*
+ * semba_gpu.h -- C ABI of libsemba_gpu.so, the B200 (sm_100a) implementation
+ * of semba-fdtd's Yee leapfrog core: E/H curl updates, CPML psi updates,
+ * electric pole-residue ADE, plane-wave TF/SF and nodal sources, with point
+ * probes.  Plain pointers and sizes only; no CUDA or torch types.
+ *
+ * Two levels:
+ *
+ *  1. The drop-in for the reference's per-step routines.  The Fortran host
+ *     keeps its set-up (findbounds, calc_G1G2Gm1Gm2, InitCPMLBorders,
+ *     InitEDispersives, InitPlaneWave, InitNodalSources) and hands the arrays
+ *     it built to sgpu_create / sgpu_init_*; every Advance_* routine of the
+ *     time loop then maps to one sgpu_advance_* call.  The field, media and
+ *     coefficient arrays are passed exactly as the Fortran host holds them
+ *     (column-major over sgg%Alloc, re-based to 0), so a bind(C) interface
+ *     can pass them without copies.
+ *
+ *  2. A problem-level host (sgpu_host_*) that restates, in C++, the set-up
+ *     of launch_simulation from an NFDE-style problem description (grid,
+ *     CPML, materials, plane waves, nodal sources, probes) and then drives
+ *     level 1.  This is the caller used by the Python package, the tests and
+ *     the benchmark in this repository.
+ *
+ * Coordinates are the reference's absolute cell indices (sgg%Alloc ranges,
+ * which start at -layers-1).  Field components are numbered 0..5 for
+ * Ex, Ey, Ez, Hx, Hy, Hz (iEx..iHz of fdetypes.F90:190, minus one).
+ *
+ * Every entry point returns SGPU_OK (0) or an error code; the text of the
+ * last error of a context is available from sgpu_last_error.  A context is
+ * not thread-safe: use one context per host thread.  Device work of a
+ * context is issued on its own CUDA stream; sgpu_synchronize waits for it.
+ */
+#ifndef SEMBA_GPU_H
+#define SEMBA_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int sgpu_status;
+#define SGPU_OK 0
+#define SGPU_ERR_ARG 1        /* bad argument or extent                     */
+#define SGPU_ERR_OOM 2        /* device or host allocation failed           */
+#define SGPU_ERR_CUDA 3       /* CUDA runtime error                         */
+#define SGPU_ERR_STATE 4      /* call out of order (e.g. advance before set-up) */
+#define SGPU_ERR_NONFINITE 5  /* NaN/Inf found by sgpu_check_finite         */
+#define SGPU_ERR_TIMEOUT 6    /* a bounded device wait ran out              */
+#define SGPU_ERR_UNSUPPORTED 7
+
+typedef struct sgpu_ctx sgpu_ctx;
+
+typedef struct { int xi, xe, yi, ye, zi, ze; } sgpu_lim;
+
+/* ======================================================================== */
+/* Level 1: drop-in for the per-step routines                               */
+/* ======================================================================== */
+
+/* Grid, coefficient tables and metric arrays, as built by launch_simulation
+ * (timestepping.F90:305-370, :565) and findbounds (timestepping.F90:2883).
+ * Replaces the field/metric allocation of timestepping.F90:375-403. */
+typedef struct {
+    sgpu_lim alloc[6];   /* sgg%Alloc(iEx..iHz)                               */
+    sgpu_lim sweep[6];   /* sgg%Sweep(iEx..iHz)                               */
+    int num_media;       /* sgg%NumMedia; tables hold num_media+1 entries     */
+    const float* g1;     /* G1, G2, GM1, GM2 of calc_G1G2Gm1Gm2 after         */
+    const float* g2;     /*   InitEDispersives has overwritten the dispersive */
+    const float* gm1;    /*   media (calc_constants.F90:36-148,               */
+    const float* gm2;    /*   electricdispersive.F90:140-142)                 */
+    const uint8_t* is_pec; /* sgg%Med(r)%Is%PEC, used by nodal sources        */
+    /* Inverse steps after calc_cpmlconstants has stretched them in the PML:
+     * idxe over alloc[Hx].x, idye over alloc[Hy].y, idze over alloc[Hz].z,
+     * idxh over alloc[Ex].x, idyh over alloc[Ey].y, idzh over alloc[Ez].z. */
+    const float *idxe, *idye, *idze, *idxh, *idyh, *idzh;
+    double dt;           /* sgg%dt                                            */
+} sgpu_grid_desc;
+
+/* On failure *out may hold a context whose sgpu_last_error explains the
+ * failure; destroy it. */
+sgpu_status sgpu_create(const sgpu_grid_desc* grid, sgpu_ctx** out);
+void sgpu_destroy(sgpu_ctx* ctx);
+const char* sgpu_last_error(const sgpu_ctx* ctx);
+sgpu_status sgpu_synchronize(sgpu_ctx* ctx);
+
+/* Media matrices sggMiEx..sggMiHz (int16, -DCompileWithInt2), column-major
+ * over alloc[comp]. */
+sgpu_status sgpu_upload_media(sgpu_ctx* ctx, int comp, const int16_t* mi);
+/* Field arrays Ex..Hz, column-major over alloc[comp]. */
+sgpu_status sgpu_upload_field(sgpu_ctx* ctx, int comp, const float* f);
+sgpu_status sgpu_download_field(sgpu_ctx* ctx, int comp, float* f);
+
+/* InitCPMLBorders (borderscpml.F90:90-473): the PMLc boxes of the six slab
+ * regions per component and the coefficient vectors of calc_cpmlconstants.
+ * Region order Down, Up, Left, Right, Back, Front (fdetypes.F90:186).  An
+ * absent face has an empty box.  p_be[a], p_ce[a], p_bm[a], p_cm[a] cover
+ * alloc[Hx].x (a=0), alloc[Hy].y (a=1), alloc[Hz].z (a=2). */
+typedef struct {
+    sgpu_lim pmlc[6][6]; /* [component][region] */
+    const float *p_be[3], *p_ce[3], *p_bm[3], *p_cm[3];
+} sgpu_cpml_desc;
+sgpu_status sgpu_init_cpml(sgpu_ctx* ctx, const sgpu_cpml_desc* d);
+
+/* InitEDispersives (electricdispersive.F90:77-298): for each electric
+ * dispersive medium its index and the complex(8) Kappa, Beta and G3 of each
+ * pole (interleaved re, im; poles of all media concatenated).  The node
+ * lists of the reference are rebuilt on the device from the media matrices
+ * (every swept E node whose medium is in the list); their state starts at
+ * zero as on a fresh start. */
+typedef struct {
+    int nmedia;
+    const int* medium_index;   /* [nmedia] */
+    const int* npoles;         /* [nmedia] */
+    const double* kappa;       /* [2 * sum(npoles)] */
+    const double* beta;
+    const double* g3;
+} sgpu_edisp_desc;
+sgpu_status sgpu_init_edisp(sgpu_ctx* ctx, const sgpu_edisp_desc* d);
+
+/* InitPlaneWave (planewaves.F90:72-770) + calc_planewaveconstants
+ * (:1494-1510) for one plane wave (one mode).  face[] holds, per face
+ * (0..5 = back, front, left, right, down, up), the flag Ilumina* and per
+ * component the limits of TrFr / IzDe / AbAr:
+ *   lim[face][comp] = {fixed index, lo1, hi1, lo2, hi2}
+ * where the two ranges are the varying coordinates in loop order
+ * (k then j for back/front, k then i for left/right, j then i for down/up).
+ * phys[comp][axis] are Punto%PhysCoor over sweep-1 .. sweep+1. */
+typedef struct {
+    int active[6];
+    int lim[6][6][5];
+    float px, py, pz, d0, cluz;
+    float fpw[6];
+    int numus;
+    float deltaevol;
+    const float* evol;          /* numus + 1 samples */
+    const float* phys[6][3];
+    int phys_lo[6][3];
+    int phys_n[6][3];
+} sgpu_planewave_desc;
+sgpu_status sgpu_add_planewave(sgpu_ctx* ctx, const sgpu_planewave_desc* d);
+
+/* InitNodalSources (nodalsources.F90:76-300): one clipped point box of one
+ * component. */
+typedef struct {
+    int comp;                   /* 0..5 */
+    int hard;
+    sgpu_lim box;
+    float amplitude;
+    int numus;
+    float deltaevol;
+    const float* evol;
+} sgpu_nodal_desc;
+sgpu_status sgpu_add_nodal(sgpu_ctx* ctx, const sgpu_nodal_desc* d);
+
+/* crea_timevector (timestepping.F90:3230-3240): tiempo(n0 .. n0+count-1). */
+sgpu_status sgpu_set_time(sgpu_ctx* ctx, int n0, int count, const double* tiempo);
+
+/* Point probes (observation.F90:2633-2668): comp_ijk holds 4 ints per
+ * probe (component, i, j, k).  Values are recorded after every whole step
+ * into a device ring of capacity_steps rows. */
+sgpu_status sgpu_set_probes(sgpu_ctx* ctx, int nprobes, const int* comp_ijk, int capacity_steps);
+/* Copy the rows recorded since the last read (at most max_steps) to out
+ * (row-major [step][probe]); *nsteps receives the number of rows and
+ * *first_n the step index n of the first row. */
+sgpu_status sgpu_read_probes(sgpu_ctx* ctx, float* out, int max_steps, int* nsteps, int* first_n);
+
+/* One call per reference routine, in the order of timestepping.F90:1286-1742. */
+sgpu_status sgpu_advance_ex(sgpu_ctx* ctx);                 /* Advance_Ex :2165 */
+sgpu_status sgpu_advance_ey(sgpu_ctx* ctx);                 /* Advance_Ey :2206 */
+sgpu_status sgpu_advance_ez(sgpu_ctx* ctx);                 /* Advance_Ez :2250 */
+sgpu_status sgpu_advance_electric_cpml(sgpu_ctx* ctx);      /* borderscpml.F90:584 */
+sgpu_status sgpu_advance_edispersive_e(sgpu_ctx* ctx);      /* electricdispersive.F90:304 */
+sgpu_status sgpu_advance_planewave_e(sgpu_ctx* ctx, int n); /* planewaves.F90:878 */
+sgpu_status sgpu_advance_nodal_e(sgpu_ctx* ctx, int n);     /* nodalsources.F90:396 */
+sgpu_status sgpu_advance_hx(sgpu_ctx* ctx);                 /* Advance_Hx :2294 */
+sgpu_status sgpu_advance_hy(sgpu_ctx* ctx);                 /* Advance_Hy :2334 */
+sgpu_status sgpu_advance_hz(sgpu_ctx* ctx);                 /* Advance_Hz :2374 */
+sgpu_status sgpu_advance_magnetic_cpml(sgpu_ctx* ctx);      /* borderscpml.F90:881 */
+sgpu_status sgpu_advance_planewave_h(sgpu_ctx* ctx, int n); /* planewaves.F90:1180 */
+sgpu_status sgpu_advance_nodal_h(sgpu_ctx* ctx, int n);     /* nodalsources.F90:584 */
+sgpu_status sgpu_update_observation(sgpu_ctx* ctx, int n);  /* observation.F90:2540 */
+
+/* Fused forms, same results bit for bit: the E half step (curl + CPML +
+ * ADE + TF/SF + nodal), the H half step (curl + CPML + TF/SF + nodal), and
+ * `count` whole steps n0 .. n0+count-1 including the probe gather, captured
+ * into a CUDA graph and replayed. */
+sgpu_status sgpu_advance_e(sgpu_ctx* ctx, int n);
+sgpu_status sgpu_advance_h(sgpu_ctx* ctx, int n);
+sgpu_status sgpu_advance_steps(sgpu_ctx* ctx, int n0, int count);
+
+/* Scans the six field components for NaN/Inf on the device; returns
+ * SGPU_ERR_NONFINITE if any is found (the host-side counterpart of the
+ * reference's energy/NaN stop, errorreport.F90:1433-1460). */
+sgpu_status sgpu_check_finite(sgpu_ctx* ctx);
+
+/* sgpu_advance_steps bracketed by CUDA events on the context's stream;
+ * *ms receives the device time of the `count` steps. */
+sgpu_status sgpu_elapsed_steps(sgpu_ctx* ctx, int n0, int count, float* ms);
+/* `count` steps launched directly with CUDA events between the phases;
+ * ms6 accumulates the device time of: E curl+CPML, ADE, E sources,
+ * H curl+CPML, H sources, probe gather. */
+sgpu_status sgpu_profile_steps(sgpu_ctx* ctx, int n0, int count, float* ms6);
+/* Algorithmic bytes of one launch of each phase of sgpu_profile_steps:
+ * compulsory field/media/psi/ADE-state traffic, without neighbour re-reads
+ * or coefficient tables. */
+sgpu_status sgpu_algorithmic_bytes(const sgpu_ctx* ctx, double* bytes6);
+/* Select the CUDA device this library's runtime uses on the calling thread
+ * (call before sgpu_create / sgpu_host_create). */
+sgpu_status sgpu_select_device(int device);
+/* Kernel launches issued per whole step (graph replays add one per chunk). */
+sgpu_status sgpu_kernels_per_step(const sgpu_ctx* ctx, int* n);
+
+/* Bytes of device memory the context holds. */
+sgpu_status sgpu_device_bytes(const sgpu_ctx* ctx, uint64_t* bytes);
+
+/* ======================================================================== */
+/* Level 2: problem-level host                                              */
+/* ======================================================================== */
+
+/* A material region in NFDE terms: kind 0 = PEC volume, 1 = isotropic
+ * dielectric volume, 2 = electric pole-residue volume.  eps/mu absolute
+ * (for a pole-residue region eps is the high-frequency permittivity).
+ * Poles: the complex64 residues a11 and b11 = minus the pole, as in
+ * preprocess_geom.F90:5196-5199. */
+typedef struct {
+    int kind;
+    float eps, sigma, mu, sigmam;
+    int npoles;
+    const float* residues;   /* 2*npoles */
+    const float* bpoles;     /* 2*npoles */
+    int nboxes;
+    const int* boxes;        /* 6*nboxes: XI XE YI YE ZI ZE inclusive */
+} sgpu_region;
+
+typedef struct {
+    int x1, y1, z1, x2, y2, z2;    /* coor1 / coor2 (cellIntervalsToCoords) */
+    float theta, phi, alpha, beta;
+    int nsamples;
+    const float* samples;
+    float dsamples;
+} sgpu_planewave_src;
+
+typedef struct {
+    int is_elec, is_hard;
+    int npoints;
+    const int* boxes;   /* 6*npoints */
+    const float* amp;   /* 3*npoints: xc yc zc */
+    int nsamples;
+    const float* samples;
+    float dsamples;
+} sgpu_nodal_src;
+
+typedef struct {
+    int nx, ny, nz;
+    const float *desx, *desy, *desz;
+    float originx, originy, originz;
+    double dt;          /* general%dt */
+    int forcecfl;       /* the -cfl switch */
+    float cfl;
+    int pml_layers[6];  /* back, front, left, right, down, up; all >= 1 */
+    float pml_order[6];
+    float pml_refl[6];
+    float alphamax, alphaorder, kappamax;   /* -pmlalpha, -pmlkappa */
+    int nregions;
+    const sgpu_region* regions;
+    int npw;
+    const sgpu_planewave_src* pw;
+    int nnodal;
+    const sgpu_nodal_src* nodal;
+    int nprobes;
+    const int* probes;  /* 4*nprobes: comp, i, j, k */
+    int probe_capacity; /* rows of the device probe ring */
+} sgpu_problem;
+
+/* Restated set-up of semba_fdtd.F90:1197-1300 and timestepping.F90:305-1014
+ * for one problem, then sgpu_create and the sgpu_init_* calls.  The time
+ * vector is generated for steps 0 .. max_steps+2.  On failure *out may hold
+ * a context whose sgpu_last_error explains it; destroy it. */
+sgpu_status sgpu_host_create(const sgpu_problem* p, int max_steps, sgpu_ctx** out);
+/* The same set-up on the host only: the context owns no device memory and
+ * serves the sgpu_host_* getters (and sgpu_host_footprint for admission
+ * control) without a GPU. */
+sgpu_status sgpu_host_plan(const sgpu_problem* p, int max_steps, sgpu_ctx** out);
+/* Device bytes sgpu_host_create would allocate for this plan: fields, media,
+ * CPML psi, ADE state and the probe ring. */
+sgpu_status sgpu_host_footprint(const sgpu_ctx* ctx, uint64_t* bytes);
+/* Results of the set-up. */
+sgpu_status sgpu_host_info(const sgpu_ctx* ctx, double* dt, int* num_media, sgpu_lim* alloc6,
+                           sgpu_lim* sweep6, sgpu_lim* sinpml6);
+/* The coefficient tables the host built (num_media+1 each). */
+sgpu_status sgpu_host_get_g(const sgpu_ctx* ctx, float* g1, float* g2, float* gm1, float* gm2);
+/* which as for the oracle: 0..5 Idxe..Idzh, 6..17 P_be, P_ce, P_bm, P_cm. */
+sgpu_status sgpu_host_get_metric(const sgpu_ctx* ctx, int which, float* out, int* lo, int* hi);
+sgpu_status sgpu_host_get_media(const sgpu_ctx* ctx, int comp, int16_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,132 @@
+/*
+ * CPU oracle for the semba-fdtd Yee / CPML / pole-residue ADE / TF-SF hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the checker for the CUDA path:
+ * it is loaded by tests/, by __graft_entry__.smoke() and by the cpu_baseline
+ * leg of bench.py, and by nothing else.  It is never the thing measured as
+ * the GPU result and the product never links it.
+ *
+ * It restates, in plain C++17 with OpenMP, the reference's algorithm:
+ *   - grid limits, PML padding and time step   (preprocess_geom.F90:5266-5737,
+ *                                                semba_fdtd.F90:1197-1300)
+ *   - media table and media matrices           (preprocess_geom.F90:421-760,
+ *                                                1085-1110, healer.F90:66-243,
+ *                                                healer.F90:961-1420)
+ *   - update coefficients                       (calc_constants.F90:36-148)
+ *   - metric arrays                             (timestepping.F90:314-370)
+ *   - CPML                                      (borderscpml.F90:90-473, 584-1176,
+ *                                                1465-1733)
+ *   - electric pole-residue ADE                 (electricdispersive.F90:77-362)
+ *   - plane-wave TF/SF                          (planewaves.F90:72-853, 878-1510)
+ *   - nodal sources                             (nodalsources.F90:76-583)
+ *   - point probes                              (observation.F90:2633-2668)
+ *   - the leapfrog loop order                   (timestepping.F90:1248-1981)
+ * following the reference's operation order and its real4/real8/complex8
+ * promotion rules.  The template parameter R is the field kind RKIND: float
+ * is the reference FP32 build, double the -DCompileWithReal8 accuracy oracle.
+ *
+ * Parity status: the reference Fortran cannot be compiled in this container
+ * (no Fortran compiler; its json-fortran/ngspice/lapack dependencies are
+ * absent), and the reference ships no golden vectors for this path, so the
+ * oracle is pinned by known-answer tests (tests/test_oracle_kat.py) and the
+ * reference's parser fixture, not by reference outputs: parity unpinned.
+ */
+#ifndef SEMBA_ORACLE_H
+#define SEMBA_ORACLE_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* A material region in NFDE terms (nfde_types.F90).  kind: 0 = PEC volume,
+ * 1 = isotropic dielectric volume, 2 = electric pole-residue volume.
+ * eps/mu are absolute (F/m, H/m) as stored by the NFDE structures; for a
+ * dispersive region eps is eps11 (the high-frequency permittivity). */
+typedef struct {
+    int kind;
+    float eps, sigma, mu, sigmam;
+    int npoles;
+    const float* residues; /* 2*npoles: complex64 residues a11 (re, im)        */
+    const float* bpoles;   /* 2*npoles: complex64 b11 = minus the pole (re, im) */
+    int nboxes;
+    const int* boxes;      /* 6*nboxes: XI XE YI YE ZI ZE, inclusive cell coords */
+} orc_region;
+
+typedef struct {
+    int x1, y1, z1, x2, y2, z2;      /* coor1 / coor2 after cellIntervalsToCoords */
+    float theta, phi, alpha, beta;   /* direction and polarisation angles       */
+    int nsamples;                    /* numus + 1                               */
+    const float* samples;
+    float dsamples;
+} orc_planewave;
+
+typedef struct {
+    int is_elec, is_hard;
+    int npoints;
+    const int* boxes;                /* 6*npoints */
+    const float* amp;                /* 3*npoints: xc, yc, zc */
+    int nsamples;
+    const float* samples;
+    float dsamples;
+} orc_nodal;
+
+typedef struct {
+    int nx, ny, nz;
+    const float *desx, *desy, *desz;
+    float originx, originy, originz;
+    double dt;                       /* general%dt from the case file */
+    int forcecfl;                    /* -cfl switch given             */
+    float cfl;
+    /* face order of the reference: back(x-), front(x+), left(y-), right(y+),
+     * down(z-), up(z+).  All faces are CPML; layers must be >= 1. */
+    int pml_layers[6];
+    float pml_order[6];
+    float pml_refl[6];
+    float alphamax, alphaorder, kappamax;
+    int nregions;
+    const orc_region* regions;
+    int npw;
+    const orc_planewave* pw;
+    int nnodal;
+    const orc_nodal* nodal;
+    int nprobes;
+    const int* probes;               /* 4*nprobes: comp(0..5 = Ex..Hz), i, j, k */
+} orc_problem;
+
+/* Extents of one component (sgg%Alloc, sgg%Sweep) in the reference's
+ * absolute cell coordinates. */
+typedef struct { int xi, xe, yi, ye, zi, ze; } orc_lim;
+
+/* Returns 0 on success.  fp64 != 0 selects the double-precision variant. */
+int orc_create(const orc_problem* p, int fp64, int nthreads, void** handle);
+void orc_destroy(void* h);
+/* Advance steps n0 .. n1-1 (the reference's loop variable n), recording
+ * probes after each step into rows [n - n0] of out (nprobes per row), if
+ * out is non-null. */
+int orc_run(void* h, int n0, int n1, float* probe_out);
+/* Grid description after set-up. */
+int orc_get_lims(void* h, orc_lim* alloc6, orc_lim* sweep6, orc_lim* sinpml6);
+double orc_get_dt(void* h);
+int orc_get_num_media(void* h);
+/* Copy a field component (0..5) into a float buffer laid out over Alloc in
+ * Fortran (column-major) order. */
+int orc_get_field(void* h, int comp, float* out);
+int orc_get_field_f64(void* h, int comp, double* out);
+int orc_get_media(void* h, int comp, short* out);
+/* Coefficient tables, for cross-checks of the set-up: g1,g2,gm1,gm2 each
+ * num_media+1 floats. */
+int orc_get_g(void* h, float* g1, float* g2, float* gm1, float* gm2);
+/* which: 0..5 = Idxe Idye Idze Idxh Idyh Idzh, 6..17 = P_be_x,y,z P_ce_x,y,z
+ * P_bm_x,y,z P_cm_x,y,z; arrays cover the Alloc range of the matching
+ * component axis (see orc_get_metric_range). */
+int orc_get_metric(void* h, int which, float* out);
+int orc_get_metric_range(void* h, int which, int* lo, int* hi);
+/* Per dispersive medium m (0-based in creation order): numpoles, kappa,
+ * beta, g3 as interleaved doubles (re, im). */
+int orc_get_edisp(void* h, int m, int* medium_index, int* npoles, double* kappa,
+                  double* beta, double* g3);
+double orc_get_time(void* h, int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,1436 @@
+// libsemba_gpu: device kernels and the level-1 C ABI (see include/semba_gpu.h).
+//
+// The per-cell arithmetic restates the reference routines named beside each
+// kernel, in their operation order, so that a build with -fmad=false
+// reproduces the reference FP32 build bit for bit.  All transcendental work
+// (exp, log, pow, trig) happens once on the host during set-up; kernels only
+// add, subtract, multiply, divide and convert, which CUDA performs with IEEE
+// round-to-nearest.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "sgpu_internal.h"
+
+using namespace sgpu;
+
+namespace sgpu {
+
+sgpu_status set_error(sgpu_ctx* c, sgpu_status code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+KGrid kgrid(const sgpu_ctx* c) {
+    KGrid g{};
+    for (int f = 0; f < 6; ++f) {
+        g.F[f] = c->F[f];
+        g.M[f] = c->M[f];
+        g.sw[f][0] = c->sweep[f].xi - c->ox;
+        g.sw[f][1] = c->sweep[f].xe - c->ox;
+        g.sw[f][2] = c->sweep[f].yi - c->oy;
+        g.sw[f][3] = c->sweep[f].ye - c->oy;
+        g.sw[f][4] = c->sweep[f].zi - c->oz;
+        g.sw[f][5] = c->sweep[f].ze - c->oz;
+    }
+    g.g1 = c->g1; g.g2 = c->g2; g.gm1 = c->gm1; g.gm2 = c->gm2;
+    g.idxe = c->idxe; g.idye = c->idye; g.idze = c->idze;
+    g.idxh = c->idxh; g.idyh = c->idyh; g.idzh = c->idzh;
+    g.pitch = c->pitch;
+    g.plane = c->plane;
+    g.nmed1 = c->num_media + 1;
+    return g;
+}
+
+}  // namespace sgpu
+
+#define CUDA_TRY(ctx, call)                                                                   \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            return set_error((ctx), SGPU_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+namespace {
+
+enum : int { kBulk = 1, kCpml = 2, kCx = 4, kCy = 8, kCz = 16, kAll = kCx | kCy | kCz };
+constexpr int kShTable = 4096;  // media entries held in shared memory
+
+__device__ __forceinline__ float* slab_ptr(const Slab& s, int i, int j, int k) {
+    if (i < s.xlo || i > s.xhi || j < s.ylo || j > s.yhi || k < s.zlo || k > s.zhi) return nullptr;
+    long long nx = s.xhi - s.xlo + 1, ny = s.yhi - s.ylo + 1;
+    return s.psi + ((i - s.xlo) + nx * ((j - s.ylo) + ny * (long long)(k - s.zlo)));
+}
+
+// True when the (x, y) column range [x0,x1]x[y0,y1] or the z range [z0,z1]
+// can touch the slab.
+__device__ __forceinline__ bool slab_touches(const Slab& s, int x0, int x1, int y0, int y1, int z0, int z1) {
+    return s.psi && x1 >= s.xlo && x0 <= s.xhi && y1 >= s.ylo && y0 <= s.yhi && z1 >= s.zlo && z0 <= s.zhi;
+}
+
+// One CPML correction of the reference (borderscpml.F90:584-1176):
+//   psi = P_b(c) * psi + diff * P_c(c) ;  F = F +- g * psi
+// applied for whichever of the two opposite slabs holds the cell.
+template <bool ADD>
+__device__ __forceinline__ float cpml_one(const Slab (&s)[2], int i, int j, int k, int c, const float* pb,
+                                          const float* pc, float diff, float g, float v, bool& touched) {
+    float* p = slab_ptr(s[0], i, j, k);
+    if (!p) p = slab_ptr(s[1], i, j, k);
+    if (p) {
+        float ps = pb[c] * (*p) + diff * pc[c];
+        *p = ps;
+        v = ADD ? v + g * ps : v - g * ps;
+        touched = true;
+    }
+    return v;
+}
+
+// Block geometry shared by the two field kernels: 32 x BY threads, each
+// owning one (i, j) column and marching over a z chunk.  x starts at local 0
+// so every warp load covers one aligned 128-byte line.
+constexpr int kBX = 32, kBY = 8;
+
+// Advance_Ex/Ey/Ez (timestepping.F90:2165-2285) fused with
+// AdvanceelectricCPML (borderscpml.F90:584-876).  Each field value is read
+// once per cell; the curl update and, in blocks that touch a PML slab, the
+// CPML corrections (in the reference's region order) are applied to the
+// register value before a single store.  Hx and Hy of plane k-1 are carried
+// in registers from the previous iteration; the i-1 neighbours come from the
+// next lower lane.
+template <int MODE, bool CP>
+__device__ __forceinline__ void efield_column(const KGrid& g, const KCpml& cp, const float* t1, const float* t2, int i, int j,
+                                              int kb, int ke, bool vx, bool vy, bool vz) {
+    const long long pitch = g.pitch, plane = g.plane;
+    float* __restrict__ Ex = g.F[0];
+    float* __restrict__ Ey = g.F[1];
+    float* __restrict__ Ez = g.F[2];
+    const float* __restrict__ Hx = g.F[3];
+    const float* __restrict__ Hy = g.F[4];
+    const float* __restrict__ Hz = g.F[5];
+    const int16_t* __restrict__ Mx = g.M[0];
+    const int16_t* __restrict__ My = g.M[1];
+    const int16_t* __restrict__ Mz = g.M[2];
+    const bool lane0 = (threadIdx.x & 31) == 0;
+    const float idyh = g.idyh[j], idxh = g.idxh[i];
+    long long c = i + pitch * j + plane * kb;
+    float hx_km = __ldg(Hx + c - plane), hy_km = __ldg(Hy + c - plane);
+    for (int k = kb; k <= ke; ++k, c += plane) {
+        const float hx = __ldg(Hx + c), hy = __ldg(Hy + c), hz = __ldg(Hz + c);
+        float hz_im = __shfl_up_sync(0xffffffffu, hz, 1);
+        float hy_im = __shfl_up_sync(0xffffffffu, hy, 1);
+        if (lane0) {
+            hz_im = __ldg(Hz + c - 1);
+            hy_im = __ldg(Hy + c - 1);
+        }
+        const float idzh = g.idzh[k];
+        if ((MODE & kCx) && vx && k >= g.sw[0][4] && k <= g.sw[0][5]) {
+            float e = Ex[c];
+            const int m = __ldg(Mx + c);
+            const float dy = hz - __ldg(Hz + c - pitch);
+            const float dz = hy - hy_km;
+            bool st = (MODE & kBulk) != 0;
+            if (MODE & kBulk) e = t1[m] * e + t2[m] * (dy * idyh - dz * idzh);
+            if (CP) {
+                const float gg = t2[m];
+                e = cpml_one<true>(cp.s[0][0], i, j, k, j, cp.pbe[1], cp.pce[1], dy, gg, e, st);
+                e = cpml_one<false>(cp.s[0][1], i, j, k, k, cp.pbe[2], cp.pce[2], dz, gg, e, st);
+            }
+            if (st) Ex[c] = e;
+        }
+        if ((MODE & kCy) && vy && k >= g.sw[1][4] && k <= g.sw[1][5]) {
+            float e = Ey[c];
+            const int m = __ldg(My + c);
+            const float dz = hx - hx_km;
+            const float dx = hz - hz_im;
+            bool st = (MODE & kBulk) != 0;
+            if (MODE & kBulk) e = t1[m] * e + t2[m] * (dz * idzh - dx * idxh);
+            if (CP) {
+                const float gg = t2[m];
+                e = cpml_one<true>(cp.s[1][0], i, j, k, k, cp.pbe[2], cp.pce[2], dz, gg, e, st);
+                e = cpml_one<false>(cp.s[1][1], i, j, k, i, cp.pbe[0], cp.pce[0], dx, gg, e, st);
+            }
+            if (st) Ey[c] = e;
+        }
+        if ((MODE & kCz) && vz && k >= g.sw[2][4] && k <= g.sw[2][5]) {
+            float e = Ez[c];
+            const int m = __ldg(Mz + c);
+            const float dx = hy - hy_im;
+            const float dy = hx - __ldg(Hx + c - pitch);
+            bool st = (MODE & kBulk) != 0;
+            if (MODE & kBulk) e = t1[m] * e + t2[m] * (dx * idxh - dy * idyh);
+            if (CP) {
+                const float gg = t2[m];
+                e = cpml_one<false>(cp.s[2][0], i, j, k, j, cp.pbe[1], cp.pce[1], dy, gg, e, st);
+                e = cpml_one<true>(cp.s[2][1], i, j, k, i, cp.pbe[0], cp.pce[0], dx, gg, e, st);
+            }
+            if (st) Ez[c] = e;
+        }
+        hx_km = hx;
+        hy_km = hy;
+    }
+}
+
+__device__ __forceinline__ bool col_in(const int* s, int i, int j) { return i >= s[0] && i <= s[1] && j >= s[2] && j <= s[3]; }
+
+template <int MODE>
+__global__ void __launch_bounds__(kBX * kBY, 4) k_efield(KGrid g, KCpml cp, int y0, int z0, int z1, int zchunk) {
+    extern __shared__ float sh[];
+    const bool use_sh = g.nmed1 <= kShTable;
+    if (use_sh) {
+        for (int t = threadIdx.x + kBX * threadIdx.y; t < g.nmed1; t += kBX * kBY) {
+            sh[t] = g.g1[t];
+            sh[g.nmed1 + t] = g.g2[t];
+        }
+    }
+    __syncthreads();
+    const float* t1 = use_sh ? sh : g.g1;
+    const float* t2 = use_sh ? sh + g.nmed1 : g.g2;
+    const int i = blockIdx.x * kBX + threadIdx.x;
+    const int jb = y0 + blockIdx.y * kBY;
+    const int j = jb + threadIdx.y;
+    const int kb = z0 + blockIdx.z * zchunk;
+    const int ke = min(kb + zchunk - 1, z1);
+    // the warp shuffles need every lane: out-of-range lanes stay in the loop
+    // with all three components disabled and clamped (in-bounds) indices
+    const bool vx = col_in(g.sw[0], i, j), vy = col_in(g.sw[1], i, j), vz = col_in(g.sw[2], i, j);
+    // i < pitch always (grid rounding stays inside the padded row); rows
+    // past the last swept row are clamped to a valid one and do no work
+    const int ic = i;
+    const int jc = min(max(j, 1), (int)(g.plane / g.pitch) - 2);
+    bool cpml_block = false;
+    if (MODE & kCpml) {
+        const int bx0 = blockIdx.x * kBX, bx1 = bx0 + kBX - 1, by1 = jb + kBY - 1;
+        for (int f = 0; f < 3; ++f)
+            for (int w = 0; w < 2; ++w)
+                for (int sd = 0; sd < 2; ++sd) cpml_block |= slab_touches(cp.s[f][w][sd], bx0, bx1, jb, by1, kb, ke);
+    }
+    if (cpml_block) efield_column<MODE, true>(g, cp, t1, t2, ic, jc, kb, ke, vx, vy, vz);
+    else if (MODE & kBulk) efield_column<MODE, false>(g, cp, t1, t2, ic, jc, kb, ke, vx, vy, vz);
+}
+
+// Advance_Hx/Hy/Hz (timestepping.F90:2294-2409) fused with
+// AdvanceMagneticCPML (borderscpml.F90:881-1176).  Ex and Ey of plane k+1
+// are loaded once and carried to the next iteration; the i+1 neighbours come
+// from the next higher lane.
+template <int MODE, bool CP>
+__device__ __forceinline__ void hfield_column(const KGrid& g, const KCpml& cp, const float* t1, const float* t2, int i, int j,
+                                              int kb, int ke, bool vx, bool vy, bool vz) {
+    const long long pitch = g.pitch, plane = g.plane;
+    const float* __restrict__ Ex = g.F[0];
+    const float* __restrict__ Ey = g.F[1];
+    const float* __restrict__ Ez = g.F[2];
+    float* __restrict__ Hx = g.F[3];
+    float* __restrict__ Hy = g.F[4];
+    float* __restrict__ Hz = g.F[5];
+    const int16_t* __restrict__ Mx = g.M[3];
+    const int16_t* __restrict__ My = g.M[4];
+    const int16_t* __restrict__ Mz = g.M[5];
+    const bool lane31 = (threadIdx.x & 31) == 31;
+    const float idye = g.idye[j], idxe = g.idxe[i];
+    long long c = i + pitch * j + plane * kb;
+    float ex_k = __ldg(Ex + c), ey_k = __ldg(Ey + c);
+    for (int k = kb; k <= ke; ++k, c += plane) {
+        const float ez = __ldg(Ez + c);
+        const float ex_kp = __ldg(Ex + c + plane), ey_kp = __ldg(Ey + c + plane);
+        float ez_ip = __shfl_down_sync(0xffffffffu, ez, 1);
+        float ey_ip = __shfl_down_sync(0xffffffffu, ey_k, 1);
+        if (lane31) {
+            ez_ip = __ldg(Ez + c + 1);
+            ey_ip = __ldg(Ey + c + 1);
+        }
+        const float idze = g.idze[k];
+        if ((MODE & kCx) && vx && k >= g.sw[3][4] && k <= g.sw[3][5]) {
+            float h = Hx[c];
+            const int m = __ldg(Mx + c);
+            const float dz = ey_kp - ey_k;
+            const float dy = __ldg(Ez + c + pitch) - ez;
+            bool st = (MODE & kBulk) != 0;
+            if (MODE & kBulk) h = t1[m] * h + t2[m] * (dz * idze - dy * idye);
+            if (CP) {
+                const float gg = t2[m];
+                h = cpml_one<false>(cp.s[3][0], i, j, k, j, cp.pbm[1], cp.pcm[1], dy, gg, h, st);
+                h = cpml_one<true>(cp.s[3][1], i, j, k, k, cp.pbm[2], cp.pcm[2], dz, gg, h, st);
+            }
+            if (st) Hx[c] = h;
+        }
+        if ((MODE & kCy) && vy && k >= g.sw[4][4] && k <= g.sw[4][5]) {
+            float h = Hy[c];
+            const int m = __ldg(My + c);
+            const float dx = ez_ip - ez;
+            const float dz = ex_kp - ex_k;
+            bool st = (MODE & kBulk) != 0;
+            if (MODE & kBulk) h = t1[m] * h + t2[m] * (dx * idxe - dz * idze);
+            if (CP) {
+                const float gg = t2[m];
+                h = cpml_one<false>(cp.s[4][0], i, j, k, k, cp.pbm[2], cp.pcm[2], dz, gg, h, st);
+                h = cpml_one<true>(cp.s[4][1], i, j, k, i, cp.pbm[0], cp.pcm[0], dx, gg, h, st);
+            }
+            if (st) Hy[c] = h;
+        }
+        if ((MODE & kCz) && vz && k >= g.sw[5][4] && k <= g.sw[5][5]) {
+            float h = Hz[c];
+            const int m = __ldg(Mz + c);
+            const float dy = __ldg(Ex + c + pitch) - ex_k;
+            const float dx = ey_ip - ey_k;
+            bool st = (MODE & kBulk) != 0;
+            if (MODE & kBulk) h = t1[m] * h + t2[m] * (dy * idye - dx * idxe);
+            if (CP) {
+                const float gg = t2[m];
+                h = cpml_one<true>(cp.s[5][0], i, j, k, j, cp.pbm[1], cp.pcm[1], dy, gg, h, st);
+                h = cpml_one<false>(cp.s[5][1], i, j, k, i, cp.pbm[0], cp.pcm[0], dx, gg, h, st);
+            }
+            if (st) Hz[c] = h;
+        }
+        ex_k = ex_kp;
+        ey_k = ey_kp;
+    }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kBX * kBY, 4) k_hfield(KGrid g, KCpml cp, int y0, int z0, int z1, int zchunk) {
+    extern __shared__ float sh[];
+    const bool use_sh = g.nmed1 <= kShTable;
+    if (use_sh) {
+        for (int t = threadIdx.x + kBX * threadIdx.y; t < g.nmed1; t += kBX * kBY) {
+            sh[t] = g.gm1[t];
+            sh[g.nmed1 + t] = g.gm2[t];
+        }
+    }
+    __syncthreads();
+    const float* t1 = use_sh ? sh : g.gm1;
+    const float* t2 = use_sh ? sh + g.nmed1 : g.gm2;
+    const int i = blockIdx.x * kBX + threadIdx.x;
+    const int jb = y0 + blockIdx.y * kBY;
+    const int j = jb + threadIdx.y;
+    const int kb = z0 + blockIdx.z * zchunk;
+    const int ke = min(kb + zchunk - 1, z1);
+    const bool vx = col_in(g.sw[3], i, j), vy = col_in(g.sw[4], i, j), vz = col_in(g.sw[5], i, j);
+    // i < pitch always (grid rounding stays inside the padded row); rows
+    // past the last swept row are clamped to a valid one and do no work
+    const int ic = i;
+    const int jc = min(max(j, 1), (int)(g.plane / g.pitch) - 2);
+    bool cpml_block = false;
+    if (MODE & kCpml) {
+        const int bx0 = blockIdx.x * kBX, bx1 = bx0 + kBX - 1, by1 = jb + kBY - 1;
+        for (int f = 3; f < 6; ++f)
+            for (int w = 0; w < 2; ++w)
+                for (int sd = 0; sd < 2; ++sd) cpml_block |= slab_touches(cp.s[f][w][sd], bx0, bx1, jb, by1, kb, ke);
+    }
+    if (cpml_block) hfield_column<MODE, true>(g, cp, t1, t2, ic, jc, kb, ke, vx, vy, vz);
+    else if (MODE & kBulk) hfield_column<MODE, false>(g, cp, t1, t2, ic, jc, kb, ke, vx, vy, vz);
+}
+
+// AdvanceEDispersiveE (electricdispersive.F90:304-362): one thread per node.
+// Conjugate poles share one state slot; the subtraction still runs once
+// per pole of the reference, in its order, and Re(conj(g)*conj(J)) equals
+// Re(g*J) exactly.  NU (the largest number of state slots of any medium) is
+// a template parameter so the states stay in registers.
+template <int NU>
+__global__ void __launch_bounds__(256) k_edisp(KGrid g, KDisp d, int comp) {
+    const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long n = d.n[comp];
+    if (q >= n) return;
+    const int idx = d.node[comp][q];
+    const DispMedium* __restrict__ md = d.media + d.med[comp][q];
+    float* F = g.F[comp];
+    double2* J = d.J[comp];
+    const int nu = md->nu;
+    double2 st[NU];
+#pragma unroll
+    for (int u = 0; u < NU; ++u) st[u] = u < nu ? J[u * n + q] : make_double2(0.0, 0.0);
+    float e = F[idx];
+    for (int p = 0; p < md->np; ++p) {
+        const int up = md->map[p];
+        double jr = 0.0, ji = 0.0;
+#pragma unroll
+        for (int u = 0; u < NU; ++u)
+            if (u == up) { jr = st[u].x; ji = st[u].y; }
+        const double2 g3 = md->g3[up];
+        const double re = g3.x * jr - g3.y * ji;
+        e = (float)((double)e - re);
+    }
+    const double dd = (double)(e - d.prev[comp][q]);
+#pragma unroll
+    for (int u = 0; u < NU; ++u) {
+        if (u < nu) {
+            const double2 kp = md->kappa[u], bt = md->beta[u];
+            const double kr = kp.x * st[u].x - kp.y * st[u].y;
+            const double ki = kp.x * st[u].y + kp.y * st[u].x;
+            const double br = (bt.x * dd) / d.dt;
+            const double bi = (bt.y * dd) / d.dt;
+            J[u * n + q] = make_double2(kr + br, ki + bi);
+        }
+    }
+    d.prev[comp][q] = e;
+    F[idx] = e;
+}
+
+__device__ __forceinline__ int step_of(const StepRef& s) { return (s.dev_n ? *s.dev_n : 0) + s.n; }
+
+// AdvancePlaneWaveE/H (planewaves.F90:878-1475) with Incid/evolucion
+// (:778-853) and AdvanceNodalE/H (nodalsources.F90:310-777): one thread per
+// touched node applies that node's contributions in the reference order.
+__global__ void k_sources(KGrid g, KSrc s, StepRef sr, const double* tiempo, int t_n0, double dt, int hside, int mask) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= s.nrows) return;
+    const int n = step_of(sr);
+    const double tn = tiempo[n - t_n0];
+    const float t = hside ? (float)(tn + (double)0.5f * dt) : (float)tn;
+    const float G21 = hside ? g.gm2[1] : g.g2[1];
+    float* F = g.F[s.row_comp[r]];
+    const int node = s.row_node[r];
+    float v = F[node];
+    for (int p = s.row_ptr[r]; p < s.row_ptr[r + 1]; ++p) {
+        const SrcEntry en = s.e[p];
+        if (!((1 << en.type) & mask)) continue;
+        const SrcTable tb = s.tab[en.table];
+        const float* ev0 = s.samples + tb.offset;
+        if (en.type == kSrcPlaneWave) {
+            float ev = 0.0f;
+            const long long nprev = (long long)((t - en.a) / tb.delta);
+            if (nprev + 1 <= tb.numus && nprev > 0)
+                ev = (ev0[nprev + 1] - ev0[nprev]) / tb.delta * ((t - en.a) - (float)nprev * tb.delta) + ev0[nprev];
+            const float inc = 0.0f + en.b * ev;
+            v = v + G21 * inc * en.c;
+        } else {
+            float ev = 0.0f;
+            const long long nprev = (long long)(t / tb.delta);
+            if (!((nprev + 1 > tb.numus) || (nprev + 1 <= 0)))
+                ev = (ev0[nprev + 1] - ev0[nprev]) / tb.delta * ((t) - (float)nprev * tb.delta) + ev0[nprev];
+            if (en.type == kSrcNodalSoft) v = v - en.a * ev;
+            else v = en.a * ev;
+        }
+    }
+    F[node] = v;
+}
+
+// UpdateObservation point probes (observation.F90:2633-2668).
+__global__ void k_probes(KGrid g, KProbes p, StepRef sr, int first_n) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= p.n) return;
+    const int n = step_of(sr);
+    const long long row = (long long)(n - first_n) % p.cap;
+    p.ring[row * p.n + q] = g.F[p.comp[q]][p.idx[q]];
+}
+
+__global__ void k_set_step(int* d, int v) { *d = v; }
+__global__ void k_fill16(int16_t* p, long long n, int16_t v) {
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) p[q] = v;
+}
+__global__ void k_add_step(int* d, int v) { *d += v; }
+
+__global__ void k_count_disp(const int16_t* M, const int16_t* slot, int pitch, long long plane, int x0, int x1, int y0,
+                             int y1, int z0, int z1, int* counts) {
+    const long long row = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int ny = y1 - y0 + 1, nz = z1 - z0 + 1;
+    if (row >= (long long)ny * nz) return;
+    const int j = y0 + (int)(row % ny), k = z0 + (int)(row / ny);
+    int cnt = 0;
+    const long long base = (long long)pitch * j + plane * k;
+    for (int i = x0; i <= x1; ++i) cnt += slot[M[base + i]] >= 0;
+    counts[row] = cnt;
+}
+
+__global__ void k_fill_disp(const int16_t* M, const int16_t* slot, int pitch, long long plane, int x0, int x1, int y0,
+                            int y1, int z0, int z1, const long long* offs, int* node, uint8_t* med) {
+    const long long row = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int ny = y1 - y0 + 1, nz = z1 - z0 + 1;
+    if (row >= (long long)ny * nz) return;
+    const int j = y0 + (int)(row % ny), k = z0 + (int)(row / ny);
+    long long o = offs[row];
+    const long long base = (long long)pitch * j + plane * k;
+    for (int i = x0; i <= x1; ++i) {
+        const int s = slot[M[base + i]];
+        if (s >= 0) {
+            node[o] = (int)(base + i);
+            med[o] = (uint8_t)s;
+            ++o;
+        }
+    }
+}
+
+__global__ void k_nonfinite(const float* a, long long n, unsigned int* flag) {
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        if (!isfinite(a[q])) {
+            atomicOr(flag, 1u);
+            return;
+        }
+}
+
+int zchunk_for(int nz, int blocks_xy) {
+    // short chunks: many waves of blocks on 148 SMs, so the last partial wave
+    // costs little; 16 planes keep the carried k-1 plane worthwhile
+    int chunk = 16;
+    while (chunk > 4 && (long long)blocks_xy * ((nz + chunk - 1) / chunk) < 148LL * 4) chunk /= 2;
+    return std::min(chunk, nz);
+}
+
+struct Launch {
+    dim3 grid, block;
+    int y0, z0, z1, zchunk;
+    size_t smem;
+};
+
+Launch plan(const sgpu_ctx* c, int c0, int c1) {
+    int x1 = -1, y0 = 1 << 30, y1 = -1, z0 = 1 << 30, z1 = -1;
+    for (int f = c0; f <= c1; ++f) {
+        x1 = std::max(x1, c->sweep[f].xe - c->ox);
+        y0 = std::min(y0, c->sweep[f].yi - c->oy); y1 = std::max(y1, c->sweep[f].ye - c->oy);
+        z0 = std::min(z0, c->sweep[f].zi - c->oz); z1 = std::max(z1, c->sweep[f].ze - c->oz);
+    }
+    Launch L;
+    L.block = dim3(kBX, kBY, 1);
+    int bx = (x1 + 1 + kBX - 1) / kBX, by = (y1 - y0 + 1 + kBY - 1) / kBY;
+    int nz = z1 - z0 + 1;
+    L.zchunk = zchunk_for(nz, bx * by);
+    L.grid = dim3(bx, by, (nz + L.zchunk - 1) / L.zchunk);
+    L.y0 = y0; L.z0 = z0; L.z1 = z1;
+    const int n1 = c->num_media + 1;
+    L.smem = n1 <= kShTable ? 2 * n1 * sizeof(float) : 0;
+    return L;
+}
+
+sgpu_status check_launch(sgpu_ctx* c, const char* what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return set_error(c, SGPU_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    return SGPU_OK;
+}
+
+template <int MODE> sgpu_status launch_e(sgpu_ctx* c) {
+    Launch L = plan(c, 0, 2);
+    k_efield<MODE><<<L.grid, L.block, L.smem, c->stream>>>(kgrid(c), c->cpml, L.y0, L.z0, L.z1, L.zchunk);
+    return check_launch(c, "k_efield");
+}
+template <int MODE> sgpu_status launch_h(sgpu_ctx* c) {
+    Launch L = plan(c, 3, 5);
+    k_hfield<MODE><<<L.grid, L.block, L.smem, c->stream>>>(kgrid(c), c->cpml, L.y0, L.z0, L.z1, L.zchunk);
+    return check_launch(c, "k_hfield");
+}
+
+bool ready(sgpu_ctx* c) {
+    for (int f = 0; f < 6; ++f)
+        if (!c->media_loaded[f]) return false;
+    return true;
+}
+
+sgpu_status build_sources(sgpu_ctx* c);
+
+template <int NU> void edisp_launch(sgpu_ctx* c, int comp, unsigned blocks) {
+    k_edisp<NU><<<blocks, 256, 0, c->stream>>>(kgrid(c), c->disp, comp);
+}
+
+sgpu_status launch_edisp(sgpu_ctx* c) {
+    if (!c->disp_on) return SGPU_OK;
+    for (int comp = 0; comp < 3; ++comp) {
+        long long n = c->disp.n[comp];
+        if (n == 0) continue;
+        const unsigned blocks = (unsigned)((n + 255) / 256);
+        switch (c->disp.nu_max) {
+            case 1: edisp_launch<1>(c, comp, blocks); break;
+            case 2: edisp_launch<2>(c, comp, blocks); break;
+            case 3: edisp_launch<3>(c, comp, blocks); break;
+            case 4: edisp_launch<4>(c, comp, blocks); break;
+            default: edisp_launch<kMaxPolesPerMedium>(c, comp, blocks); break;
+        }
+        sgpu_status s = check_launch(c, "k_edisp");
+        if (s) return s;
+    }
+    return SGPU_OK;
+}
+
+constexpr int kMaskPW = 1 << kSrcPlaneWave, kMaskNodal = (1 << kSrcNodalSoft) | (1 << kSrcNodalHard),
+              kMaskAll = kMaskPW | kMaskNodal;
+
+sgpu_status launch_sources(sgpu_ctx* c, int side, StepRef sr, int mask = kMaskAll) {
+    if (c->src_dirty) {
+        sgpu_status s = build_sources(c);
+        if (s) return s;
+    }
+    const KSrc& k = c->src[side];
+    if (k.nrows == 0) return SGPU_OK;
+    if (!c->d_tiempo) return set_error(c, SGPU_ERR_STATE, "time vector not set (sgpu_set_time)");
+    if (!sr.dev_n && (sr.n < c->t_n0 || sr.n >= c->t_n0 + c->d_tiempo_count))
+        return set_error(c, SGPU_ERR_ARG, "step outside the time vector");
+    int threads = 128;
+    int blocks = (k.nrows + threads - 1) / threads;
+    k_sources<<<blocks, threads, 0, c->stream>>>(kgrid(c), k, sr, c->d_tiempo, c->t_n0, c->dt, side, mask);
+    return check_launch(c, "k_sources");
+}
+
+sgpu_status launch_probes(sgpu_ctx* c, StepRef sr) {
+    if (c->probes.n == 0) return SGPU_OK;
+    int threads = 128;
+    int blocks = (c->probes.n + threads - 1) / threads;
+    k_probes<<<blocks, threads, 0, c->stream>>>(kgrid(c), c->probes, sr, c->probe_first_n);
+    return check_launch(c, "k_probes");
+}
+
+sgpu_status half_e(sgpu_ctx* c, StepRef sr) {
+    sgpu_status s = c->cpml.on ? launch_e<kBulk | kCpml | kAll>(c) : launch_e<kBulk | kAll>(c);
+    if (s) return s;
+    if ((s = launch_edisp(c))) return s;
+    return launch_sources(c, 0, sr);
+}
+
+sgpu_status half_h(sgpu_ctx* c, StepRef sr) {
+    sgpu_status s = c->cpml.on ? launch_h<kBulk | kCpml | kAll>(c) : launch_h<kBulk | kAll>(c);
+    if (s) return s;
+    return launch_sources(c, 1, sr);
+}
+
+sgpu_status whole_step(sgpu_ctx* c, StepRef sr) {
+    sgpu_status s = half_e(c, sr);
+    if (s) return s;
+    if ((s = half_h(c, sr))) return s;
+    return launch_probes(c, sr);
+}
+
+template <class T> sgpu_status dalloc(sgpu_ctx* c, T** p, size_t n, std::vector<void*>* track = nullptr) {
+    *p = nullptr;
+    if (n == 0) return SGPU_OK;
+    cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return set_error(c, SGPU_ERR_OOM, std::string("cudaMalloc of ") + std::to_string(n * sizeof(T)) + " bytes failed");
+    }
+    if (track) track->push_back(*p);
+    return SGPU_OK;
+}
+
+template <class T> sgpu_status h2d(sgpu_ctx* c, T* d, const T* h, size_t n) {
+    if (n == 0) return SGPU_OK;
+    CUDA_TRY(c, cudaMemcpyAsync(d, h, n * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+    return SGPU_OK;
+}
+
+void free_list(std::vector<void*>& v) {
+    for (void* p : v) cudaFree(p);
+    v.clear();
+}
+
+cudaMemcpy3DParms copy_parms(sgpu_ctx* c, int comp, void* host, void* dev, size_t esz, bool up) {
+    const sgpu_lim& a = c->alloc[comp];
+    size_t ax = a.xe - a.xi + 1, ay = a.ye - a.yi + 1, az = a.ze - a.zi + 1;
+    cudaMemcpy3DParms p{};
+    cudaPitchedPtr hp = make_cudaPitchedPtr(host, ax * esz, ax * esz, ay);
+    cudaPitchedPtr dp = make_cudaPitchedPtr(dev, (size_t)c->pitch * esz, (size_t)c->nxa * esz, c->nya);
+    if (up) { p.srcPtr = hp; p.dstPtr = dp; p.kind = cudaMemcpyHostToDevice; }
+    else { p.srcPtr = dp; p.dstPtr = hp; p.kind = cudaMemcpyDeviceToHost; }
+    p.extent = make_cudaExtent(ax * esz, ay, az);
+    return p;
+}
+
+}  // namespace
+
+// ===========================================================================
+// Level-1 C ABI
+// ===========================================================================
+extern "C" {
+
+const char* sgpu_last_error(const sgpu_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+sgpu_status sgpu_create(const sgpu_grid_desc* d, sgpu_ctx** out) {
+    if (!d || !out) return SGPU_ERR_ARG;
+    *out = nullptr;
+    sgpu_ctx* c = new (std::nothrow) sgpu_ctx();
+    if (!c) return SGPU_ERR_OOM;
+    auto fail = [&](sgpu_status s) {
+        // keep the context alive so the caller can read the message
+        *out = c;
+        return s;
+    };
+    for (int f = 0; f < 6; ++f) {
+        c->alloc[f] = d->alloc[f];
+        c->sweep[f] = d->sweep[f];
+        const sgpu_lim& a = d->alloc[f];
+        const sgpu_lim& w = d->sweep[f];
+        if (a.xe < a.xi || a.ye < a.yi || a.ze < a.zi)
+            return fail(set_error(c, SGPU_ERR_ARG, "empty Alloc range"));
+        if (w.xi <= a.xi || w.xe >= a.xe || w.yi <= a.yi || w.ye >= a.ye || w.zi <= a.zi || w.ze >= a.ze)
+            return fail(set_error(c, SGPU_ERR_ARG, "Sweep must lie strictly inside Alloc"));
+        if (a.xi != d->alloc[0].xi || a.yi != d->alloc[0].yi || a.zi != d->alloc[0].zi)
+            return fail(set_error(c, SGPU_ERR_ARG, "components must share the lower Alloc bounds"));
+    }
+    if (d->num_media < 1 || d->num_media > 32767)
+        return fail(set_error(c, SGPU_ERR_ARG, "num_media out of range"));
+    c->ox = d->alloc[0].xi; c->oy = d->alloc[0].yi; c->oz = d->alloc[0].zi;
+    for (int f = 0; f < 6; ++f) {
+        c->nxa = std::max(c->nxa, d->alloc[f].xe - c->ox + 1);
+        c->nya = std::max(c->nya, d->alloc[f].ye - c->oy + 1);
+        c->nza = std::max(c->nza, d->alloc[f].ze - c->oz + 1);
+    }
+    c->pitch = (c->nxa + 31) / 32 * 32;
+    c->plane = (long long)c->pitch * c->nya;
+    c->vol = c->plane * c->nza;
+    if (c->vol >= (1LL << 31)) return fail(set_error(c, SGPU_ERR_UNSUPPORTED, "grid exceeds 2^31 padded cells"));
+    c->num_media = d->num_media;
+    c->dt = d->dt;
+    cudaError_t e = cudaGetDevice(&c->device);
+    if (e != cudaSuccess) return fail(set_error(c, SGPU_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e)));
+    e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return fail(set_error(c, SGPU_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e)));
+    sgpu_status s;
+    for (int f = 0; f < 6; ++f) {
+        if ((s = dalloc(c, &c->F[f], c->vol))) return fail(s);
+        if ((s = dalloc(c, &c->M[f], c->vol))) return fail(s);
+        CUDA_TRY(c, cudaMemsetAsync(c->F[f], 0, c->vol * sizeof(float), c->stream));
+        // padding cells keep medium 1 (vacuum), as the reference initialises
+        // every media matrix before assigning regions
+    }
+    const int n1 = d->num_media + 1;
+    c->h_g1.assign(d->g1, d->g1 + n1); c->h_g2.assign(d->g2, d->g2 + n1);
+    c->h_gm1.assign(d->gm1, d->gm1 + n1); c->h_gm2.assign(d->gm2, d->gm2 + n1);
+    c->h_pec.assign(n1, 0);
+    if (d->is_pec) c->h_pec.assign(d->is_pec, d->is_pec + n1);
+    else c->h_pec[0] = 1;
+    if ((s = dalloc(c, &c->g1, n1)) || (s = dalloc(c, &c->g2, n1)) || (s = dalloc(c, &c->gm1, n1)) || (s = dalloc(c, &c->gm2, n1)))
+        return fail(s);
+    if ((s = h2d(c, c->g1, d->g1, n1)) || (s = h2d(c, c->g2, d->g2, n1)) || (s = h2d(c, c->gm1, d->gm1, n1)) ||
+        (s = h2d(c, c->gm2, d->gm2, n1)))
+        return fail(s);
+    // metric arrays, re-indexed to local coordinates over the padded box
+    struct M1 { const float* src; int lo, hi, origin, len; std::vector<float>* h; float** dv; };
+    // x metrics span the padded pitch: lanes past the last column read them
+    M1 ms[6] = {{d->idxe, d->alloc[3].xi, d->alloc[3].xe, c->ox, c->pitch, &c->h_idxe, &c->idxe},
+                {d->idye, d->alloc[4].yi, d->alloc[4].ye, c->oy, c->nya, &c->h_idye, &c->idye},
+                {d->idze, d->alloc[5].zi, d->alloc[5].ze, c->oz, c->nza, &c->h_idze, &c->idze},
+                {d->idxh, d->alloc[0].xi, d->alloc[0].xe, c->ox, c->pitch, &c->h_idxh, &c->idxh},
+                {d->idyh, d->alloc[1].yi, d->alloc[1].ye, c->oy, c->nya, &c->h_idyh, &c->idyh},
+                {d->idzh, d->alloc[2].zi, d->alloc[2].ze, c->oz, c->nza, &c->h_idzh, &c->idzh}};
+    for (M1& m : ms) {
+        if (!m.src) return fail(set_error(c, SGPU_ERR_ARG, "missing metric array"));
+        m.h->assign(m.len, 0.0f);
+        for (int i = m.lo; i <= m.hi; ++i) (*m.h)[i - m.origin] = m.src[i - m.lo];
+        if ((s = dalloc(c, m.dv, m.len))) return fail(s);
+        if ((s = h2d(c, *m.dv, m.h->data(), m.len))) return fail(s);
+    }
+    if ((s = dalloc(c, &c->d_step, 1))) return fail(s);
+    if ((s = dalloc(c, &c->d_flag, 1))) return fail(s);
+    CUDA_TRY(c, cudaMemsetAsync(c->d_step, 0, sizeof(int), c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    *out = c;
+    return SGPU_OK;
+}
+
+void sgpu_destroy(sgpu_ctx* c) {
+    if (!c) return;
+    if (c->host_only) {
+        if (c->host && c->host_free) c->host_free(c->host);
+        delete c;
+        return;
+    }
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->graph) cudaGraphExecDestroy(c->graph);
+    for (int f = 0; f < 6; ++f) {
+        cudaFree(c->F[f]);
+        cudaFree(c->M[f]);
+    }
+    cudaFree(c->g1); cudaFree(c->g2); cudaFree(c->gm1); cudaFree(c->gm2);
+    cudaFree(c->idxe); cudaFree(c->idye); cudaFree(c->idze);
+    cudaFree(c->idxh); cudaFree(c->idyh); cudaFree(c->idzh);
+    cudaFree(c->d_tiempo); cudaFree(c->d_step); cudaFree(c->d_flag);
+    free_list(c->cpml_allocs);
+    free_list(c->disp_allocs);
+    free_list(c->src_allocs[0]);
+    free_list(c->src_allocs[1]);
+    free_list(c->probe_allocs);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->host && c->host_free) c->host_free(c->host);
+    delete c;
+}
+
+sgpu_status sgpu_synchronize(sgpu_ctx* c) {
+    if (!c) return SGPU_ERR_ARG;
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_upload_media(sgpu_ctx* c, int comp, const int16_t* mi) {
+    if (!c || !mi || comp < 0 || comp > 5) return set_error(c, SGPU_ERR_ARG, "bad media upload");
+    const sgpu_lim& a = c->alloc[comp];
+    long long n = (long long)(a.xe - a.xi + 1) * (a.ye - a.yi + 1) * (a.ze - a.zi + 1);
+    for (long long q = 0; q < n; ++q)
+        if (mi[q] < 0 || mi[q] > c->num_media) return set_error(c, SGPU_ERR_ARG, "media index outside 0..num_media");
+    // unused padding of the common box is vacuum
+    k_fill16<<<148 * 8, 256, 0, c->stream>>>(c->M[comp], c->vol, (int16_t)1);
+    sgpu_status fs = check_launch(c, "k_fill16");
+    if (fs) return fs;
+    cudaMemcpy3DParms p = copy_parms(c, comp, (void*)mi, c->M[comp], sizeof(int16_t), true);
+    CUDA_TRY(c, cudaMemcpy3DAsync(&p, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    c->media_loaded[comp] = true;
+    c->src_dirty = true;
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_upload_field(sgpu_ctx* c, int comp, const float* f) {
+    if (!c || !f || comp < 0 || comp > 5) return set_error(c, SGPU_ERR_ARG, "bad field upload");
+    cudaMemcpy3DParms p = copy_parms(c, comp, (void*)f, c->F[comp], sizeof(float), true);
+    CUDA_TRY(c, cudaMemcpy3DAsync(&p, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_download_field(sgpu_ctx* c, int comp, float* f) {
+    if (!c || !f || comp < 0 || comp > 5) return set_error(c, SGPU_ERR_ARG, "bad field download");
+    cudaMemcpy3DParms p = copy_parms(c, comp, f, c->F[comp], sizeof(float), false);
+    CUDA_TRY(c, cudaMemcpy3DAsync(&p, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_init_cpml(sgpu_ctx* c, const sgpu_cpml_desc* d) {
+    if (!c || !d) return set_error(c, SGPU_ERR_ARG, "null cpml descriptor");
+    free_list(c->cpml_allocs);
+    KCpml& k = c->cpml;
+    k = KCpml{};
+    sgpu_status s;
+    const int lens[3] = {c->nxa, c->nya, c->nza};
+    const int org[3] = {c->ox, c->oy, c->oz};
+    const sgpu_lim* ah[3] = {&c->alloc[3], &c->alloc[4], &c->alloc[5]};
+    for (int a = 0; a < 3; ++a) {
+        int lo = a == 0 ? ah[a]->xi : (a == 1 ? ah[a]->yi : ah[a]->zi);
+        int hi = a == 0 ? ah[a]->xe : (a == 1 ? ah[a]->ye : ah[a]->ze);
+        const float* src[4] = {d->p_be[a], d->p_ce[a], d->p_bm[a], d->p_cm[a]};
+        const float** dst[4] = {&k.pbe[a], &k.pce[a], &k.pbm[a], &k.pcm[a]};
+        for (int w = 0; w < 4; ++w) {
+            if (!src[w]) return set_error(c, SGPU_ERR_ARG, "missing CPML coefficient vector");
+            std::vector<float> h(lens[a], w == 0 || w == 2 ? 1.0f : 0.0f);
+            for (int i = lo; i <= hi; ++i) h[i - org[a]] = src[w][i - lo];
+            float* dv;
+            if ((s = dalloc(c, &dv, lens[a], &c->cpml_allocs))) return s;
+            if ((s = h2d(c, dv, h.data(), h.size()))) return s;
+            *dst[w] = dv;
+        }
+    }
+    // psi kinds per component: (region pair of the first correction, of the second)
+    // regions: 0 Down 1 Up 2 Left 3 Right 4 Back 5 Front
+    const int pairs[6][2] = {{2, 0}, {0, 4}, {2, 4}, {2, 0}, {0, 4}, {2, 4}};
+    bool any = false;
+    for (int f = 0; f < 6; ++f)
+        for (int w = 0; w < 2; ++w)
+            for (int side = 0; side < 2; ++side) {
+                const sgpu_lim& b = d->pmlc[f][pairs[f][w] + side];
+                Slab& sl = k.s[f][w][side];
+                sl = Slab{b.xi - c->ox, b.xe - c->ox, b.yi - c->oy, b.ye - c->oy, b.zi - c->oz, b.ze - c->oz, nullptr};
+                if (b.xe < b.xi || b.ye < b.yi || b.ze < b.zi) {
+                    sl = Slab{1, 0, 1, 0, 1, 0, nullptr};
+                    continue;
+                }
+                size_t n = (size_t)(b.xe - b.xi + 1) * (b.ye - b.yi + 1) * (b.ze - b.zi + 1);
+                if ((s = dalloc(c, &sl.psi, n, &c->cpml_allocs))) return s;
+                CUDA_TRY(c, cudaMemsetAsync(sl.psi, 0, n * sizeof(float), c->stream));
+                any = true;
+            }
+    k.on = any ? 1 : 0;
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_init_edisp(sgpu_ctx* c, const sgpu_edisp_desc* d) {
+    if (!c || !d) return set_error(c, SGPU_ERR_ARG, "null edisp descriptor");
+    if (!ready(c)) return set_error(c, SGPU_ERR_STATE, "upload the media matrices before sgpu_init_edisp");
+    free_list(c->disp_allocs);
+    c->disp = KDisp{};
+    c->disp_on = false;
+    if (d->nmedia <= 0) return SGPU_OK;
+    if (d->nmedia > 255) return set_error(c, SGPU_ERR_UNSUPPORTED, "more than 255 dispersive media");
+    std::vector<DispMedium> media(d->nmedia);
+    std::vector<int16_t> slot(c->num_media + 1, -1);
+    int off = 0, nu_max = 0;
+    for (int m = 0; m < d->nmedia; ++m) {
+        int np = d->npoles[m];
+        if (np < 0 || np > kMaxPolesPerMedium) return set_error(c, SGPU_ERR_UNSUPPORTED, "too many poles in a medium");
+        int idx = d->medium_index[m];
+        if (idx < 1 || idx > c->num_media) return set_error(c, SGPU_ERR_ARG, "dispersive medium index out of range");
+        slot[idx] = (int16_t)m;
+        DispMedium& dm = media[m];
+        dm = DispMedium{};
+        dm.np = np;
+        dm.nu = 0;
+        for (int p = 0; p < np; ++p) {
+            const double* K = d->kappa + 2 * (off + p);
+            const double* B = d->beta + 2 * (off + p);
+            const double* G = d->g3 + 2 * (off + p);
+            int found = -1;
+            // a pole whose coefficients are the exact conjugates of an earlier
+            // pole keeps the conjugate state: fold it onto that slot
+            for (int u = 0; u < dm.nu && found < 0; ++u)
+                if (dm.kappa[u].x == K[0] && dm.kappa[u].y == -K[1] && dm.beta[u].x == B[0] && dm.beta[u].y == -B[1] &&
+                    dm.g3[u].x == G[0] && dm.g3[u].y == -G[1] && K[1] != 0.0)
+                    found = u;
+            if (found >= 0) {
+                dm.map[p] = found;
+            } else {
+                dm.kappa[dm.nu] = make_double2(K[0], K[1]);
+                dm.beta[dm.nu] = make_double2(B[0], B[1]);
+                dm.g3[dm.nu] = make_double2(G[0], G[1]);
+                dm.map[p] = dm.nu++;
+            }
+        }
+        nu_max = std::max(nu_max, dm.nu);
+        off += np;
+    }
+    sgpu_status s;
+    DispMedium* dmedia;
+    int16_t* dslot;
+    if ((s = dalloc(c, &dmedia, media.size(), &c->disp_allocs))) return s;
+    if ((s = h2d(c, dmedia, media.data(), media.size()))) return s;
+    if ((s = dalloc(c, &dslot, slot.size(), &c->disp_allocs))) return s;
+    if ((s = h2d(c, dslot, slot.data(), slot.size()))) return s;
+    KDisp& k = c->disp;
+    k.media = dmedia;
+    k.slot_of_medium = dslot;
+    k.nu_max = nu_max;
+    k.dt = c->dt;
+    for (int comp = 0; comp < 3; ++comp) {
+        int x0 = c->sweep[comp].xi - c->ox, x1 = c->sweep[comp].xe - c->ox;
+        int y0 = c->sweep[comp].yi - c->oy, y1 = c->sweep[comp].ye - c->oy;
+        int z0 = c->sweep[comp].zi - c->oz, z1 = c->sweep[comp].ze - c->oz;
+        long long rows = (long long)(y1 - y0 + 1) * (z1 - z0 + 1);
+        int* dcount;
+        if ((s = dalloc(c, &dcount, rows))) return s;
+        k_count_disp<<<(unsigned)((rows + 255) / 256), 256, 0, c->stream>>>(c->M[comp], dslot, c->pitch, c->plane, x0, x1,
+                                                                            y0, y1, z0, z1, dcount);
+        if ((s = check_launch(c, "k_count_disp"))) { cudaFree(dcount); return s; }
+        std::vector<int> cnt(rows);
+        cudaError_t e = cudaMemcpyAsync(cnt.data(), dcount, rows * sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) { cudaFree(dcount); return set_error(c, SGPU_ERR_CUDA, cudaGetErrorString(e)); }
+        cudaFree(dcount);
+        std::vector<long long> offs(rows);
+        long long tot = 0;
+        for (long long r = 0; r < rows; ++r) { offs[r] = tot; tot += cnt[r]; }
+        k.n[comp] = tot;
+        if (tot == 0) continue;
+        long long* doffs;
+        if ((s = dalloc(c, &doffs, rows))) return s;
+        if ((s = h2d(c, doffs, offs.data(), rows))) { cudaFree(doffs); return s; }
+        int* node;
+        uint8_t* med;
+        float* prev;
+        double2* J;
+        if ((s = dalloc(c, &node, tot, &c->disp_allocs)) || (s = dalloc(c, &med, tot, &c->disp_allocs)) ||
+            (s = dalloc(c, &prev, tot, &c->disp_allocs)) || (s = dalloc(c, &J, (size_t)tot * std::max(1, nu_max), &c->disp_allocs))) {
+            cudaFree(doffs);
+            return s;
+        }
+        k_fill_disp<<<(unsigned)((rows + 255) / 256), 256, 0, c->stream>>>(c->M[comp], dslot, c->pitch, c->plane, x0, x1, y0,
+                                                                           y1, z0, z1, doffs, node, med);
+        if ((s = check_launch(c, "k_fill_disp"))) { cudaFree(doffs); return s; }
+        CUDA_TRY(c, cudaMemsetAsync(prev, 0, tot * sizeof(float), c->stream));
+        CUDA_TRY(c, cudaMemsetAsync(J, 0, (size_t)tot * std::max(1, nu_max) * sizeof(double2), c->stream));
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+        cudaFree(doffs);
+        k.node[comp] = node;
+        k.med[comp] = med;
+        k.prev[comp] = prev;
+        k.J[comp] = J;
+    }
+    c->disp_on = (k.n[0] + k.n[1] + k.n[2]) > 0;
+    return SGPU_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Sources (plane waves and nodal sources)
+namespace {
+
+int add_table(sgpu_ctx* c, const float* ev, int numus, float delta, int is_pw) {
+    sgpu_ctx::HostSrcTable t;
+    t.samples.assign(ev, ev + numus + 1);
+    t.numus = numus;
+    t.delta = delta;
+    t.is_pw = is_pw;
+    c->src_tables.push_back(t);
+    return (int)c->src_tables.size() - 1;
+}
+
+long long lin(const sgpu_ctx* c, int i, int j, int k) {
+    return (long long)(i - c->ox) + (long long)c->pitch * (j - c->oy) + c->plane * (long long)(k - c->oz);
+}
+
+sgpu_status build_sources(sgpu_ctx* c) {
+    for (int side = 0; side < 2; ++side) {
+        free_list(c->src_allocs[side]);
+        c->src[side] = KSrc{};
+        std::vector<sgpu_ctx::HostEntry> es = c->src_host[side];
+        if (es.empty()) continue;
+        // group by (component, node) keeping the reference order inside a group
+        std::stable_sort(es.begin(), es.end(), [](const sgpu_ctx::HostEntry& a, const sgpu_ctx::HostEntry& b) {
+            if (a.comp != b.comp) return a.comp < b.comp;
+            if (a.node != b.node) return a.node < b.node;
+            return a.order < b.order;
+        });
+        std::vector<int> rnode, rcomp, rptr;
+        std::vector<SrcEntry> ent;
+        for (size_t q = 0; q < es.size(); ++q) {
+            if (q == 0 || es[q].node != es[q - 1].node || es[q].comp != es[q - 1].comp) {
+                rnode.push_back((int)es[q].node);
+                rcomp.push_back(es[q].comp);
+                rptr.push_back((int)ent.size());
+            }
+            ent.push_back(es[q].e);
+        }
+        rptr.push_back((int)ent.size());
+        std::vector<SrcTable> tabs;
+        std::vector<float> samples;
+        for (const auto& t : c->src_tables) {
+            tabs.push_back(SrcTable{t.numus, t.delta, (int)samples.size(), t.is_pw});
+            samples.insert(samples.end(), t.samples.begin(), t.samples.end());
+        }
+        KSrc& k = c->src[side];
+        sgpu_status s;
+        int *drn, *drc, *drp;
+        SrcEntry* de;
+        SrcTable* dt;
+        float* dsm;
+        std::vector<void*>& tr = c->src_allocs[side];
+        if ((s = dalloc(c, &drn, rnode.size(), &tr)) || (s = dalloc(c, &drc, rcomp.size(), &tr)) ||
+            (s = dalloc(c, &drp, rptr.size(), &tr)) || (s = dalloc(c, &de, ent.size(), &tr)) ||
+            (s = dalloc(c, &dt, tabs.size(), &tr)) || (s = dalloc(c, &dsm, samples.size(), &tr)))
+            return s;
+        if ((s = h2d(c, drn, rnode.data(), rnode.size())) || (s = h2d(c, drc, rcomp.data(), rcomp.size())) ||
+            (s = h2d(c, drp, rptr.data(), rptr.size())) || (s = h2d(c, de, ent.data(), ent.size())) ||
+            (s = h2d(c, dt, tabs.data(), tabs.size())) || (s = h2d(c, dsm, samples.data(), samples.size())))
+            return s;
+        k.nrows = (int)rnode.size();
+        k.row_node = drn;
+        k.row_comp = drc;
+        k.row_ptr = drp;
+        k.e = de;
+        k.tab = dt;
+        k.samples = dsm;
+    }
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    c->src_dirty = false;
+    return SGPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+sgpu_status sgpu_add_planewave(sgpu_ctx* c, const sgpu_planewave_desc* d) {
+    if (!c || !d || !d->evol) return set_error(c, SGPU_ERR_ARG, "bad plane-wave descriptor");
+    const int tab = add_table(c, d->evol, d->numus, d->deltaevol, 1);
+    enum { EX = 0, EY, EZ, HX, HY, HZ };
+    // Per face, per side (E: planewaves.F90:914-1170, H: :1215-1470):
+    // {component, incident field, offset along the face normal, sign}.
+    struct Part { int comp, fld, off, sign; };
+    const Part eparts[6][2] = {{{EZ, HY, -1, -1}, {EY, HZ, -1, +1}},   // back
+                               {{EZ, HY, 0, +1}, {EY, HZ, 0, -1}},     // front
+                               {{EX, HZ, -1, -1}, {EZ, HX, -1, +1}},   // left
+                               {{EZ, HX, 0, -1}, {EX, HZ, 0, +1}},     // right
+                               {{EX, HY, -1, +1}, {EY, HX, -1, -1}},   // down
+                               {{EX, HY, 0, -1}, {EY, HX, 0, +1}}};    // up
+    const Part hparts[6][2] = {{{HZ, EY, +1, +1}, {HY, EZ, +1, -1}},
+                               {{HZ, EY, 0, -1}, {HY, EZ, 0, +1}},
+                               {{HX, EZ, +1, +1}, {HZ, EX, +1, -1}},
+                               {{HX, EZ, 0, -1}, {HZ, EX, 0, +1}},
+                               {{HX, EY, +1, -1}, {HY, EX, +1, +1}},
+                               {{HX, EY, 0, +1}, {HY, EX, 0, -1}}};
+    for (int side = 0; side < 2; ++side) {
+        for (int face = 0; face < 6; ++face) {
+            if (!d->active[face]) continue;
+            const int axis = face / 2;  // 0 x (back/front), 1 y (left/right), 2 z (down/up)
+            for (int pi = 0; pi < 2; ++pi) {
+                const Part P = side == 0 ? eparts[face][pi] : hparts[face][pi];
+                const int* L = d->lim[face][P.comp];
+                const int fixed = L[0];
+                // Id of the face: Idxh/Idyh/Idzh (E) or Idxe/Idye/Idze (H) at the fixed index
+                const std::vector<float>* idv[2][3] = {{&c->h_idxh, &c->h_idyh, &c->h_idzh}, {&c->h_idxe, &c->h_idye, &c->h_idze}};
+                const int org[3] = {c->ox, c->oy, c->oz};
+                const float Id = (*idv[side][axis])[fixed - org[axis]];
+                for (int a = L[1]; a <= L[2]; ++a)
+                    for (int b = L[3]; b <= L[4]; ++b) {
+                        int i, j, k;
+                        if (axis == 0) { i = fixed; k = a; j = b; }
+                        else if (axis == 1) { j = fixed; k = a; i = b; }
+                        else { k = fixed; j = a; i = b; }
+                        int si = i, sj = j, sk = k;
+                        if (axis == 0) si += P.off; else if (axis == 1) sj += P.off; else sk += P.off;
+                        // Incid: d = (x*px + y*py + z*pz) - d0 ; the kernel uses d/cluz
+                        const int fl = P.fld;
+                        const int ci[3] = {si, sj, sk};
+                        float xyz[3];
+                        for (int ax = 0; ax < 3; ++ax) {
+                            int q = ci[ax] - d->phys_lo[fl][ax];
+                            if (q < 0 || q >= d->phys_n[fl][ax]) return set_error(c, SGPU_ERR_ARG, "plane-wave node outside PhysCoor");
+                            xyz[ax] = d->phys[fl][ax][q];
+                        }
+                        const float dd = (xyz[0] * d->px + xyz[1] * d->py + xyz[2] * d->pz) - d->d0;
+                        sgpu_ctx::HostEntry he;
+                        he.node = lin(c, i, j, k);
+                        he.comp = P.comp;
+                        he.order = c->src_seq++;
+                        he.e.comp = P.comp;
+                        he.e.type = kSrcPlaneWave;
+                        he.e.table = tab;
+                        he.e.a = dd / d->cluz;
+                        he.e.b = d->fpw[fl];
+                        he.e.c = P.sign > 0 ? Id : -Id;
+                        c->src_host[side].push_back(he);
+                    }
+            }
+        }
+    }
+    c->src_dirty = true;
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_add_nodal(sgpu_ctx* c, const sgpu_nodal_desc* d) {
+    if (!c || !d || !d->evol || d->comp < 0 || d->comp > 5) return set_error(c, SGPU_ERR_ARG, "bad nodal descriptor");
+    if (!c->media_loaded[d->comp]) return set_error(c, SGPU_ERR_STATE, "upload the media matrices before sgpu_add_nodal");
+    const int tab = add_table(c, d->evol, d->numus, d->deltaevol, 0);
+    const bool elec = d->comp < 3;
+    const int side = elec ? 0 : 1;
+    const sgpu_lim& b = d->box;
+    for (int k = b.zi; k <= b.ze; ++k)
+        for (int j = b.yi; j <= b.ye; ++j)
+            for (int i = b.xi; i <= b.xe; ++i) {
+                int16_t m;
+                long long node = lin(c, i, j, k);
+                CUDA_TRY(c, cudaMemcpy(&m, c->M[d->comp] + node, sizeof(int16_t), cudaMemcpyDeviceToHost));
+                // electric sources skip PEC media (nodalsources.F90:455-470)
+                if (elec && c->h_pec[m]) continue;
+                sgpu_ctx::HostEntry he;
+                he.node = node;
+                he.comp = d->comp;
+                he.order = c->src_seq++;
+                he.e.comp = d->comp;
+                he.e.table = tab;
+                he.e.b = 0; he.e.c = 0;
+                if (d->hard) {
+                    he.e.type = kSrcNodalHard;
+                    he.e.a = d->amplitude;
+                } else {
+                    he.e.type = kSrcNodalSoft;
+                    const int a = d->comp % 3;
+                    float I1, I2;
+                    if (elec) {
+                        I1 = a == 0 ? c->h_idyh[j - c->oy] : c->h_idxh[i - c->ox];
+                        I2 = a == 2 ? c->h_idyh[j - c->oy] : c->h_idzh[k - c->oz];
+                    } else {
+                        I1 = a == 0 ? c->h_idye[j - c->oy] : c->h_idxe[i - c->ox];
+                        I2 = a == 2 ? c->h_idye[j - c->oy] : c->h_idze[k - c->oz];
+                    }
+                    const float g = elec ? c->h_g2[m] : c->h_gm2[m];
+                    he.e.a = g * I1 * I2 * d->amplitude;
+                }
+                c->src_host[side].push_back(he);
+            }
+    c->src_dirty = true;
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_set_time(sgpu_ctx* c, int n0, int count, const double* t) {
+    if (!c || !t || count <= 0) return set_error(c, SGPU_ERR_ARG, "bad time vector");
+    cudaFree(c->d_tiempo);
+    c->d_tiempo = nullptr;
+    sgpu_status s;
+    if ((s = dalloc(c, &c->d_tiempo, count))) return s;
+    if ((s = h2d(c, c->d_tiempo, t, count))) return s;
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    c->t_n0 = n0;
+    c->d_tiempo_count = count;
+    c->h_tiempo.assign(t, t + count);
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_set_probes(sgpu_ctx* c, int np, const int* cijk, int cap) {
+    if (!c || np < 0 || (np > 0 && (!cijk || cap <= 0))) return set_error(c, SGPU_ERR_ARG, "bad probe set");
+    free_list(c->probe_allocs);
+    c->probes = KProbes{};
+    c->probe_written = c->probe_read = 0;
+    c->probe_first_n = -1;
+    if (np == 0) return SGPU_OK;
+    std::vector<int> comp(np);
+    std::vector<long long> idx(np);
+    for (int q = 0; q < np; ++q) {
+        int f = cijk[4 * q];
+        if (f < 0 || f > 5) return set_error(c, SGPU_ERR_ARG, "probe component out of range");
+        const sgpu_lim& a = c->alloc[f];
+        int i = cijk[4 * q + 1], j = cijk[4 * q + 2], k = cijk[4 * q + 3];
+        if (i < a.xi || i > a.xe || j < a.yi || j > a.ye || k < a.zi || k > a.ze)
+            return set_error(c, SGPU_ERR_ARG, "probe outside Alloc");
+        comp[q] = f;
+        idx[q] = lin(c, i, j, k);
+    }
+    sgpu_status s;
+    int* dc;
+    long long* di;
+    float* ring;
+    if ((s = dalloc(c, &dc, np, &c->probe_allocs)) || (s = dalloc(c, &di, np, &c->probe_allocs)) ||
+        (s = dalloc(c, &ring, (size_t)np * cap, &c->probe_allocs)))
+        return s;
+    if ((s = h2d(c, dc, comp.data(), np)) || (s = h2d(c, di, idx.data(), np))) return s;
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    c->probes = KProbes{np, dc, di, ring, cap};
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_read_probes(sgpu_ctx* c, float* out, int max_steps, int* nsteps, int* first_n) {
+    if (!c || !nsteps) return set_error(c, SGPU_ERR_ARG, "bad probe read");
+    *nsteps = 0;
+    if (first_n) *first_n = c->probe_first_n + (int)c->probe_read;
+    if (c->probes.n == 0) return SGPU_OK;
+    long long pending = c->probe_written - c->probe_read;
+    long long take = std::min<long long>(pending, max_steps);
+    if (take <= 0) return SGPU_OK;
+    if (!out) return set_error(c, SGPU_ERR_ARG, "null output");
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    const int np = c->probes.n, cap = c->probes.cap;
+    for (long long r = 0; r < take; ++r) {
+        long long row = (c->probe_read + r) % cap;
+        CUDA_TRY(c, cudaMemcpy(out + r * np, c->probes.ring + row * np, np * sizeof(float), cudaMemcpyDeviceToHost));
+    }
+    c->probe_read += take;
+    *nsteps = (int)take;
+    return SGPU_OK;
+}
+
+namespace {
+sgpu_status note_probe_rows(sgpu_ctx* c, int n0, int count) {
+    if (c->probes.n == 0) return SGPU_OK;
+    if (c->probe_first_n < 0) c->probe_first_n = n0;
+    if (n0 != c->probe_first_n + c->probe_written)
+        return set_error(c, SGPU_ERR_STATE, "probe rows must be recorded for consecutive steps");
+    if (c->probe_written + count - c->probe_read > c->probes.cap)
+        return set_error(c, SGPU_ERR_STATE, "probe ring full: read the probes first");
+    return SGPU_OK;
+}
+}  // namespace
+
+#define SGPU_READY(c)                                                                            \
+    do {                                                                                         \
+        if (!(c)) return SGPU_ERR_ARG;                                                           \
+        if (!ready(c)) return set_error((c), SGPU_ERR_STATE, "media matrices not uploaded");      \
+    } while (0)
+
+sgpu_status sgpu_advance_ex(sgpu_ctx* c) { SGPU_READY(c); return launch_e<kBulk | kCx>(c); }
+sgpu_status sgpu_advance_ey(sgpu_ctx* c) { SGPU_READY(c); return launch_e<kBulk | kCy>(c); }
+sgpu_status sgpu_advance_ez(sgpu_ctx* c) { SGPU_READY(c); return launch_e<kBulk | kCz>(c); }
+sgpu_status sgpu_advance_electric_cpml(sgpu_ctx* c) {
+    SGPU_READY(c);
+    return c->cpml.on ? launch_e<kCpml | kAll>(c) : SGPU_OK;
+}
+sgpu_status sgpu_advance_edispersive_e(sgpu_ctx* c) { SGPU_READY(c); return launch_edisp(c); }
+sgpu_status sgpu_advance_planewave_e(sgpu_ctx* c, int n) {
+    SGPU_READY(c);
+    return launch_sources(c, 0, StepRef{nullptr, n}, kMaskPW);
+}
+sgpu_status sgpu_advance_nodal_e(sgpu_ctx* c, int n) {
+    SGPU_READY(c);
+    return launch_sources(c, 0, StepRef{nullptr, n}, kMaskNodal);
+}
+sgpu_status sgpu_advance_hx(sgpu_ctx* c) { SGPU_READY(c); return launch_h<kBulk | kCx>(c); }
+sgpu_status sgpu_advance_hy(sgpu_ctx* c) { SGPU_READY(c); return launch_h<kBulk | kCy>(c); }
+sgpu_status sgpu_advance_hz(sgpu_ctx* c) { SGPU_READY(c); return launch_h<kBulk | kCz>(c); }
+sgpu_status sgpu_advance_magnetic_cpml(sgpu_ctx* c) {
+    SGPU_READY(c);
+    return c->cpml.on ? launch_h<kCpml | kAll>(c) : SGPU_OK;
+}
+sgpu_status sgpu_advance_planewave_h(sgpu_ctx* c, int n) {
+    SGPU_READY(c);
+    return launch_sources(c, 1, StepRef{nullptr, n}, kMaskPW);
+}
+sgpu_status sgpu_advance_nodal_h(sgpu_ctx* c, int n) {
+    SGPU_READY(c);
+    return launch_sources(c, 1, StepRef{nullptr, n}, kMaskNodal);
+}
+sgpu_status sgpu_update_observation(sgpu_ctx* c, int n) {
+    SGPU_READY(c);
+    sgpu_status s = note_probe_rows(c, n, 1);
+    if (s) return s;
+    s = launch_probes(c, StepRef{nullptr, n});
+    if (!s && c->probes.n) c->probe_written += 1;
+    return s;
+}
+
+sgpu_status sgpu_advance_e(sgpu_ctx* c, int n) { SGPU_READY(c); return half_e(c, StepRef{nullptr, n}); }
+sgpu_status sgpu_advance_h(sgpu_ctx* c, int n) { SGPU_READY(c); return half_h(c, StepRef{nullptr, n}); }
+
+sgpu_status sgpu_advance_steps(sgpu_ctx* c, int n0, int count) {
+    SGPU_READY(c);
+    if (count <= 0) return SGPU_OK;
+    if (c->src_dirty) {
+        sgpu_status s = build_sources(c);
+        if (s) return s;
+    }
+    const bool has_src = c->src[0].nrows + c->src[1].nrows > 0;
+    if (has_src && (n0 < c->t_n0 || n0 + count > c->t_n0 + c->d_tiempo_count))
+        return set_error(c, SGPU_ERR_ARG, "steps outside the time vector");
+    sgpu_status s = note_probe_rows(c, n0, count);
+    if (s) return s;
+    const int chunk = std::min(count, 32);
+    if (!c->graph || c->graph_steps != chunk) {
+        if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
+        cudaGraph_t g;
+        CUDA_TRY(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        sgpu_status cs = SGPU_OK;
+        for (int q = 0; q < chunk && !cs; ++q) cs = whole_step(c, StepRef{c->d_step, q});
+        if (!cs) {
+            k_add_step<<<1, 1, 0, c->stream>>>(c->d_step, chunk);
+            cs = check_launch(c, "k_add_step");
+        }
+        cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+        if (cs) { if (e == cudaSuccess) cudaGraphDestroy(g); return cs; }
+        if (e != cudaSuccess) return set_error(c, SGPU_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&c->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) { c->graph = nullptr; return set_error(c, SGPU_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e)); }
+        c->graph_steps = chunk;
+    }
+    k_set_step<<<1, 1, 0, c->stream>>>(c->d_step, n0);
+    if ((s = check_launch(c, "k_set_step"))) return s;
+    int done = 0;
+    while (count - done >= chunk) {
+        CUDA_TRY(c, cudaGraphLaunch(c->graph, c->stream));
+        done += chunk;
+    }
+    for (; done < count; ++done)
+        if ((s = whole_step(c, StepRef{nullptr, n0 + done}))) return s;
+    if (c->probes.n) c->probe_written += count;
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_elapsed_steps(sgpu_ctx* c, int n0, int count, float* ms) {
+    SGPU_READY(c);
+    if (!ms) return set_error(c, SGPU_ERR_ARG, "null output");
+    cudaEvent_t a, b;
+    CUDA_TRY(c, cudaEventCreate(&a));
+    CUDA_TRY(c, cudaEventCreate(&b));
+    CUDA_TRY(c, cudaEventRecord(a, c->stream));
+    sgpu_status s = sgpu_advance_steps(c, n0, count);
+    CUDA_TRY(c, cudaEventRecord(b, c->stream));
+    CUDA_TRY(c, cudaEventSynchronize(b));
+    CUDA_TRY(c, cudaEventElapsedTime(ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return s;
+}
+
+sgpu_status sgpu_profile_steps(sgpu_ctx* c, int n0, int count, float* ms6) {
+    SGPU_READY(c);
+    if (!ms6) return set_error(c, SGPU_ERR_ARG, "null output");
+    sgpu_status s = note_probe_rows(c, n0, count);
+    if (s) return s;
+    if (c->src_dirty && (s = build_sources(c))) return s;
+    cudaEvent_t ev[7];
+    for (auto& e : ev) CUDA_TRY(c, cudaEventCreate(&e));
+    for (int q = 0; q < 6; ++q) ms6[q] = 0.0f;
+    for (int n = n0; n < n0 + count && !s; ++n) {
+        StepRef sr{nullptr, n};
+        cudaEventRecord(ev[0], c->stream);
+        s = c->cpml.on ? launch_e<kBulk | kCpml | kAll>(c) : launch_e<kBulk | kAll>(c);
+        cudaEventRecord(ev[1], c->stream);
+        if (!s) s = launch_edisp(c);
+        cudaEventRecord(ev[2], c->stream);
+        if (!s) s = launch_sources(c, 0, sr);
+        cudaEventRecord(ev[3], c->stream);
+        if (!s) s = c->cpml.on ? launch_h<kBulk | kCpml | kAll>(c) : launch_h<kBulk | kAll>(c);
+        cudaEventRecord(ev[4], c->stream);
+        if (!s) s = launch_sources(c, 1, sr);
+        cudaEventRecord(ev[5], c->stream);
+        if (!s) s = launch_probes(c, sr);
+        cudaEventRecord(ev[6], c->stream);
+        CUDA_TRY(c, cudaEventSynchronize(ev[6]));
+        for (int q = 0; q < 6; ++q) {
+            float t = 0;
+            cudaEventElapsedTime(&t, ev[q], ev[q + 1]);
+            ms6[q] += t;
+        }
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    if (!s && c->probes.n) c->probe_written += count;
+    return s;
+}
+
+sgpu_status sgpu_algorithmic_bytes(const sgpu_ctx* c, double* b6) {
+    if (!c || !b6) return SGPU_ERR_ARG;
+    auto cells = [](const sgpu_lim& l) { return (double)(l.xe - l.xi + 1) * (l.ye - l.yi + 1) * (l.ze - l.zi + 1); };
+    auto psi_bytes = [&](int c0) {
+        double b = 0;
+        for (int f = c0; f < c0 + 3; ++f)
+            for (int w = 0; w < 2; ++w)
+                for (int sd = 0; sd < 2; ++sd) {
+                    const Slab& sl = c->cpml.s[f][w][sd];
+                    if (sl.psi) b += 8.0 * (sl.xhi - sl.xlo + 1) * (sl.yhi - sl.ylo + 1) * (sl.zhi - sl.zlo + 1);
+                }
+        return b;
+    };
+    // E (H) half step: every swept node of the three updated components is
+    // read and written once (8 B) with its int16 medium (2 B), and each node
+    // of the three other components is read once (4 B); psi points are read
+    // and written (8 B).  Neighbour re-reads and coefficient tables are not
+    // counted.
+    double e = 0, h = 0;
+    for (int f = 0; f < 3; ++f) e += cells(c->sweep[f]) * 10.0 + cells(c->sweep[f + 3]) * 4.0;
+    for (int f = 3; f < 6; ++f) h += cells(c->sweep[f]) * 10.0 + cells(c->sweep[f - 3]) * 4.0;
+    b6[0] = e + psi_bytes(0);
+    // ADE node: index 4 + medium slot 1 + E 8 + previous E 8 + 32 per state slot
+    double nodes = 0;
+    for (int comp = 0; comp < 3; ++comp) nodes += (double)c->disp.n[comp];
+    b6[1] = c->disp_on ? nodes * (21.0 + 32.0 * c->disp.nu_max) : 0.0;
+    b6[2] = 0;
+    b6[3] = h + psi_bytes(3);
+    b6[4] = 0;
+    b6[5] = 8.0 * c->probes.n;
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_select_device(int device) {
+    return cudaSetDevice(device) == cudaSuccess ? SGPU_OK : SGPU_ERR_CUDA;
+}
+
+sgpu_status sgpu_kernels_per_step(const sgpu_ctx* c, int* n) {
+    if (!c || !n) return SGPU_ERR_ARG;
+    int k = 2;  // E and H field kernels
+    for (int comp = 0; comp < 3; ++comp) k += c->disp_on && c->disp.n[comp] > 0;
+    k += c->src[0].nrows > 0;
+    k += c->src[1].nrows > 0;
+    k += c->probes.n > 0;
+    *n = k;
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_check_finite(sgpu_ctx* c) {
+    if (!c) return SGPU_ERR_ARG;
+    CUDA_TRY(c, cudaMemsetAsync(c->d_flag, 0, sizeof(unsigned int), c->stream));
+    for (int f = 0; f < 6; ++f) {
+        k_nonfinite<<<148 * 8, 256, 0, c->stream>>>(c->F[f], c->vol, c->d_flag);
+        sgpu_status s = check_launch(c, "k_nonfinite");
+        if (s) return s;
+    }
+    unsigned int flag = 0;
+    CUDA_TRY(c, cudaMemcpyAsync(&flag, c->d_flag, sizeof(flag), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    if (flag) return set_error(c, SGPU_ERR_NONFINITE, "non-finite field value found");
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_device_bytes(const sgpu_ctx* c, uint64_t* bytes) {
+    if (!c || !bytes) return SGPU_ERR_ARG;
+    uint64_t b = (uint64_t)c->vol * 6 * (sizeof(float) + sizeof(int16_t));
+    for (int f = 0; f < 6; ++f)
+        for (int w = 0; w < 2; ++w)
+            for (int s = 0; s < 2; ++s) {
+                const Slab& sl = c->cpml.s[f][w][s];
+                if (sl.psi) b += (uint64_t)(sl.xhi - sl.xlo + 1) * (sl.yhi - sl.ylo + 1) * (sl.zhi - sl.zlo + 1) * 4;
+            }
+    for (int comp = 0; comp < 3; ++comp)
+        b += (uint64_t)c->disp.n[comp] * (4 + 1 + 4 + 16 * (uint64_t)std::max(1, c->disp.nu_max));
+    *bytes = b;
+    return SGPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,185 @@
+// Internal structures of libsemba_gpu.so (not part of the C ABI).
+//
+// Device layout: the six field components and the six media matrices share
+// one padded box, the union of the components' sgg%Alloc ranges.  Local
+// index l = absolute - origin on every axis, where origin is the common
+// lower Alloc bound (-layers-1); a component whose Alloc range is one cell
+// shorter simply leaves the last slab unused.  Rows are padded to a
+// multiple of 32 floats so every row starts on a 128-byte boundary.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/semba_gpu.h"
+
+namespace sgpu {
+
+constexpr int kMaxPolesPerMedium = 8;
+
+// A CPML slab in local coordinates with its psi array (dense over the box,
+// x fastest).
+struct Slab {
+    int xlo, xhi, ylo, yhi, zlo, zhi;
+    float* psi;
+};
+
+// Kernel view of the grid: fields, media, coefficient tables, metrics and
+// the sweep boxes, all in local coordinates.
+struct KGrid {
+    float* F[6];
+    const int16_t* M[6];
+    const float *g1, *g2, *gm1, *gm2;
+    const float *idxe, *idye, *idze, *idxh, *idyh, *idzh;
+    int pitch;
+    long long plane;
+    int sw[6][6];  // [comp][xlo xhi ylo yhi zlo zhi]
+    int nmed1;     // num_media + 1
+};
+
+// psi kinds, two per component in the order the reference applies them:
+//   Ex: y(+) z(-)   Ey: z(+) x(-)   Ez: y(-) x(+)
+//   Hx: y(-) z(+)   Hy: z(-) x(+)   Hz: y(+) x(-)
+struct KCpml {
+    const float *pbe[3], *pce[3], *pbm[3], *pcm[3];
+    Slab s[6][2][2];  // [comp][which of the two][lo side, hi side]
+    int on;
+};
+
+// Electric pole-residue media (folded conjugate pairs share one state).
+struct DispMedium {
+    int np;                       // poles of the reference
+    int nu;                       // unique poles carrying state
+    int map[kMaxPolesPerMedium];  // pole -> unique state slot
+    double2 kappa[kMaxPolesPerMedium], beta[kMaxPolesPerMedium], g3[kMaxPolesPerMedium];
+};
+
+struct KDisp {
+    const int* node[3];           // linear local index per node
+    const uint8_t* med[3];        // dispersive-medium slot per node
+    float* prev[3];
+    double2* J[3];                // [unique slot][node]
+    long long n[3];
+    const DispMedium* media;
+    const int16_t* slot_of_medium;  // media index -> slot (-1 none)
+    int nu_max;
+    double dt;
+};
+
+// One source contribution applied after the curl/CPML/ADE work of a half
+// step, in the reference's order (plane-wave faces, then nodal sources).
+enum { kSrcPlaneWave = 0, kSrcNodalSoft = 1, kSrcNodalHard = 2 };
+struct SrcEntry {
+    int comp;
+    int type;
+    int table;
+    float a, b, c;  // plane wave: a = d/c, b = fpw, c = +-Id ; soft: a = G2*I1*I2*amp ; hard: a = amp
+};
+struct SrcTable {
+    int numus;
+    float delta;
+    int offset;  // into the concatenated samples
+    int is_pw;
+};
+struct KSrc {
+    int nrows;
+    const int* row_node;   // local linear index of each node
+    const int* row_comp;
+    const int* row_ptr;    // nrows + 1
+    const SrcEntry* e;
+    const SrcTable* tab;
+    const float* samples;
+};
+
+struct KProbes {
+    int n;
+    const int* comp;
+    const long long* idx;
+    float* ring;
+    int cap;
+};
+
+struct StepRef {
+    const int* dev_n;  // if non-null, the step index is read from here
+    int n;
+};
+
+}  // namespace sgpu
+
+struct sgpu_ctx {
+    std::string err;
+    cudaStream_t stream = nullptr;
+    int device = 0;
+    // geometry
+    sgpu_lim alloc[6], sweep[6];
+    int ox = 0, oy = 0, oz = 0;
+    int nxa = 0, nya = 0, nza = 0;
+    int pitch = 0;
+    long long plane = 0, vol = 0;
+    int num_media = 0;
+    double dt = 0;
+    // device buffers
+    float* F[6] = {};
+    int16_t* M[6] = {};
+    float *g1 = nullptr, *g2 = nullptr, *gm1 = nullptr, *gm2 = nullptr;
+    float *idxe = nullptr, *idye = nullptr, *idze = nullptr, *idxh = nullptr, *idyh = nullptr, *idzh = nullptr;
+    std::vector<float> h_g1, h_g2, h_gm1, h_gm2;
+    std::vector<uint8_t> h_pec;
+    std::vector<float> h_idxe, h_idye, h_idze, h_idxh, h_idyh, h_idzh;  // local-indexed
+    bool media_loaded[6] = {};
+    // CPML
+    sgpu::KCpml cpml{};
+    std::vector<void*> cpml_allocs;
+    // ADE
+    bool disp_on = false;
+    sgpu::KDisp disp{};
+    std::vector<void*> disp_allocs;
+    // sources
+    struct HostSrcTable {
+        std::vector<float> samples;
+        int numus;
+        float delta;
+        int is_pw;
+    };
+    std::vector<HostSrcTable> src_tables;
+    struct HostEntry {
+        long long node;
+        int comp;
+        int order;  // sequence number (reference order)
+        sgpu::SrcEntry e;
+    };
+    std::vector<HostEntry> src_host[2];  // [E side, H side]
+    sgpu::KSrc src[2]{};
+    std::vector<void*> src_allocs[2];
+    bool src_dirty = true;
+    int src_seq = 0;
+    // time
+    std::vector<double> h_tiempo;
+    int t_n0 = 0;
+    double* d_tiempo = nullptr;
+    int d_tiempo_count = 0;
+    int* d_step = nullptr;
+    // probes
+    sgpu::KProbes probes{};
+    std::vector<void*> probe_allocs;
+    long long probe_written = 0;  // rows written in total
+    long long probe_read = 0;
+    int probe_first_n = -1;
+    // graph
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+    // scratch
+    unsigned int* d_flag = nullptr;
+    // level-2 host data kept for inspection; host_only contexts (from
+    // sgpu_host_plan) own no device resources
+    bool host_only = false;
+    void* host = nullptr;
+    void (*host_free)(void*) = nullptr;
+};
+
+namespace sgpu {
+sgpu_status set_error(sgpu_ctx* c, sgpu_status code, const std::string& msg);
+KGrid kgrid(const sgpu_ctx* c);
+}  // namespace sgpu

@@ -1,0 +1,188 @@
+"""Solver: one FDTD problem on one GPU through libsemba_gpu.
+
+Three ways to advance, all bit-identical:
+
+* ``mode="graph"`` (default) -- ``sgpu_advance_steps``: whole steps replayed
+  from a CUDA graph of up to 32 captured steps;
+* ``mode="fused"`` -- ``sgpu_advance_e`` / ``sgpu_advance_h`` /
+  ``sgpu_update_observation`` per step;
+* ``mode="routines"`` -- one call per reference routine, in the order of
+  timestepping.F90:1286-1742 (Advance_Ex, Ey, Ez, AdvanceelectricCPML,
+  AdvanceEDispersiveE, AdvancePlaneWaveE, AdvanceNodalE, Advance_Hx, Hy, Hz,
+  AdvanceMagneticCPML, AdvancePlaneWaveH, AdvanceNodalH, UpdateObservation).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .case import Problem
+
+
+class Solver:
+    def __init__(self, problem: Problem, variant: str = "exact", probe_capacity: int = 1024,
+                 max_steps: int | None = None):
+        self.problem = problem
+        self.lib = _lib.load(variant)
+        self.variant = variant
+        self.probe_capacity = probe_capacity
+        desc, self._keep = problem.to_desc(probe_capacity)
+        self.max_steps = int(max_steps if max_steps is not None else problem.nsteps)
+        h = C.c_void_p()
+        rc = self.lib.sgpu_host_create(C.byref(desc), self.max_steps, C.byref(h))
+        self._h = h
+        if rc:
+            msg = self.lib.sgpu_last_error(h).decode() if h.value else ""
+            self.close()
+            raise _lib.SembaGpuError(f"sgpu_host_create failed ({_lib.ERRORS.get(rc, rc)}): {msg}")
+        self.n = 0
+        dt = C.c_double()
+        nm = C.c_int()
+        a6, s6, q6 = (_lib.Lim * 6)(), (_lib.Lim * 6)(), (_lib.Lim * 6)()
+        self._check(self.lib.sgpu_host_info(h, C.byref(dt), C.byref(nm), a6, s6, q6))
+        self.dt = dt.value
+        self.num_media = nm.value
+        self.alloc = [a.tuple() for a in a6]
+        self.sweep = [s.tuple() for s in s6]
+        self.sinpml = [q.tuple() for q in q6]
+        self.nprobes = len(problem.probes)
+        self._probe_rows: list[np.ndarray] = []
+
+    # -- plumbing ----------------------------------------------------------
+    def _check(self, rc: int, what: str = "") -> None:
+        if rc:
+            msg = self.lib.sgpu_last_error(self._h).decode()
+            raise _lib.SembaGpuError(f"{what or 'libsemba_gpu'} failed ({_lib.ERRORS.get(rc, rc)}): {msg}")
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self.lib.sgpu_destroy(self._h)
+        self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    # -- stepping ----------------------------------------------------------
+    def step(self, count: int = 1, mode: str = "graph") -> None:
+        """Advance `count` whole steps from the current step index."""
+        if self.n + count > self.max_steps + 1:
+            raise _lib.SembaGpuError("beyond the time vector built at creation (max_steps)")
+        lib, h = self.lib, self._h
+        done = 0
+        while done < count:
+            room = self.probe_capacity - self._pending() if self.nprobes else count - done
+            if room <= 0:
+                self._drain()
+                continue
+            k = min(count - done, room)
+            n0 = self.n
+            if mode == "graph":
+                self._check(lib.sgpu_advance_steps(h, n0, k), "sgpu_advance_steps")
+            elif mode == "fused":
+                for n in range(n0, n0 + k):
+                    self._check(lib.sgpu_advance_e(h, n), "sgpu_advance_e")
+                    self._check(lib.sgpu_advance_h(h, n), "sgpu_advance_h")
+                    self._check(lib.sgpu_update_observation(h, n), "sgpu_update_observation")
+            elif mode == "routines":
+                for n in range(n0, n0 + k):
+                    for f in (lib.sgpu_advance_ex, lib.sgpu_advance_ey, lib.sgpu_advance_ez,
+                              lib.sgpu_advance_electric_cpml, lib.sgpu_advance_edispersive_e):
+                        self._check(f(h))
+                    self._check(lib.sgpu_advance_planewave_e(h, n))
+                    self._check(lib.sgpu_advance_nodal_e(h, n))
+                    for f in (lib.sgpu_advance_hx, lib.sgpu_advance_hy, lib.sgpu_advance_hz,
+                              lib.sgpu_advance_magnetic_cpml):
+                        self._check(f(h))
+                    self._check(lib.sgpu_advance_planewave_h(h, n))
+                    self._check(lib.sgpu_advance_nodal_h(h, n))
+                    self._check(lib.sgpu_update_observation(h, n))
+            else:
+                raise ValueError(mode)
+            self.n += k
+            done += k
+            if self.nprobes and self._pending() >= self.probe_capacity:
+                self._drain()
+
+    def _pending(self) -> int:
+        return self.n - sum(len(r) for r in self._probe_rows)
+
+    def _drain(self) -> None:
+        if not self.nprobes:
+            return
+        buf = np.empty((self.probe_capacity, self.nprobes), np.float32)
+        ns, first = C.c_int(), C.c_int()
+        self._check(self.lib.sgpu_read_probes(self._h, buf.ctypes.data_as(_lib.c_float_p), self.probe_capacity,
+                                              C.byref(ns), C.byref(first)), "sgpu_read_probes")
+        if ns.value:
+            self._probe_rows.append(buf[: ns.value].copy())
+
+    def run(self, nsteps: int | None = None, mode: str = "graph") -> np.ndarray:
+        """Run the remaining steps (or `nsteps`) and return the probe traces."""
+        nsteps = self.problem.nsteps + 1 - self.n if nsteps is None else nsteps
+        self.step(nsteps, mode=mode)
+        return self.probes()
+
+    def probes(self) -> np.ndarray:
+        """All probe rows recorded so far, [step, probe] (FP32)."""
+        self._drain()
+        if not self._probe_rows:
+            return np.zeros((0, self.nprobes), np.float32)
+        return np.concatenate(self._probe_rows, axis=0)
+
+    def synchronize(self) -> None:
+        self._check(self.lib.sgpu_synchronize(self._h), "sgpu_synchronize")
+
+    # -- data --------------------------------------------------------------
+    def field(self, comp: int) -> np.ndarray:
+        """Field component (0..5) over its Alloc range, Fortran order, as a
+        3-D array indexed [i, j, k] relative to the Alloc lower corner."""
+        xi, xe, yi, ye, zi, ze = self.alloc[comp]
+        out = np.empty((ze - zi + 1, ye - yi + 1, xe - xi + 1), np.float32)
+        self._check(self.lib.sgpu_download_field(self._h, comp, out.ctypes.data_as(_lib.c_float_p)), "download")
+        return out.transpose(2, 1, 0)
+
+    def media(self, comp: int) -> np.ndarray:
+        xi, xe, yi, ye, zi, ze = self.alloc[comp]
+        out = np.empty((ze - zi + 1, ye - yi + 1, xe - xi + 1), np.int16)
+        self._check(self.lib.sgpu_host_get_media(self._h, comp, out.ctypes.data_as(C.POINTER(C.c_int16))), "media")
+        return out.transpose(2, 1, 0)
+
+    def g_tables(self):
+        n = self.num_media + 1
+        arrs = [np.empty(n, np.float32) for _ in range(4)]
+        self._check(self.lib.sgpu_host_get_g(self._h, *[a.ctypes.data_as(_lib.c_float_p) for a in arrs]))
+        return arrs
+
+    def metric(self, which: int):
+        lo, hi = C.c_int(), C.c_int()
+        self._check(self.lib.sgpu_host_get_metric(self._h, which, None, C.byref(lo), C.byref(hi)))
+        out = np.empty(hi.value - lo.value + 1, np.float32)
+        self._check(self.lib.sgpu_host_get_metric(self._h, which, out.ctypes.data_as(_lib.c_float_p), None, None))
+        return lo.value, out
+
+    def check_finite(self) -> bool:
+        rc = self.lib.sgpu_check_finite(self._h)
+        if rc == 5:
+            return False
+        self._check(rc, "sgpu_check_finite")
+        return True
+
+    def device_bytes(self) -> int:
+        b = C.c_uint64()
+        self._check(self.lib.sgpu_device_bytes(self._h, C.byref(b)))
+        return b.value

@@ -1,0 +1,31 @@
+"""Scaled variants of the benchmark configurations for parity tests."""
+from functools import lru_cache
+from pathlib import Path
+import tempfile
+
+from semba_fdtd_b200 import casegen, read_case
+
+_DIR = Path(tempfile.mkdtemp(prefix="semba_cases_"))
+
+
+@lru_cache(maxsize=None)
+def small(n=24, steps=120, layers=6):
+    """Plain small: vacuum, CPML, TF/SF plane wave, Ex/Hy probes."""
+    return read_case(casegen.plain_small(_DIR / f"small{n}", n=n, steps=steps, inset=5, nprobes=4, layers=layers))
+
+
+@lru_cache(maxsize=None)
+def mid(n=40, steps=120, layers=5):
+    """Plain mid: lossy sphere and PEC/dielectric blocks inside the TF/SF box."""
+    return read_case(casegen.plain_mid(_DIR / f"mid{n}", n=n, steps=steps, inset=6, radius=max(3, n // 5), nblocks=6,
+                                       nprobes=12, layers=layers, edge=(2, max(3, n // 5))))
+
+
+@lru_cache(maxsize=None)
+def disp(n=32, steps=120, layers=5):
+    """Dispersive: graded mesh, pole-residue blocks, soft Ez dipole."""
+    return read_case(casegen.dispersive_large(_DIR / f"disp{n}", n=n, steps=steps, layers=layers,
+                                              edge=(4, max(5, n // 3)), nprobes=6))
+
+
+ALL = {"small": small, "mid": mid, "disp": disp}

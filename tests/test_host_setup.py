@@ -1,0 +1,90 @@
+"""CPU tests of the C ABI library's host side (no GPU needed): the library
+loads and exports every entry point of include/semba_gpu.h, and the level-2
+set-up (sgpu_host_plan) produces exactly the oracle's dt, coefficient tables,
+metric/CPML vectors and media matrices."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from cases import ALL
+from semba_fdtd_b200 import _lib
+
+import oracle
+
+
+def test_library_exports_every_declared_symbol():
+    for variant in ("exact", "fast"):
+        lib = C.CDLL(str(_lib.lib_path(variant)))
+        missing = [s for s in _lib.exported_symbols() if not hasattr(lib, s)]
+        assert not missing, f"{variant}: {missing}"
+
+
+def _plan(pb):
+    lib = _lib.load()
+    d, keep = pb.to_desc()
+    h = C.c_void_p()
+    assert lib.sgpu_host_plan(C.byref(d), pb.nsteps, C.byref(h)) == 0
+    return lib, h
+
+
+@pytest.mark.parametrize("name", list(ALL))
+def test_host_plan_matches_oracle_setup(name):
+    pb = ALL[name]()
+    lib, h = _plan(pb)
+    try:
+        o = oracle.Oracle(pb)
+        dt, nm = C.c_double(), C.c_int()
+        a6, s6, q6 = (_lib.Lim * 6)(), (_lib.Lim * 6)(), (_lib.Lim * 6)()
+        assert lib.sgpu_host_info(h, C.byref(dt), C.byref(nm), a6, s6, q6) == 0
+        # NFDE2sgg time step and the media count after CreatePMLmatrix
+        assert dt.value == o.dt
+        assert nm.value == o.num_media
+        assert [a.tuple() for a in a6] == o.alloc
+        assert [s.tuple() for s in s6] == o.sweep
+        assert [q.tuple() for q in q6] == o.sinpml
+        n1 = nm.value + 1
+        hg = [np.empty(n1, np.float32) for _ in range(4)]
+        lib.sgpu_host_get_g(h, *[x.ctypes.data_as(_lib.c_float_p) for x in hg])
+        for a, b in zip(hg, o.g_tables()):
+            np.testing.assert_array_equal(a, b)
+        for w in range(18):
+            lo, hi = C.c_int(), C.c_int()
+            lib.sgpu_host_get_metric(h, w, None, C.byref(lo), C.byref(hi))
+            arr = np.empty(hi.value - lo.value + 1, np.float32)
+            lib.sgpu_host_get_metric(h, w, arr.ctypes.data_as(_lib.c_float_p), None, None)
+            olo, oarr = o.metric(w)
+            assert olo == lo.value
+            np.testing.assert_array_equal(arr, oarr)
+        for c in range(6):
+            xi, xe, yi, ye, zi, ze = a6[c].tuple()
+            m = np.empty((ze - zi + 1, ye - yi + 1, xe - xi + 1), np.int16)
+            lib.sgpu_host_get_media(h, c, m.ctypes.data_as(C.POINTER(C.c_int16)))
+            np.testing.assert_array_equal(m, o.media(c).transpose(2, 1, 0))
+    finally:
+        lib.sgpu_destroy(h)
+
+
+def test_footprint_counts_fields_media_and_ade_state():
+    pb = ALL["disp"]()
+    lib, h = _plan(pb)
+    try:
+        b = C.c_uint64()
+        assert lib.sgpu_host_footprint(h, C.byref(b)) == 0
+        cells = pb.swept_cells
+        # at least 6 fields x 4 B and 6 media x 2 B per swept cell
+        assert b.value >= cells * 36
+    finally:
+        lib.sgpu_destroy(h)
+
+
+def test_plan_rejects_bad_problems():
+    pb = ALL["small"]()
+    lib = _lib.load()
+    d, keep = pb.to_desc()
+    d.pml_layers[0] = 0
+    h = C.c_void_p()
+    assert lib.sgpu_host_plan(C.byref(d), 10, C.byref(h)) == 1
+    d, keep = pb.to_desc()
+    d.nx = 1
+    assert lib.sgpu_host_plan(C.byref(d), 10, C.byref(h)) == 1
