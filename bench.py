@@ -200,7 +200,7 @@ def run_ours(args):
         return float(t.item())
 
     # ---- device-resident throughput ------------------------------------
-    s = Solver(pb, probe_capacity=max(1024, K + W + 8))
+    s = Solver(pb, probe_capacity=max(1024, K + W + 8), kernel_family=args.family)
     s.step(W)
     s.synchronize()
     ms = C.c_float()
@@ -225,7 +225,8 @@ def run_ours(args):
     bytes6 = (C.c_double * 6)()
     lib.sgpu_algorithmic_bytes(s.handle, bytes6)
     names = ["efield_curl_cpml", "edispersive_ade", "sources_e", "hfield_curl_cpml", "sources_h", "probes"]
-    kern = ["k_efield", "k_edisp", "k_sources", "k_hfield", "k_sources", "k_probes"]
+    fe, fh = ("k_tma_efield", "k_tma_hfield") if args.family == 1 else ("k_efield", "k_hfield")
+    kern = [fe, "k_edisp", "k_sources", fh, "k_sources", "k_probes"]
     avg_ms = [phases[q] / K for q in range(6)]
     dom = int(np.argmax(avg_ms))
     peak, peak_kind = measured_hbm_peak()
@@ -234,7 +235,7 @@ def run_ours(args):
     s.close()
 
     # ---- end to end through the C ABI with host buffers -----------------
-    e2e = None if args.quick else run_e2e(pb, K, lib)
+    e2e = None if args.quick else run_e2e(pb, K, lib, args.family)
 
     value = allsum(cells * K) / (t_ms * 1e-3) / 1e9
     if rank != 0:
@@ -247,7 +248,8 @@ def run_ours(args):
             "data": "synthetic",
             "config": {"workload": label, "swept_cells": cells, "parallelism": f"replicas{world}",
                        "l2": "inputs larger than L2 (fields alone %.1f GB)" % (cells * 24 / 1e9),
-                       "build": "-fmad=false (bit-exact)"},
+                       "build": "-fmad=false (bit-exact)",
+                       "field_kernels": "TMA-pipelined" if args.family == 1 else "register-marching"},
             "hbm_frac_step": (step_bytes / (t_ms / K * 1e-3) / 1e9) / peak,
             "roofline": {"bound": "hbm", "kernel": kern[dom], "phase": names[dom], "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
@@ -268,12 +270,12 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def run_e2e(pb, K, lib):
+def run_e2e(pb, K, lib, family):
     """Host problem -> device (set-up, media and initial fields from host
     buffers) -> K steps -> probe traces and final fields back to host."""
     from semba_fdtd_b200 import Solver
     t0 = time.perf_counter()
-    s = Solver(pb, probe_capacity=max(1024, K + 8))
+    s = Solver(pb, probe_capacity=max(1024, K + 8), kernel_family=family)
     h2d = 0
     for c in range(6):
         xi, xe, yi, ye, zi, ze = s.alloc[c]
@@ -309,6 +311,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="dispersive_large", choices=list(CONFIGS))
     ap.add_argument("--n", type=int, default=None, help="scale the configuration (cells per axis)")
+    ap.add_argument("--family", type=int, default=1, choices=[0, 1],
+                    help="field kernels: 1 TMA-pipelined (default), 0 register-marching")
     ap.add_argument("--quick", action="store_true", help="skip the end-to-end and CPU-baseline legs (profiling runs)")
     args = ap.parse_args()
     if args.impl == "reference":

@@ -188,6 +188,12 @@ sgpu_status sgpu_advance_e(sgpu_ctx* ctx, int n);
 sgpu_status sgpu_advance_h(sgpu_ctx* ctx, int n);
 sgpu_status sgpu_advance_steps(sgpu_ctx* ctx, int n0, int count);
 
+/* Field-kernel family of the fused half steps: 1 (default when the driver
+ * provides tensor maps) streams each tile's planes through a shared-memory
+ * ring with TMA bulk-tensor loads; 0 uses register-marching kernels with
+ * plain loads.  Both give identical results. */
+sgpu_status sgpu_set_kernel_family(sgpu_ctx* ctx, int family);
+
 /* Scans the six field components for NaN/Inf on the device; returns
  * SGPU_ERR_NONFINITE if any is found (the host-side counterpart of the
  * reference's energy/NaN stop, errorreport.F90:1433-1460). */

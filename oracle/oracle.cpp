@@ -1347,6 +1347,19 @@ int orc_get_field(void* hv, int comp, float* out) {
     return 0;
 }
 
+int orc_set_field(void* hv, int comp, const float* in) {
+    Handle* h = (Handle*)hv;
+    if (comp < 0 || comp > 5) return 1;
+    if (h->fp64) {
+        auto& v = h->sd->F[comp].v;
+        for (size_t i = 0; i < v.size(); ++i) v[i] = in[i];
+    } else {
+        auto& v = h->sf->F[comp].v;
+        std::memcpy(v.data(), in, v.size() * sizeof(float));
+    }
+    return 0;
+}
+
 int orc_get_field_f64(void* hv, int comp, double* out) {
     Handle* h = (Handle*)hv;
     if (comp < 0 || comp > 5) return 1;

@@ -111,6 +111,8 @@ int orc_get_num_media(void* h);
  * Fortran (column-major) order. */
 int orc_get_field(void* h, int comp, float* out);
 int orc_get_field_f64(void* h, int comp, double* out);
+/* Overwrite a field component (known-answer tests set initial states). */
+int orc_set_field(void* h, int comp, const float* in);
 int orc_get_media(void* h, int comp, short* out);
 /* Coefficient tables, for cross-checks of the set-up: g1,g2,gm1,gm2 each
  * num_media+1 floats. */

@@ -85,6 +85,7 @@ def load():
         lib.orc_get_field.argtypes = [vp, C.c_int, C.POINTER(C.c_float)]
         lib.orc_get_field_f64.argtypes = [vp, C.c_int, C.POINTER(C.c_double)]
         lib.orc_get_media.argtypes = [vp, C.c_int, C.POINTER(C.c_short)]
+        lib.orc_set_field.argtypes = [vp, C.c_int, C.POINTER(C.c_float)]
         lib.orc_get_g.argtypes = [vp] + [C.POINTER(C.c_float)] * 4
         lib.orc_get_metric.argtypes = [vp, C.c_int, C.POINTER(C.c_float)]
         lib.orc_get_metric_range.argtypes = [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
@@ -200,6 +201,11 @@ class Oracle:
             out = np.empty(shape, np.float32)
             self.lib.orc_get_field(self._h, comp, out.ctypes.data_as(C.POINTER(C.c_float)))
         return out.transpose(2, 1, 0)
+
+    def set_field(self, comp: int, arr: np.ndarray) -> None:
+        """Overwrite a component with an [i, j, k] array over its Alloc range."""
+        a = np.ascontiguousarray(np.asarray(arr, np.float32).transpose(2, 1, 0))
+        self.lib.orc_set_field(self._h, comp, a.ctypes.data_as(C.POINTER(C.c_float)))
 
     def media(self, comp: int) -> np.ndarray:
         xi, xe, yi, ye, zi, ze = self.alloc[comp]

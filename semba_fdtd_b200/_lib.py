@@ -115,6 +115,7 @@ def _declare(lib: C.CDLL) -> None:
         "sgpu_kernels_per_step": ([vp, c_int_p], C.c_int),
         "sgpu_algorithmic_bytes": ([vp, c_double_p], C.c_int),
         "sgpu_select_device": ([C.c_int], C.c_int),
+        "sgpu_set_kernel_family": ([vp, C.c_int], C.c_int),
         "sgpu_host_create": ([C.POINTER(ProblemDesc), C.c_int, C.POINTER(vp)], C.c_int),
         "sgpu_host_plan": ([C.POINTER(ProblemDesc), C.c_int, C.POINTER(vp)], C.c_int),
         "sgpu_host_footprint": ([vp, C.POINTER(C.c_uint64)], C.c_int),

@@ -101,6 +101,7 @@ class Problem:
     probe_names: list = field(default_factory=list)
     origin: tuple = (0.0, 0.0, 0.0)
     name: str = "case"
+    boundary: str = "pml"
 
     @property
     def swept_cells(self) -> int:
@@ -236,9 +237,9 @@ def read_case(path: str | Path) -> Problem:
 
     gen = js.get("general", {})
     bnd = js.get("boundary", {}).get("all", {})
-    if bnd.get("type", "pml") != "pml":
-        raise ValueError("only CPML boundaries are supported on this path")
-    L = int(bnd.get("layers", 8))
+    btype = bnd.get("type", "pml")
+    # other boundary kinds are read (layers 0) and refused by the solver
+    L = int(bnd.get("layers", 8)) if btype == "pml" else 0
     order = float(bnd.get("order", 2.0))
     refl = float(bnd.get("reflection", 0.001))
     pb = Problem(nx=nx, ny=ny, nz=nz, desx=des("x", nx), desy=des("y", ny), desz=des("z", nz),
@@ -246,7 +247,7 @@ def read_case(path: str | Path) -> Problem:
                  forcecfl="cfl" in gen, cfl=float(gen.get("cfl", 1.0)),
                  pml_layers=(L,) * 6, pml_order=(order,) * 6, pml_refl=(refl,) * 6,
                  alphamax=float(bnd.get("pmlAlpha", 0.0)), alphaorder=float(bnd.get("pmlAlphaOrder", 1.0)),
-                 kappamax=float(bnd.get("pmlKappa", 1.0)), name=path.name.split(".")[0])
+                 kappamax=float(bnd.get("pmlKappa", 1.0)), name=path.name.split(".")[0], boundary=btype)
     coords = {c["id"]: c["relativePosition"] for c in js["mesh"].get("coordinates", [])}
     elems = {e["id"]: e for e in js["mesh"].get("elements", [])}
     mats = {m["id"]: m for m in js.get("materials", [])}

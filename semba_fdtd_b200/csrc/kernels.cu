@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "sgpu_internal.h"
+#include "tma_fields.cuh"
 
 using namespace sgpu;
 
@@ -326,6 +327,214 @@ __global__ void __launch_bounds__(kBX * kBY, 4) k_hfield(KGrid g, KCpml cp, int 
     else if (MODE & kBulk) hfield_column<MODE, false>(g, cp, t1, t2, ic, jc, kb, ke, vx, vy, vz);
 }
 
+// ---------------------------------------------------------------------------
+// TMA-pipelined fused kernels (fast path of the E and H half steps).
+// Same per-cell arithmetic as efield_column / hfield_column, from shared
+// memory instead of global loads.
+
+// Every lane waits on the barrier (each needs the acquire); the warp then
+// agrees on the outcome so all lanes leave together on a timeout.
+__device__ __forceinline__ bool warp_wait(unsigned bar, unsigned parity, int* err, int code) {
+    const bool ok = mbar_wait(bar, parity, err, code);
+    return __all_sync(0xffffffffu, ok);
+}
+
+template <bool CP>
+__device__ __forceinline__ void e_consume(const TmaCta& t, const KGrid& g, const KCpml& cp, const float* t1, const float* t2,
+                                          int* err) {
+    const int w = t.warp, l = t.lane;
+    const int i = t.ib + l, j = t.jb + w;
+    const int nya = (int)(g.plane / g.pitch);
+    const bool vx = col_in(g.sw[0], i, j), vy = col_in(g.sw[1], i, j), vz = col_in(g.sw[2], i, j);
+    const float idyh = g.idyh[min(j, nya - 1)], idxh = g.idxh[i];
+    const long long pitch = g.pitch, plane = g.plane;
+    for (int k = t.kb; k <= t.ke; ++k) {
+        const int pidx = k - (t.kb - 1);
+        const int s = pidx % kStages, sp = (pidx - 1) % kStages;
+        if (k == t.kb && !warp_wait(t.full0, 0, err, 2)) return;
+        if (!warp_wait(t.full0 + 8 * s, (pidx / kStages) & 1, err, 1)) return;
+        const unsigned char* st = t.ring + s * kStageBytes;
+        const unsigned char* pv = t.ring + sp * kStageBytes;
+        const float* HX = (const float*)(st + kOffA);
+        const float* HY = (const float*)(st + kOffB);
+        const float* HZ = (const float*)(st + kOffC);
+        const float* HXp = (const float*)(pv + kOffA);
+        const float* HYp = (const float*)(pv + kOffB);
+        const float* EF = (const float*)(st + kOffF);
+        const int16_t* MF = (const int16_t*)(st + kOffM);
+        constexpr int fs = align128(kBoxF) / 4, ms = align128(kBoxM) / 2;
+        const float hx = HX[(w + 1) * kTX + l], hx_jm = HX[w * kTX + l], hx_km = HXp[(w + 1) * kTX + l];
+        const float hy = HY[w * kHaloW + l + 4], hy_im = HY[w * kHaloW + l + 3], hy_km = HYp[w * kHaloW + l + 4];
+        const float hz = HZ[(w + 1) * kHaloW + l + 4], hz_jm = HZ[w * kHaloW + l + 4], hz_im = HZ[(w + 1) * kHaloW + l + 3];
+        const float idzh = g.idzh[k];
+        const long long c = i + pitch * j + plane * k;
+        const int o = w * kTX + l;
+        if (vx && k >= g.sw[0][4] && k <= g.sw[0][5]) {
+            float e = EF[o];
+            const int m = MF[o];
+            const float dy = hz - hz_jm, dz = hy - hy_km;
+            e = t1[m] * e + t2[m] * (dy * idyh - dz * idzh);
+            if (CP) {
+                bool st_ = true;
+                e = cpml_one<true>(cp.s[0][0], i, j, k, j, cp.pbe[1], cp.pce[1], dy, t2[m], e, st_);
+                e = cpml_one<false>(cp.s[0][1], i, j, k, k, cp.pbe[2], cp.pce[2], dz, t2[m], e, st_);
+            }
+            g.F[0][c] = e;
+        }
+        if (vy && k >= g.sw[1][4] && k <= g.sw[1][5]) {
+            float e = EF[fs + o];
+            const int m = MF[ms + o];
+            const float dz = hx - hx_km, dx = hz - hz_im;
+            e = t1[m] * e + t2[m] * (dz * idzh - dx * idxh);
+            if (CP) {
+                bool st_ = true;
+                e = cpml_one<true>(cp.s[1][0], i, j, k, k, cp.pbe[2], cp.pce[2], dz, t2[m], e, st_);
+                e = cpml_one<false>(cp.s[1][1], i, j, k, i, cp.pbe[0], cp.pce[0], dx, t2[m], e, st_);
+            }
+            g.F[1][c] = e;
+        }
+        if (vz && k >= g.sw[2][4] && k <= g.sw[2][5]) {
+            float e = EF[2 * fs + o];
+            const int m = MF[2 * ms + o];
+            const float dx = hy - hy_im, dy = hx - hx_jm;
+            e = t1[m] * e + t2[m] * (dx * idxh - dy * idyh);
+            if (CP) {
+                bool st_ = true;
+                e = cpml_one<false>(cp.s[2][0], i, j, k, j, cp.pbe[1], cp.pce[1], dy, t2[m], e, st_);
+                e = cpml_one<true>(cp.s[2][1], i, j, k, i, cp.pbe[0], cp.pce[0], dx, t2[m], e, st_);
+            }
+            g.F[2][c] = e;
+        }
+        __syncwarp();
+        if (l == 0) mbar_arrive(t.empty0 + 8 * sp);  // plane k-1 is no longer needed
+    }
+}
+
+template <bool CP>
+__device__ __forceinline__ void h_consume(const TmaCta& t, const KGrid& g, const KCpml& cp, const float* t1, const float* t2,
+                                          int* err) {
+    const int w = t.warp, l = t.lane;
+    const int i = t.ib + l, j = t.jb + w;
+    const int nya = (int)(g.plane / g.pitch);
+    const bool vx = col_in(g.sw[3], i, j), vy = col_in(g.sw[4], i, j), vz = col_in(g.sw[5], i, j);
+    const float idye = g.idye[min(j, nya - 1)], idxe = g.idxe[i];
+    const long long pitch = g.pitch, plane = g.plane;
+    for (int k = t.kb; k <= t.ke; ++k) {
+        const int pidx = k - t.kb;
+        const int s = pidx % kStages, sn = (pidx + 1) % kStages;
+        if (!warp_wait(t.full0 + 8 * s, (pidx / kStages) & 1, err, 3)) return;
+        if (!warp_wait(t.full0 + 8 * sn, ((pidx + 1) / kStages) & 1, err, 4)) return;
+        const unsigned char* st = t.ring + s * kStageBytes;
+        const unsigned char* nx = t.ring + sn * kStageBytes;
+        const float* EX = (const float*)(st + kOffA);
+        const float* EY = (const float*)(st + kOffB);
+        const float* EZ = (const float*)(st + kOffC);
+        const float* EXn = (const float*)(nx + kOffA);
+        const float* EYn = (const float*)(nx + kOffB);
+        const float* HF = (const float*)(st + kOffF);
+        const int16_t* MF = (const int16_t*)(st + kOffM);
+        constexpr int fs = align128(kBoxF) / 4, ms = align128(kBoxM) / 2;
+        const float ex = EX[w * kTX + l], ex_jp = EX[(w + 1) * kTX + l], ex_kp = EXn[w * kTX + l];
+        const float ey = EY[w * kHaloW + l], ey_ip = EY[w * kHaloW + l + 1], ey_kp = EYn[w * kHaloW + l];
+        const float ez = EZ[w * kHaloW + l], ez_ip = EZ[w * kHaloW + l + 1], ez_jp = EZ[(w + 1) * kHaloW + l];
+        const float idze = g.idze[k];
+        const long long c = i + pitch * j + plane * k;
+        const int o = w * kTX + l;
+        if (vx && k >= g.sw[3][4] && k <= g.sw[3][5]) {
+            float h = HF[o];
+            const int m = MF[o];
+            const float dz = ey_kp - ey, dy = ez_jp - ez;
+            h = t1[m] * h + t2[m] * (dz * idze - dy * idye);
+            if (CP) {
+                bool st_ = true;
+                h = cpml_one<false>(cp.s[3][0], i, j, k, j, cp.pbm[1], cp.pcm[1], dy, t2[m], h, st_);
+                h = cpml_one<true>(cp.s[3][1], i, j, k, k, cp.pbm[2], cp.pcm[2], dz, t2[m], h, st_);
+            }
+            g.F[3][c] = h;
+        }
+        if (vy && k >= g.sw[4][4] && k <= g.sw[4][5]) {
+            float h = HF[fs + o];
+            const int m = MF[ms + o];
+            const float dx = ez_ip - ez, dz = ex_kp - ex;
+            h = t1[m] * h + t2[m] * (dx * idxe - dz * idze);
+            if (CP) {
+                bool st_ = true;
+                h = cpml_one<false>(cp.s[4][0], i, j, k, k, cp.pbm[2], cp.pcm[2], dz, t2[m], h, st_);
+                h = cpml_one<true>(cp.s[4][1], i, j, k, i, cp.pbm[0], cp.pcm[0], dx, t2[m], h, st_);
+            }
+            g.F[4][c] = h;
+        }
+        if (vz && k >= g.sw[5][4] && k <= g.sw[5][5]) {
+            float h = HF[2 * fs + o];
+            const int m = MF[2 * ms + o];
+            const float dy = ex_jp - ex, dx = ey_ip - ey;
+            h = t1[m] * h + t2[m] * (dy * idye - dx * idxe);
+            if (CP) {
+                bool st_ = true;
+                h = cpml_one<true>(cp.s[5][0], i, j, k, j, cp.pbm[1], cp.pcm[1], dy, t2[m], h, st_);
+                h = cpml_one<false>(cp.s[5][1], i, j, k, i, cp.pbm[0], cp.pcm[0], dx, t2[m], h, st_);
+            }
+            g.F[5][c] = h;
+        }
+        __syncwarp();
+        if (l == 0) mbar_arrive(t.empty0 + 8 * s);  // plane k is no longer needed
+    }
+}
+
+__device__ __forceinline__ const float* tma_tables(unsigned char* smem, const float* a, const float* b, int nmed1) {
+    float* tab = (float*)(smem + kTmaSmem);
+    if (nmed1 <= kShTable) {
+        for (int q = threadIdx.x; q < nmed1; q += blockDim.x) {
+            tab[q] = a[q];
+            tab[nmed1 + q] = b[q];
+        }
+        return tab;
+    }
+    return nullptr;
+}
+
+__global__ void __launch_bounds__(kTmaThreads, 3)
+    k_tma_efield(KGrid g, KCpml cp, const __grid_constant__ TMaps tm, int y0, int z0, int z1, int zchunk, int* err) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const float* tab = tma_tables(smem, g.g1, g.g2, g.nmed1);
+    const TmaCta t = tma_cta_setup(smem, y0, z0, z1, zchunk);
+    if (t.warp == kConsumerWarps) {
+        tma_produce(t, tm, t.kb - 1, t.ke, t.kb - 1, err);
+        return;
+    }
+    const float* t1 = tab ? tab : g.g1;
+    const float* t2 = tab ? tab + g.nmed1 : g.g2;
+    bool cpml_block = false;
+    if (cp.on)
+        for (int f = 0; f < 3; ++f)
+            for (int w = 0; w < 2; ++w)
+                for (int sd = 0; sd < 2; ++sd)
+                    cpml_block |= slab_touches(cp.s[f][w][sd], t.ib, t.ib + kTX - 1, t.jb, t.jb + kTY - 1, t.kb, t.ke);
+    if (cpml_block) e_consume<true>(t, g, cp, t1, t2, err);
+    else e_consume<false>(t, g, cp, t1, t2, err);
+}
+
+__global__ void __launch_bounds__(kTmaThreads, 3)
+    k_tma_hfield(KGrid g, KCpml cp, const __grid_constant__ TMaps tm, int y0, int z0, int z1, int zchunk, int* err) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const float* tab = tma_tables(smem, g.gm1, g.gm2, g.nmed1);
+    const TmaCta t = tma_cta_setup(smem, y0, z0, z1, zchunk);
+    if (t.warp == kConsumerWarps) {
+        tma_produce_h(t, tm, t.kb, t.ke + 1, t.ke + 1, err);
+        return;
+    }
+    const float* t1 = tab ? tab : g.gm1;
+    const float* t2 = tab ? tab + g.nmed1 : g.gm2;
+    bool cpml_block = false;
+    if (cp.on)
+        for (int f = 3; f < 6; ++f)
+            for (int w = 0; w < 2; ++w)
+                for (int sd = 0; sd < 2; ++sd)
+                    cpml_block |= slab_touches(cp.s[f][w][sd], t.ib, t.ib + kTX - 1, t.jb, t.jb + kTY - 1, t.kb, t.ke);
+    if (cpml_block) h_consume<true>(t, g, cp, t1, t2, err);
+    else h_consume<false>(t, g, cp, t1, t2, err);
+}
+
 // AdvanceEDispersiveE (electricdispersive.F90:304-362): one thread per node.
 // Conjugate poles share one state slot; the subtraction still runs once
 // per pole of the reference, in its order, and Re(conj(g)*conj(J)) equals
@@ -513,6 +722,82 @@ template <int MODE> sgpu_status launch_h(sgpu_ctx* c) {
     return check_launch(c, "k_hfield");
 }
 
+constexpr int kTmaChunk = 32;
+
+sgpu_status launch_tma(sgpu_ctx* c, bool hside) {
+    Launch L = plan(c, hside ? 3 : 0, hside ? 5 : 2);
+    int x1 = -1;
+    for (int f = hside ? 3 : 0; f < (hside ? 6 : 3); ++f) x1 = std::max(x1, c->sweep[f].xe - c->ox);
+    const int bx = (x1 + 1 + kTX - 1) / kTX;
+    int y1 = -1;
+    for (int f = hside ? 3 : 0; f < (hside ? 6 : 3); ++f) y1 = std::max(y1, c->sweep[f].ye - c->oy);
+    const int by = (y1 - L.y0 + 1 + kTY - 1) / kTY;
+    const int nz = L.z1 - L.z0 + 1;
+    int chunk = kTmaChunk;
+    while (chunk > 8 && (long long)bx * by * ((nz + chunk - 1) / chunk) < 148LL * 4) chunk /= 2;
+    chunk = std::min(chunk, nz);
+    dim3 grid(bx, by, (nz + chunk - 1) / chunk);
+    const int n1 = c->num_media + 1;
+    const size_t smem = kTmaSmem + (n1 <= kShTable ? 2 * n1 * sizeof(float) : 0);
+    if (hside)
+        k_tma_hfield<<<grid, kTmaThreads, smem, c->stream>>>(kgrid(c), c->cpml, c->tmh, L.y0, L.z0, L.z1, chunk, c->d_err);
+    else
+        k_tma_efield<<<grid, kTmaThreads, smem, c->stream>>>(kgrid(c), c->cpml, c->tme, L.y0, L.z0, L.z1, chunk, c->d_err);
+    return check_launch(c, hside ? "k_tma_hfield" : "k_tma_efield");
+}
+
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*,
+                                 const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                 CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encoder() {
+    static EncodeTiled fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiled)p;
+        cudaGetLastError();
+    }
+    return fn;
+}
+
+// A 3-D tiled map over one padded array with a (bx, by, 1) box.
+bool encode_map(const sgpu_ctx* c, CUtensorMap* m, void* base, bool int16, int bx, int by) {
+    EncodeTiled fn = encoder();
+    if (!fn) return false;
+    const cuuint64_t esz = int16 ? 2 : 4;
+    const cuuint64_t dims[3] = {(cuuint64_t)c->pitch, (cuuint64_t)c->nya, (cuuint64_t)c->nza};
+    const cuuint64_t strides[2] = {(cuuint64_t)c->pitch * esz, (cuuint64_t)c->plane * esz};
+    const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
+    const cuuint32_t es[3] = {1, 1, 1};
+    return fn(m, int16 ? CU_TENSOR_MAP_DATA_TYPE_UINT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, es,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+bool build_tensor_maps(sgpu_ctx* c) {
+    bool ok = true;
+    // E kernel: Hx (32x9), Hy (36x8), Hz (36x9), Ex Ey Ez, Mx My Mz
+    ok = ok && encode_map(c, &c->tme.m[0], c->F[3], false, kTX, kTY + 1);
+    ok = ok && encode_map(c, &c->tme.m[1], c->F[4], false, kHaloW, kTY);
+    ok = ok && encode_map(c, &c->tme.m[2], c->F[5], false, kHaloW, kTY + 1);
+    // H kernel: Ex (32x9), Ey (36x8), Ez (36x9), Hx Hy Hz, MHx MHy MHz
+    ok = ok && encode_map(c, &c->tmh.m[0], c->F[0], false, kTX, kTY + 1);
+    ok = ok && encode_map(c, &c->tmh.m[1], c->F[1], false, kHaloW, kTY);
+    ok = ok && encode_map(c, &c->tmh.m[2], c->F[2], false, kHaloW, kTY + 1);
+    for (int q = 0; q < 3; ++q) {
+        ok = ok && encode_map(c, &c->tme.m[3 + q], c->F[q], false, kTX, kTY);
+        ok = ok && encode_map(c, &c->tme.m[6 + q], c->M[q], true, kTX, kTY);
+        ok = ok && encode_map(c, &c->tmh.m[3 + q], c->F[3 + q], false, kTX, kTY);
+        ok = ok && encode_map(c, &c->tmh.m[6 + q], c->M[3 + q], true, kTX, kTY);
+    }
+    return ok;
+}
+
 bool ready(sgpu_ctx* c) {
     for (int f = 0; f < 6; ++f)
         if (!c->media_loaded[f]) return false;
@@ -571,15 +856,25 @@ sgpu_status launch_probes(sgpu_ctx* c, StepRef sr) {
     return check_launch(c, "k_probes");
 }
 
+sgpu_status field_e(sgpu_ctx* c) {
+    if (c->family == 1 && c->tma_ready) return launch_tma(c, false);
+    return c->cpml.on ? launch_e<kBulk | kCpml | kAll>(c) : launch_e<kBulk | kAll>(c);
+}
+
+sgpu_status field_h(sgpu_ctx* c) {
+    if (c->family == 1 && c->tma_ready) return launch_tma(c, true);
+    return c->cpml.on ? launch_h<kBulk | kCpml | kAll>(c) : launch_h<kBulk | kAll>(c);
+}
+
 sgpu_status half_e(sgpu_ctx* c, StepRef sr) {
-    sgpu_status s = c->cpml.on ? launch_e<kBulk | kCpml | kAll>(c) : launch_e<kBulk | kAll>(c);
+    sgpu_status s = field_e(c);
     if (s) return s;
     if ((s = launch_edisp(c))) return s;
     return launch_sources(c, 0, sr);
 }
 
 sgpu_status half_h(sgpu_ctx* c, StepRef sr) {
-    sgpu_status s = c->cpml.on ? launch_h<kBulk | kCpml | kAll>(c) : launch_h<kBulk | kAll>(c);
+    sgpu_status s = field_h(c);
     if (s) return s;
     return launch_sources(c, 1, sr);
 }
@@ -713,6 +1008,15 @@ sgpu_status sgpu_create(const sgpu_grid_desc* d, sgpu_ctx** out) {
     }
     if ((s = dalloc(c, &c->d_step, 1))) return fail(s);
     if ((s = dalloc(c, &c->d_flag, 1))) return fail(s);
+    if ((s = dalloc(c, &c->d_err, 1))) return fail(s);
+    CUDA_TRY(c, cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
+    c->tma_ready = build_tensor_maps(c);
+    if (c->tma_ready) {
+        const int smax = (int)(kTmaSmem + 2 * kShTable * sizeof(float));
+        c->tma_ready = cudaFuncSetAttribute(k_tma_efield, cudaFuncAttributeMaxDynamicSharedMemorySize, smax) == cudaSuccess &&
+                       cudaFuncSetAttribute(k_tma_hfield, cudaFuncAttributeMaxDynamicSharedMemorySize, smax) == cudaSuccess;
+        cudaGetLastError();
+    }
     CUDA_TRY(c, cudaMemsetAsync(c->d_step, 0, sizeof(int), c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     *out = c;
@@ -735,7 +1039,7 @@ void sgpu_destroy(sgpu_ctx* c) {
     cudaFree(c->g1); cudaFree(c->g2); cudaFree(c->gm1); cudaFree(c->gm2);
     cudaFree(c->idxe); cudaFree(c->idye); cudaFree(c->idze);
     cudaFree(c->idxh); cudaFree(c->idyh); cudaFree(c->idzh);
-    cudaFree(c->d_tiempo); cudaFree(c->d_step); cudaFree(c->d_flag);
+    cudaFree(c->d_tiempo); cudaFree(c->d_step); cudaFree(c->d_flag); cudaFree(c->d_err);
     free_list(c->cpml_allocs);
     free_list(c->disp_allocs);
     free_list(c->src_allocs[0]);
@@ -749,6 +1053,25 @@ void sgpu_destroy(sgpu_ctx* c) {
 sgpu_status sgpu_synchronize(sgpu_ctx* c) {
     if (!c) return SGPU_ERR_ARG;
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    if (c->d_err) {
+        int e = 0;
+        CUDA_TRY(c, cudaMemcpy(&e, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (e) {
+            CUDA_TRY(c, cudaMemset(c->d_err, 0, sizeof(int)));
+            return set_error(c, SGPU_ERR_TIMEOUT, "a bounded wait in a pipelined kernel expired (code " + std::to_string(e) + ")");
+        }
+    }
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_set_kernel_family(sgpu_ctx* c, int family) {
+    if (!c || family < 0 || family > 1) return SGPU_ERR_ARG;
+    if (family == 1 && !c->tma_ready) return set_error(c, SGPU_ERR_UNSUPPORTED, "TMA tensor maps unavailable");
+    c->family = family;
+    if (c->graph) {
+        cudaGraphExecDestroy(c->graph);
+        c->graph = nullptr;
+    }
     return SGPU_OK;
 }
 
@@ -1331,13 +1654,13 @@ sgpu_status sgpu_profile_steps(sgpu_ctx* c, int n0, int count, float* ms6) {
     for (int n = n0; n < n0 + count && !s; ++n) {
         StepRef sr{nullptr, n};
         cudaEventRecord(ev[0], c->stream);
-        s = c->cpml.on ? launch_e<kBulk | kCpml | kAll>(c) : launch_e<kBulk | kAll>(c);
+        s = field_e(c);
         cudaEventRecord(ev[1], c->stream);
         if (!s) s = launch_edisp(c);
         cudaEventRecord(ev[2], c->stream);
         if (!s) s = launch_sources(c, 0, sr);
         cudaEventRecord(ev[3], c->stream);
-        if (!s) s = c->cpml.on ? launch_h<kBulk | kCpml | kAll>(c) : launch_h<kBulk | kAll>(c);
+        if (!s) s = field_h(c);
         cudaEventRecord(ev[4], c->stream);
         if (!s) s = launch_sources(c, 1, sr);
         cudaEventRecord(ev[5], c->stream);
@@ -1417,6 +1740,10 @@ sgpu_status sgpu_check_finite(sgpu_ctx* c) {
     if (flag) return set_error(c, SGPU_ERR_NONFINITE, "non-finite field value found");
     return SGPU_OK;
 }
+
+}  // extern "C"
+
+extern "C" {
 
 sgpu_status sgpu_device_bytes(const sgpu_ctx* c, uint64_t* bytes) {
     if (!c || !bytes) return SGPU_ERR_ARG;

@@ -7,6 +7,7 @@
 // shorter simply leaves the last slab unused.  Rows are padded to a
 // multiple of 32 floats so every row starts on a 128-byte boundary.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -101,6 +102,11 @@ struct KProbes {
     int cap;
 };
 
+// Tensor maps of one fused TMA kernel (see tma_fields.cuh for the order).
+struct alignas(64) TMaps {
+    CUtensorMap m[9];
+};
+
 struct StepRef {
     const int* dev_n;  // if non-null, the step index is read from here
     int n;
@@ -172,6 +178,11 @@ struct sgpu_ctx {
     int graph_steps = 0;
     // scratch
     unsigned int* d_flag = nullptr;
+    // TMA-pipelined fused kernels: tensor maps and the bounded-wait error word
+    sgpu::TMaps tme{}, tmh{};
+    bool tma_ready = false;
+    int family = 1;  // 1: TMA-pipelined fused kernels when available, 0: register-marching kernels
+    int* d_err = nullptr;
     // level-2 host data kept for inspection; host_only contexts (from
     // sgpu_host_plan) own no device resources
     bool host_only = false;

@@ -23,7 +23,7 @@ from .case import Problem
 
 class Solver:
     def __init__(self, problem: Problem, variant: str = "exact", probe_capacity: int = 1024,
-                 max_steps: int | None = None):
+                 max_steps: int | None = None, kernel_family: int | None = None):
         self.problem = problem
         self.lib = _lib.load(variant)
         self.variant = variant
@@ -49,6 +49,8 @@ class Solver:
         self.sinpml = [q.tuple() for q in q6]
         self.nprobes = len(problem.probes)
         self._probe_rows: list[np.ndarray] = []
+        if kernel_family is not None:
+            self._check(self.lib.sgpu_set_kernel_family(h, int(kernel_family)), "sgpu_set_kernel_family")
 
     # -- plumbing ----------------------------------------------------------
     def _check(self, rc: int, what: str = "") -> None:
@@ -139,6 +141,7 @@ class Solver:
 
     def probes(self) -> np.ndarray:
         """All probe rows recorded so far, [step, probe] (FP32)."""
+        self.synchronize()
         self._drain()
         if not self._probe_rows:
             return np.zeros((0, self.nprobes), np.float32)
@@ -146,6 +149,10 @@ class Solver:
 
     def synchronize(self) -> None:
         self._check(self.lib.sgpu_synchronize(self._h), "sgpu_synchronize")
+
+    def set_kernel_family(self, family: int) -> None:
+        """1: TMA-pipelined fused field kernels (default); 0: register-marching."""
+        self._check(self.lib.sgpu_set_kernel_family(self._h, int(family)), "sgpu_set_kernel_family")
 
     # -- data --------------------------------------------------------------
     def field(self, comp: int) -> np.ndarray:

@@ -4,7 +4,7 @@ The exact library (-fmad=false) must reproduce the oracle's FP32 probe
 traces and final fields bit for bit; the three stepping forms (per-routine
 drop-ins, fused half steps, graph-replayed steps) must agree bit for bit;
 the FMA library must stay within 1e-5 relative L2 of the exact one on every
-probe trace."""
+probe trace that FP32 arithmetic resolves (see the FMA test)."""
 import numpy as np
 import pytest
 
@@ -31,12 +31,13 @@ def _run_oracle(pb, steps):
     return o, tr
 
 
+@pytest.mark.parametrize("family", [1, 0], ids=["tma", "regs"])
 @pytest.mark.parametrize("name", list(ALL))
-def test_bit_exact_against_oracle(name):
+def test_bit_exact_against_oracle(name, family):
     pb = ALL[name]()
     steps = pb.nsteps + 1
     o, otr = _run_oracle(pb, steps)
-    with Solver(pb) as s:
+    with Solver(pb, kernel_family=family) as s:
         gtr = s.run()
         assert gtr.shape == otr.shape
         np.testing.assert_array_equal(gtr, otr)
@@ -63,11 +64,17 @@ def test_stepping_forms_agree(name):
 @pytest.mark.parametrize("name", list(ALL))
 def test_fma_build_within_tolerance(name):
     """The FMA build against the bit-exact build, both against the FP64
-    accuracy oracle.  Every probe trace must be within 1e-5 relative L2 of
-    the exact build, or -- for traces dominated by cancellation residue, such
-    as scattered-field probes that record only the TF/SF box's numerical
-    dispersion leakage -- no further from the exact build than the exact FP32
-    build itself is from the FP64 oracle."""
+    accuracy oracle.
+
+    A probe trace is *resolved* when the exact FP32 build itself stays within
+    REL_L2_FMA of the FP64 oracle; on every resolved trace the FMA build must
+    be within REL_L2_FMA relative L2 of the exact build.  A trace that the
+    FP32 arithmetic does not resolve (for example a scattered-field probe
+    outside the TF/SF box, which records only the box's discretisation
+    leakage, a cancellation residue) carries FP32 rounding noise of the same
+    size in both builds; there the FMA build must be no further from the
+    FP64 oracle than twice the exact build's distance.  Every case must have
+    resolved traces, so the 1e-5 bar is never vacuous."""
     pb = ALL[name]()
     with Solver(pb) as s:
         exact = s.run()
@@ -75,15 +82,20 @@ def test_fma_build_within_tolerance(name):
         fast = s.run()
     ref64 = oracle.Oracle(pb, fp64=True)
     f64 = ref64.step(pb.nsteps + 1)
-    report = []
+    rows = []
     for q in range(exact.shape[1]):
         if not np.any(exact[:, q]):
             continue
         d_fast = _rel_l2(fast[:, q], exact[:, q])
-        d_fp32 = _rel_l2(exact[:, q], f64[:, q])
-        report.append((q, d_fast, d_fp32))
-        assert d_fast <= max(REL_L2_FMA, d_fp32), f"probe {q}: fma-vs-exact {d_fast:.3e}, fp32-vs-fp64 {d_fp32:.3e}"
-    print(f"{name}: (probe, rel L2 fma vs exact, rel L2 fp32 vs fp64) = {report}")
+        e32 = _rel_l2(exact[:, q], f64[:, q])
+        efma = _rel_l2(fast[:, q], f64[:, q])
+        rows.append((q, e32 <= REL_L2_FMA, d_fast, e32, efma))
+    table = "\n".join(f"  probe {q:3d} {'resolved' if r else 'noise   '} fma-vs-exact {d:.3e} "
+                       f"exact-vs-fp64 {e:.3e} fma-vs-fp64 {f:.3e}" for q, r, d, e, f in rows)
+    print(f"{name}:\n{table}")
+    assert any(r for _, r, *_ in rows), f"no resolved probe trace:\n{table}"
+    bad = [q for q, r, d, e, f in rows if (d > REL_L2_FMA if r else f > 2 * e)]
+    assert not bad, f"probes {bad} out of tolerance:\n{table}"
 
 
 def test_probe_ring_wraps_and_drains():
