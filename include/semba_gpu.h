@@ -48,6 +48,7 @@ typedef int sgpu_status;
 #define SGPU_ERR_NONFINITE 5  /* NaN/Inf found by sgpu_check_finite         */
 #define SGPU_ERR_TIMEOUT 6    /* a bounded device wait ran out              */
 #define SGPU_ERR_UNSUPPORTED 7
+#define SGPU_ERR_SIZE 8       /* input larger than the entry point's stated maximum */
 
 typedef struct sgpu_ctx sgpu_ctx;
 
@@ -215,6 +216,27 @@ sgpu_status sgpu_algorithmic_bytes(const sgpu_ctx* ctx, double* bytes6);
 sgpu_status sgpu_select_device(int device);
 /* Kernel launches issued per whole step (graph replays add one per chunk). */
 sgpu_status sgpu_kernels_per_step(const sgpu_ctx* ctx, int* n);
+
+/* Non-finite scan that allocates no device memory.  No counterpart in the
+ * reference: it is for callers that cannot call cudaMalloc where they need
+ * the check (a host whose device memory belongs to its own pool allocator, a
+ * service loop that forbids allocation after start-up, a watchdog checking a
+ * buffer it does not own).  Counts the NaN/Inf values among the n floats at
+ * the device pointer `data` (memory of the calling thread's current device)
+ * and returns the count and the index of the first one (-1 when none) in
+ * host memory.  `stream` is a cudaStream_t passed as a pointer (NULL: the
+ * legacy default stream); the call waits for that stream.
+ *   - n may be at most 268,435,456 (4096 x 65536); larger n returns
+ *     SGPU_ERR_SIZE without touching the data.
+ *   - Scratch is a file-scope __device__ array of 512 KiB that every device
+ *     loading this library holds until exit.  Its device address is taken
+ *     with cudaGetSymbolAddress on the first call on each device, so make
+ *     that first call before any stream capture.
+ *   - Every call shares the scratch: calls whose work overlaps on a device
+ *     (different host threads, or streams that run concurrently) race and
+ *     may return each other's results; serialise them. */
+sgpu_status sgpu_scan_nonfinite_noalloc(const float* data, uint64_t n, void* stream, uint64_t* count,
+                                        int64_t* first_index);
 
 /* Bytes of device memory the context holds. */
 sgpu_status sgpu_device_bytes(const sgpu_ctx* ctx, uint64_t* bytes);

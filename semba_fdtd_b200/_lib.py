@@ -63,7 +63,7 @@ class GridDesc(C.Structure):
 
 
 ERRORS = {0: "ok", 1: "bad argument", 2: "out of memory", 3: "CUDA error", 4: "call out of order",
-          5: "non-finite field", 6: "timeout", 7: "unsupported"}
+          5: "non-finite field", 6: "timeout", 7: "unsupported", 8: "size above the stated maximum"}
 
 
 class SembaGpuError(RuntimeError):
@@ -116,6 +116,7 @@ def _declare(lib: C.CDLL) -> None:
         "sgpu_algorithmic_bytes": ([vp, c_double_p], C.c_int),
         "sgpu_select_device": ([C.c_int], C.c_int),
         "sgpu_set_kernel_family": ([vp, C.c_int], C.c_int),
+        "sgpu_scan_nonfinite_noalloc": ([vp, C.c_uint64, vp, C.POINTER(C.c_uint64), C.POINTER(C.c_int64)], C.c_int),
         "sgpu_host_create": ([C.POINTER(ProblemDesc), C.c_int, C.POINTER(vp)], C.c_int),
         "sgpu_host_plan": ([C.POINTER(ProblemDesc), C.c_int, C.POINTER(vp)], C.c_int),
         "sgpu_host_footprint": ([vp, C.POINTER(C.c_uint64)], C.c_int),

@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -1742,6 +1743,120 @@ sgpu_status sgpu_check_finite(sgpu_ctx* c) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Non-finite scan that allocates nothing.
+//
+// sgpu_check_finite keeps its result word in memory the context allocated at
+// creation.  sgpu_scan_nonfinite_noalloc is the same scan for callers that
+// may not allocate device memory when they run it: a Fortran or framework
+// host whose device memory belongs to its own pool allocator, a service loop
+// that forbids cudaMalloc/cudaFree after start-up, or a watchdog that checks
+// a field buffer someone else owns.  Its scratch is the file-scope array
+// below: every device that loads this library holds it (8 B per block of
+// 4096 elements, 512 KiB in all) until the process exits, and every call
+// shares it.
+namespace {
+
+constexpr int kScanChunk = 4096;      // elements scanned by one block
+constexpr int kScanMaxBlocks = 65536;  // one scratch word per block
+constexpr unsigned long long kScanMaxElems = (unsigned long long)kScanChunk * kScanMaxBlocks;  // 268,435,456
+
+// [b] = (non-finite count of block b) << 32 | first offset in the block
+//       (0xffffffff when none); [kScanMaxBlocks] = the reduced result.
+// Every entry a call reads is written earlier in that call, so nothing has
+// to start at zero.
+static __device__ __align__(256) unsigned long long g_scan_scratch[kScanMaxBlocks + 1];
+
+__global__ void k_scan_partial(const float* a, unsigned long long n, unsigned long long* part) {
+    __shared__ unsigned int cnt, first;
+    if (threadIdx.x == 0) {
+        cnt = 0;
+        first = 0xffffffffu;
+    }
+    __syncthreads();
+    const unsigned long long base = (unsigned long long)blockIdx.x * kScanChunk;
+    for (int t = threadIdx.x; t < kScanChunk; t += blockDim.x) {
+        const unsigned long long q = base + t;
+        if (q < n && !isfinite(a[q])) {
+            atomicAdd(&cnt, 1u);
+            atomicMin(&first, (unsigned int)t);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) part[blockIdx.x] = ((unsigned long long)cnt << 32) | first;
+}
+
+__global__ void k_scan_reduce(unsigned long long* part, int nblocks) {
+    __shared__ unsigned int total, first;
+    if (threadIdx.x == 0) {
+        total = 0;
+        first = 0xffffffffu;
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+        const unsigned long long v = part[b];
+        const unsigned int cnt = (unsigned int)(v >> 32), f = (unsigned int)(v & 0xffffffffu);
+        if (cnt) {
+            atomicAdd(&total, cnt);
+            atomicMin(&first, (unsigned int)b * kScanChunk + f);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) part[kScanMaxBlocks] = ((unsigned long long)total << 32) | first;
+}
+
+constexpr int kScanMaxDevices = 64;
+std::mutex g_scan_mu;
+unsigned long long* g_scan_ptr[kScanMaxDevices] = {};
+
+}  // namespace
+
+extern "C" sgpu_status sgpu_scan_nonfinite_noalloc(const float* data, uint64_t n, void* stream, uint64_t* count,
+                                                  int64_t* first_index) {
+    if (!count || !first_index || (n > 0 && !data)) return SGPU_ERR_ARG;
+    if (n > kScanMaxElems) return SGPU_ERR_SIZE;
+    *count = 0;
+    *first_index = -1;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kScanMaxDevices) return SGPU_ERR_CUDA;
+    if (n == 0) return SGPU_OK;
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, data) != cudaSuccess) {
+        cudaGetLastError();
+        return SGPU_ERR_ARG;
+    }
+    if ((attr.type != cudaMemoryTypeDevice && attr.type != cudaMemoryTypeManaged) || attr.device != dev)
+        return SGPU_ERR_ARG;  // not device memory of the calling thread's current device
+    unsigned long long* scratch = nullptr;
+    {
+        // once per device, with that device current: the device address of
+        // the file-scope array (its host-side name is only a stand-in)
+        std::lock_guard<std::mutex> lock(g_scan_mu);
+        if (!g_scan_ptr[dev]) {
+            void* p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_scan_scratch) != cudaSuccess || !p) {
+                cudaGetLastError();
+                return SGPU_ERR_CUDA;
+            }
+            g_scan_ptr[dev] = (unsigned long long*)p;
+        }
+        scratch = g_scan_ptr[dev];
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const int nblocks = (int)((n + kScanChunk - 1) / kScanChunk);
+    k_scan_partial<<<nblocks, 256, 0, s>>>(data, n, scratch);
+    k_scan_reduce<<<1, 1024, 0, s>>>(scratch, nblocks);
+    if (cudaGetLastError() != cudaSuccess) return SGPU_ERR_CUDA;
+    unsigned long long res = 0;
+    if (cudaMemcpyAsync(&res, scratch + kScanMaxBlocks, sizeof(res), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return SGPU_ERR_CUDA;
+    *count = res >> 32;
+    const unsigned int f = (unsigned int)(res & 0xffffffffu);
+    *first_index = (*count > 0 && f != 0xffffffffu) ? (int64_t)f : -1;
+    return SGPU_OK;
+}
 
 extern "C" {
 
