@@ -223,10 +223,17 @@ def write_waveform(path: Path, dt: float, values: np.ndarray) -> None:
             fh.write(f"{float(a):.9e} {float(b):.9e}\n")
 
 
-def read_case(path: str | Path) -> Problem:
+def read_case(path: str | Path, search: tuple = ()) -> Problem:
+    """Read a case file.  Waveform (``magnitudeFile``) names are looked up in
+    the case file's directory first, then in each directory of `search`."""
     path = Path(path)
     js = json.loads(path.read_text())
-    base = path.parent
+
+    def wave_path(name: str) -> Path:
+        for d in (path.parent, *map(Path, search)):
+            if (d / name).exists():
+                return d / name
+        raise FileNotFoundError(f"waveform {name!r} not found next to {path.name} or in {list(search)}")
     grid = js["mesh"]["grid"]
     nx, ny, nz = (int(v) for v in grid["numberOfCells"])
     steps = grid["steps"]
@@ -288,7 +295,7 @@ def read_case(path: str | Path) -> Problem:
             pb.planewaves.append(PlaneWave(coor1=(box[0], box[2], box[4]), coor2=(box[1], box[3], box[5]),
                                            theta=float(s["direction"]["theta"]), phi=float(s["direction"]["phi"]),
                                            alpha=float(s["polarization"]["theta"]), beta=float(s["polarization"]["phi"]),
-                                           wave=read_waveform(base / s["magnitudeFile"])))
+                                           wave=read_waveform(wave_path(s["magnitudeFile"]))))
         elif s["type"] == "nodalSource":
             bx, amp = [], []
             for i in s["elementIds"]:
@@ -301,7 +308,7 @@ def read_case(path: str | Path) -> Problem:
                     amp.append(a3)
             pb.nodals.append(NodalSource(is_elec=s.get("field", "electric") == "electric", is_hard=bool(s.get("hard", True)),
                                          boxes=np.asarray(bx, np.int32), amp=np.asarray(amp, np.float32),
-                                         wave=read_waveform(base / s["magnitudeFile"])))
+                                         wave=read_waveform(wave_path(s["magnitudeFile"]))))
         else:
             raise ValueError(f"source type {s['type']!r} is outside this path")
     probes, names = [], []

@@ -1,0 +1,175 @@
+"""Known-answer tests that pin the CPU oracle (no GPU).
+
+The reference Fortran cannot be built here and its tests hold no golden
+vectors for this path, so the oracle is pinned by physics and by the
+reference's own parser fixture:
+
+* one step from a linear Hz ramp gives the analytic discrete curl
+  (staggering, G2 of vacuum, metric arrays; timestepping.F90:2165-2285);
+* a vacuum plane wave through an empty TF/SF box: unit incident amplitude
+  inside, scattered field below -40 dB outside (planewaves.F90:878-1475);
+* CPML reflection against a domain large enough to have none in the window
+  (borderscpml.F90:584-1176, 1465-1733);
+* Debye relaxation of a uniform field in a single-real-pole medium converges
+  to the analytic solution (electricdispersive.F90:77-362);
+* FP32 against FP64 oracle per probe;
+* the reference's parser fixture test/smbjson/test_read_planewave.F90 on
+  testData/cases/planewave.fdtd.json (skipped where that tree is absent).
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle
+from semba_fdtd_b200.case import EPS0, NodalSource, PlaneWave, Problem, Region, Waveform, read_case
+
+ETA0 = 376.730313668
+
+
+def _box(n, steps, layers, dx=0.01):
+    d = np.full(n, dx, np.float32)
+    return Problem(nx=n, ny=n, nz=n, desx=d, desy=d.copy(), desz=d.copy(), nsteps=steps, forcecfl=True, cfl=0.8,
+                   pml_layers=(layers,) * 6, pml_order=(3.0,) * 6, pml_refl=(1e-6,) * 6)
+
+
+def _dt():
+    return oracle.Oracle(_box(8, 1, 4), fp64=True).dt
+
+
+def _fill(o, comp, fn):
+    xi, xe, yi, ye, zi, ze = o.alloc[comp]
+    i, j, k = np.meshgrid(np.arange(xi, xe + 1), np.arange(yi, ye + 1), np.arange(zi, ze + 1), indexing="ij")
+    o.set_field(comp, fn(i, j, k).astype(np.float32))
+
+
+def test_one_step_curl_of_a_ramp_is_exact():
+    """Hz = j (absolute cell index), everything else zero.  After one step,
+    in the interior: Ex = G2(vacuum) * Idyh(j) exactly, Ey = Ez = 0, Hz
+    unchanged, Hx = Hy = 0 (curl E vanishes where Ex is uniform)."""
+    n, L = 12, 4
+    o = oracle.Oracle(_box(n, 1, L))
+    _fill(o, 5, lambda i, j, k: j.astype(np.float32))
+    o.step(1)
+    g1, g2, gm1, gm2 = o.g_tables()
+    assert g1[1] == np.float32(1.0) and gm1[1] == np.float32(1.0)
+    assert g2[1] == np.float32(np.float64(o.dt) / np.float64(EPS0))
+    lo, idyh = o.metric(4)
+
+    def interior(comp):
+        xi, _, yi, _, zi, _ = o.alloc[comp]
+        f = o.field(comp)
+        return f[2 - xi:n - 2 - xi, 2 - yi:n - 2 - yi, 2 - zi:n - 2 - zi]
+
+    ex = interior(0)
+    want = (g2[1] * idyh[np.arange(2, n - 2) - lo]).astype(np.float32)
+    np.testing.assert_array_equal(ex, np.broadcast_to(want[None, :, None], ex.shape))
+    assert not np.any(interior(1)) and not np.any(interior(2))
+    assert not np.any(interior(3)[1:-1, 1:-1, 1:-1]) and not np.any(interior(4)[1:-1, 1:-1, 1:-1])
+    hz = interior(5)
+    np.testing.assert_array_equal(hz[:, 1:-1, :], np.broadcast_to(np.arange(3, n - 3, dtype=np.float32)[None, :, None],
+                                                                  hz[:, 1:-1, :].shape))
+
+
+def _gauss(dt, steps, sigma, t0):
+    ds = dt / 4
+    t = np.arange(int(steps * dt / ds) + 2) * ds
+    return Waveform(np.exp(-((t - t0) ** 2) / (2 * sigma * sigma)).astype(np.float32), np.float32(ds))
+
+
+def test_tfsf_unit_incident_and_quiet_scattered_region():
+    n, steps, sig = 30, 260, 200e-12
+    pb = _box(n, steps, 8)
+    pb.planewaves = [PlaneWave((6, 6, 6), (23, 23, 23), 0.0, 0.0, float(np.float32(np.pi / 2)), 0.0,
+                               _gauss(_dt(), steps, sig, 4 * sig))]
+    # Ex and Hy at the centre (total field); Ex upstream, downstream, lateral (scattered field)
+    pb.probes = np.array([[0, 15, 15, 15], [4, 15, 15, 15], [0, 15, 15, 3], [0, 15, 15, 26], [0, 2, 15, 15]], np.int32)
+    tr = oracle.Oracle(pb, fp64=True).step(steps).astype(np.float64)
+    peak = np.abs(tr[:, 0]).max()
+    assert abs(peak - 1.0) < 0.01
+    assert abs(np.abs(tr[:, 1]).max() * ETA0 - 1.0) < 0.01
+    for q in (2, 3, 4):
+        assert np.abs(tr[:, q]).max() / peak < 1e-2, f"probe {q} leaks"
+
+
+def _dipole(n, c, probe, steps, dt, sig):
+    pb = _box(n, steps, 10)
+    ds = dt / 4
+    t = np.arange(int(steps * dt / ds) + 2) * ds
+    x = (t - 4 * sig) / sig
+    w = Waveform((-x * np.exp(-0.5 * x * x)).astype(np.float32), np.float32(ds))
+    pb.nodals = [NodalSource(True, False, np.array([[c] * 6], np.int32), np.array([[0, 0, 1]], np.float32), w)]
+    pb.probes = np.array([[2, *probe]], np.int32)
+    return pb
+
+
+def test_cpml_reflection_below_60_db():
+    """Soft Ez dipole, probe 4 cells from the CPML of a 24^3 box, against the
+    same source and probe in a 64^3 box whose boundary echo cannot reach the
+    probe within the 110 steps."""
+    dt, steps = _dt(), 110
+    sig = 8 * dt
+    small = oracle.Oracle(_dipole(24, 12, (12, 12, 20), steps, dt, sig), fp64=True).step(steps)[:, 0].astype(np.float64)
+    big = oracle.Oracle(_dipole(64, 32, (32, 32, 40), steps, dt, sig), fp64=True).step(steps)[:, 0].astype(np.float64)
+    assert np.abs(big).max() > 1.0
+    assert np.abs(small - big).max() / np.abs(big).max() < 1e-3
+
+
+def _debye_error(m, n=40, steps=18):
+    pb = _box(n, steps, 4)
+    dt = oracle.Oracle(pb, fp64=True).dt
+    eps_inf, eps_s = 2.0, 6.0
+    tau_e = m * dt
+    tau = tau_e * eps_s / eps_inf
+    a = -1.0 / tau
+    r = (eps_s - eps_inf) * float(EPS0) / tau
+    pb.regions = [Region(kind=2, boxes=np.array([[0, n - 1] * 3], np.int32), eps=float(np.float32(eps_inf) * EPS0),
+                         residues=np.array([r], np.complex64), bpoles=np.array([-a], np.complex64))]
+    pb.probes = np.array([[0, n // 2, n // 2, n // 2]], np.int32)
+    o = oracle.Oracle(pb, fp64=True)
+    for c in range(3):
+        _fill(o, c, lambda i, j, k: np.ones(i.shape))
+    tr = o.step(steps)[:, 0].astype(np.float64)
+    t = np.arange(steps) * dt
+    exact = eps_inf / eps_s + (1 - eps_inf / eps_s) * np.exp(-t / tau_e)
+    return np.abs(tr - exact).max()
+
+
+def test_debye_relaxation_converges_to_analytic():
+    """A uniform E = 1 switched on at t = 0 in a single-real-pole medium
+    (eps_inf 2, eps_s 6) with no curl relaxes as
+    E(t) = eps_inf/eps_s + (1 - eps_inf/eps_s) exp(-t/tau_E),
+    tau_E = tau eps_inf/eps_s (the ADE state lags the field by one step)."""
+    e12, e24 = _debye_error(12), _debye_error(24)
+    assert e24 < 5e-3
+    assert e12 / e24 > 2.0
+
+
+def test_fp32_tracks_fp64():
+    n, steps, sig = 24, 160, 200e-12
+    pb = _box(n, steps, 6)
+    pb.planewaves = [PlaneWave((5, 5, 5), (18, 18, 18), 0.0, 0.0, float(np.float32(np.pi / 2)), 0.0,
+                               _gauss(_dt(), steps, sig, 4 * sig))]
+    pb.probes = np.array([[0, 12, 12, 12], [4, 12, 12, 12], [0, 9, 14, 11]], np.int32)
+    a = oracle.Oracle(pb).step(steps).astype(np.float64)
+    b = oracle.Oracle(pb, fp64=True).step(steps).astype(np.float64)
+    for q in range(3):
+        assert np.linalg.norm(a[:, q] - b[:, q]) / np.linalg.norm(b[:, q]) < 1e-5
+
+
+REF = Path("/root/reference")
+
+
+@pytest.mark.skipif(not (REF / "testData/cases/planewave.fdtd.json").exists(), reason="reference tree absent")
+def test_reader_matches_reference_parser_fixture():
+    """Expected values of test/smbjson/test_read_planewave.F90:24-96."""
+    pb = read_case(REF / "testData/cases/planewave.fdtd.json", search=(REF / "testData/excitations",))
+    assert pb.dt == pytest.approx(10e-12) and pb.nsteps == 2000
+    assert (pb.nx, pb.ny, pb.nz) == (10, 10, 10)
+    for d in (pb.desx, pb.desy, pb.desz):
+        assert d.shape == (10,) and np.all(d == np.float32(0.1))
+    assert pb.boundary == "mur"
+    (w,) = pb.planewaves
+    assert tuple(int(v) for v in w.coor1) == (1, 1, 1) and tuple(int(v) for v in w.coor2) == (8, 8, 8)
+    assert (w.theta, w.phi, w.beta) == (0.0, 0.0, 0.0) and w.alpha == pytest.approx(1.5708)
+    np.testing.assert_array_equal(pb.probes, [[0, 4, 4, 4], [1, 4, 4, 4], [2, 4, 4, 4]])
