@@ -35,7 +35,7 @@ def _stale(target: Path) -> bool:
     if not target.exists():
         return True
     t = target.stat().st_mtime
-    deps = [CSRC / s for s in SOURCES] + list(CSRC.glob("*.h")) + [HERE.parent / "include" / "semba_gpu.h", Path(__file__)]
+    deps = [CSRC / s for s in SOURCES] + list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + [HERE.parent / "include" / "semba_gpu.h", Path(__file__)]
     return any(d.stat().st_mtime > t for d in deps if d.exists())
 
 

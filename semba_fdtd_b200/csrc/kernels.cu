@@ -18,9 +18,11 @@
 #include <vector>
 
 #include "sgpu_internal.h"
+#include "stencil.cuh"
 #include "tma_fields.cuh"
 
 using namespace sgpu;
+using namespace sgpu::dev;
 
 namespace sgpu {
 
@@ -61,125 +63,6 @@ KGrid kgrid(const sgpu_ctx* c) {
 
 namespace {
 
-enum : int { kBulk = 1, kCpml = 2, kCx = 4, kCy = 8, kCz = 16, kAll = kCx | kCy | kCz };
-constexpr int kShTable = 4096;  // media entries held in shared memory
-
-__device__ __forceinline__ float* slab_ptr(const Slab& s, int i, int j, int k) {
-    if (i < s.xlo || i > s.xhi || j < s.ylo || j > s.yhi || k < s.zlo || k > s.zhi) return nullptr;
-    long long nx = s.xhi - s.xlo + 1, ny = s.yhi - s.ylo + 1;
-    return s.psi + ((i - s.xlo) + nx * ((j - s.ylo) + ny * (long long)(k - s.zlo)));
-}
-
-// True when the (x, y) column range [x0,x1]x[y0,y1] or the z range [z0,z1]
-// can touch the slab.
-__device__ __forceinline__ bool slab_touches(const Slab& s, int x0, int x1, int y0, int y1, int z0, int z1) {
-    return s.psi && x1 >= s.xlo && x0 <= s.xhi && y1 >= s.ylo && y0 <= s.yhi && z1 >= s.zlo && z0 <= s.zhi;
-}
-
-// One CPML correction of the reference (borderscpml.F90:584-1176):
-//   psi = P_b(c) * psi + diff * P_c(c) ;  F = F +- g * psi
-// applied for whichever of the two opposite slabs holds the cell.
-template <bool ADD>
-__device__ __forceinline__ float cpml_one(const Slab (&s)[2], int i, int j, int k, int c, const float* pb,
-                                          const float* pc, float diff, float g, float v, bool& touched) {
-    float* p = slab_ptr(s[0], i, j, k);
-    if (!p) p = slab_ptr(s[1], i, j, k);
-    if (p) {
-        float ps = pb[c] * (*p) + diff * pc[c];
-        *p = ps;
-        v = ADD ? v + g * ps : v - g * ps;
-        touched = true;
-    }
-    return v;
-}
-
-// Block geometry shared by the two field kernels: 32 x BY threads, each
-// owning one (i, j) column and marching over a z chunk.  x starts at local 0
-// so every warp load covers one aligned 128-byte line.
-constexpr int kBX = 32, kBY = 8;
-
-// Advance_Ex/Ey/Ez (timestepping.F90:2165-2285) fused with
-// AdvanceelectricCPML (borderscpml.F90:584-876).  Each field value is read
-// once per cell; the curl update and, in blocks that touch a PML slab, the
-// CPML corrections (in the reference's region order) are applied to the
-// register value before a single store.  Hx and Hy of plane k-1 are carried
-// in registers from the previous iteration; the i-1 neighbours come from the
-// next lower lane.
-template <int MODE, bool CP>
-__device__ __forceinline__ void efield_column(const KGrid& g, const KCpml& cp, const float* t1, const float* t2, int i, int j,
-                                              int kb, int ke, bool vx, bool vy, bool vz) {
-    const long long pitch = g.pitch, plane = g.plane;
-    float* __restrict__ Ex = g.F[0];
-    float* __restrict__ Ey = g.F[1];
-    float* __restrict__ Ez = g.F[2];
-    const float* __restrict__ Hx = g.F[3];
-    const float* __restrict__ Hy = g.F[4];
-    const float* __restrict__ Hz = g.F[5];
-    const int16_t* __restrict__ Mx = g.M[0];
-    const int16_t* __restrict__ My = g.M[1];
-    const int16_t* __restrict__ Mz = g.M[2];
-    const bool lane0 = (threadIdx.x & 31) == 0;
-    const float idyh = g.idyh[j], idxh = g.idxh[i];
-    long long c = i + pitch * j + plane * kb;
-    float hx_km = __ldg(Hx + c - plane), hy_km = __ldg(Hy + c - plane);
-    for (int k = kb; k <= ke; ++k, c += plane) {
-        const float hx = __ldg(Hx + c), hy = __ldg(Hy + c), hz = __ldg(Hz + c);
-        float hz_im = __shfl_up_sync(0xffffffffu, hz, 1);
-        float hy_im = __shfl_up_sync(0xffffffffu, hy, 1);
-        if (lane0) {
-            hz_im = __ldg(Hz + c - 1);
-            hy_im = __ldg(Hy + c - 1);
-        }
-        const float idzh = g.idzh[k];
-        if ((MODE & kCx) && vx && k >= g.sw[0][4] && k <= g.sw[0][5]) {
-            float e = Ex[c];
-            const int m = __ldg(Mx + c);
-            const float dy = hz - __ldg(Hz + c - pitch);
-            const float dz = hy - hy_km;
-            bool st = (MODE & kBulk) != 0;
-            if (MODE & kBulk) e = t1[m] * e + t2[m] * (dy * idyh - dz * idzh);
-            if (CP) {
-                const float gg = t2[m];
-                e = cpml_one<true>(cp.s[0][0], i, j, k, j, cp.pbe[1], cp.pce[1], dy, gg, e, st);
-                e = cpml_one<false>(cp.s[0][1], i, j, k, k, cp.pbe[2], cp.pce[2], dz, gg, e, st);
-            }
-            if (st) Ex[c] = e;
-        }
-        if ((MODE & kCy) && vy && k >= g.sw[1][4] && k <= g.sw[1][5]) {
-            float e = Ey[c];
-            const int m = __ldg(My + c);
-            const float dz = hx - hx_km;
-            const float dx = hz - hz_im;
-            bool st = (MODE & kBulk) != 0;
-            if (MODE & kBulk) e = t1[m] * e + t2[m] * (dz * idzh - dx * idxh);
-            if (CP) {
-                const float gg = t2[m];
-                e = cpml_one<true>(cp.s[1][0], i, j, k, k, cp.pbe[2], cp.pce[2], dz, gg, e, st);
-                e = cpml_one<false>(cp.s[1][1], i, j, k, i, cp.pbe[0], cp.pce[0], dx, gg, e, st);
-            }
-            if (st) Ey[c] = e;
-        }
-        if ((MODE & kCz) && vz && k >= g.sw[2][4] && k <= g.sw[2][5]) {
-            float e = Ez[c];
-            const int m = __ldg(Mz + c);
-            const float dx = hy - hy_im;
-            const float dy = hx - __ldg(Hx + c - pitch);
-            bool st = (MODE & kBulk) != 0;
-            if (MODE & kBulk) e = t1[m] * e + t2[m] * (dx * idxh - dy * idyh);
-            if (CP) {
-                const float gg = t2[m];
-                e = cpml_one<false>(cp.s[2][0], i, j, k, j, cp.pbe[1], cp.pce[1], dy, gg, e, st);
-                e = cpml_one<true>(cp.s[2][1], i, j, k, i, cp.pbe[0], cp.pce[0], dx, gg, e, st);
-            }
-            if (st) Ez[c] = e;
-        }
-        hx_km = hx;
-        hy_km = hy;
-    }
-}
-
-__device__ __forceinline__ bool col_in(const int* s, int i, int j) { return i >= s[0] && i <= s[1] && j >= s[2] && j <= s[3]; }
-
 template <int MODE>
 __global__ void __launch_bounds__(kBX * kBY, 4) k_efield(KGrid g, KCpml cp, int y0, int z0, int z1, int zchunk) {
     extern __shared__ float sh[];
@@ -214,84 +97,6 @@ __global__ void __launch_bounds__(kBX * kBY, 4) k_efield(KGrid g, KCpml cp, int 
     }
     if (cpml_block) efield_column<MODE, true>(g, cp, t1, t2, ic, jc, kb, ke, vx, vy, vz);
     else if (MODE & kBulk) efield_column<MODE, false>(g, cp, t1, t2, ic, jc, kb, ke, vx, vy, vz);
-}
-
-// Advance_Hx/Hy/Hz (timestepping.F90:2294-2409) fused with
-// AdvanceMagneticCPML (borderscpml.F90:881-1176).  Ex and Ey of plane k+1
-// are loaded once and carried to the next iteration; the i+1 neighbours come
-// from the next higher lane.
-template <int MODE, bool CP>
-__device__ __forceinline__ void hfield_column(const KGrid& g, const KCpml& cp, const float* t1, const float* t2, int i, int j,
-                                              int kb, int ke, bool vx, bool vy, bool vz) {
-    const long long pitch = g.pitch, plane = g.plane;
-    const float* __restrict__ Ex = g.F[0];
-    const float* __restrict__ Ey = g.F[1];
-    const float* __restrict__ Ez = g.F[2];
-    float* __restrict__ Hx = g.F[3];
-    float* __restrict__ Hy = g.F[4];
-    float* __restrict__ Hz = g.F[5];
-    const int16_t* __restrict__ Mx = g.M[3];
-    const int16_t* __restrict__ My = g.M[4];
-    const int16_t* __restrict__ Mz = g.M[5];
-    const bool lane31 = (threadIdx.x & 31) == 31;
-    const float idye = g.idye[j], idxe = g.idxe[i];
-    long long c = i + pitch * j + plane * kb;
-    float ex_k = __ldg(Ex + c), ey_k = __ldg(Ey + c);
-    for (int k = kb; k <= ke; ++k, c += plane) {
-        const float ez = __ldg(Ez + c);
-        const float ex_kp = __ldg(Ex + c + plane), ey_kp = __ldg(Ey + c + plane);
-        float ez_ip = __shfl_down_sync(0xffffffffu, ez, 1);
-        float ey_ip = __shfl_down_sync(0xffffffffu, ey_k, 1);
-        if (lane31) {
-            ez_ip = __ldg(Ez + c + 1);
-            ey_ip = __ldg(Ey + c + 1);
-        }
-        const float idze = g.idze[k];
-        if ((MODE & kCx) && vx && k >= g.sw[3][4] && k <= g.sw[3][5]) {
-            float h = Hx[c];
-            const int m = __ldg(Mx + c);
-            const float dz = ey_kp - ey_k;
-            const float dy = __ldg(Ez + c + pitch) - ez;
-            bool st = (MODE & kBulk) != 0;
-            if (MODE & kBulk) h = t1[m] * h + t2[m] * (dz * idze - dy * idye);
-            if (CP) {
-                const float gg = t2[m];
-                h = cpml_one<false>(cp.s[3][0], i, j, k, j, cp.pbm[1], cp.pcm[1], dy, gg, h, st);
-                h = cpml_one<true>(cp.s[3][1], i, j, k, k, cp.pbm[2], cp.pcm[2], dz, gg, h, st);
-            }
-            if (st) Hx[c] = h;
-        }
-        if ((MODE & kCy) && vy && k >= g.sw[4][4] && k <= g.sw[4][5]) {
-            float h = Hy[c];
-            const int m = __ldg(My + c);
-            const float dx = ez_ip - ez;
-            const float dz = ex_kp - ex_k;
-            bool st = (MODE & kBulk) != 0;
-            if (MODE & kBulk) h = t1[m] * h + t2[m] * (dx * idxe - dz * idze);
-            if (CP) {
-                const float gg = t2[m];
-                h = cpml_one<false>(cp.s[4][0], i, j, k, k, cp.pbm[2], cp.pcm[2], dz, gg, h, st);
-                h = cpml_one<true>(cp.s[4][1], i, j, k, i, cp.pbm[0], cp.pcm[0], dx, gg, h, st);
-            }
-            if (st) Hy[c] = h;
-        }
-        if ((MODE & kCz) && vz && k >= g.sw[5][4] && k <= g.sw[5][5]) {
-            float h = Hz[c];
-            const int m = __ldg(Mz + c);
-            const float dy = __ldg(Ex + c + pitch) - ex_k;
-            const float dx = ey_ip - ey_k;
-            bool st = (MODE & kBulk) != 0;
-            if (MODE & kBulk) h = t1[m] * h + t2[m] * (dy * idye - dx * idxe);
-            if (CP) {
-                const float gg = t2[m];
-                h = cpml_one<true>(cp.s[5][0], i, j, k, j, cp.pbm[1], cp.pcm[1], dy, gg, h, st);
-                h = cpml_one<false>(cp.s[5][1], i, j, k, i, cp.pbm[0], cp.pcm[0], dx, gg, h, st);
-            }
-            if (st) Hz[c] = h;
-        }
-        ex_k = ex_kp;
-        ey_k = ey_kp;
-    }
 }
 
 template <int MODE>
@@ -333,155 +138,6 @@ __global__ void __launch_bounds__(kBX * kBY, 4) k_hfield(KGrid g, KCpml cp, int 
 // Same per-cell arithmetic as efield_column / hfield_column, from shared
 // memory instead of global loads.
 
-// Every lane waits on the barrier (each needs the acquire); the warp then
-// agrees on the outcome so all lanes leave together on a timeout.
-__device__ __forceinline__ bool warp_wait(unsigned bar, unsigned parity, int* err, int code) {
-    const bool ok = mbar_wait(bar, parity, err, code);
-    return __all_sync(0xffffffffu, ok);
-}
-
-template <bool CP>
-__device__ __forceinline__ void e_consume(const TmaCta& t, const KGrid& g, const KCpml& cp, const float* t1, const float* t2,
-                                          int* err) {
-    const int w = t.warp, l = t.lane;
-    const int i = t.ib + l, j = t.jb + w;
-    const int nya = (int)(g.plane / g.pitch);
-    const bool vx = col_in(g.sw[0], i, j), vy = col_in(g.sw[1], i, j), vz = col_in(g.sw[2], i, j);
-    const float idyh = g.idyh[min(j, nya - 1)], idxh = g.idxh[i];
-    const long long pitch = g.pitch, plane = g.plane;
-    for (int k = t.kb; k <= t.ke; ++k) {
-        const int pidx = k - (t.kb - 1);
-        const int s = pidx % kStages, sp = (pidx - 1) % kStages;
-        if (k == t.kb && !warp_wait(t.full0, 0, err, 2)) return;
-        if (!warp_wait(t.full0 + 8 * s, (pidx / kStages) & 1, err, 1)) return;
-        const unsigned char* st = t.ring + s * kStageBytes;
-        const unsigned char* pv = t.ring + sp * kStageBytes;
-        const float* HX = (const float*)(st + kOffA);
-        const float* HY = (const float*)(st + kOffB);
-        const float* HZ = (const float*)(st + kOffC);
-        const float* HXp = (const float*)(pv + kOffA);
-        const float* HYp = (const float*)(pv + kOffB);
-        const float* EF = (const float*)(st + kOffF);
-        const int16_t* MF = (const int16_t*)(st + kOffM);
-        constexpr int fs = align128(kBoxF) / 4, ms = align128(kBoxM) / 2;
-        const float hx = HX[(w + 1) * kTX + l], hx_jm = HX[w * kTX + l], hx_km = HXp[(w + 1) * kTX + l];
-        const float hy = HY[w * kHaloW + l + 4], hy_im = HY[w * kHaloW + l + 3], hy_km = HYp[w * kHaloW + l + 4];
-        const float hz = HZ[(w + 1) * kHaloW + l + 4], hz_jm = HZ[w * kHaloW + l + 4], hz_im = HZ[(w + 1) * kHaloW + l + 3];
-        const float idzh = g.idzh[k];
-        const long long c = i + pitch * j + plane * k;
-        const int o = w * kTX + l;
-        if (vx && k >= g.sw[0][4] && k <= g.sw[0][5]) {
-            float e = EF[o];
-            const int m = MF[o];
-            const float dy = hz - hz_jm, dz = hy - hy_km;
-            e = t1[m] * e + t2[m] * (dy * idyh - dz * idzh);
-            if (CP) {
-                bool st_ = true;
-                e = cpml_one<true>(cp.s[0][0], i, j, k, j, cp.pbe[1], cp.pce[1], dy, t2[m], e, st_);
-                e = cpml_one<false>(cp.s[0][1], i, j, k, k, cp.pbe[2], cp.pce[2], dz, t2[m], e, st_);
-            }
-            g.F[0][c] = e;
-        }
-        if (vy && k >= g.sw[1][4] && k <= g.sw[1][5]) {
-            float e = EF[fs + o];
-            const int m = MF[ms + o];
-            const float dz = hx - hx_km, dx = hz - hz_im;
-            e = t1[m] * e + t2[m] * (dz * idzh - dx * idxh);
-            if (CP) {
-                bool st_ = true;
-                e = cpml_one<true>(cp.s[1][0], i, j, k, k, cp.pbe[2], cp.pce[2], dz, t2[m], e, st_);
-                e = cpml_one<false>(cp.s[1][1], i, j, k, i, cp.pbe[0], cp.pce[0], dx, t2[m], e, st_);
-            }
-            g.F[1][c] = e;
-        }
-        if (vz && k >= g.sw[2][4] && k <= g.sw[2][5]) {
-            float e = EF[2 * fs + o];
-            const int m = MF[2 * ms + o];
-            const float dx = hy - hy_im, dy = hx - hx_jm;
-            e = t1[m] * e + t2[m] * (dx * idxh - dy * idyh);
-            if (CP) {
-                bool st_ = true;
-                e = cpml_one<false>(cp.s[2][0], i, j, k, j, cp.pbe[1], cp.pce[1], dy, t2[m], e, st_);
-                e = cpml_one<true>(cp.s[2][1], i, j, k, i, cp.pbe[0], cp.pce[0], dx, t2[m], e, st_);
-            }
-            g.F[2][c] = e;
-        }
-        __syncwarp();
-        if (l == 0) mbar_arrive(t.empty0 + 8 * sp);  // plane k-1 is no longer needed
-    }
-}
-
-template <bool CP>
-__device__ __forceinline__ void h_consume(const TmaCta& t, const KGrid& g, const KCpml& cp, const float* t1, const float* t2,
-                                          int* err) {
-    const int w = t.warp, l = t.lane;
-    const int i = t.ib + l, j = t.jb + w;
-    const int nya = (int)(g.plane / g.pitch);
-    const bool vx = col_in(g.sw[3], i, j), vy = col_in(g.sw[4], i, j), vz = col_in(g.sw[5], i, j);
-    const float idye = g.idye[min(j, nya - 1)], idxe = g.idxe[i];
-    const long long pitch = g.pitch, plane = g.plane;
-    for (int k = t.kb; k <= t.ke; ++k) {
-        const int pidx = k - t.kb;
-        const int s = pidx % kStages, sn = (pidx + 1) % kStages;
-        if (!warp_wait(t.full0 + 8 * s, (pidx / kStages) & 1, err, 3)) return;
-        if (!warp_wait(t.full0 + 8 * sn, ((pidx + 1) / kStages) & 1, err, 4)) return;
-        const unsigned char* st = t.ring + s * kStageBytes;
-        const unsigned char* nx = t.ring + sn * kStageBytes;
-        const float* EX = (const float*)(st + kOffA);
-        const float* EY = (const float*)(st + kOffB);
-        const float* EZ = (const float*)(st + kOffC);
-        const float* EXn = (const float*)(nx + kOffA);
-        const float* EYn = (const float*)(nx + kOffB);
-        const float* HF = (const float*)(st + kOffF);
-        const int16_t* MF = (const int16_t*)(st + kOffM);
-        constexpr int fs = align128(kBoxF) / 4, ms = align128(kBoxM) / 2;
-        const float ex = EX[w * kTX + l], ex_jp = EX[(w + 1) * kTX + l], ex_kp = EXn[w * kTX + l];
-        const float ey = EY[w * kHaloW + l], ey_ip = EY[w * kHaloW + l + 1], ey_kp = EYn[w * kHaloW + l];
-        const float ez = EZ[w * kHaloW + l], ez_ip = EZ[w * kHaloW + l + 1], ez_jp = EZ[(w + 1) * kHaloW + l];
-        const float idze = g.idze[k];
-        const long long c = i + pitch * j + plane * k;
-        const int o = w * kTX + l;
-        if (vx && k >= g.sw[3][4] && k <= g.sw[3][5]) {
-            float h = HF[o];
-            const int m = MF[o];
-            const float dz = ey_kp - ey, dy = ez_jp - ez;
-            h = t1[m] * h + t2[m] * (dz * idze - dy * idye);
-            if (CP) {
-                bool st_ = true;
-                h = cpml_one<false>(cp.s[3][0], i, j, k, j, cp.pbm[1], cp.pcm[1], dy, t2[m], h, st_);
-                h = cpml_one<true>(cp.s[3][1], i, j, k, k, cp.pbm[2], cp.pcm[2], dz, t2[m], h, st_);
-            }
-            g.F[3][c] = h;
-        }
-        if (vy && k >= g.sw[4][4] && k <= g.sw[4][5]) {
-            float h = HF[fs + o];
-            const int m = MF[ms + o];
-            const float dx = ez_ip - ez, dz = ex_kp - ex;
-            h = t1[m] * h + t2[m] * (dx * idxe - dz * idze);
-            if (CP) {
-                bool st_ = true;
-                h = cpml_one<false>(cp.s[4][0], i, j, k, k, cp.pbm[2], cp.pcm[2], dz, t2[m], h, st_);
-                h = cpml_one<true>(cp.s[4][1], i, j, k, i, cp.pbm[0], cp.pcm[0], dx, t2[m], h, st_);
-            }
-            g.F[4][c] = h;
-        }
-        if (vz && k >= g.sw[5][4] && k <= g.sw[5][5]) {
-            float h = HF[2 * fs + o];
-            const int m = MF[2 * ms + o];
-            const float dy = ex_jp - ex, dx = ey_ip - ey;
-            h = t1[m] * h + t2[m] * (dy * idye - dx * idxe);
-            if (CP) {
-                bool st_ = true;
-                h = cpml_one<true>(cp.s[5][0], i, j, k, j, cp.pbm[1], cp.pcm[1], dy, t2[m], h, st_);
-                h = cpml_one<false>(cp.s[5][1], i, j, k, i, cp.pbm[0], cp.pcm[0], dx, t2[m], h, st_);
-            }
-            g.F[5][c] = h;
-        }
-        __syncwarp();
-        if (l == 0) mbar_arrive(t.empty0 + 8 * s);  // plane k is no longer needed
-    }
-}
-
 __device__ __forceinline__ const float* tma_tables(unsigned char* smem, const float* a, const float* b, int nmed1) {
     float* tab = (float*)(smem + kTmaSmem);
     if (nmed1 <= kShTable) {
@@ -500,7 +156,7 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
     const float* tab = tma_tables(smem, g.g1, g.g2, g.nmed1);
     const TmaCta t = tma_cta_setup(smem, y0, z0, z1, zchunk);
     if (t.warp == kConsumerWarps) {
-        tma_produce(t, tm, t.kb - 1, t.ke, t.kb - 1, err);
+        if (t.lane == 0) tma_drain(t, (unsigned)tma_issue(t, tm.m, 0, t.kb - 1, t.ke, t.kb - 1, false, err), err, 12);
         return;
     }
     const float* t1 = tab ? tab : g.g1;
@@ -511,8 +167,8 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
             for (int w = 0; w < 2; ++w)
                 for (int sd = 0; sd < 2; ++sd)
                     cpml_block |= slab_touches(cp.s[f][w][sd], t.ib, t.ib + kTX - 1, t.jb, t.jb + kTY - 1, t.kb, t.ke);
-    if (cpml_block) e_consume<true>(t, g, cp, t1, t2, err);
-    else e_consume<false>(t, g, cp, t1, t2, err);
+    if (cpml_block) e_consume<true>(t, 0, g, cp, t1, t2, err, false);
+    else e_consume<false>(t, 0, g, cp, t1, t2, err, false);
 }
 
 __global__ void __launch_bounds__(kTmaThreads, 3)
@@ -521,7 +177,7 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
     const float* tab = tma_tables(smem, g.gm1, g.gm2, g.nmed1);
     const TmaCta t = tma_cta_setup(smem, y0, z0, z1, zchunk);
     if (t.warp == kConsumerWarps) {
-        tma_produce_h(t, tm, t.kb, t.ke + 1, t.ke + 1, err);
+        if (t.lane == 0) tma_drain(t, (unsigned)tma_issue(t, tm.m, 0, t.kb, t.ke + 1, t.ke + 1, true, err), err, 14);
         return;
     }
     const float* t1 = tab ? tab : g.gm1;
@@ -532,101 +188,29 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
             for (int w = 0; w < 2; ++w)
                 for (int sd = 0; sd < 2; ++sd)
                     cpml_block |= slab_touches(cp.s[f][w][sd], t.ib, t.ib + kTX - 1, t.jb, t.jb + kTY - 1, t.kb, t.ke);
-    if (cpml_block) h_consume<true>(t, g, cp, t1, t2, err);
-    else h_consume<false>(t, g, cp, t1, t2, err);
+    if (cpml_block) h_consume<true>(t, 0, g, cp, t1, t2, err, false);
+    else h_consume<false>(t, 0, g, cp, t1, t2, err, false);
 }
 
-// AdvanceEDispersiveE (electricdispersive.F90:304-362): one thread per node.
-// Conjugate poles share one state slot; the subtraction still runs once
-// per pole of the reference, in its order, and Re(conj(g)*conj(J)) equals
-// Re(g*J) exactly.  NU (the largest number of state slots of any medium) is
-// a template parameter so the states stay in registers.
 template <int NU>
 __global__ void __launch_bounds__(256) k_edisp(KGrid g, KDisp d, int comp) {
     const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    const long long n = d.n[comp];
-    if (q >= n) return;
-    const int idx = d.node[comp][q];
-    const DispMedium* __restrict__ md = d.media + d.med[comp][q];
-    float* F = g.F[comp];
-    double2* J = d.J[comp];
-    const int nu = md->nu;
-    double2 st[NU];
-#pragma unroll
-    for (int u = 0; u < NU; ++u) st[u] = u < nu ? J[u * n + q] : make_double2(0.0, 0.0);
-    float e = F[idx];
-    for (int p = 0; p < md->np; ++p) {
-        const int up = md->map[p];
-        double jr = 0.0, ji = 0.0;
-#pragma unroll
-        for (int u = 0; u < NU; ++u)
-            if (u == up) { jr = st[u].x; ji = st[u].y; }
-        const double2 g3 = md->g3[up];
-        const double re = g3.x * jr - g3.y * ji;
-        e = (float)((double)e - re);
-    }
-    const double dd = (double)(e - d.prev[comp][q]);
-#pragma unroll
-    for (int u = 0; u < NU; ++u) {
-        if (u < nu) {
-            const double2 kp = md->kappa[u], bt = md->beta[u];
-            const double kr = kp.x * st[u].x - kp.y * st[u].y;
-            const double ki = kp.x * st[u].y + kp.y * st[u].x;
-            const double br = (bt.x * dd) / d.dt;
-            const double bi = (bt.y * dd) / d.dt;
-            J[u * n + q] = make_double2(kr + br, ki + bi);
-        }
-    }
-    d.prev[comp][q] = e;
-    F[idx] = e;
+    if (q < d.n[comp]) edisp_node<NU>(g, d, comp, q);
 }
 
-__device__ __forceinline__ int step_of(const StepRef& s) { return (s.dev_n ? *s.dev_n : 0) + s.n; }
 
 // AdvancePlaneWaveE/H (planewaves.F90:878-1475) with Incid/evolucion
 // (:778-853) and AdvanceNodalE/H (nodalsources.F90:310-777): one thread per
 // touched node applies that node's contributions in the reference order.
 __global__ void k_sources(KGrid g, KSrc s, StepRef sr, const double* tiempo, int t_n0, double dt, int hside, int mask) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= s.nrows) return;
-    const int n = step_of(sr);
-    const double tn = tiempo[n - t_n0];
-    const float t = hside ? (float)(tn + (double)0.5f * dt) : (float)tn;
-    const float G21 = hside ? g.gm2[1] : g.g2[1];
-    float* F = g.F[s.row_comp[r]];
-    const int node = s.row_node[r];
-    float v = F[node];
-    for (int p = s.row_ptr[r]; p < s.row_ptr[r + 1]; ++p) {
-        const SrcEntry en = s.e[p];
-        if (!((1 << en.type) & mask)) continue;
-        const SrcTable tb = s.tab[en.table];
-        const float* ev0 = s.samples + tb.offset;
-        if (en.type == kSrcPlaneWave) {
-            float ev = 0.0f;
-            const long long nprev = (long long)((t - en.a) / tb.delta);
-            if (nprev + 1 <= tb.numus && nprev > 0)
-                ev = (ev0[nprev + 1] - ev0[nprev]) / tb.delta * ((t - en.a) - (float)nprev * tb.delta) + ev0[nprev];
-            const float inc = 0.0f + en.b * ev;
-            v = v + G21 * inc * en.c;
-        } else {
-            float ev = 0.0f;
-            const long long nprev = (long long)(t / tb.delta);
-            if (!((nprev + 1 > tb.numus) || (nprev + 1 <= 0)))
-                ev = (ev0[nprev + 1] - ev0[nprev]) / tb.delta * ((t) - (float)nprev * tb.delta) + ev0[nprev];
-            if (en.type == kSrcNodalSoft) v = v - en.a * ev;
-            else v = en.a * ev;
-        }
-    }
-    F[node] = v;
+    if (r < s.nrows) source_row(g, s, step_of(sr), tiempo, t_n0, dt, hside, mask, r);
 }
 
 // UpdateObservation point probes (observation.F90:2633-2668).
 __global__ void k_probes(KGrid g, KProbes p, StepRef sr, int first_n) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= p.n) return;
-    const int n = step_of(sr);
-    const long long row = (long long)(n - first_n) % p.cap;
-    p.ring[row * p.n + q] = g.F[p.comp[q]][p.idx[q]];
+    if (q < p.n) probe_one(g, p, step_of(sr), first_n, q);
 }
 
 __global__ void k_set_step(int* d, int v) { *d = v; }

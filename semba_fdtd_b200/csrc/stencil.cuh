@@ -1,0 +1,385 @@
+// Per-cell device arithmetic shared by the single-problem kernels
+// (kernels.cu) and the batched kernels (batch.cu).  Each function restates
+// one reference routine in its operation order; nothing here rounds
+// differently from a separate multiply and add, so a -fmad=false build
+// reproduces the reference FP32 build bit for bit.
+#pragma once
+#include "sgpu_internal.h"
+
+namespace sgpu {
+namespace dev {
+
+enum : int { kBulk = 1, kCpml = 2, kCx = 4, kCy = 8, kCz = 16, kAll = kCx | kCy | kCz };
+constexpr int kShTable = 4096;  // media entries held in shared memory
+
+__device__ __forceinline__ float* slab_ptr(const Slab& s, int i, int j, int k) {
+    if (i < s.xlo || i > s.xhi || j < s.ylo || j > s.yhi || k < s.zlo || k > s.zhi) return nullptr;
+    long long nx = s.xhi - s.xlo + 1, ny = s.yhi - s.ylo + 1;
+    return s.psi + ((i - s.xlo) + nx * ((j - s.ylo) + ny * (long long)(k - s.zlo)));
+}
+
+// True when the (x, y) column range [x0,x1]x[y0,y1] or the z range [z0,z1]
+// can touch the slab.
+__device__ __forceinline__ bool slab_touches(const Slab& s, int x0, int x1, int y0, int y1, int z0, int z1) {
+    return s.psi && x1 >= s.xlo && x0 <= s.xhi && y1 >= s.ylo && y0 <= s.yhi && z1 >= s.zlo && z0 <= s.zhi;
+}
+
+// Slab masks: a tile only looks up the slabs that can hold its cells.  Bit
+// 4*q + 2*kind + side stands for slab cp.s[c0+q][kind][side] of the three
+// components c0..c0+2 of a half step.  cpml_tile_mask keeps the slabs whose
+// x-y extent meets the tile's columns (once per tile); cpml_plane_mask keeps
+// those whose z extent holds plane k (once per plane).  Both are uniform
+// over the tile, so a plane that touches no slab runs the bulk path.
+__device__ __forceinline__ unsigned cpml_tile_mask(const KCpml& cp, int c0, int x0, int x1, int y0, int y1) {
+    unsigned m = 0;
+    if (!cp.on) return 0;
+#pragma unroll
+    for (int n = 0; n < 12; ++n) {
+        const Slab& s = cp.s[c0 + (n >> 2)][(n >> 1) & 1][n & 1];
+        if (s.psi && x1 >= s.xlo && x0 <= s.xhi && y1 >= s.ylo && y0 <= s.yhi) m |= 1u << n;
+    }
+    return m;
+}
+__device__ __forceinline__ unsigned cpml_plane_mask(const KCpml& cp, int c0, unsigned tile, int k) {
+    unsigned m = 0;
+#pragma unroll
+    for (int n = 0; n < 12; ++n) {
+        const Slab& s = cp.s[c0 + (n >> 2)][(n >> 1) & 1][n & 1];
+        if (((tile >> n) & 1) && k >= s.zlo && k <= s.zhi) m |= 1u << n;
+    }
+    return m;
+}
+
+// Slabs by the axis their coefficients run along (the same for the E and H
+// sides): x -- comp 1 kind 1, comp 2 kind 1; y -- comp 0 kind 0, comp 2
+// kind 0; z -- comp 0 kind 1, comp 1 kind 0.
+constexpr unsigned kCpmlX = 0xCC0u, kCpmlY = 0x303u, kCpmlZ = 0x03Cu;
+
+// Per-thread CPML view of one tile: `col` flags the slabs whose x-y extent
+// holds the thread's column (i, j), and the P_b / P_c values indexed by i
+// and j are loaded once (only where some slab needs them, so i and j are in
+// range).
+struct CpmlCol {
+    unsigned col;
+    float bx, cx, by, cy;
+};
+__device__ __forceinline__ CpmlCol cpml_col(const KCpml& cp, int c0, unsigned tile, int i, int j) {
+    CpmlCol r;
+    r.col = 0;
+#pragma unroll
+    for (int n = 0; n < 12; ++n) {
+        const Slab& s = cp.s[c0 + (n >> 2)][(n >> 1) & 1][n & 1];
+        if (((tile >> n) & 1) && i >= s.xlo && i <= s.xhi && j >= s.ylo && j <= s.yhi) r.col |= 1u << n;
+    }
+    const bool h = c0 != 0;
+    r.bx = r.cx = r.by = r.cy = 0.0f;
+    if (r.col & kCpmlX) {
+        r.bx = (h ? cp.pbm[0] : cp.pbe[0])[i];
+        r.cx = (h ? cp.pcm[0] : cp.pce[0])[i];
+    }
+    if (r.col & kCpmlY) {
+        r.by = (h ? cp.pbm[1] : cp.pbe[1])[j];
+        r.cy = (h ? cp.pcm[1] : cp.pce[1])[j];
+    }
+    return r;
+}
+
+// One CPML correction of the reference (borderscpml.F90:584-1176):
+//   psi = P_b(c) * psi + diff * P_c(c) ;  F = F +- g * psi
+// for the slab pair whose two live bits are `live2` (side 0 first; the two
+// sides lie at opposite ends of the axis and share no cell), with the
+// P_b(c) / P_c(c) values already loaded.
+template <bool ADD>
+__device__ __forceinline__ float cpml_pair(const Slab (&s)[2], unsigned live2, int i, int j, int k, float pb, float pc,
+                                           float diff, float g, float v, bool& touched) {
+    if (live2) {
+        const bool a = live2 & 1;
+        float* const psi = a ? s[0].psi : s[1].psi;
+        const int xlo = a ? s[0].xlo : s[1].xlo, xhi = a ? s[0].xhi : s[1].xhi;
+        const int ylo = a ? s[0].ylo : s[1].ylo, yhi = a ? s[0].yhi : s[1].yhi;
+        const int zlo = a ? s[0].zlo : s[1].zlo;
+        float* p = psi + ((i - xlo) + (long long)(xhi - xlo + 1) * ((j - ylo) + (long long)(yhi - ylo + 1) * (k - zlo)));
+        const float ps = pb * (*p) + diff * pc;
+        *p = ps;
+        v = ADD ? v + g * ps : v - g * ps;
+        touched = true;
+    }
+    return v;
+}
+
+// Block geometry shared by the two field kernels: 32 x BY threads, each
+// owning one (i, j) column and marching over a z chunk.  x starts at local 0
+// so every warp load covers one aligned 128-byte line.
+constexpr int kBX = 32, kBY = 8;
+
+// Advance_Ex/Ey/Ez (timestepping.F90:2165-2285) fused with
+// AdvanceelectricCPML (borderscpml.F90:584-876).  Each field value is read
+// once per cell; the curl update and, in blocks that touch a PML slab, the
+// CPML corrections (in the reference's region order) are applied to the
+// register value before a single store.  Hx and Hy of plane k-1 are carried
+// in registers from the previous iteration; the i-1 neighbours come from the
+// next lower lane.
+template <int MODE, bool CP>
+__device__ __forceinline__ void efield_column(const KGrid& g, const KCpml& cp, const float* t1, const float* t2, int i, int j,
+                                              int kb, int ke, bool vx, bool vy, bool vz) {
+    const long long pitch = g.pitch, plane = g.plane;
+    float* __restrict__ Ex = g.F[0];
+    float* __restrict__ Ey = g.F[1];
+    float* __restrict__ Ez = g.F[2];
+    const float* __restrict__ Hx = g.F[3];
+    const float* __restrict__ Hy = g.F[4];
+    const float* __restrict__ Hz = g.F[5];
+    const int16_t* __restrict__ Mx = g.M[0];
+    const int16_t* __restrict__ My = g.M[1];
+    const int16_t* __restrict__ Mz = g.M[2];
+    const bool lane0 = (threadIdx.x & 31) == 0;
+    const float idyh = g.idyh[j], idxh = g.idxh[i];
+    long long c = i + pitch * j + plane * kb;
+    float hx_km = __ldg(Hx + c - plane), hy_km = __ldg(Hy + c - plane);
+    // slabs that can hold this block's cells (its 32 x blockDim.y columns);
+    // threads on clamped rows store nothing, so their mask does not matter
+    const int bx0 = i & ~31, by0 = j - (int)threadIdx.y;
+    const unsigned tmask = CP ? cpml_tile_mask(cp, 0, bx0, bx0 + 31, by0, by0 + (int)blockDim.y - 1) : 0u;
+    const CpmlCol cc = CP ? cpml_col(cp, 0, tmask, i, j) : CpmlCol{};
+    for (int k = kb; k <= ke; ++k, c += plane) {
+        const unsigned pm = CP ? cpml_plane_mask(cp, 0, cc.col, k) : 0u;
+        float bz = 0.0f, cz = 0.0f;
+        if (CP && (pm & kCpmlZ)) {
+            bz = cp.pbe[2][k];
+            cz = cp.pce[2][k];
+        }
+        const float hx = __ldg(Hx + c), hy = __ldg(Hy + c), hz = __ldg(Hz + c);
+        float hz_im = __shfl_up_sync(0xffffffffu, hz, 1);
+        float hy_im = __shfl_up_sync(0xffffffffu, hy, 1);
+        if (lane0) {
+            hz_im = __ldg(Hz + c - 1);
+            hy_im = __ldg(Hy + c - 1);
+        }
+        const float idzh = g.idzh[k];
+        if ((MODE & kCx) && vx && k >= g.sw[0][4] && k <= g.sw[0][5]) {
+            float e = Ex[c];
+            const int m = __ldg(Mx + c);
+            const float dy = hz - __ldg(Hz + c - pitch);
+            const float dz = hy - hy_km;
+            bool st = (MODE & kBulk) != 0;
+            if (MODE & kBulk) e = t1[m] * e + t2[m] * (dy * idyh - dz * idzh);
+            if (CP && pm) {
+                const float gg = t2[m];
+                e = cpml_pair<true>(cp.s[0][0], pm & 3, i, j, k, cc.by, cc.cy, dy, gg, e, st);
+                e = cpml_pair<false>(cp.s[0][1], (pm >> 2) & 3, i, j, k, bz, cz, dz, gg, e, st);
+            }
+            if (st) Ex[c] = e;
+        }
+        if ((MODE & kCy) && vy && k >= g.sw[1][4] && k <= g.sw[1][5]) {
+            float e = Ey[c];
+            const int m = __ldg(My + c);
+            const float dz = hx - hx_km;
+            const float dx = hz - hz_im;
+            bool st = (MODE & kBulk) != 0;
+            if (MODE & kBulk) e = t1[m] * e + t2[m] * (dz * idzh - dx * idxh);
+            if (CP && pm) {
+                const float gg = t2[m];
+                e = cpml_pair<true>(cp.s[1][0], (pm >> 4) & 3, i, j, k, bz, cz, dz, gg, e, st);
+                e = cpml_pair<false>(cp.s[1][1], (pm >> 6) & 3, i, j, k, cc.bx, cc.cx, dx, gg, e, st);
+            }
+            if (st) Ey[c] = e;
+        }
+        if ((MODE & kCz) && vz && k >= g.sw[2][4] && k <= g.sw[2][5]) {
+            float e = Ez[c];
+            const int m = __ldg(Mz + c);
+            const float dx = hy - hy_im;
+            const float dy = hx - __ldg(Hx + c - pitch);
+            bool st = (MODE & kBulk) != 0;
+            if (MODE & kBulk) e = t1[m] * e + t2[m] * (dx * idxh - dy * idyh);
+            if (CP && pm) {
+                const float gg = t2[m];
+                e = cpml_pair<false>(cp.s[2][0], (pm >> 8) & 3, i, j, k, cc.by, cc.cy, dy, gg, e, st);
+                e = cpml_pair<true>(cp.s[2][1], (pm >> 10) & 3, i, j, k, cc.bx, cc.cx, dx, gg, e, st);
+            }
+            if (st) Ez[c] = e;
+        }
+        hx_km = hx;
+        hy_km = hy;
+    }
+}
+
+
+__device__ __forceinline__ bool col_in(const int* s, int i, int j) { return i >= s[0] && i <= s[1] && j >= s[2] && j <= s[3]; }
+
+// Advance_Hx/Hy/Hz (timestepping.F90:2294-2409) fused with
+// AdvanceMagneticCPML (borderscpml.F90:881-1176).  Ex and Ey of plane k+1
+// are loaded once and carried to the next iteration; the i+1 neighbours come
+// from the next higher lane.
+template <int MODE, bool CP>
+__device__ __forceinline__ void hfield_column(const KGrid& g, const KCpml& cp, const float* t1, const float* t2, int i, int j,
+                                              int kb, int ke, bool vx, bool vy, bool vz) {
+    const long long pitch = g.pitch, plane = g.plane;
+    const float* __restrict__ Ex = g.F[0];
+    const float* __restrict__ Ey = g.F[1];
+    const float* __restrict__ Ez = g.F[2];
+    float* __restrict__ Hx = g.F[3];
+    float* __restrict__ Hy = g.F[4];
+    float* __restrict__ Hz = g.F[5];
+    const int16_t* __restrict__ Mx = g.M[3];
+    const int16_t* __restrict__ My = g.M[4];
+    const int16_t* __restrict__ Mz = g.M[5];
+    const bool lane31 = (threadIdx.x & 31) == 31;
+    const float idye = g.idye[j], idxe = g.idxe[i];
+    long long c = i + pitch * j + plane * kb;
+    float ex_k = __ldg(Ex + c), ey_k = __ldg(Ey + c);
+    const int bx0 = i & ~31, by0 = j - (int)threadIdx.y;
+    const unsigned tmask = CP ? cpml_tile_mask(cp, 3, bx0, bx0 + 31, by0, by0 + (int)blockDim.y - 1) : 0u;
+    const CpmlCol cc = CP ? cpml_col(cp, 3, tmask, i, j) : CpmlCol{};
+    for (int k = kb; k <= ke; ++k, c += plane) {
+        const unsigned pm = CP ? cpml_plane_mask(cp, 3, cc.col, k) : 0u;
+        float bz = 0.0f, cz = 0.0f;
+        if (CP && (pm & kCpmlZ)) {
+            bz = cp.pbm[2][k];
+            cz = cp.pcm[2][k];
+        }
+        const float ez = __ldg(Ez + c);
+        const float ex_kp = __ldg(Ex + c + plane), ey_kp = __ldg(Ey + c + plane);
+        float ez_ip = __shfl_down_sync(0xffffffffu, ez, 1);
+        float ey_ip = __shfl_down_sync(0xffffffffu, ey_k, 1);
+        if (lane31) {
+            ez_ip = __ldg(Ez + c + 1);
+            ey_ip = __ldg(Ey + c + 1);
+        }
+        const float idze = g.idze[k];
+        if ((MODE & kCx) && vx && k >= g.sw[3][4] && k <= g.sw[3][5]) {
+            float h = Hx[c];
+            const int m = __ldg(Mx + c);
+            const float dz = ey_kp - ey_k;
+            const float dy = __ldg(Ez + c + pitch) - ez;
+            bool st = (MODE & kBulk) != 0;
+            if (MODE & kBulk) h = t1[m] * h + t2[m] * (dz * idze - dy * idye);
+            if (CP && pm) {
+                const float gg = t2[m];
+                h = cpml_pair<false>(cp.s[3][0], pm & 3, i, j, k, cc.by, cc.cy, dy, gg, h, st);
+                h = cpml_pair<true>(cp.s[3][1], (pm >> 2) & 3, i, j, k, bz, cz, dz, gg, h, st);
+            }
+            if (st) Hx[c] = h;
+        }
+        if ((MODE & kCy) && vy && k >= g.sw[4][4] && k <= g.sw[4][5]) {
+            float h = Hy[c];
+            const int m = __ldg(My + c);
+            const float dx = ez_ip - ez;
+            const float dz = ex_kp - ex_k;
+            bool st = (MODE & kBulk) != 0;
+            if (MODE & kBulk) h = t1[m] * h + t2[m] * (dx * idxe - dz * idze);
+            if (CP && pm) {
+                const float gg = t2[m];
+                h = cpml_pair<false>(cp.s[4][0], (pm >> 4) & 3, i, j, k, bz, cz, dz, gg, h, st);
+                h = cpml_pair<true>(cp.s[4][1], (pm >> 6) & 3, i, j, k, cc.bx, cc.cx, dx, gg, h, st);
+            }
+            if (st) Hy[c] = h;
+        }
+        if ((MODE & kCz) && vz && k >= g.sw[5][4] && k <= g.sw[5][5]) {
+            float h = Hz[c];
+            const int m = __ldg(Mz + c);
+            const float dy = __ldg(Ex + c + pitch) - ex_k;
+            const float dx = ey_ip - ey_k;
+            bool st = (MODE & kBulk) != 0;
+            if (MODE & kBulk) h = t1[m] * h + t2[m] * (dy * idye - dx * idxe);
+            if (CP && pm) {
+                const float gg = t2[m];
+                h = cpml_pair<true>(cp.s[5][0], (pm >> 8) & 3, i, j, k, cc.by, cc.cy, dy, gg, h, st);
+                h = cpml_pair<false>(cp.s[5][1], (pm >> 10) & 3, i, j, k, cc.bx, cc.cx, dx, gg, h, st);
+            }
+            if (st) Hz[c] = h;
+        }
+        ex_k = ex_kp;
+        ey_k = ey_kp;
+    }
+}
+
+
+// AdvanceEDispersiveE (electricdispersive.F90:304-362): one thread per node.
+// Conjugate poles share one state slot; the subtraction still runs once
+// per pole of the reference, in its order, and Re(conj(g)*conj(J)) equals
+// Re(g*J) exactly.  NU (the largest number of state slots of any medium) is
+// a template parameter so the states stay in registers.
+template <int NU>
+__device__ __forceinline__ void edisp_node(const KGrid& g, const KDisp& d, int comp, long long q) {
+    const long long n = d.n[comp];
+    const int idx = d.node[comp][q];
+    const DispMedium* __restrict__ md = d.media + d.med[comp][q];
+    float* F = g.F[comp];
+    double2* J = d.J[comp];
+    const int nu = md->nu;
+    double2 st[NU];
+#pragma unroll
+    for (int u = 0; u < NU; ++u) st[u] = u < nu ? J[u * n + q] : make_double2(0.0, 0.0);
+    float e = F[idx];
+    for (int p = 0; p < md->np; ++p) {
+        const int up = md->map[p];
+        double jr = 0.0, ji = 0.0;
+#pragma unroll
+        for (int u = 0; u < NU; ++u)
+            if (u == up) { jr = st[u].x; ji = st[u].y; }
+        const double2 g3 = md->g3[up];
+        const double re = g3.x * jr - g3.y * ji;
+        e = (float)((double)e - re);
+    }
+    const double dd = (double)(e - d.prev[comp][q]);
+#pragma unroll
+    for (int u = 0; u < NU; ++u) {
+        if (u < nu) {
+            const double2 kp = md->kappa[u], bt = md->beta[u];
+            const double kr = kp.x * st[u].x - kp.y * st[u].y;
+            const double ki = kp.x * st[u].y + kp.y * st[u].x;
+            const double br = (bt.x * dd) / d.dt;
+            const double bi = (bt.y * dd) / d.dt;
+            J[u * n + q] = make_double2(kr + br, ki + bi);
+        }
+    }
+    d.prev[comp][q] = e;
+    F[idx] = e;
+}
+
+__device__ __forceinline__ int step_of(const StepRef& s) { return (s.dev_n ? *s.dev_n : 0) + s.n; }
+
+// AdvancePlaneWaveE/H (planewaves.F90:878-1475) with Incid/evolucion
+// (:778-853) and AdvanceNodalE/H (nodalsources.F90:310-777): source row r
+// (one touched node) applies that node's contributions in the reference
+// order.
+__device__ __forceinline__ void source_row(const KGrid& g, const KSrc& s, int n, const double* tiempo, int t_n0, double dt,
+                                           int hside, int mask, int r) {
+    const double tn = tiempo[n - t_n0];
+    const float t = hside ? (float)(tn + (double)0.5f * dt) : (float)tn;
+    const float G21 = hside ? g.gm2[1] : g.g2[1];
+    float* F = g.F[s.row_comp[r]];
+    const int node = s.row_node[r];
+    float v = F[node];
+    for (int p = s.row_ptr[r]; p < s.row_ptr[r + 1]; ++p) {
+        const SrcEntry en = s.e[p];
+        if (!((1 << en.type) & mask)) continue;
+        const SrcTable tb = s.tab[en.table];
+        const float* ev0 = s.samples + tb.offset;
+        if (en.type == kSrcPlaneWave) {
+            float ev = 0.0f;
+            const long long nprev = (long long)((t - en.a) / tb.delta);
+            if (nprev + 1 <= tb.numus && nprev > 0)
+                ev = (ev0[nprev + 1] - ev0[nprev]) / tb.delta * ((t - en.a) - (float)nprev * tb.delta) + ev0[nprev];
+            const float inc = 0.0f + en.b * ev;
+            v = v + G21 * inc * en.c;
+        } else {
+            float ev = 0.0f;
+            const long long nprev = (long long)(t / tb.delta);
+            if (!((nprev + 1 > tb.numus) || (nprev + 1 <= 0)))
+                ev = (ev0[nprev + 1] - ev0[nprev]) / tb.delta * ((t) - (float)nprev * tb.delta) + ev0[nprev];
+            if (en.type == kSrcNodalSoft) v = v - en.a * ev;
+            else v = en.a * ev;
+        }
+    }
+    F[node] = v;
+}
+
+// UpdateObservation point probes (observation.F90:2633-2668).
+__device__ __forceinline__ void probe_one(const KGrid& g, const KProbes& p, int n, int first_n, int q) {
+    const long long row = (long long)(n - first_n) % p.cap;
+    p.ring[row * p.n + q] = g.F[p.comp[q]][p.idx[q]];
+}
+
+}  // namespace dev
+}  // namespace sgpu

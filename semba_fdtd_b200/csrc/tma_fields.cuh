@@ -1,5 +1,6 @@
 // TMA-pipelined curl + CPML kernels (the fused fast path of the E and H half
-// steps).  Included by kernels.cu; relies on its Slab/KGrid/KCpml helpers.
+// steps) and their persistent batched form.  Included by kernels.cu and
+// batch.cu; the per-cell helpers come from stencil.cuh.
 //
 // Each CTA owns a 32 x 8 tile of (i, j) columns and marches a z chunk.  One
 // producer warp streams every plane the tile needs -- the H (or E) tiles with
@@ -16,7 +17,10 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include "stencil.cuh"
+
 namespace sgpu {
+using namespace sgpu::dev;
 
 constexpr int kTX = 32, kTY = 8;          // tile (threads per row, rows)
 constexpr int kStages = 4;                // shared-memory ring depth
@@ -116,60 +120,218 @@ __device__ __forceinline__ TmaCta tma_cta_setup(unsigned char* smem, int y0, int
     return t;
 }
 
-// Producer: planes p0 .. p1 into the ring; `edge` is the plane that carries
-// only the first two arrays (the E kernel's k-1 plane, the H kernel's k+1).
-__device__ __forceinline__ void tma_produce(const TmaCta& t, const TMaps& tm, int p0, int p1, int edge, int* err) {
-    if (t.lane != 0) return;
-    int issued = 0;
-    bool ok = true;
-    for (int p = p0; p <= p1 && ok; ++p) {
-        const int pidx = p - p0, s = pidx % kStages, u = pidx / kStages;
-        if (u >= 1 && !mbar_wait(t.empty0 + 8 * s, (u - 1) & 1, err, 11)) { ok = false; break; }
+// Producer (lane 0 of the producer warp): planes p0 .. p1 of one work item
+// into the ring; the item's first plane has the running plane number G0 (a
+// plane lands in stage G % kStages; its n-th use of that stage is phase n).
+// `edge` is the plane that carries only the first two arrays (the E side's
+// k-1 plane, the H side's k+1 plane).  Tile origins: E side Hx (ib, jb-1),
+// Hy (ib-4, jb), Hz (ib-4, jb-1), own fields and media (ib, jb); H side all
+// at (ib, jb).  Returns the number of planes issued: fewer than p1-p0+1 when
+// a bounded wait ran out.
+__device__ __forceinline__ int tma_issue(const TmaCta& t, const CUtensorMap* maps, unsigned G0, int p0, int p1, int edge,
+                                         bool hside, int* err) {
+    for (int p = p0; p <= p1; ++p) {
+        const unsigned G = G0 + (unsigned)(p - p0), s = G % kStages, u = G / kStages;
+        if (u >= 1 && !mbar_wait(t.empty0 + 8 * s, (u - 1) & 1, err, hside ? 13 : 11)) return p - p0;
         const unsigned bar = t.full0 + 8 * s;
         unsigned char* st = t.ring + s * kStageBytes;
         const bool part = p == edge;
         mbar_expect_tx(bar, part ? kTxEdge : kTxFull);
-        tma_load3(smem_u32(st + kOffA), &tm.m[0], t.ib, t.jb - 1, p, bar);  // first array (halo in y)
-        tma_load3(smem_u32(st + kOffB), &tm.m[1], t.ib - 4, t.jb, p, bar);  // second (halo in x)
+        const int xh = hside ? t.ib : t.ib - 4, ya = hside ? t.jb : t.jb - 1;
+        tma_load3(smem_u32(st + kOffA), &maps[0], t.ib, ya, p, bar);  // first array (halo in y)
+        tma_load3(smem_u32(st + kOffB), &maps[1], xh, t.jb, p, bar);  // second (halo in x)
         if (!part) {
-            tma_load3(smem_u32(st + kOffC), &tm.m[2], t.ib - 4, t.jb - 1, p, bar);
-            for (int q = 0; q < 3; ++q) tma_load3(smem_u32(st + kOffF + q * align128(kBoxF)), &tm.m[3 + q], t.ib, t.jb, p, bar);
-            for (int q = 0; q < 3; ++q) tma_load3(smem_u32(st + kOffM + q * align128(kBoxM)), &tm.m[6 + q], t.ib, t.jb, p, bar);
+            tma_load3(smem_u32(st + kOffC), &maps[2], xh, ya, p, bar);
+            for (int q = 0; q < 3; ++q) tma_load3(smem_u32(st + kOffF + q * align128(kBoxF)), &maps[3 + q], t.ib, t.jb, p, bar);
+            for (int q = 0; q < 3; ++q) tma_load3(smem_u32(st + kOffM + q * align128(kBoxM)), &maps[6 + q], t.ib, t.jb, p, bar);
         }
-        ++issued;
     }
-    // nothing may be in flight into this CTA's shared memory when it exits
-    const int first = issued > kStages ? issued - kStages : 0;
-    for (int pidx = first; pidx < issued; ++pidx)
-        mbar_wait(t.full0 + 8 * (pidx % kStages), (pidx / kStages) & 1, err, 12);
+    return p1 - p0 + 1;
 }
 
-// The H kernel's tiles start at x = ib (no -x halo) and its y halo is +1, so
-// its maps are encoded with those origins; the producer passes coordinates
-// through these two helpers.
-__device__ __forceinline__ void tma_produce_h(const TmaCta& t, const TMaps& tm, int p0, int p1, int edge, int* err) {
-    if (t.lane != 0) return;
-    int issued = 0;
-    bool ok = true;
-    for (int p = p0; p <= p1 && ok; ++p) {
-        const int pidx = p - p0, s = pidx % kStages, u = pidx / kStages;
-        if (u >= 1 && !mbar_wait(t.empty0 + 8 * s, (u - 1) & 1, err, 13)) { ok = false; break; }
-        const unsigned bar = t.full0 + 8 * s;
-        unsigned char* st = t.ring + s * kStageBytes;
-        const bool part = p == edge;
-        mbar_expect_tx(bar, part ? kTxEdge : kTxFull);
-        tma_load3(smem_u32(st + kOffA), &tm.m[0], t.ib, t.jb, p, bar);  // Ex rows jb..jb+8
-        tma_load3(smem_u32(st + kOffB), &tm.m[1], t.ib, t.jb, p, bar);  // Ey x ib..ib+35
-        if (!part) {
-            tma_load3(smem_u32(st + kOffC), &tm.m[2], t.ib, t.jb, p, bar);  // Ez x ib..ib+35, rows jb..jb+8
-            for (int q = 0; q < 3; ++q) tma_load3(smem_u32(st + kOffF + q * align128(kBoxF)), &tm.m[3 + q], t.ib, t.jb, p, bar);
-            for (int q = 0; q < 3; ++q) tma_load3(smem_u32(st + kOffM + q * align128(kBoxM)), &tm.m[6 + q], t.ib, t.jb, p, bar);
+// Nothing may be in flight into the CTA's shared memory when it exits: wait
+// (bounded) for the last loads of the `issued` planes numbered 0..issued-1.
+__device__ __forceinline__ void tma_drain(const TmaCta& t, unsigned issued, int* err, int code) {
+    const unsigned first = issued > (unsigned)kStages ? issued - kStages : 0;
+    for (unsigned G = first; G < issued; ++G) mbar_wait(t.full0 + 8 * (G % kStages), (G / kStages) & 1, err, code);
+}
+
+// Every lane waits on the barrier (each needs the acquire); the warp then
+// agrees on the outcome so all lanes leave together on a timeout.
+__device__ __forceinline__ bool warp_wait(unsigned bar, unsigned parity, int* err, int code) {
+    const bool ok = mbar_wait(bar, parity, err, code);
+    return __all_sync(0xffffffffu, ok);
+}
+
+__device__ __forceinline__ void warp_release(const TmaCta& t, unsigned G) {
+    __syncwarp();
+    if (t.lane == 0) mbar_arrive(t.empty0 + 8 * (G % kStages));
+}
+
+// Consumers of the E side: Advance_Ex/Ey/Ez + AdvanceelectricCPML from the
+// ring, the same per-cell arithmetic as efield_column.  The item's planes are
+// G0 (k = kb-1, edge) and G0+1+(k-kb).  Plane k-1 is released once plane k is
+// done; with `release_last` the item's last plane is released too (a
+// persistent CTA goes on to another item).  False on a timeout.
+template <bool CP>
+__device__ __forceinline__ bool e_consume(const TmaCta& t, unsigned G0, const KGrid& g, const KCpml& cp, const float* t1,
+                                          const float* t2, int* err, bool release_last) {
+    const int w = t.warp, l = t.lane;
+    const int i = t.ib + l, j = t.jb + w;
+    const int nya = (int)(g.plane / g.pitch);
+    const bool vx = col_in(g.sw[0], i, j), vy = col_in(g.sw[1], i, j), vz = col_in(g.sw[2], i, j);
+    const float idyh = g.idyh[min(j, nya - 1)], idxh = g.idxh[i];
+    const long long pitch = g.pitch, plane = g.plane;
+    const unsigned tmask = CP ? cpml_tile_mask(cp, 0, t.ib, t.ib + kTX - 1, t.jb, t.jb + kTY - 1) : 0u;
+    const CpmlCol cc = CP ? cpml_col(cp, 0, tmask, i, j) : CpmlCol{};
+    for (int k = t.kb; k <= t.ke; ++k) {
+        const unsigned Gk = G0 + 1 + (unsigned)(k - t.kb), Gp = Gk - 1;
+        const unsigned s = Gk % kStages, sp = Gp % kStages;
+        // slabs holding cell (i, j, k), and the P_b / P_c pair indexed by k
+        const unsigned pm = CP ? cpml_plane_mask(cp, 0, cc.col, k) : 0u;
+        float bz = 0.0f, cz = 0.0f;
+        if (CP && (pm & kCpmlZ)) {
+            bz = cp.pbe[2][k];
+            cz = cp.pce[2][k];
         }
-        ++issued;
+        if (k == t.kb && !warp_wait(t.full0 + 8 * sp, (Gp / kStages) & 1, err, 2)) return false;
+        if (!warp_wait(t.full0 + 8 * s, (Gk / kStages) & 1, err, 1)) return false;
+        const unsigned char* st = t.ring + s * kStageBytes;
+        const unsigned char* pv = t.ring + sp * kStageBytes;
+        const float* HX = (const float*)(st + kOffA);
+        const float* HY = (const float*)(st + kOffB);
+        const float* HZ = (const float*)(st + kOffC);
+        const float* HXp = (const float*)(pv + kOffA);
+        const float* HYp = (const float*)(pv + kOffB);
+        const float* EF = (const float*)(st + kOffF);
+        const int16_t* MF = (const int16_t*)(st + kOffM);
+        constexpr int fs = align128(kBoxF) / 4, ms = align128(kBoxM) / 2;
+        const float hx = HX[(w + 1) * kTX + l], hx_jm = HX[w * kTX + l], hx_km = HXp[(w + 1) * kTX + l];
+        const float hy = HY[w * kHaloW + l + 4], hy_im = HY[w * kHaloW + l + 3], hy_km = HYp[w * kHaloW + l + 4];
+        const float hz = HZ[(w + 1) * kHaloW + l + 4], hz_jm = HZ[w * kHaloW + l + 4], hz_im = HZ[(w + 1) * kHaloW + l + 3];
+        const float idzh = g.idzh[k];
+        const long long c = i + pitch * j + plane * k;
+        const int o = w * kTX + l;
+        bool st_ = true;
+        if (vx && k >= g.sw[0][4] && k <= g.sw[0][5]) {
+            float e = EF[o];
+            const int m = MF[o];
+            const float dy = hz - hz_jm, dz = hy - hy_km;
+            e = t1[m] * e + t2[m] * (dy * idyh - dz * idzh);
+            if (CP && pm) {
+                e = cpml_pair<true>(cp.s[0][0], pm & 3, i, j, k, cc.by, cc.cy, dy, t2[m], e, st_);
+                e = cpml_pair<false>(cp.s[0][1], (pm >> 2) & 3, i, j, k, bz, cz, dz, t2[m], e, st_);
+            }
+            g.F[0][c] = e;
+        }
+        if (vy && k >= g.sw[1][4] && k <= g.sw[1][5]) {
+            float e = EF[fs + o];
+            const int m = MF[ms + o];
+            const float dz = hx - hx_km, dx = hz - hz_im;
+            e = t1[m] * e + t2[m] * (dz * idzh - dx * idxh);
+            if (CP && pm) {
+                e = cpml_pair<true>(cp.s[1][0], (pm >> 4) & 3, i, j, k, bz, cz, dz, t2[m], e, st_);
+                e = cpml_pair<false>(cp.s[1][1], (pm >> 6) & 3, i, j, k, cc.bx, cc.cx, dx, t2[m], e, st_);
+            }
+            g.F[1][c] = e;
+        }
+        if (vz && k >= g.sw[2][4] && k <= g.sw[2][5]) {
+            float e = EF[2 * fs + o];
+            const int m = MF[2 * ms + o];
+            const float dx = hy - hy_im, dy = hx - hx_jm;
+            e = t1[m] * e + t2[m] * (dx * idxh - dy * idyh);
+            if (CP && pm) {
+                e = cpml_pair<false>(cp.s[2][0], (pm >> 8) & 3, i, j, k, cc.by, cc.cy, dy, t2[m], e, st_);
+                e = cpml_pair<true>(cp.s[2][1], (pm >> 10) & 3, i, j, k, cc.bx, cc.cx, dx, t2[m], e, st_);
+            }
+            g.F[2][c] = e;
+        }
+        warp_release(t, Gp);  // plane k-1 is no longer needed
     }
-    const int first = issued > kStages ? issued - kStages : 0;
-    for (int pidx = first; pidx < issued; ++pidx)
-        mbar_wait(t.full0 + 8 * (pidx % kStages), (pidx / kStages) & 1, err, 14);
+    if (release_last) warp_release(t, G0 + 1 + (unsigned)(t.ke - t.kb));
+    return true;
+}
+
+// Consumers of the H side: Advance_Hx/Hy/Hz + AdvanceMagneticCPML from the
+// ring (hfield_column's arithmetic).  The item's planes are G0+(k-kb) for
+// k = kb..ke+1 (ke+1 the edge); plane k is released once it is done.
+template <bool CP>
+__device__ __forceinline__ bool h_consume(const TmaCta& t, unsigned G0, const KGrid& g, const KCpml& cp, const float* t1,
+                                          const float* t2, int* err, bool release_last) {
+    const int w = t.warp, l = t.lane;
+    const int i = t.ib + l, j = t.jb + w;
+    const int nya = (int)(g.plane / g.pitch);
+    const bool vx = col_in(g.sw[3], i, j), vy = col_in(g.sw[4], i, j), vz = col_in(g.sw[5], i, j);
+    const float idye = g.idye[min(j, nya - 1)], idxe = g.idxe[i];
+    const long long pitch = g.pitch, plane = g.plane;
+    const unsigned tmask = CP ? cpml_tile_mask(cp, 3, t.ib, t.ib + kTX - 1, t.jb, t.jb + kTY - 1) : 0u;
+    const CpmlCol cc = CP ? cpml_col(cp, 3, tmask, i, j) : CpmlCol{};
+    for (int k = t.kb; k <= t.ke; ++k) {
+        const unsigned Gk = G0 + (unsigned)(k - t.kb), Gn = Gk + 1;
+        const unsigned s = Gk % kStages, sn = Gn % kStages;
+        // slabs holding cell (i, j, k), and the P_b / P_c pair indexed by k
+        const unsigned pm = CP ? cpml_plane_mask(cp, 3, cc.col, k) : 0u;
+        float bz = 0.0f, cz = 0.0f;
+        if (CP && (pm & kCpmlZ)) {
+            bz = cp.pbm[2][k];
+            cz = cp.pcm[2][k];
+        }
+        if (!warp_wait(t.full0 + 8 * s, (Gk / kStages) & 1, err, 3)) return false;
+        if (!warp_wait(t.full0 + 8 * sn, (Gn / kStages) & 1, err, 4)) return false;
+        const unsigned char* st = t.ring + s * kStageBytes;
+        const unsigned char* nx = t.ring + sn * kStageBytes;
+        const float* EX = (const float*)(st + kOffA);
+        const float* EY = (const float*)(st + kOffB);
+        const float* EZ = (const float*)(st + kOffC);
+        const float* EXn = (const float*)(nx + kOffA);
+        const float* EYn = (const float*)(nx + kOffB);
+        const float* HF = (const float*)(st + kOffF);
+        const int16_t* MF = (const int16_t*)(st + kOffM);
+        constexpr int fs = align128(kBoxF) / 4, ms = align128(kBoxM) / 2;
+        const float ex = EX[w * kTX + l], ex_jp = EX[(w + 1) * kTX + l], ex_kp = EXn[w * kTX + l];
+        const float ey = EY[w * kHaloW + l], ey_ip = EY[w * kHaloW + l + 1], ey_kp = EYn[w * kHaloW + l];
+        const float ez = EZ[w * kHaloW + l], ez_ip = EZ[w * kHaloW + l + 1], ez_jp = EZ[(w + 1) * kHaloW + l];
+        const float idze = g.idze[k];
+        const long long c = i + pitch * j + plane * k;
+        const int o = w * kTX + l;
+        bool st_ = true;
+        if (vx && k >= g.sw[3][4] && k <= g.sw[3][5]) {
+            float h = HF[o];
+            const int m = MF[o];
+            const float dz = ey_kp - ey, dy = ez_jp - ez;
+            h = t1[m] * h + t2[m] * (dz * idze - dy * idye);
+            if (CP && pm) {
+                h = cpml_pair<false>(cp.s[3][0], pm & 3, i, j, k, cc.by, cc.cy, dy, t2[m], h, st_);
+                h = cpml_pair<true>(cp.s[3][1], (pm >> 2) & 3, i, j, k, bz, cz, dz, t2[m], h, st_);
+            }
+            g.F[3][c] = h;
+        }
+        if (vy && k >= g.sw[4][4] && k <= g.sw[4][5]) {
+            float h = HF[fs + o];
+            const int m = MF[ms + o];
+            const float dx = ez_ip - ez, dz = ex_kp - ex;
+            h = t1[m] * h + t2[m] * (dx * idxe - dz * idze);
+            if (CP && pm) {
+                h = cpml_pair<false>(cp.s[4][0], (pm >> 4) & 3, i, j, k, bz, cz, dz, t2[m], h, st_);
+                h = cpml_pair<true>(cp.s[4][1], (pm >> 6) & 3, i, j, k, cc.bx, cc.cx, dx, t2[m], h, st_);
+            }
+            g.F[4][c] = h;
+        }
+        if (vz && k >= g.sw[5][4] && k <= g.sw[5][5]) {
+            float h = HF[2 * fs + o];
+            const int m = MF[2 * ms + o];
+            const float dy = ex_jp - ex, dx = ey_ip - ey;
+            h = t1[m] * h + t2[m] * (dy * idye - dx * idxe);
+            if (CP && pm) {
+                h = cpml_pair<true>(cp.s[5][0], (pm >> 8) & 3, i, j, k, cc.by, cc.cy, dy, t2[m], h, st_);
+                h = cpml_pair<false>(cp.s[5][1], (pm >> 10) & 3, i, j, k, cc.bx, cc.cx, dx, t2[m], h, st_);
+            }
+            g.F[5][c] = h;
+        }
+        warp_release(t, Gk);  // plane k is no longer needed
+    }
+    if (release_last) warp_release(t, G0 + 1 + (unsigned)(t.ke - t.kb));
+    return true;
 }
 
 }  // namespace sgpu
