@@ -321,6 +321,68 @@ sgpu_status sgpu_host_get_g(const sgpu_ctx* ctx, float* g1, float* g2, float* gm
 sgpu_status sgpu_host_get_metric(const sgpu_ctx* ctx, int which, float* out, int* lo, int* hi);
 sgpu_status sgpu_host_get_media(const sgpu_ctx* ctx, int comp, int16_t* out);
 
+/* ------------------------------------------------------------------------
+ * Batched form (no counterpart in the reference, which runs one problem per
+ * process).  Many independent problems of uneven sizes live in one device
+ * arena and advance together: every phase of a step is one persistent
+ * kernel over flattened work lists of all instances, and whole steps are
+ * replayed from a CUDA graph of 32 captured steps.  Each instance advances
+ * with the same per-cell arithmetic as sgpu_host_create, so its probe traces
+ * and fields are bit-identical to a solo run.  Instances join at step 0 when
+ * added (between calls that advance the batch) and stop after their last
+ * step while others go on; the batch's own step counter advances for all.
+ * ------------------------------------------------------------------------ */
+typedef struct sgpu_batch sgpu_batch;
+
+/* One arena of arena_bytes of device memory (one cudaMalloc) on the current
+ * device, room for max_instances instances. */
+sgpu_status sgpu_batch_create(uint64_t arena_bytes, int max_instances, sgpu_batch** out);
+void sgpu_batch_destroy(sgpu_batch* b);
+const char* sgpu_batch_last_error(const sgpu_batch* b);
+/* Set up a problem inside the arena: from `p`, or from `plan` (a host-only
+ * context of sgpu_host_plan, consumed: destroy it afterwards as usual).  The
+ * instance runs steps 0..nsteps and keeps every probe row on the device.
+ * SGPU_ERR_OOM when the arena has no room (nothing is left allocated). */
+sgpu_status sgpu_batch_add(sgpu_batch* b, const sgpu_problem* p, sgpu_ctx* plan, int nsteps, int* slot);
+/* Free an instance's arena memory and slot (waits for queued work). */
+sgpu_status sgpu_batch_remove(sgpu_batch* b, int slot);
+/* Queue nsteps batch steps (graph replays of 32, the rest one by one). */
+sgpu_status sgpu_batch_advance(sgpu_batch* b, int nsteps);
+/* Wait for queued work; SGPU_ERR_TIMEOUT if a bounded wait ran out. */
+sgpu_status sgpu_batch_synchronize(sgpu_batch* b);
+/* sgpu_batch_advance timed on the device with CUDA events (waits). */
+sgpu_status sgpu_batch_elapsed(sgpu_batch* b, int nsteps, float* ms);
+/* Steps an instance has completed (queued work counted) and its total. */
+sgpu_status sgpu_batch_slot_info(const sgpu_batch* b, int slot, int* steps_done, int* steps_total, int* nprobes);
+/* Probe rows 0..rows-1 of an instance ([step][probe] floats; waits). */
+sgpu_status sgpu_batch_read_probes(sgpu_batch* b, int slot, float* out, int max_rows, int* rows);
+/* The instance's context, for sgpu_download_field and the like (waits). */
+sgpu_status sgpu_batch_instance(sgpu_batch* b, int slot, sgpu_ctx** ctx);
+/* Arena capacity, bytes in use and the largest free block. */
+sgpu_status sgpu_batch_memory(sgpu_batch* b, uint64_t* capacity, uint64_t* in_use, uint64_t* largest_free);
+/* Device bytes one instance of this plan takes in a batch arena (every
+ * buffer rounded to the arena's 256-byte grain, whole probe traces), and
+ * its largest single buffer. */
+sgpu_status sgpu_batch_footprint(const sgpu_ctx* plan, uint64_t* bytes, uint64_t* largest);
+/* Field kernels of the batch: 1 (default) the persistent TMA-pipelined
+ * kernels (each instance's tensor maps in global memory), 0 the
+ * register-marching kernels.  Both give identical results. */
+sgpu_status sgpu_batch_set_kernel_family(sgpu_batch* b, int family);
+/* Launch shape: z-chunk length of the field work items for the three size
+ * classes (Alloc z extent <= 80, <= 160, larger) and persistent CTAs per SM.
+ * Either may be NULL / 0 to keep the current value. */
+sgpu_status sgpu_batch_set_tuning(sgpu_batch* b, const int* chunk3, int ctas_per_sm);
+sgpu_status sgpu_batch_get_tuning(const sgpu_batch* b, int* chunk3, int* ctas_per_sm);
+/* Online autotuner: times steps_per_trial real steps of the live instances
+ * per candidate (CTAs per SM in 2,3,4,6, then z chunk 4..64 per size class
+ * present) and keeps the fastest.  The trials advance the instances. */
+sgpu_status sgpu_batch_autotune(sgpu_batch* b, int steps_per_trial, int* chunk3, int* ctas_per_sm);
+/* Device time of each phase summed over nsteps real steps launched one by
+ * one: E field + CPML, ADE, E sources, H field + CPML, H sources, probes. */
+sgpu_status sgpu_batch_profile_steps(sgpu_batch* b, int nsteps, float* ms6);
+/* The batch step counter (steps queued so far). */
+sgpu_status sgpu_batch_steps(const sgpu_batch* b, int* counter);
+
 #ifdef __cplusplus
 }
 #endif

@@ -124,6 +124,25 @@ def _declare(lib: C.CDLL) -> None:
         "sgpu_host_get_g": ([vp, c_float_p, c_float_p, c_float_p, c_float_p], C.c_int),
         "sgpu_host_get_metric": ([vp, C.c_int, c_float_p, c_int_p, c_int_p], C.c_int),
         "sgpu_host_get_media": ([vp, C.c_int, C.POINTER(C.c_int16)], C.c_int),
+        "sgpu_batch_create": ([C.c_uint64, C.c_int, C.POINTER(vp)], C.c_int),
+        "sgpu_batch_destroy": ([vp], None),
+        "sgpu_batch_last_error": ([vp], C.c_char_p),
+        "sgpu_batch_add": ([vp, C.POINTER(ProblemDesc), vp, C.c_int, c_int_p], C.c_int),
+        "sgpu_batch_remove": ([vp, C.c_int], C.c_int),
+        "sgpu_batch_advance": ([vp, C.c_int], C.c_int),
+        "sgpu_batch_synchronize": ([vp], C.c_int),
+        "sgpu_batch_elapsed": ([vp, C.c_int, c_float_p], C.c_int),
+        "sgpu_batch_slot_info": ([vp, C.c_int, c_int_p, c_int_p, c_int_p], C.c_int),
+        "sgpu_batch_read_probes": ([vp, C.c_int, c_float_p, C.c_int, c_int_p], C.c_int),
+        "sgpu_batch_instance": ([vp, C.c_int, C.POINTER(vp)], C.c_int),
+        "sgpu_batch_memory": ([vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)], C.c_int),
+        "sgpu_batch_footprint": ([vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)], C.c_int),
+        "sgpu_batch_set_kernel_family": ([vp, C.c_int], C.c_int),
+        "sgpu_batch_set_tuning": ([vp, c_int_p, C.c_int], C.c_int),
+        "sgpu_batch_get_tuning": ([vp, c_int_p, c_int_p], C.c_int),
+        "sgpu_batch_autotune": ([vp, C.c_int, c_int_p, c_int_p], C.c_int),
+        "sgpu_batch_profile_steps": ([vp, C.c_int, c_float_p], C.c_int),
+        "sgpu_batch_steps": ([vp, c_int_p], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)

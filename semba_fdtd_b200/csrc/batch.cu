@@ -1,0 +1,931 @@
+// Batched form: many independent FDTD problems of uneven sizes advanced
+// together on one GPU.
+//
+// * Every instance is an ordinary context (the same device layout and
+//   set-up as a single problem) whose buffers are carved out of one device
+//   arena (first fit, 256-byte aligned, coalescing free list).
+// * A descriptor table on the device holds each instance's grid, CPML, ADE,
+//   source and probe views plus its step offset; flattened work lists hold
+//   (instance, tile, z chunk) items for the field kernels and node / row /
+//   probe ranges for the other phases.
+// * One persistent kernel per phase walks its work list; an instance's step
+//   index is the batch's device step counter plus the instance's offset, and
+//   an instance outside 0..last step does nothing.  So instances can join at
+//   any chunk boundary and finish at any step while the graph of 32 captured
+//   steps stays valid: changing the batch only rewrites the tables.
+// * The per-cell arithmetic is the single-problem code (stencil.cuh,
+//   tma_fields.cuh), so an instance gives the same bits alone, in any mix
+//   and on the plain path.
+// * The z-chunk length of the field work items is chosen per size class and
+//   the persistent grid size per batch by an online autotuner that times real
+//   steps (results do not depend on either choice).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <map>
+#include <mutex>
+#include <new>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "sgpu_internal.h"
+#include "stencil.cuh"
+#include "tma_fields.cuh"
+
+using namespace sgpu;
+using namespace sgpu::dev;
+
+// ---------------------------------------------------------------------------
+// Arena
+
+struct sgpu::Arena {
+    char* base = nullptr;
+    size_t cap = 0;
+    size_t in_use = 0;
+    std::map<size_t, size_t> free_;            // offset -> size, address ordered
+    std::unordered_map<size_t, size_t> used_;  // offset -> size
+    std::mutex mu;
+};
+
+namespace sgpu {
+namespace {
+constexpr size_t kArenaAlign = 256;
+}
+}  // namespace sgpu
+
+void* sgpu::arena_alloc(Arena* a, size_t bytes) {
+    if (!a || bytes == 0) return nullptr;
+    const size_t need = (bytes + kArenaAlign - 1) / kArenaAlign * kArenaAlign;
+    std::lock_guard<std::mutex> lock(a->mu);
+    for (auto it = a->free_.begin(); it != a->free_.end(); ++it) {
+        if (it->second < need) continue;
+        const size_t off = it->first, rest = it->second - need;
+        a->free_.erase(it);
+        if (rest) a->free_[off + need] = rest;
+        a->used_[off] = need;
+        a->in_use += need;
+        return a->base + off;
+    }
+    return nullptr;
+}
+
+void sgpu::arena_free(Arena* a, void* p) {
+    if (!a || !p) return;
+    std::lock_guard<std::mutex> lock(a->mu);
+    const size_t off = (size_t)((char*)p - a->base);
+    auto u = a->used_.find(off);
+    if (u == a->used_.end()) return;
+    size_t start = off, size = u->second;
+    a->in_use -= size;
+    a->used_.erase(u);
+    auto next = a->free_.lower_bound(start);
+    if (next != a->free_.end() && next->first == start + size) {
+        size += next->second;
+        next = a->free_.erase(next);
+    }
+    if (next != a->free_.begin()) {
+        auto prev = std::prev(next);
+        if (prev->first + prev->second == start) {
+            start = prev->first;
+            size += prev->second;
+            a->free_.erase(prev);
+        }
+    }
+    a->free_[start] = size;
+}
+
+namespace sgpu {
+namespace {
+
+size_t arena_largest(Arena* a) {
+    std::lock_guard<std::mutex> lock(a->mu);
+    size_t m = 0;
+    for (auto& f : a->free_) m = std::max(m, f.second);
+    return m;
+}
+
+// ---------------------------------------------------------------------------
+// Device tables
+
+struct InstDesc {
+    KGrid g;
+    KCpml cp;
+    KDisp d;
+    KSrc src[2];
+    KProbes pr;
+    const double* tiempo;
+    double dt;
+    int step_off;  // instance step n = batch counter + step_off
+    int last_n;    // steps 0..last_n are advanced; -1: inactive slot
+};
+
+struct FieldItem {
+    int slot, ib, jb, kb, ke, cp;
+};
+struct RangeItem {
+    int slot, sub;     // sub: E component (ADE) or side (sources)
+    long long q0, q1;  // node / row / probe range
+};
+
+enum : int { kCntE = 0, kCntH, kCntNode, kCntSrcE, kCntSrcH, kCntProbe, kNumCounts };
+
+constexpr int kNodeChunk = 2048;  // ADE nodes per work item
+constexpr int kRowChunk = 128;    // source rows / probes per work item
+constexpr int kPhaseThreads = 256;
+
+__device__ __forceinline__ int inst_step(const InstDesc& D, const int* G, bool* on) {
+    const int n = *G + D.step_off;
+    *on = n >= 0 && n <= D.last_n;
+    return n;
+}
+
+// Per-warp copy of an instance's grid (and CPML) view into shared memory:
+// the field kernels then read slab bounds, pointers and sweep limits with
+// shared loads instead of global ones, and no warp waits for another.
+struct WarpView {
+    KGrid g;
+    KCpml cp;
+};
+template <class T> __device__ __forceinline__ void warp_copy(T* dst, const T* src, int lane) {
+    static_assert(sizeof(T) % 4 == 0, "word copy");
+    const int* s = (const int*)src;
+    int* d = (int*)dst;
+    for (int q = lane; q < (int)(sizeof(T) / 4); q += 32) d[q] = s[q];
+}
+__device__ __forceinline__ const WarpView& stage_view(WarpView* slot, const InstDesc& D, bool cpml, int lane) {
+    __syncwarp();  // the warp is done with the previous item's view
+    warp_copy(&slot->g, &D.g, lane);
+    if (cpml) warp_copy(&slot->cp, &D.cp, lane);
+    __syncwarp();
+    return *slot;
+}
+
+// Advance_Ex/Ey/Ez + AdvanceelectricCPML (SIDE 0) or Advance_Hx/Hy/Hz +
+// AdvanceMagneticCPML (SIDE 1) over every active instance's tiles, with the
+// register-marching columns.
+template <int SIDE>
+__global__ void __launch_bounds__(kBX * kBY, 4)
+    k_batch_field(const InstDesc* __restrict__ descs, const FieldItem* __restrict__ items, const int* counts, const int* G) {
+    __shared__ WarpView views[kBY];
+    const int n_items = counts[SIDE == 0 ? kCntE : kCntH];
+    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+        const FieldItem w = items[it];
+        const InstDesc& D = descs[w.slot];
+        bool on;
+        inst_step(D, G, &on);
+        if (!on) continue;
+        const WarpView& V = stage_view(&views[threadIdx.y], D, w.cp != 0, threadIdx.x);
+        const KGrid& g = V.g;
+        const int i = w.ib + threadIdx.x, j = w.jb + threadIdx.y;
+        const int jc = min(max(j, 1), (int)(g.plane / g.pitch) - 2);
+        constexpr int MODE = kBulk | kCpml | kAll;
+        if (SIDE == 0) {
+            const bool vx = col_in(g.sw[0], i, j), vy = col_in(g.sw[1], i, j), vz = col_in(g.sw[2], i, j);
+            if (w.cp) efield_column<MODE, true>(g, V.cp, g.g1, g.g2, i, jc, w.kb, w.ke, vx, vy, vz);
+            else efield_column<MODE, false>(g, V.cp, g.g1, g.g2, i, jc, w.kb, w.ke, vx, vy, vz);
+        } else {
+            const bool vx = col_in(g.sw[3], i, j), vy = col_in(g.sw[4], i, j), vz = col_in(g.sw[5], i, j);
+            if (w.cp) hfield_column<MODE, true>(g, V.cp, g.gm1, g.gm2, i, jc, w.kb, w.ke, vx, vy, vz);
+            else hfield_column<MODE, false>(g, V.cp, g.gm1, g.gm2, i, jc, w.kb, w.ke, vx, vy, vz);
+        }
+    }
+}
+
+// The same half steps through the TMA ring (tma_fields.cuh) as one
+// persistent kernel: each CTA walks its work items in order and the ring's
+// running plane number carries on from item to item, so the producer warp
+// fetches the next item's planes while the consumers finish the current one.
+// Each instance's tensor maps live in global memory (written by the host
+// before the launch) and are acquired through the tensormap proxy before
+// their first use in the CTA.
+__device__ __forceinline__ void tensormap_acquire(const CUtensorMap* m) {
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"((unsigned long long)m) : "memory");
+}
+
+template <int SIDE>
+__global__ void __launch_bounds__(kTmaThreads, 3)
+    k_batch_tma_field(const InstDesc* __restrict__ descs, const TMaps* __restrict__ maps, const FieldItem* __restrict__ items,
+                      const int* counts, const int* G, int* err) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ WarpView views[kConsumerWarps];
+    TmaCta t = tma_cta_setup(smem, 0, 0, 0, 1);
+    const int n_items = counts[SIDE == 0 ? kCntE : kCntH];
+    const bool producer = t.warp == kConsumerWarps;
+    unsigned gp = 0;  // running plane number of the ring
+    int fenced = -1;
+    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+        const FieldItem w = items[it];
+        const InstDesc& D = descs[w.slot];
+        bool on;
+        inst_step(D, G, &on);
+        if (!on) continue;
+        t.ib = w.ib;
+        t.jb = w.jb;
+        t.kb = w.kb;
+        t.ke = w.ke;
+        const int np = w.ke - w.kb + 2;  // the item's planes, edge plane included
+        if (producer) {
+            if (t.lane == 0) {
+                const CUtensorMap* m = maps[2 * w.slot + SIDE].m;
+                if (fenced != w.slot) {
+                    for (int q = 0; q < 9; ++q) tensormap_acquire(&m[q]);
+                    fenced = w.slot;
+                }
+                const int got = SIDE == 0 ? tma_issue(t, m, gp, w.kb - 1, w.ke, w.kb - 1, false, err)
+                                          : tma_issue(t, m, gp, w.kb, w.ke + 1, w.ke + 1, true, err);
+                if (got < np) {
+                    tma_drain(t, gp + (unsigned)got, err, 15);
+                    return;
+                }
+            }
+        } else {
+            const WarpView& V = stage_view(&views[t.warp], D, w.cp != 0, t.lane);
+            const KGrid& g = V.g;
+            bool ok;
+            if (SIDE == 0)
+                ok = w.cp ? e_consume<true>(t, gp, g, V.cp, g.g1, g.g2, err, true)
+                          : e_consume<false>(t, gp, g, V.cp, g.g1, g.g2, err, true);
+            else
+                ok = w.cp ? h_consume<true>(t, gp, g, V.cp, g.gm1, g.gm2, err, true)
+                          : h_consume<false>(t, gp, g, V.cp, g.gm1, g.gm2, err, true);
+            if (!ok) return;
+        }
+        gp += (unsigned)np;
+    }
+    if (producer && t.lane == 0) tma_drain(t, gp, err, 15);
+}
+
+// AdvanceEDispersiveE over node ranges of every active instance.
+template <int NU>
+__global__ void __launch_bounds__(kPhaseThreads)
+    k_batch_edisp(const InstDesc* __restrict__ descs, const RangeItem* __restrict__ items, const int* counts, const int* G) {
+    const int n_items = counts[kCntNode];
+    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+        const RangeItem w = items[it];
+        const InstDesc& D = descs[w.slot];
+        bool on;
+        inst_step(D, G, &on);
+        if (!on) continue;
+        for (long long q = w.q0 + threadIdx.x; q < w.q1; q += blockDim.x) edisp_node<NU>(D.g, D.d, w.sub, q);
+    }
+}
+
+// Plane-wave and nodal sources of one half step.
+__global__ void __launch_bounds__(kPhaseThreads)
+    k_batch_sources(const InstDesc* __restrict__ descs, const RangeItem* __restrict__ items, const int* counts, const int* G,
+                    int side) {
+    const int n_items = counts[side == 0 ? kCntSrcE : kCntSrcH];
+    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+        const RangeItem w = items[it];
+        const InstDesc& D = descs[w.slot];
+        bool on;
+        const int n = inst_step(D, G, &on);
+        if (!on) continue;
+        const long long r = w.q0 + threadIdx.x;
+        if (r < w.q1)
+            source_row(D.g, D.src[side], n, D.tiempo, 0, D.dt, side,
+                       (1 << kSrcPlaneWave) | (1 << kSrcNodalSoft) | (1 << kSrcNodalHard), (int)r);
+    }
+}
+
+// Point probes, one row per step of each instance (the whole trace stays on
+// the device).
+__global__ void __launch_bounds__(kPhaseThreads)
+    k_batch_probes(const InstDesc* __restrict__ descs, const RangeItem* __restrict__ items, const int* counts, const int* G) {
+    const int n_items = counts[kCntProbe];
+    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+        const RangeItem w = items[it];
+        const InstDesc& D = descs[w.slot];
+        bool on;
+        const int n = inst_step(D, G, &on);
+        if (!on) continue;
+        const long long q = w.q0 + threadIdx.x;
+        if (q < w.q1) probe_one(D.g, D.pr, n, 0, (int)q);
+    }
+}
+
+// The batch counter moves on by one step.
+__global__ void k_batch_tick(int* G) { *G += 1; }
+
+struct Slot {
+    sgpu_ctx* ctx = nullptr;
+    int start = 0;   // batch counter value at the instance's step 0
+    int nsteps = 0;  // last step index advanced (steps 0..nsteps)
+    int size_class = 0;
+};
+
+bool touches_any(const KCpml& cp, int c0, int x0, int x1, int y0, int y1, int z0, int z1) {
+    if (!cp.on) return false;
+    for (int f = c0; f < c0 + 3; ++f)
+        for (int w = 0; w < 2; ++w)
+            for (int sd = 0; sd < 2; ++sd) {
+                const Slab& s = cp.s[f][w][sd];
+                if (s.psi && x1 >= s.xlo && x0 <= s.xhi && y1 >= s.ylo && y0 <= s.yhi && z1 >= s.zlo && z0 <= s.zhi)
+                    return true;
+            }
+    return false;
+}
+
+}  // namespace
+}  // namespace sgpu
+
+constexpr int kNumClasses = 3;
+
+struct sgpu_batch {
+    std::string err;
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    sgpu::Arena arena;
+    int max_slots = 0;
+    std::vector<Slot> slots;
+    // device tables (plain cudaMalloc: they outlive every instance)
+    InstDesc* d_desc = nullptr;
+    TMaps* d_maps = nullptr;  // [slot][E side, H side]
+    int* d_err = nullptr;     // bounded-wait error word of the TMA kernels
+    int* d_counts = nullptr;
+    int* d_G = nullptr;
+    FieldItem* d_field[2] = {};
+    RangeItem* d_node = nullptr;
+    RangeItem* d_src[2] = {};
+    RangeItem* d_probe = nullptr;
+    size_t cap_field[2] = {}, cap_node = 0, cap_src[2] = {}, cap_probe = 0;
+    int family = 1;  // 1: TMA-pipelined field kernels, 0: register-marching
+    std::vector<char> has_maps;
+    bool dirty = true;         // work lists must be rebuilt before the next step
+    std::vector<char> listed;  // slots whose work is in the current lists
+    int G = 0;                 // host mirror of the device step counter
+    int nu_max = 1;
+    // launch shape
+    int chunk[kNumClasses] = {16, 16, 32};
+    int ctas_per_sm = 4;
+    // graph of kGraphSteps steps
+    cudaGraphExec_t graph = nullptr;
+    int graph_nu = 0, graph_ctas = 0;
+    bool graph_tma = false;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace sgpu {
+namespace {
+
+constexpr int kGraphSteps = 32;
+
+sgpu_status berr(sgpu_batch* b, sgpu_status code, const std::string& msg) {
+    if (b) b->err = msg;
+    return code;
+}
+
+#define BTRY(b, call)                                                                                           \
+    do {                                                                                                        \
+        cudaError_t e_ = (call);                                                                                \
+        if (e_ != cudaSuccess) return berr((b), SGPU_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+int size_class_of(const sgpu_ctx* c) { return c->nza <= 80 ? 0 : c->nza <= 160 ? 1 : 2; }
+
+InstDesc make_desc(const Slot& s, bool active) {
+    InstDesc D{};
+    sgpu_ctx* c = s.ctx;
+    D.g = kgrid(c);
+    D.cp = c->cpml;
+    D.d = c->disp;
+    if (!c->disp_on) D.d.n[0] = D.d.n[1] = D.d.n[2] = 0;
+    D.src[0] = c->src[0];
+    D.src[1] = c->src[1];
+    D.pr = c->probes;
+    D.tiempo = c->d_tiempo;
+    D.dt = c->dt;
+    D.step_off = -s.start;
+    D.last_n = active ? s.nsteps : -1;
+    return D;
+}
+
+template <class T> sgpu_status ensure(sgpu_batch* b, T** p, size_t* cap, size_t n) {
+    if (n <= *cap && *p) return SGPU_OK;
+    size_t want = std::max<size_t>(std::max<size_t>(n, 2 * *cap), 256);
+    T* q = nullptr;
+    BTRY(b, cudaStreamSynchronize(b->stream));
+    BTRY(b, cudaMalloc((void**)&q, want * sizeof(T)));
+    if (*p) cudaFree(*p);
+    *p = q;
+    *cap = want;
+    if (b->graph) {  // a captured graph holds the old pointer
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    return SGPU_OK;
+}
+
+template <class T> sgpu_status upload(sgpu_batch* b, T* d, const std::vector<T>& h) {
+    if (h.empty()) return SGPU_OK;
+    BTRY(b, cudaMemcpyAsync(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, b->stream));
+    return SGPU_OK;
+}
+
+// An instance still has steps to run at the batch counter value G.
+bool running(const Slot& s, int G) { return s.ctx && G - s.start <= s.nsteps; }
+
+// Rebuild the flattened work lists from the instances that still run.
+sgpu_status rebuild(sgpu_batch* b) {
+    std::vector<FieldItem> fi[2];
+    std::vector<RangeItem> node, src[2], probe;
+    int nu = 1;
+    b->listed.assign(b->slots.size(), 0);
+    for (int sl = 0; sl < (int)b->slots.size(); ++sl) {
+        const Slot& s = b->slots[sl];
+        if (!running(s, b->G)) continue;
+        b->listed[sl] = 1;
+        sgpu_ctx* c = s.ctx;
+        const int chunk = b->chunk[s.size_class];
+        for (int side = 0; side < 2; ++side) {
+            const int c0 = side ? 3 : 0;
+            int x1 = -1, y0 = 1 << 30, y1 = -1, z0 = 1 << 30, z1 = -1;
+            for (int f = c0; f < c0 + 3; ++f) {
+                x1 = std::max(x1, c->sweep[f].xe - c->ox);
+                y0 = std::min(y0, c->sweep[f].yi - c->oy);
+                y1 = std::max(y1, c->sweep[f].ye - c->oy);
+                z0 = std::min(z0, c->sweep[f].zi - c->oz);
+                z1 = std::max(z1, c->sweep[f].ze - c->oz);
+            }
+            for (int kb = z0; kb <= z1; kb += chunk) {
+                const int ke = std::min(kb + chunk - 1, z1);
+                for (int jb = y0; jb <= y1; jb += kBY)
+                    for (int ib = 0; ib <= x1; ib += kBX)
+                        fi[side].push_back(FieldItem{sl, ib, jb, kb, ke,
+                                                     touches_any(c->cpml, c0, ib, ib + kBX - 1, jb, jb + kBY - 1, kb, ke) ? 1 : 0});
+            }
+        }
+        if (c->disp_on) {
+            nu = std::max(nu, c->disp.nu_max);
+            for (int comp = 0; comp < 3; ++comp)
+                for (long long q = 0; q < c->disp.n[comp]; q += kNodeChunk)
+                    node.push_back(RangeItem{sl, comp, q, std::min<long long>(q + kNodeChunk, c->disp.n[comp])});
+        }
+        for (int side = 0; side < 2; ++side)
+            for (long long r = 0; r < c->src[side].nrows; r += kRowChunk)
+                src[side].push_back(RangeItem{sl, side, r, std::min<long long>(r + kRowChunk, c->src[side].nrows)});
+        for (long long q = 0; q < c->probes.n; q += kRowChunk)
+            probe.push_back(RangeItem{sl, 0, q, std::min<long long>(q + kRowChunk, c->probes.n)});
+    }
+    sgpu_status s;
+    for (int side = 0; side < 2; ++side) {
+        if ((s = ensure(b, &b->d_field[side], &b->cap_field[side], fi[side].size()))) return s;
+        if ((s = ensure(b, &b->d_src[side], &b->cap_src[side], src[side].size()))) return s;
+    }
+    if ((s = ensure(b, &b->d_node, &b->cap_node, node.size())) || (s = ensure(b, &b->d_probe, &b->cap_probe, probe.size())))
+        return s;
+    if ((s = upload(b, b->d_field[0], fi[0])) || (s = upload(b, b->d_field[1], fi[1])) || (s = upload(b, b->d_node, node)) ||
+        (s = upload(b, b->d_src[0], src[0])) || (s = upload(b, b->d_src[1], src[1])) || (s = upload(b, b->d_probe, probe)))
+        return s;
+    std::vector<int> counts(kNumCounts);
+    counts[kCntE] = (int)fi[0].size();
+    counts[kCntH] = (int)fi[1].size();
+    counts[kCntNode] = (int)node.size();
+    counts[kCntSrcE] = (int)src[0].size();
+    counts[kCntSrcH] = (int)src[1].size();
+    counts[kCntProbe] = (int)probe.size();
+    if ((s = upload(b, b->d_counts, counts))) return s;
+    if (nu > b->nu_max) b->nu_max = nu;
+    // the copies read the host vectors; wait before they go out of scope
+    BTRY(b, cudaStreamSynchronize(b->stream));
+    b->dirty = false;
+    return SGPU_OK;
+}
+
+// Finished instances leave the work lists at the next chunk boundary (their
+// memory and results stay until sgpu_batch_remove).
+void drop_finished(sgpu_batch* b) {
+    if (b->listed.size() != b->slots.size()) {
+        b->dirty = true;
+        return;
+    }
+    for (size_t sl = 0; sl < b->slots.size(); ++sl)
+        if (b->listed[sl] && !running(b->slots[sl], b->G)) {
+            b->dirty = true;
+            return;
+        }
+}
+
+// The TMA kernels serve the batch when every listed instance has tensor maps.
+bool use_tma(const sgpu_batch* b) {
+    if (b->family != 1) return false;
+    for (size_t sl = 0; sl < b->listed.size(); ++sl)
+        if (b->listed[sl] && !b->has_maps[sl]) return false;
+    return true;
+}
+
+template <int NU> void edisp_batch(sgpu_batch* b, int grid) {
+    k_batch_edisp<NU><<<grid, kPhaseThreads, 0, b->stream>>>(b->d_desc, b->d_node, b->d_counts, b->d_G);
+}
+
+// One whole step of every instance in the order of timestepping.F90 (E curl +
+// CPML, ADE, E sources, H curl + CPML, H sources, probes).  With `marks`, an
+// event is recorded after each of the six phases.
+sgpu_status enqueue_step(sgpu_batch* b, cudaEvent_t* marks = nullptr) {
+    const int grid = b->num_sms * b->ctas_per_sm;
+    const int tgrid = b->num_sms * std::min(b->ctas_per_sm, 3);
+    const dim3 blk(kBX, kBY);
+    const bool tma = use_tma(b);
+    auto mark = [&](int q) {
+        if (marks) cudaEventRecord(marks[q], b->stream);
+    };
+    if (tma)
+        k_batch_tma_field<0><<<tgrid, kTmaThreads, kTmaSmem, b->stream>>>(b->d_desc, b->d_maps, b->d_field[0], b->d_counts,
+                                                                          b->d_G, b->d_err);
+    else
+        k_batch_field<0><<<grid, blk, 0, b->stream>>>(b->d_desc, b->d_field[0], b->d_counts, b->d_G);
+    mark(0);
+    switch (b->nu_max) {
+        case 1: edisp_batch<1>(b, grid); break;
+        case 2: edisp_batch<2>(b, grid); break;
+        case 3: edisp_batch<3>(b, grid); break;
+        case 4: edisp_batch<4>(b, grid); break;
+        default: edisp_batch<kMaxPolesPerMedium>(b, grid); break;
+    }
+    mark(1);
+    k_batch_sources<<<grid, kPhaseThreads, 0, b->stream>>>(b->d_desc, b->d_src[0], b->d_counts, b->d_G, 0);
+    mark(2);
+    if (tma)
+        k_batch_tma_field<1><<<tgrid, kTmaThreads, kTmaSmem, b->stream>>>(b->d_desc, b->d_maps, b->d_field[1], b->d_counts,
+                                                                          b->d_G, b->d_err);
+    else
+        k_batch_field<1><<<grid, blk, 0, b->stream>>>(b->d_desc, b->d_field[1], b->d_counts, b->d_G);
+    mark(3);
+    k_batch_sources<<<grid, kPhaseThreads, 0, b->stream>>>(b->d_desc, b->d_src[1], b->d_counts, b->d_G, 1);
+    mark(4);
+    k_batch_probes<<<grid, kPhaseThreads, 0, b->stream>>>(b->d_desc, b->d_probe, b->d_counts, b->d_G);
+    k_batch_tick<<<1, 1, 0, b->stream>>>(b->d_G);
+    mark(5);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return berr(b, SGPU_ERR_CUDA, std::string("batched step launch: ") + cudaGetErrorString(e));
+    return SGPU_OK;
+}
+
+sgpu_status ensure_graph(sgpu_batch* b) {
+    if (b->graph && b->graph_nu == b->nu_max && b->graph_ctas == b->ctas_per_sm && b->graph_tma == use_tma(b)) return SGPU_OK;
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    BTRY(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    sgpu_status s = SGPU_OK;
+    for (int q = 0; q < kGraphSteps && !s; ++q) s = enqueue_step(b);
+    cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    if (s) {
+        if (g) cudaGraphDestroy(g);
+        return s;
+    }
+    if (e != cudaSuccess) return berr(b, SGPU_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        b->graph = nullptr;
+        return berr(b, SGPU_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    }
+    b->graph_nu = b->nu_max;
+    b->graph_ctas = b->ctas_per_sm;
+    b->graph_tma = use_tma(b);
+    return SGPU_OK;
+}
+
+sgpu_status advance(sgpu_batch* b, int nsteps, bool use_graph) {
+    sgpu_status s;
+    drop_finished(b);
+    if (b->dirty && (s = rebuild(b))) return s;
+    int done = 0;
+    if (use_graph && nsteps >= kGraphSteps) {
+        if ((s = ensure_graph(b))) return s;
+        for (; done + kGraphSteps <= nsteps; done += kGraphSteps) BTRY(b, cudaGraphLaunch(b->graph, b->stream));
+    }
+    for (; done < nsteps; ++done)
+        if ((s = enqueue_step(b))) return s;
+    b->G += nsteps;
+    return SGPU_OK;
+}
+
+// The TMA kernels record an expired bounded wait in d_err.
+sgpu_status check_err(sgpu_batch* b) {
+    int e = 0;
+    BTRY(b, cudaMemcpy(&e, b->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) {
+        BTRY(b, cudaMemset(b->d_err, 0, sizeof(int)));
+        return berr(b, SGPU_ERR_TIMEOUT, "a bounded wait in a pipelined batch kernel expired (code " + std::to_string(e) + ")");
+    }
+    return SGPU_OK;
+}
+
+bool valid_slot(const sgpu_batch* b, int slot) {
+    return b && slot >= 0 && slot < (int)b->slots.size() && b->slots[slot].ctx;
+}
+
+}  // namespace
+}  // namespace sgpu
+
+extern "C" {
+
+sgpu_status sgpu_batch_create(uint64_t arena_bytes, int max_instances, sgpu_batch** out) {
+    if (!out || arena_bytes == 0 || max_instances < 1) return SGPU_ERR_ARG;
+    *out = nullptr;
+    sgpu_batch* b = new (std::nothrow) sgpu_batch();
+    if (!b) return SGPU_ERR_OOM;
+    *out = b;
+    BTRY(b, cudaGetDevice(&b->device));
+    cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, b->device);
+    BTRY(b, cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    void* base = nullptr;
+    if (cudaMalloc(&base, arena_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return berr(b, SGPU_ERR_OOM, "arena of " + std::to_string(arena_bytes) + " bytes could not be allocated");
+    }
+    b->arena.base = (char*)base;
+    b->arena.cap = arena_bytes / kArenaAlign * kArenaAlign;
+    b->arena.free_[0] = b->arena.cap;
+    b->max_slots = max_instances;
+    b->slots.resize(max_instances);
+    b->has_maps.assign(max_instances, 0);
+    BTRY(b, cudaMalloc((void**)&b->d_desc, sizeof(InstDesc) * max_instances));
+    BTRY(b, cudaMalloc((void**)&b->d_maps, sizeof(TMaps) * 2 * max_instances));
+    BTRY(b, cudaMalloc((void**)&b->d_err, sizeof(int)));
+    BTRY(b, cudaMalloc((void**)&b->d_counts, sizeof(int) * kNumCounts));
+    BTRY(b, cudaMalloc((void**)&b->d_G, sizeof(int)));
+    BTRY(b, cudaMemsetAsync(b->d_err, 0, sizeof(int), b->stream));
+    BTRY(b, cudaMemsetAsync(b->d_counts, 0, sizeof(int) * kNumCounts, b->stream));
+    BTRY(b, cudaMemsetAsync(b->d_G, 0, sizeof(int), b->stream));
+    std::vector<InstDesc> off(max_instances);
+    for (auto& d : off) d.last_n = -1;
+    BTRY(b, cudaMemcpyAsync(b->d_desc, off.data(), sizeof(InstDesc) * max_instances, cudaMemcpyHostToDevice, b->stream));
+    BTRY(b, cudaEventCreate(&b->ev0));
+    BTRY(b, cudaEventCreate(&b->ev1));
+    BTRY(b, cudaStreamSynchronize(b->stream));
+    return SGPU_OK;
+}
+
+void sgpu_batch_destroy(sgpu_batch* b) {
+    if (!b) return;
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    for (Slot& s : b->slots)
+        if (s.ctx) sgpu_destroy(s.ctx);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    cudaFree(b->d_desc);
+    cudaFree(b->d_maps);
+    cudaFree(b->d_err);
+    cudaFree(b->d_counts);
+    cudaFree(b->d_G);
+    for (int s = 0; s < 2; ++s) {
+        cudaFree(b->d_field[s]);
+        cudaFree(b->d_src[s]);
+    }
+    cudaFree(b->d_node);
+    cudaFree(b->d_probe);
+    if (b->arena.base) cudaFree(b->arena.base);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+const char* sgpu_batch_last_error(const sgpu_batch* b) { return b ? b->err.c_str() : "null batch"; }
+
+sgpu_status sgpu_batch_add(sgpu_batch* b, const sgpu_problem* p, sgpu_ctx* plan, int nsteps, int* slot) {
+    if (!b || !slot || (!p && !plan) || nsteps < 0) return berr(b, SGPU_ERR_ARG, "bad sgpu_batch_add arguments");
+    *slot = -1;
+    int sl = -1;
+    for (int q = 0; q < b->max_slots; ++q)
+        if (!b->slots[q].ctx) {
+            sl = q;
+            break;
+        }
+    if (sl < 0) return berr(b, SGPU_ERR_OOM, "no free instance slot");
+    // everything in flight finishes before set-up work joins the stream
+    BTRY(b, cudaStreamSynchronize(b->stream));
+    sgpu_ctx* c = nullptr;
+    sgpu_status s = host_create_in(p, plan, nsteps, &b->arena, b->stream, &c);
+    if (!s) s = rebuild_sources(c);
+    if (s) {
+        b->err = c ? c->err : "instance set-up failed";
+        if (c) sgpu_destroy(c);
+        return s;
+    }
+    Slot& S = b->slots[sl];
+    S.ctx = c;
+    S.start = b->G;
+    S.nsteps = nsteps;
+    S.size_class = size_class_of(c);
+    InstDesc D = make_desc(S, true);
+    BTRY(b, cudaMemcpyAsync(b->d_desc + sl, &D, sizeof(InstDesc), cudaMemcpyHostToDevice, b->stream));
+    b->has_maps[sl] = c->tma_ready ? 1 : 0;
+    TMaps m2[2] = {c->tme, c->tmh};
+    if (c->tma_ready) BTRY(b, cudaMemcpyAsync(b->d_maps + 2 * sl, m2, sizeof(m2), cudaMemcpyHostToDevice, b->stream));
+    BTRY(b, cudaStreamSynchronize(b->stream));
+    b->dirty = true;
+    *slot = sl;
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_batch_remove(sgpu_batch* b, int slot) {
+    if (!valid_slot(b, slot)) return berr(b, SGPU_ERR_ARG, "no instance in that slot");
+    BTRY(b, cudaStreamSynchronize(b->stream));
+    InstDesc off{};
+    off.last_n = -1;
+    BTRY(b, cudaMemcpyAsync(b->d_desc + slot, &off, sizeof(InstDesc), cudaMemcpyHostToDevice, b->stream));
+    BTRY(b, cudaStreamSynchronize(b->stream));
+    sgpu_destroy(b->slots[slot].ctx);
+    b->slots[slot] = Slot{};
+    b->has_maps[slot] = 0;
+    b->dirty = true;
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_batch_advance(sgpu_batch* b, int nsteps) {
+    if (!b || nsteps < 0) return SGPU_ERR_ARG;
+    return advance(b, nsteps, true);
+}
+
+sgpu_status sgpu_batch_synchronize(sgpu_batch* b) {
+    if (!b) return SGPU_ERR_ARG;
+    BTRY(b, cudaStreamSynchronize(b->stream));
+    return check_err(b);
+}
+
+sgpu_status sgpu_batch_set_kernel_family(sgpu_batch* b, int family) {
+    if (!b || family < 0 || family > 1) return SGPU_ERR_ARG;
+    b->family = family;
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_batch_elapsed(sgpu_batch* b, int nsteps, float* ms) {
+    if (!b || !ms || nsteps < 0) return SGPU_ERR_ARG;
+    sgpu_status s;
+    drop_finished(b);
+    if (b->dirty && (s = rebuild(b))) return s;
+    if (nsteps >= kGraphSteps && (s = ensure_graph(b))) return s;
+    BTRY(b, cudaEventRecord(b->ev0, b->stream));
+    if ((s = advance(b, nsteps, true))) return s;
+    BTRY(b, cudaEventRecord(b->ev1, b->stream));
+    BTRY(b, cudaEventSynchronize(b->ev1));
+    BTRY(b, cudaEventElapsedTime(ms, b->ev0, b->ev1));
+    return check_err(b);
+}
+
+sgpu_status sgpu_batch_slot_info(const sgpu_batch* b, int slot, int* steps_done, int* steps_total, int* nprobes) {
+    if (!valid_slot(b, slot)) return SGPU_ERR_ARG;
+    const Slot& S = b->slots[slot];
+    const int done = std::min(std::max(b->G - S.start, 0), S.nsteps + 1);
+    if (steps_done) *steps_done = done;
+    if (steps_total) *steps_total = S.nsteps + 1;
+    if (nprobes) *nprobes = S.ctx->probes.n;
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_batch_read_probes(sgpu_batch* b, int slot, float* out, int max_rows, int* rows) {
+    if (!valid_slot(b, slot) || !rows) return berr(b, SGPU_ERR_ARG, "bad probe read");
+    const Slot& S = b->slots[slot];
+    const int done = std::min(std::max(b->G - S.start, 0), S.nsteps + 1);
+    const int take = std::min(done, max_rows);
+    *rows = take;
+    if (take <= 0 || S.ctx->probes.n == 0) return SGPU_OK;
+    if (!out) return berr(b, SGPU_ERR_ARG, "null output");
+    BTRY(b, cudaStreamSynchronize(b->stream));
+    BTRY(b, cudaMemcpy(out, S.ctx->probes.ring, sizeof(float) * (size_t)take * S.ctx->probes.n, cudaMemcpyDeviceToHost));
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_batch_instance(sgpu_batch* b, int slot, sgpu_ctx** ctx) {
+    if (!valid_slot(b, slot) || !ctx) return SGPU_ERR_ARG;
+    BTRY(b, cudaStreamSynchronize(b->stream));
+    *ctx = b->slots[slot].ctx;
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_batch_memory(sgpu_batch* b, uint64_t* capacity, uint64_t* in_use, uint64_t* largest_free) {
+    if (!b) return SGPU_ERR_ARG;
+    if (capacity) *capacity = b->arena.cap;
+    if (in_use) {
+        std::lock_guard<std::mutex> lock(b->arena.mu);
+        *in_use = b->arena.in_use;
+    }
+    if (largest_free) *largest_free = arena_largest(&b->arena);
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_batch_set_tuning(sgpu_batch* b, const int* chunk3, int ctas_per_sm) {
+    if (!b) return SGPU_ERR_ARG;
+    if (chunk3)
+        for (int q = 0; q < kNumClasses; ++q) {
+            if (chunk3[q] < 1 || chunk3[q] > 1024) return berr(b, SGPU_ERR_ARG, "z chunk out of range");
+            if (b->chunk[q] != chunk3[q]) b->dirty = true;
+            b->chunk[q] = chunk3[q];
+        }
+    if (ctas_per_sm) {
+        if (ctas_per_sm < 1 || ctas_per_sm > 8) return berr(b, SGPU_ERR_ARG, "CTAs per SM out of range");
+        b->ctas_per_sm = ctas_per_sm;
+    }
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_batch_get_tuning(const sgpu_batch* b, int* chunk3, int* ctas_per_sm) {
+    if (!b) return SGPU_ERR_ARG;
+    if (chunk3)
+        for (int q = 0; q < kNumClasses; ++q) chunk3[q] = b->chunk[q];
+    if (ctas_per_sm) *ctas_per_sm = b->ctas_per_sm;
+    return SGPU_OK;
+}
+
+// Online autotuner: every trial advances the live instances by real steps
+// (results do not depend on the launch shape), timed with CUDA events; the
+// persistent grid size is chosen first, then each size class's z chunk by
+// coordinate descent.
+sgpu_status sgpu_batch_autotune(sgpu_batch* b, int steps_per_trial, int* chunk3, int* ctas_per_sm) {
+    if (!b || steps_per_trial < 1) return SGPU_ERR_ARG;
+    sgpu_status s;
+    auto trial = [&](float* ms) -> sgpu_status {
+        sgpu_status r;
+        drop_finished(b);
+        if (b->dirty && (r = rebuild(b))) return r;
+        if ((r = advance(b, 1, false))) return r;  // the first launch of a new shape is not timed
+        BTRY(b, cudaEventRecord(b->ev0, b->stream));
+        if ((r = advance(b, steps_per_trial, false))) return r;
+        BTRY(b, cudaEventRecord(b->ev1, b->stream));
+        BTRY(b, cudaEventSynchronize(b->ev1));
+        BTRY(b, cudaEventElapsedTime(ms, b->ev0, b->ev1));
+        return check_err(b);
+    };
+    bool present[kNumClasses] = {};
+    for (const Slot& sl : b->slots)
+        if (sl.ctx) present[sl.size_class] = true;
+    float best = 0;
+    int best_ctas = b->ctas_per_sm;
+    for (int ctas : {2, 3, 4, 6}) {
+        b->ctas_per_sm = ctas;
+        float ms = 0;
+        if ((s = trial(&ms))) return s;
+        if (ctas == 2 || ms < best) {
+            best = ms;
+            best_ctas = ctas;
+        }
+    }
+    b->ctas_per_sm = best_ctas;
+    for (int cl = 0; cl < kNumClasses; ++cl) {
+        if (!present[cl]) continue;
+        int best_chunk = b->chunk[cl];
+        float best_ms = -1;
+        for (int ch : {4, 8, 16, 32, 64}) {
+            if (b->chunk[cl] != ch) b->dirty = true;
+            b->chunk[cl] = ch;
+            float ms = 0;
+            if ((s = trial(&ms))) return s;
+            if (best_ms < 0 || ms < best_ms) {
+                best_ms = ms;
+                best_chunk = ch;
+            }
+        }
+        if (b->chunk[cl] != best_chunk) b->dirty = true;
+        b->chunk[cl] = best_chunk;
+    }
+    if (chunk3)
+        for (int q = 0; q < kNumClasses; ++q) chunk3[q] = b->chunk[q];
+    if (ctas_per_sm) *ctas_per_sm = b->ctas_per_sm;
+    return SGPU_OK;
+}
+
+// Device time of each phase summed over nsteps steps launched one by one
+// (ms6: E field, ADE, E sources, H field, H sources, probes + counter).
+// The steps are real steps of the live instances.
+sgpu_status sgpu_batch_profile_steps(sgpu_batch* b, int nsteps, float* ms6) {
+    if (!b || !ms6 || nsteps < 0) return SGPU_ERR_ARG;
+    sgpu_status s = SGPU_OK;
+    drop_finished(b);
+    if (b->dirty && (s = rebuild(b))) return s;
+    cudaEvent_t ev[7];
+    for (auto& e : ev) BTRY(b, cudaEventCreate(&e));
+    for (int q = 0; q < 6; ++q) ms6[q] = 0;
+    for (int n = 0; n < nsteps && !s; ++n) {
+        cudaEventRecord(ev[6], b->stream);
+        if ((s = enqueue_step(b, ev))) break;
+        b->G += 1;
+        if (cudaEventSynchronize(ev[5]) != cudaSuccess) {
+            s = berr(b, SGPU_ERR_CUDA, "profiled step failed");
+            break;
+        }
+        float t;
+        cudaEventElapsedTime(&t, ev[6], ev[0]);
+        ms6[0] += t;
+        for (int q = 1; q < 6; ++q) {
+            cudaEventElapsedTime(&t, ev[q - 1], ev[q]);
+            ms6[q] += t;
+        }
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    return s ? s : check_err(b);
+}
+
+sgpu_status sgpu_batch_steps(const sgpu_batch* b, int* counter) {
+    if (!b || !counter) return SGPU_ERR_ARG;
+    *counter = b->G;
+    return SGPU_OK;
+}
+
+}  // extern "C"

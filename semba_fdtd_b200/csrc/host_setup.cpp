@@ -217,49 +217,71 @@ void pml_media(HostState& h) {
         const Box& r = reach[f];
         const int lo_src[3] = {inner.x0, inner.y0, inner.z0};
         const int hi_src[3] = {inner.x1 + in_lo[f][0] - 1, inner.y1 + in_lo[f][1] - 1, inner.z1 + in_lo[f][2] - 1};
-        // along x
-        for (int j = r.y0; j <= r.y1; ++j)
-            for (int k = r.z0; k <= r.z1; ++k) {
-                for (int i = r.x0; i <= inner.x0 - 1; ++i) m.at(i, j, k) = neg(m.at(lo_src[0], j, k));
-                for (int i = inner.x1 + in_lo[f][0]; i <= r.x1; ++i) m.at(i, j, k) = neg(m.at(hi_src[0], j, k));
-            }
-        // along y, over the whole x reach (edges)
-        for (int i = r.x0; i <= r.x1; ++i)
-            for (int k = r.z0; k <= r.z1; ++k) {
-                for (int j = r.y0; j <= inner.y0 - 1; ++j) m.at(i, j, k) = neg(m.at(i, lo_src[1], k));
-                for (int j = inner.y1 + in_lo[f][1]; j <= r.y1; ++j) m.at(i, j, k) = neg(m.at(i, hi_src[1], k));
-            }
-        // along z, over the whole x and y reach (corners)
-        for (int i = r.x0; i <= r.x1; ++i)
+        // along x (rows are contiguous: k, then j, then the two i ranges)
+        for (int k = r.z0; k <= r.z1; ++k)
             for (int j = r.y0; j <= r.y1; ++j) {
-                for (int k = r.z0; k <= inner.z0 - 1; ++k) m.at(i, j, k) = neg(m.at(i, j, lo_src[2]));
-                for (int k = inner.z1 + in_lo[f][2]; k <= r.z1; ++k) m.at(i, j, k) = neg(m.at(i, j, hi_src[2]));
+                int16_t* row = &m.at(r.x0, j, k) - r.x0;  // row[i] is cell (i, j, k)
+                const int16_t lo = neg(row[lo_src[0]]), hi = neg(row[hi_src[0]]);
+                for (int i = r.x0; i <= inner.x0 - 1; ++i) row[i] = lo;
+                for (int i = inner.x1 + in_lo[f][0]; i <= r.x1; ++i) row[i] = hi;
             }
+        // along y, over the whole x reach (edges): whole rows copied
+        auto copy_row = [&](int16_t* dst, const int16_t* src) {
+            for (int i = r.x0; i <= r.x1; ++i) dst[i] = neg(src[i]);
+        };
+        for (int k = r.z0; k <= r.z1; ++k) {
+            const int16_t* slo = &m.at(r.x0, lo_src[1], k) - r.x0;
+            const int16_t* shi = &m.at(r.x0, hi_src[1], k) - r.x0;
+            for (int j = r.y0; j <= inner.y0 - 1; ++j) copy_row(&m.at(r.x0, j, k) - r.x0, slo);
+            for (int j = inner.y1 + in_lo[f][1]; j <= r.y1; ++j) copy_row(&m.at(r.x0, j, k) - r.x0, shi);
+        }
+        // along z, over the whole x and y reach (corners): whole planes copied
+        for (int k = r.z0; k <= inner.z0 - 1; ++k)
+            for (int j = r.y0; j <= r.y1; ++j) copy_row(&m.at(r.x0, j, k) - r.x0, &m.at(r.x0, j, lo_src[2]) - r.x0);
+        for (int k = inner.z1 + in_lo[f][2]; k <= r.z1; ++k)
+            for (int j = r.y0; j <= r.y1; ++j) copy_row(&m.at(r.x0, j, k) - r.x0, &m.at(r.x0, j, hi_src[2]) - r.x0);
     }
+    // Only the extruded shell can hold negative (to be copied) entries; the
+    // scans below visit it row by row in the k, j, i order of a full sweep,
+    // so copies are numbered in order of first appearance exactly as a full
+    // sweep numbers them.
+    auto shell_rows = [&](int f, auto&& fn) {
+        MediaMat& m = h.mm[f];
+        const Box& r = reach[f];
+        const int xa = inner.x0, xb = inner.x1 + in_lo[f][0] - 1;
+        const int ya = inner.y0, yb = inner.y1 + in_lo[f][1] - 1;
+        const int za = inner.z0, zb = inner.z1 + in_lo[f][2] - 1;
+        for (int k = r.z0; k <= r.z1; ++k)
+            for (int j = r.y0; j <= r.y1; ++j) {
+                int16_t* row = &m.at(r.x0, j, k) - r.x0;
+                if (k < za || k > zb || j < ya || j > yb) {
+                    fn(row, r.x0, r.x1);
+                } else {
+                    fn(row, r.x0, std::min(r.x1, xa - 1));
+                    fn(row, std::max(r.x0, xb + 1), r.x1);
+                }
+            }
+    };
     std::vector<int> copy_of(h.num_media + 1, 0);
     int next = h.num_media;
-    for (int f = 0; f < 6; ++f) {
-        const Box& r = reach[f];
-        for (int k = r.z0; k <= r.z1; ++k)
-            for (int j = r.y0; j <= r.y1; ++j)
-                for (int i = r.x0; i <= r.x1; ++i) {
-                    int v = h.mm[f].at(i, j, k);
-                    if (v < 0 && copy_of[-v] == 0) copy_of[-v] = ++next;
-                }
-    }
+    for (int f = 0; f < 6; ++f)
+        shell_rows(f, [&](int16_t* row, int i0, int i1) {
+            for (int i = i0; i <= i1; ++i) {
+                const int v = row[i];
+                if (v < 0 && copy_of[-v] == 0) copy_of[-v] = ++next;
+            }
+        });
     h.med.resize(next + 1);
-    for (int f = 0; f < 6; ++f) {
-        const Box& r = reach[f];
-        for (int k = r.z0; k <= r.z1; ++k)
-            for (int j = r.y0; j <= r.y1; ++j)
-                for (int i = r.x0; i <= r.x1; ++i) {
-                    int16_t& v = h.mm[f].at(i, j, k);
-                    if (v < 0) {
-                        h.med[copy_of[-v]] = h.med[-v];
-                        v = (int16_t)copy_of[-v];
-                    }
+    for (int f = 0; f < 6; ++f)
+        shell_rows(f, [&](int16_t* row, int i0, int i1) {
+            for (int i = i0; i <= i1; ++i) {
+                const int v = row[i];
+                if (v < 0) {
+                    h.med[copy_of[-v]] = h.med[-v];
+                    row[i] = (int16_t)copy_of[-v];
                 }
-    }
+            }
+        });
     h.num_media = next;
 }
 
@@ -704,7 +726,7 @@ HostState* make_plan(const sgpu_problem* p, int max_steps, sgpu_status* rc) {
 }
 
 // Hand the plan to the level-1 entry points.
-sgpu_status realize(HostState* h, sgpu_ctx** out) {
+sgpu_status realize(HostState* h, sgpu::Arena* arena, cudaStream_t stream, sgpu_ctx** out) {
     sgpu_grid_desc g{};
     for (int f = 0; f < 6; ++f) {
         g.alloc[f] = to_lim(h->alloc[f]);
@@ -717,7 +739,7 @@ sgpu_status realize(HostState* h, sgpu_ctx** out) {
     g.idxh = h->idxh.v.data(); g.idyh = h->idyh.v.data(); g.idzh = h->idzh.v.data();
     g.dt = h->dt;
     sgpu_ctx* c = nullptr;
-    sgpu_status s = sgpu_create(&g, &c);
+    sgpu_status s = sgpu::create_in(&g, arena, stream, &c);
     *out = c;
     if (s) { delete h; return s; }
     c->host = h;
@@ -774,7 +796,7 @@ sgpu_status sgpu_host_create(const sgpu_problem* p, int max_steps, sgpu_ctx** ou
     sgpu_status rc;
     HostState* h = make_plan(p, max_steps, &rc);
     if (!h) return rc;
-    return realize(h, out);
+    return realize(h, nullptr, nullptr, out);
 }
 
 sgpu_status sgpu_host_footprint(const sgpu_ctx* c, uint64_t* bytes) {
@@ -819,6 +841,103 @@ sgpu_status sgpu_host_footprint(const sgpu_ctx* c, uint64_t* bytes) {
     }
     b += (uint64_t)h->probes.size() / 4 * h->probe_cap * 4;
     *bytes = b;
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_batch_footprint(const sgpu_ctx* c, uint64_t* bytes, uint64_t* largest) {
+    if (!c || !c->host || !bytes) return SGPU_ERR_ARG;
+    const HostState* h = (const HostState*)c->host;
+    uint64_t total = 0, big = 0;
+    auto buf = [&](uint64_t b) {
+        if (!b) return;
+        b = (b + 255) / 256 * 256;  // the arena's grain
+        total += b;
+        big = std::max(big, b);
+    };
+    long long nxa = 0, nya = 0, nza = 0;
+    for (int f = 0; f < 6; ++f) {
+        nxa = std::max<long long>(nxa, h->alloc[f].x1 - h->alloc[0].x0 + 1);
+        nya = std::max<long long>(nya, h->alloc[f].y1 - h->alloc[0].y0 + 1);
+        nza = std::max<long long>(nza, h->alloc[f].z1 - h->alloc[0].z0 + 1);
+    }
+    const long long pitch = (nxa + 31) / 32 * 32, vol = pitch * nya * nza;
+    for (int f = 0; f < 6; ++f) {
+        buf((uint64_t)vol * 4);  // field
+        buf((uint64_t)vol * 2);  // media
+    }
+    const uint64_t n1 = (uint64_t)h->num_media + 1;
+    for (int q = 0; q < 4; ++q) buf(n1 * 4);  // G1 G2 GM1 GM2
+    for (long long n : {pitch, nya, nza, pitch, nya, nza}) buf((uint64_t)n * 4);  // metrics
+    for (int q = 0; q < 3; ++q) buf(4);  // step, flag and error words
+    // CPML: the twelve per-axis vectors and the psi slabs
+    for (int a = 0; a < 3; ++a)
+        for (const Vec* v : {&h->pbe[a], &h->pce[a], &h->pbm[a], &h->pcm[a]}) buf((uint64_t)v->v.size() * 4 + 64);
+    for (int f = 0; f < 6; ++f)
+        for (int reg = 0; reg < 6; ++reg) {
+            const sgpu_lim& l = h->cd.pmlc[f][reg];
+            if (l.xe >= l.xi && l.ye >= l.yi && l.ze >= l.zi)
+                buf((uint64_t)(l.xe - l.xi + 1) * (l.ye - l.yi + 1) * (l.ze - l.zi + 1) * 4);
+        }
+    // ADE: per component node list, slot, previous field and state; the
+    // per-row count/offset scratch of the set-up is live at the same time
+    if (!h->didx.empty()) {
+        std::vector<char> disp(h->num_media + 1, 0);
+        int nu = 0;
+        for (size_t m = 0; m < h->didx.size(); ++m) {
+            disp[h->didx[m]] = 1;
+            nu = std::max(nu, h->dnp[m]);
+        }
+        buf(h->didx.size() * 512 + 64);  // medium table
+        buf(n1 * 2);                      // slot of medium
+        for (int f = 0; f < 3; ++f) {
+            uint64_t nodes = 0;
+            const Box& w = h->sweep[f];
+            if (h->mm[f].v.empty()) {
+                nodes = (uint64_t)vol;
+            } else {
+                MediaMat& m = const_cast<MediaMat&>(h->mm[f]);
+                for (int k = w.z0; k <= w.z1; ++k)
+                    for (int j = w.y0; j <= w.y1; ++j)
+                        for (int i = w.x0; i <= w.x1; ++i) nodes += disp[m.at(i, j, k)];
+            }
+            const uint64_t rows = (uint64_t)(w.y1 - w.y0 + 1) * (w.z1 - w.z0 + 1);
+            buf(nodes * 4);
+            buf(nodes * 1);
+            buf(nodes * 4);
+            buf(nodes * 16 * (uint64_t)std::max(1, nu));
+            buf(rows * 8);
+            buf(rows * 4);
+        }
+    }
+    // sources: every plane-wave face node and nodal point is at most one row
+    uint64_t rows = 0, samples = 0;
+    for (const sgpu_planewave_desc& d : h->pw) {
+        for (int f = 0; f < 6; ++f)
+            for (int comp = 0; comp < 6; ++comp) {
+                const int* l = d.lim[f][comp];
+                if (l[2] >= l[1] && l[4] >= l[3]) rows += (uint64_t)(l[2] - l[1] + 1) * (l[4] - l[3] + 1);
+            }
+        samples += (uint64_t)d.numus + 1;
+    }
+    for (const sgpu_nodal_desc& d : h->nodal) {
+        rows += (uint64_t)(d.box.xe - d.box.xi + 1) * (d.box.ye - d.box.yi + 1) * (d.box.ze - d.box.zi + 1);
+        samples += (uint64_t)d.numus + 1;
+    }
+    for (int side = 0; side < 2; ++side) {
+        buf(rows * 4);
+        buf(rows * 4);
+        buf(rows * 4 + 4);
+        buf(rows * 24);
+        buf((h->pw.size() + h->nodal.size()) * 16);
+        buf(samples * 4);
+    }
+    buf((uint64_t)(h->max_steps + 3) * 8);  // time vector
+    const uint64_t np = h->probes.size() / 4;
+    buf(np * 4);
+    buf(np * 8);
+    buf(np * (uint64_t)(h->max_steps + 1) * 4);  // whole traces
+    *bytes = total;
+    if (largest) *largest = big;
     return SGPU_OK;
 }
 
@@ -879,3 +998,21 @@ sgpu_status sgpu_host_get_media(const sgpu_ctx* c, int comp, int16_t* out) {
 }
 
 }  // extern "C"
+
+sgpu_status sgpu::host_create_in(const sgpu_problem* p, sgpu_ctx* plan, int max_steps, Arena* arena, cudaStream_t stream,
+                                 sgpu_ctx** out) {
+    if (!out) return SGPU_ERR_ARG;
+    *out = nullptr;
+    HostState* h = nullptr;
+    if (plan) {
+        if (!plan->host_only || !plan->host) return SGPU_ERR_ARG;
+        h = (HostState*)plan->host;
+        plan->host = nullptr;  // the realized context owns it now
+    } else {
+        sgpu_status rc;
+        h = make_plan(p, max_steps, &rc);
+        if (!h) return rc;
+    }
+    if (arena) h->probe_cap = h->max_steps + 1;
+    return realize(h, arena, stream, out);
+}

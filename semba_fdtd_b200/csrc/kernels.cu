@@ -471,15 +471,29 @@ sgpu_status whole_step(sgpu_ctx* c, StepRef sr) {
     return launch_probes(c, sr);
 }
 
+void* dev_malloc(sgpu_ctx* c, size_t bytes) {
+    if (c->arena) return arena_alloc(c->arena, bytes);
+    void* p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return p;
+}
+
+void dev_free(sgpu_ctx* c, void* p) {
+    if (!p) return;
+    if (c->arena) arena_free(c->arena, p);
+    else cudaFree(p);
+}
+
 template <class T> sgpu_status dalloc(sgpu_ctx* c, T** p, size_t n, std::vector<void*>* track = nullptr) {
     *p = nullptr;
     if (n == 0) return SGPU_OK;
-    cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
-    if (e != cudaSuccess) {
-        *p = nullptr;
-        cudaGetLastError();
-        return set_error(c, SGPU_ERR_OOM, std::string("cudaMalloc of ") + std::to_string(n * sizeof(T)) + " bytes failed");
-    }
+    *p = (T*)dev_malloc(c, n * sizeof(T));
+    if (!*p)
+        return set_error(c, SGPU_ERR_OOM, std::string(c->arena ? "arena" : "cudaMalloc") + " allocation of " +
+                                              std::to_string(n * sizeof(T)) + " bytes failed");
     if (track) track->push_back(*p);
     return SGPU_OK;
 }
@@ -490,8 +504,8 @@ template <class T> sgpu_status h2d(sgpu_ctx* c, T* d, const T* h, size_t n) {
     return SGPU_OK;
 }
 
-void free_list(std::vector<void*>& v) {
-    for (void* p : v) cudaFree(p);
+void free_list(sgpu_ctx* c, std::vector<void*>& v) {
+    for (void* p : v) dev_free(c, p);
     v.clear();
 }
 
@@ -516,11 +530,14 @@ extern "C" {
 
 const char* sgpu_last_error(const sgpu_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
-sgpu_status sgpu_create(const sgpu_grid_desc* d, sgpu_ctx** out) {
+}  // extern "C"
+
+sgpu_status sgpu::create_in(const sgpu_grid_desc* d, Arena* arena, cudaStream_t stream, sgpu_ctx** out) {
     if (!d || !out) return SGPU_ERR_ARG;
     *out = nullptr;
     sgpu_ctx* c = new (std::nothrow) sgpu_ctx();
     if (!c) return SGPU_ERR_OOM;
+    c->arena = arena;
     auto fail = [&](sgpu_status s) {
         // keep the context alive so the caller can read the message
         *out = c;
@@ -554,8 +571,13 @@ sgpu_status sgpu_create(const sgpu_grid_desc* d, sgpu_ctx** out) {
     c->dt = d->dt;
     cudaError_t e = cudaGetDevice(&c->device);
     if (e != cudaSuccess) return fail(set_error(c, SGPU_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e)));
-    e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
-    if (e != cudaSuccess) return fail(set_error(c, SGPU_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e)));
+    if (stream) {
+        c->stream = stream;
+        c->own_stream = false;
+    } else {
+        e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return fail(set_error(c, SGPU_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e)));
+    }
     sgpu_status s;
     for (int f = 0; f < 6; ++f) {
         if ((s = dalloc(c, &c->F[f], c->vol))) return fail(s);
@@ -608,6 +630,10 @@ sgpu_status sgpu_create(const sgpu_grid_desc* d, sgpu_ctx** out) {
     return SGPU_OK;
 }
 
+extern "C" {
+
+sgpu_status sgpu_create(const sgpu_grid_desc* d, sgpu_ctx** out) { return create_in(d, nullptr, nullptr, out); }
+
 void sgpu_destroy(sgpu_ctx* c) {
     if (!c) return;
     if (c->host_only) {
@@ -618,19 +644,19 @@ void sgpu_destroy(sgpu_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->graph) cudaGraphExecDestroy(c->graph);
     for (int f = 0; f < 6; ++f) {
-        cudaFree(c->F[f]);
-        cudaFree(c->M[f]);
+        dev_free(c, c->F[f]);
+        dev_free(c, c->M[f]);
     }
-    cudaFree(c->g1); cudaFree(c->g2); cudaFree(c->gm1); cudaFree(c->gm2);
-    cudaFree(c->idxe); cudaFree(c->idye); cudaFree(c->idze);
-    cudaFree(c->idxh); cudaFree(c->idyh); cudaFree(c->idzh);
-    cudaFree(c->d_tiempo); cudaFree(c->d_step); cudaFree(c->d_flag); cudaFree(c->d_err);
-    free_list(c->cpml_allocs);
-    free_list(c->disp_allocs);
-    free_list(c->src_allocs[0]);
-    free_list(c->src_allocs[1]);
-    free_list(c->probe_allocs);
-    if (c->stream) cudaStreamDestroy(c->stream);
+    dev_free(c, c->g1); dev_free(c, c->g2); dev_free(c, c->gm1); dev_free(c, c->gm2);
+    dev_free(c, c->idxe); dev_free(c, c->idye); dev_free(c, c->idze);
+    dev_free(c, c->idxh); dev_free(c, c->idyh); dev_free(c, c->idzh);
+    dev_free(c, c->d_tiempo); dev_free(c, c->d_step); dev_free(c, c->d_flag); dev_free(c, c->d_err);
+    free_list(c, c->cpml_allocs);
+    free_list(c, c->disp_allocs);
+    free_list(c, c->src_allocs[0]);
+    free_list(c, c->src_allocs[1]);
+    free_list(c, c->probe_allocs);
+    if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);
     if (c->host && c->host_free) c->host_free(c->host);
     delete c;
 }
@@ -696,7 +722,7 @@ sgpu_status sgpu_download_field(sgpu_ctx* c, int comp, float* f) {
 
 sgpu_status sgpu_init_cpml(sgpu_ctx* c, const sgpu_cpml_desc* d) {
     if (!c || !d) return set_error(c, SGPU_ERR_ARG, "null cpml descriptor");
-    free_list(c->cpml_allocs);
+    free_list(c, c->cpml_allocs);
     KCpml& k = c->cpml;
     k = KCpml{};
     sgpu_status s;
@@ -745,7 +771,7 @@ sgpu_status sgpu_init_cpml(sgpu_ctx* c, const sgpu_cpml_desc* d) {
 sgpu_status sgpu_init_edisp(sgpu_ctx* c, const sgpu_edisp_desc* d) {
     if (!c || !d) return set_error(c, SGPU_ERR_ARG, "null edisp descriptor");
     if (!ready(c)) return set_error(c, SGPU_ERR_STATE, "upload the media matrices before sgpu_init_edisp");
-    free_list(c->disp_allocs);
+    free_list(c, c->disp_allocs);
     c->disp = KDisp{};
     c->disp_on = false;
     if (d->nmedia <= 0) return SGPU_OK;
@@ -807,12 +833,12 @@ sgpu_status sgpu_init_edisp(sgpu_ctx* c, const sgpu_edisp_desc* d) {
         if ((s = dalloc(c, &dcount, rows))) return s;
         k_count_disp<<<(unsigned)((rows + 255) / 256), 256, 0, c->stream>>>(c->M[comp], dslot, c->pitch, c->plane, x0, x1,
                                                                             y0, y1, z0, z1, dcount);
-        if ((s = check_launch(c, "k_count_disp"))) { cudaFree(dcount); return s; }
+        if ((s = check_launch(c, "k_count_disp"))) { dev_free(c, dcount); return s; }
         std::vector<int> cnt(rows);
         cudaError_t e = cudaMemcpyAsync(cnt.data(), dcount, rows * sizeof(int), cudaMemcpyDeviceToHost, c->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-        if (e != cudaSuccess) { cudaFree(dcount); return set_error(c, SGPU_ERR_CUDA, cudaGetErrorString(e)); }
-        cudaFree(dcount);
+        if (e != cudaSuccess) { dev_free(c, dcount); return set_error(c, SGPU_ERR_CUDA, cudaGetErrorString(e)); }
+        dev_free(c, dcount);
         std::vector<long long> offs(rows);
         long long tot = 0;
         for (long long r = 0; r < rows; ++r) { offs[r] = tot; tot += cnt[r]; }
@@ -820,23 +846,23 @@ sgpu_status sgpu_init_edisp(sgpu_ctx* c, const sgpu_edisp_desc* d) {
         if (tot == 0) continue;
         long long* doffs;
         if ((s = dalloc(c, &doffs, rows))) return s;
-        if ((s = h2d(c, doffs, offs.data(), rows))) { cudaFree(doffs); return s; }
+        if ((s = h2d(c, doffs, offs.data(), rows))) { dev_free(c, doffs); return s; }
         int* node;
         uint8_t* med;
         float* prev;
         double2* J;
         if ((s = dalloc(c, &node, tot, &c->disp_allocs)) || (s = dalloc(c, &med, tot, &c->disp_allocs)) ||
             (s = dalloc(c, &prev, tot, &c->disp_allocs)) || (s = dalloc(c, &J, (size_t)tot * std::max(1, nu_max), &c->disp_allocs))) {
-            cudaFree(doffs);
+            dev_free(c, doffs);
             return s;
         }
         k_fill_disp<<<(unsigned)((rows + 255) / 256), 256, 0, c->stream>>>(c->M[comp], dslot, c->pitch, c->plane, x0, x1, y0,
                                                                            y1, z0, z1, doffs, node, med);
-        if ((s = check_launch(c, "k_fill_disp"))) { cudaFree(doffs); return s; }
+        if ((s = check_launch(c, "k_fill_disp"))) { dev_free(c, doffs); return s; }
         CUDA_TRY(c, cudaMemsetAsync(prev, 0, tot * sizeof(float), c->stream));
         CUDA_TRY(c, cudaMemsetAsync(J, 0, (size_t)tot * std::max(1, nu_max) * sizeof(double2), c->stream));
         CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-        cudaFree(doffs);
+        dev_free(c, doffs);
         k.node[comp] = node;
         k.med[comp] = med;
         k.prev[comp] = prev;
@@ -868,7 +894,7 @@ long long lin(const sgpu_ctx* c, int i, int j, int k) {
 
 sgpu_status build_sources(sgpu_ctx* c) {
     for (int side = 0; side < 2; ++side) {
-        free_list(c->src_allocs[side]);
+        free_list(c, c->src_allocs[side]);
         c->src[side] = KSrc{};
         std::vector<sgpu_ctx::HostEntry> es = c->src_host[side];
         if (es.empty()) continue;
@@ -1042,7 +1068,7 @@ sgpu_status sgpu_add_nodal(sgpu_ctx* c, const sgpu_nodal_desc* d) {
 
 sgpu_status sgpu_set_time(sgpu_ctx* c, int n0, int count, const double* t) {
     if (!c || !t || count <= 0) return set_error(c, SGPU_ERR_ARG, "bad time vector");
-    cudaFree(c->d_tiempo);
+    dev_free(c, c->d_tiempo);
     c->d_tiempo = nullptr;
     sgpu_status s;
     if ((s = dalloc(c, &c->d_tiempo, count))) return s;
@@ -1056,7 +1082,7 @@ sgpu_status sgpu_set_time(sgpu_ctx* c, int n0, int count, const double* t) {
 
 sgpu_status sgpu_set_probes(sgpu_ctx* c, int np, const int* cijk, int cap) {
     if (!c || np < 0 || (np > 0 && (!cijk || cap <= 0))) return set_error(c, SGPU_ERR_ARG, "bad probe set");
-    free_list(c->probe_allocs);
+    free_list(c, c->probe_allocs);
     c->probes = KProbes{};
     c->probe_written = c->probe_read = 0;
     c->probe_first_n = -1;
@@ -1460,3 +1486,8 @@ sgpu_status sgpu_device_bytes(const sgpu_ctx* c, uint64_t* bytes) {
 }
 
 }  // extern "C"
+
+sgpu_status sgpu::rebuild_sources(sgpu_ctx* c) {
+    if (!c->src_dirty) return SGPU_OK;
+    return build_sources(c);
+}

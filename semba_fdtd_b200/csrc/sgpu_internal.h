@@ -112,11 +112,19 @@ struct StepRef {
     int n;
 };
 
+// Device memory arena of a batch (batch.cu): contexts created inside a batch
+// take every device buffer from it instead of cudaMalloc.
+struct Arena;
+void* arena_alloc(Arena* a, size_t bytes);
+void arena_free(Arena* a, void* p);
+
 }  // namespace sgpu
 
 struct sgpu_ctx {
     std::string err;
     cudaStream_t stream = nullptr;
+    bool own_stream = true;          // false inside a batch (the batch's stream)
+    sgpu::Arena* arena = nullptr;    // non-null inside a batch
     int device = 0;
     // geometry
     sgpu_lim alloc[6], sweep[6];
@@ -193,4 +201,14 @@ struct sgpu_ctx {
 namespace sgpu {
 sgpu_status set_error(sgpu_ctx* c, sgpu_status code, const std::string& msg);
 KGrid kgrid(const sgpu_ctx* c);
+// sgpu_create with an optional arena and an external stream (batches).
+sgpu_status create_in(const sgpu_grid_desc* d, Arena* arena, cudaStream_t stream, sgpu_ctx** out);
+// sgpu_host_create into an arena/stream; `plan` (from sgpu_host_plan) is
+// consumed when non-null, else the problem is planned first.  Inside an
+// arena every probe keeps its whole trace (nsteps + 1 rows).
+sgpu_status host_create_in(const sgpu_problem* p, sgpu_ctx* plan, int max_steps, Arena* arena, cudaStream_t stream,
+                           sgpu_ctx** out);
+// Source lists built on the device now (normally built lazily before the
+// first launch that needs them).
+sgpu_status rebuild_sources(sgpu_ctx* c);
 }  // namespace sgpu
