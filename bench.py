@@ -43,6 +43,10 @@ CONFIGS = {
     "dispersive_large": ("dispersive_large", {}, "512^3 graded 1-3 mm, CPML 12 (536^3 swept), 30% 2-pair pole-residue, soft Ez dipole"),
     "plain_mid": ("plain_mid", {}, "256^3 dx 5 mm, CPML 12, lossy sphere + 20 PEC/dielectric blocks, TF/SF plane wave"),
     "plain_small": ("plain_small", {}, "64^3 dx 1 cm, CPML 10, TF/SF plane wave"),
+    "batched": (None, {}, "64 instances (seed 6): edges log-U[32,160] per axis, CPML 8, 1-6 dielectric blocks, "
+                          "seeded plane wave, steps U{500..3000}"),
+    "served": (None, {}, "Poisson stream (seed 7): edges log-U[48,256], CPML 10, 0-2 pole-residue blocks, soft dipole, "
+                         "4-32 probes, steps U{500..4000} x steps_scale"),
 }
 CPU_SAMPLE_N = 160  # the reference arm and cpu_baseline run this scaled sample
 
@@ -303,6 +307,116 @@ def run_e2e(pb, K, lib, family):
             "includes": "host set-up, media + initial-field upload, K graph steps, probe and final-field download"}
 
 
+def _stream_batched(n_inst: int, seed: int = 6):
+    from semba_fdtd_b200 import casegen, read_case
+    rng = np.random.default_rng(seed)
+    d = Path(tempfile.mkdtemp(prefix="semba_batched_"))
+    return [read_case(casegen.batch_instance(d, q, rng)) for q in range(n_inst)]
+
+
+def _stream_served(n_req: int, rate: float, steps_scale: float, seed: int = 7):
+    from semba_fdtd_b200 import casegen, read_case
+    from semba_fdtd_b200.serve import Request, poisson_arrivals
+    rng = np.random.default_rng(seed)
+    d = Path(tempfile.mkdtemp(prefix="semba_served_"))
+    arr = poisson_arrivals(n_req, rate, seed)
+    reqs = []
+    for q in range(n_req):
+        steps = max(1, int(round(int(rng.integers(500, 4001)) * steps_scale)))
+        pb = read_case(casegen.served_request(d, q, rng, steps=steps))
+        reqs.append(Request(rid=q, arrival=float(arr[q]), problem=pb, nsteps=steps))
+    return reqs
+
+
+def _cells_steps(pb, nsteps):
+    return pb.swept_cells * (nsteps + 1)
+
+
+def run_batched(args):
+    """The 64-instance stream as one batch (autotuned, 32-step graph chunks)
+    against the same instances one at a time through Solver.  Both arms
+    include host set-up, device upload and probe read-back; solves/s is
+    instances / wall time."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from semba_fdtd_b200 import Solver
+    from semba_fdtd_b200.batch import Batch, Plan
+    rank, local, world = env_rank()
+    if rank != 0:
+        return
+    pbs = _stream_batched(args.instances)
+    work = sum(_cells_steps(pb, pb.nsteps) for pb in pbs)
+    # plain arm: one solve at a time
+    t0 = time.perf_counter()
+    for pb in ([] if args.skip_plain else pbs):
+        with Solver(pb, probe_capacity=pb.nsteps + 1) as s:
+            s.step(pb.nsteps + 1)
+            s.probes()
+    t_plain = time.perf_counter() - t0 if not args.skip_plain else float("nan")
+    # batched arm
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 1)) as pool:  # host set-up in parallel
+            plans = list(pool.map(Plan, pbs))
+        arena = int(sum(p.footprint for p in plans) * 1.05) + (64 << 20)
+        with Batch(arena, len(pbs) + 1, kernel_family=args.batch_family) as b:
+            slots = [b.add(p) for p in plans]
+            chunks, ctas = b.autotune(2)
+            phases = b.profile(8)  # real steps, per-phase device time with every instance live
+            dev_ms = 0.0
+            while any(not b.done(x) for x in slots):
+                left = max(b.info(x)[1] - b.info(x)[0] for x in slots)
+                dev_ms += b.elapsed(min(256, max(32, left)))
+            for x in slots:
+                b.probes(x)
+        t_batch = time.perf_counter() - t0
+    line = {"metric": "solves/s", "value": len(pbs) / t_batch, "unit": "solves/s", "n_gpus": 1, "steps": None,
+            "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "impl": "batched",
+            "config": {"workload": CONFIGS["batched"][2], "instances": len(pbs), "cell_updates": work,
+                       "arena_bytes": arena, "tuned_chunks": chunks, "tuned_ctas_per_sm": ctas,
+                       "field_kernels": "TMA-pipelined persistent" if args.batch_family == 1 else "register-marching"},
+            "plain_one_at_a_time": {"solves_per_s": len(pbs) / t_plain if not args.skip_plain else None,
+                                    "seconds": None if args.skip_plain else t_plain,
+                                    "gcell_upd_s": None if args.skip_plain else work / t_plain / 1e9},
+            "batched": {"seconds": t_batch, "gcell_upd_s": work / t_batch / 1e9, "device_step_ms_total": dev_ms,
+                        "device_gcell_upd_s": work / (dev_ms * 1e-3) / 1e9 if dev_ms else None,
+                        "phase_ms_8_steps_all_live": dict(zip(["e_field", "ade", "e_sources", "h_field", "h_sources",
+                                                               "probes"], phases))},
+            "speedup_vs_plain": None if args.skip_plain else t_plain / t_batch, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
+def run_served(args):
+    """A Poisson stream (step counts scaled) served with continuous batching
+    against the same stream served one solve at a time through Solver."""
+    from semba_fdtd_b200.serve import Server, run_plain
+    rank, local, world = env_rank()
+    if rank != 0:
+        return
+    reqs = _stream_served(args.requests, args.rate, args.steps_scale)
+    work = sum(_cells_steps(r.problem, r.nsteps) for r in reqs)
+    plain = run_plain(reqs, keep_traces=False).summary()
+    for r in reqs:
+        r.plan = None
+    with ClockSampler(local) as clk:
+        srv = Server(arena_bytes=int(args.arena_gb * (1 << 30)), max_instances=512, chunk=32, backfill=32,
+                     autotune=True)
+        try:
+            st = srv.run(reqs, keep_traces=False).summary()
+        finally:
+            srv.close()
+    line = {"metric": "solves/s", "value": st["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "steps": None,
+            "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "impl": "served",
+            "config": {"workload": CONFIGS["served"][2], "requests": len(reqs), "rate_per_s": args.rate,
+                       "steps_scale": args.steps_scale, "cell_updates": work, "hbm_budget_gb": args.arena_gb},
+            "served": st, "plain_one_at_a_time": plain,
+            "speedup_vs_plain": (st["solves_per_s"] / plain["solves_per_s"]) if plain["solves_per_s"] else None,
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -314,9 +428,21 @@ def main():
     ap.add_argument("--family", type=int, default=1, choices=[0, 1],
                     help="field kernels: 1 TMA-pipelined (default), 0 register-marching")
     ap.add_argument("--quick", action="store_true", help="skip the end-to-end and CPU-baseline legs (profiling runs)")
+    ap.add_argument("--instances", type=int, default=64, help="batched: instances in the stream")
+    ap.add_argument("--skip-plain", action="store_true", help="batched: leave out the one-at-a-time arm (profiling)")
+    ap.add_argument("--batch-family", type=int, default=1, choices=[0, 1],
+                    help="batched: field kernels, 1 TMA-pipelined persistent (default), 0 register-marching")
+    ap.add_argument("--requests", type=int, default=160, help="served: requests in the stream")
+    ap.add_argument("--rate", type=float, default=32.0, help="served: Poisson arrival rate (1/s)")
+    ap.add_argument("--steps-scale", type=float, default=0.25, help="served: scale of the drawn step counts")
+    ap.add_argument("--arena-gb", type=float, default=150.0, help="served: HBM budget of the arena")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.config == "batched":
+        run_batched(args)
+    elif args.config == "served":
+        run_served(args)
     else:
         run_ours(args)
 
