@@ -60,16 +60,26 @@ constexpr unsigned kCpmlX = 0xCC0u, kCpmlY = 0x303u, kCpmlZ = 0x03Cu;
 // and j are loaded once (only where some slab needs them, so i and j are in
 // range).
 struct CpmlCol {
-    unsigned col;
+    unsigned col;    // slabs holding the column
+    unsigned zall;   // ... of them, those holding every plane kb..ke
     float bx, cx, by, cy;
+    // slabs holding cell (i, j, k) of the column, kb <= k <= ke
+    __device__ __forceinline__ unsigned live(const KCpml& cp, int c0, int k) const {
+        const unsigned zsome = col & ~zall;
+        return zsome ? zall | cpml_plane_mask(cp, c0, zsome, k) : zall;
+    }
 };
-__device__ __forceinline__ CpmlCol cpml_col(const KCpml& cp, int c0, unsigned tile, int i, int j) {
+__device__ __forceinline__ CpmlCol cpml_col(const KCpml& cp, int c0, unsigned tile, int i, int j, int kb, int ke) {
     CpmlCol r;
     r.col = 0;
+    r.zall = 0;
 #pragma unroll
     for (int n = 0; n < 12; ++n) {
         const Slab& s = cp.s[c0 + (n >> 2)][(n >> 1) & 1][n & 1];
-        if (((tile >> n) & 1) && i >= s.xlo && i <= s.xhi && j >= s.ylo && j <= s.yhi) r.col |= 1u << n;
+        if (((tile >> n) & 1) && i >= s.xlo && i <= s.xhi && j >= s.ylo && j <= s.yhi) {
+            r.col |= 1u << n;
+            if (s.zlo <= kb && s.zhi >= ke) r.zall |= 1u << n;
+        }
     }
     const bool h = c0 != 0;
     r.bx = r.cx = r.by = r.cy = 0.0f;
@@ -140,9 +150,9 @@ __device__ __forceinline__ void efield_column(const KGrid& g, const KCpml& cp, c
     // threads on clamped rows store nothing, so their mask does not matter
     const int bx0 = i & ~31, by0 = j - (int)threadIdx.y;
     const unsigned tmask = CP ? cpml_tile_mask(cp, 0, bx0, bx0 + 31, by0, by0 + (int)blockDim.y - 1) : 0u;
-    const CpmlCol cc = CP ? cpml_col(cp, 0, tmask, i, j) : CpmlCol{};
+    const CpmlCol cc = CP ? cpml_col(cp, 0, tmask, i, j, kb, ke) : CpmlCol{};
     for (int k = kb; k <= ke; ++k, c += plane) {
-        const unsigned pm = CP ? cpml_plane_mask(cp, 0, cc.col, k) : 0u;
+        const unsigned pm = CP ? cc.live(cp, 0, k) : 0u;
         float bz = 0.0f, cz = 0.0f;
         if (CP && (pm & kCpmlZ)) {
             bz = cp.pbe[2][k];
@@ -229,9 +239,9 @@ __device__ __forceinline__ void hfield_column(const KGrid& g, const KCpml& cp, c
     float ex_k = __ldg(Ex + c), ey_k = __ldg(Ey + c);
     const int bx0 = i & ~31, by0 = j - (int)threadIdx.y;
     const unsigned tmask = CP ? cpml_tile_mask(cp, 3, bx0, bx0 + 31, by0, by0 + (int)blockDim.y - 1) : 0u;
-    const CpmlCol cc = CP ? cpml_col(cp, 3, tmask, i, j) : CpmlCol{};
+    const CpmlCol cc = CP ? cpml_col(cp, 3, tmask, i, j, kb, ke) : CpmlCol{};
     for (int k = kb; k <= ke; ++k, c += plane) {
-        const unsigned pm = CP ? cpml_plane_mask(cp, 3, cc.col, k) : 0u;
+        const unsigned pm = CP ? cc.live(cp, 3, k) : 0u;
         float bz = 0.0f, cz = 0.0f;
         if (CP && (pm & kCpmlZ)) {
             bz = cp.pbm[2][k];

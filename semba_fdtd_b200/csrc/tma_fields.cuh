@@ -183,12 +183,12 @@ __device__ __forceinline__ bool e_consume(const TmaCta& t, unsigned G0, const KG
     const float idyh = g.idyh[min(j, nya - 1)], idxh = g.idxh[i];
     const long long pitch = g.pitch, plane = g.plane;
     const unsigned tmask = CP ? cpml_tile_mask(cp, 0, t.ib, t.ib + kTX - 1, t.jb, t.jb + kTY - 1) : 0u;
-    const CpmlCol cc = CP ? cpml_col(cp, 0, tmask, i, j) : CpmlCol{};
+    const CpmlCol cc = CP ? cpml_col(cp, 0, tmask, i, j, t.kb, t.ke) : CpmlCol{};
     for (int k = t.kb; k <= t.ke; ++k) {
         const unsigned Gk = G0 + 1 + (unsigned)(k - t.kb), Gp = Gk - 1;
         const unsigned s = Gk % kStages, sp = Gp % kStages;
         // slabs holding cell (i, j, k), and the P_b / P_c pair indexed by k
-        const unsigned pm = CP ? cpml_plane_mask(cp, 0, cc.col, k) : 0u;
+        const unsigned pm = CP ? cc.live(cp, 0, k) : 0u;
         float bz = 0.0f, cz = 0.0f;
         if (CP && (pm & kCpmlZ)) {
             bz = cp.pbe[2][k];
@@ -265,12 +265,12 @@ __device__ __forceinline__ bool h_consume(const TmaCta& t, unsigned G0, const KG
     const float idye = g.idye[min(j, nya - 1)], idxe = g.idxe[i];
     const long long pitch = g.pitch, plane = g.plane;
     const unsigned tmask = CP ? cpml_tile_mask(cp, 3, t.ib, t.ib + kTX - 1, t.jb, t.jb + kTY - 1) : 0u;
-    const CpmlCol cc = CP ? cpml_col(cp, 3, tmask, i, j) : CpmlCol{};
+    const CpmlCol cc = CP ? cpml_col(cp, 3, tmask, i, j, t.kb, t.ke) : CpmlCol{};
     for (int k = t.kb; k <= t.ke; ++k) {
         const unsigned Gk = G0 + (unsigned)(k - t.kb), Gn = Gk + 1;
         const unsigned s = Gk % kStages, sn = Gn % kStages;
         // slabs holding cell (i, j, k), and the P_b / P_c pair indexed by k
-        const unsigned pm = CP ? cpml_plane_mask(cp, 3, cc.col, k) : 0u;
+        const unsigned pm = CP ? cc.live(cp, 3, k) : 0u;
         float bz = 0.0f, cz = 0.0f;
         if (CP && (pm & kCpmlZ)) {
             bz = cp.pbm[2][k];
