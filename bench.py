@@ -356,25 +356,32 @@ def run_batched(args):
     # batched arm
     with ClockSampler(local) as clk:
         t0 = time.perf_counter()
+        marks = {}
         with ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 1)) as pool:  # host set-up in parallel
             plans = list(pool.map(Plan, pbs))
+        marks["plan"] = time.perf_counter() - t0
         arena = int(sum(p.footprint for p in plans) * 1.05) + (64 << 20)
         with Batch(arena, len(pbs) + 1, kernel_family=args.batch_family) as b:
             slots = [b.add(p) for p in plans]
+            marks["add"] = time.perf_counter() - t0
             chunks, ctas = b.autotune(2)
             phases = b.profile(8)  # real steps, per-phase device time with every instance live
+            marks["tune"] = time.perf_counter() - t0
             dev_ms = 0.0
             while any(not b.done(x) for x in slots):
                 left = max(b.info(x)[1] - b.info(x)[0] for x in slots)
                 dev_ms += b.elapsed(min(256, max(32, left)))
+            marks["steps"] = time.perf_counter() - t0
             for x in slots:
                 b.probes(x)
+            marks["read"] = time.perf_counter() - t0
         t_batch = time.perf_counter() - t0
     line = {"metric": "solves/s", "value": len(pbs) / t_batch, "unit": "solves/s", "n_gpus": 1, "steps": None,
             "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "impl": "batched",
             "config": {"workload": CONFIGS["batched"][2], "instances": len(pbs), "cell_updates": work,
                        "arena_bytes": arena, "tuned_chunks": chunks, "tuned_ctas_per_sm": ctas,
+                       "batched_arm_marks_s": marks,
                        "field_kernels": "TMA-pipelined persistent" if args.batch_family == 1 else "register-marching"},
             "plain_one_at_a_time": {"solves_per_s": len(pbs) / t_plain if not args.skip_plain else None,
                                     "seconds": None if args.skip_plain else t_plain,

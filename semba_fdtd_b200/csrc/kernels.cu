@@ -214,9 +214,6 @@ __global__ void k_probes(KGrid g, KProbes p, StepRef sr, int first_n) {
 }
 
 __global__ void k_set_step(int* d, int v) { *d = v; }
-__global__ void k_fill16(int16_t* p, long long n, int16_t v) {
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) p[q] = v;
-}
 __global__ void k_add_step(int* d, int v) { *d += v; }
 
 __global__ void k_count_disp(const int16_t* M, const int16_t* slot, int pitch, long long plane, int x0, int x1, int y0,
@@ -509,17 +506,6 @@ void free_list(sgpu_ctx* c, std::vector<void*>& v) {
     v.clear();
 }
 
-cudaMemcpy3DParms copy_parms(sgpu_ctx* c, int comp, void* host, void* dev, size_t esz, bool up) {
-    const sgpu_lim& a = c->alloc[comp];
-    size_t ax = a.xe - a.xi + 1, ay = a.ye - a.yi + 1, az = a.ze - a.zi + 1;
-    cudaMemcpy3DParms p{};
-    cudaPitchedPtr hp = make_cudaPitchedPtr(host, ax * esz, ax * esz, ay);
-    cudaPitchedPtr dp = make_cudaPitchedPtr(dev, (size_t)c->pitch * esz, (size_t)c->nxa * esz, c->nya);
-    if (up) { p.srcPtr = hp; p.dstPtr = dp; p.kind = cudaMemcpyHostToDevice; }
-    else { p.srcPtr = dp; p.dstPtr = hp; p.kind = cudaMemcpyDeviceToHost; }
-    p.extent = make_cudaExtent(ax * esz, ay, az);
-    return p;
-}
 
 }  // namespace
 
@@ -689,34 +675,54 @@ sgpu_status sgpu_set_kernel_family(sgpu_ctx* c, int family) {
 sgpu_status sgpu_upload_media(sgpu_ctx* c, int comp, const int16_t* mi) {
     if (!c || !mi || comp < 0 || comp > 5) return set_error(c, SGPU_ERR_ARG, "bad media upload");
     const sgpu_lim& a = c->alloc[comp];
-    long long n = (long long)(a.xe - a.xi + 1) * (a.ye - a.yi + 1) * (a.ze - a.zi + 1);
-    for (long long q = 0; q < n; ++q)
-        if (mi[q] < 0 || mi[q] > c->num_media) return set_error(c, SGPU_ERR_ARG, "media index outside 0..num_media");
+    const long long ax = a.xe - a.xi + 1, ay = a.ye - a.yi + 1, az = a.ze - a.zi + 1;
+    const long long n = ax * ay * az;
+    int lo = 0x7fff, hi = 0;
+    for (long long q = 0; q < n; ++q) {
+        lo = std::min(lo, (int)mi[q]);
+        hi = std::max(hi, (int)mi[q]);
+    }
+    if (lo < 0 || hi > c->num_media) return set_error(c, SGPU_ERR_ARG, "media index outside 0..num_media");
+    // the padded device layout built on the host and sent in one copy; the
     // unused padding of the common box is vacuum
-    k_fill16<<<148 * 8, 256, 0, c->stream>>>(c->M[comp], c->vol, (int16_t)1);
-    sgpu_status fs = check_launch(c, "k_fill16");
-    if (fs) return fs;
-    cudaMemcpy3DParms p = copy_parms(c, comp, (void*)mi, c->M[comp], sizeof(int16_t), true);
-    CUDA_TRY(c, cudaMemcpy3DAsync(&p, c->stream));
+    std::vector<int16_t> buf((size_t)c->vol, (int16_t)1);
+    for (long long k = 0; k < az; ++k)
+        for (long long j = 0; j < ay; ++j)
+            std::memcpy(&buf[(size_t)(c->pitch * j + c->plane * k)], mi + ax * (j + ay * k), (size_t)ax * sizeof(int16_t));
+    CUDA_TRY(c, cudaMemcpyAsync(c->M[comp], buf.data(), buf.size() * sizeof(int16_t), cudaMemcpyHostToDevice, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     c->media_loaded[comp] = true;
     c->src_dirty = true;
     return SGPU_OK;
 }
 
+// Field copies go through a host image of the padded device array in one
+// contiguous transfer (a row-by-row copy of short rows is far slower).  The
+// padding outside a component's Alloc range is zero on the device and stays
+// zero.
 sgpu_status sgpu_upload_field(sgpu_ctx* c, int comp, const float* f) {
     if (!c || !f || comp < 0 || comp > 5) return set_error(c, SGPU_ERR_ARG, "bad field upload");
-    cudaMemcpy3DParms p = copy_parms(c, comp, (void*)f, c->F[comp], sizeof(float), true);
-    CUDA_TRY(c, cudaMemcpy3DAsync(&p, c->stream));
+    const sgpu_lim& a = c->alloc[comp];
+    const long long ax = a.xe - a.xi + 1, ay = a.ye - a.yi + 1, az = a.ze - a.zi + 1;
+    std::vector<float> buf((size_t)c->vol, 0.0f);
+    for (long long k = 0; k < az; ++k)
+        for (long long j = 0; j < ay; ++j)
+            std::memcpy(&buf[(size_t)(c->pitch * j + c->plane * k)], f + ax * (j + ay * k), (size_t)ax * sizeof(float));
+    CUDA_TRY(c, cudaMemcpyAsync(c->F[comp], buf.data(), buf.size() * sizeof(float), cudaMemcpyHostToDevice, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     return SGPU_OK;
 }
 
 sgpu_status sgpu_download_field(sgpu_ctx* c, int comp, float* f) {
     if (!c || !f || comp < 0 || comp > 5) return set_error(c, SGPU_ERR_ARG, "bad field download");
-    cudaMemcpy3DParms p = copy_parms(c, comp, f, c->F[comp], sizeof(float), false);
-    CUDA_TRY(c, cudaMemcpy3DAsync(&p, c->stream));
+    const sgpu_lim& a = c->alloc[comp];
+    const long long ax = a.xe - a.xi + 1, ay = a.ye - a.yi + 1, az = a.ze - a.zi + 1;
+    std::vector<float> buf((size_t)c->vol);
+    CUDA_TRY(c, cudaMemcpyAsync(buf.data(), c->F[comp], buf.size() * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    for (long long k = 0; k < az; ++k)
+        for (long long j = 0; j < ay; ++j)
+            std::memcpy(f + ax * (j + ay * k), &buf[(size_t)(c->pitch * j + c->plane * k)], (size_t)ax * sizeof(float));
     return SGPU_OK;
 }
 
@@ -896,18 +902,22 @@ sgpu_status build_sources(sgpu_ctx* c) {
     for (int side = 0; side < 2; ++side) {
         free_list(c, c->src_allocs[side]);
         c->src[side] = KSrc{};
-        std::vector<sgpu_ctx::HostEntry> es = c->src_host[side];
+        const std::vector<sgpu_ctx::HostEntry>& es = c->src_host[side];
         if (es.empty()) continue;
-        // group by (component, node) keeping the reference order inside a group
-        std::stable_sort(es.begin(), es.end(), [](const sgpu_ctx::HostEntry& a, const sgpu_ctx::HostEntry& b) {
-            if (a.comp != b.comp) return a.comp < b.comp;
-            if (a.node != b.node) return a.node < b.node;
-            return a.order < b.order;
-        });
+        if (es.size() >= (1u << 30)) return set_error(c, SGPU_ERR_UNSUPPORTED, "too many source contributions");
+        // group by (component, node) keeping the reference order inside a
+        // group: entries are stored in that order, so sorting the keys
+        // (component, node, position) is a stable grouping
+        std::vector<uint64_t> key(es.size());
+        for (size_t q = 0; q < es.size(); ++q)
+            key[q] = (((uint64_t)es[q].comp * (uint64_t)c->vol + (uint64_t)es[q].node) << 30) | (uint64_t)q;
+        std::sort(key.begin(), key.end());
         std::vector<int> rnode, rcomp, rptr;
         std::vector<SrcEntry> ent;
-        for (size_t q = 0; q < es.size(); ++q) {
-            if (q == 0 || es[q].node != es[q - 1].node || es[q].comp != es[q - 1].comp) {
+        ent.reserve(es.size());
+        for (size_t r = 0; r < key.size(); ++r) {
+            const size_t q = (size_t)(key[r] & ((1u << 30) - 1));
+            if (r == 0 || (key[r] >> 30) != (key[r - 1] >> 30)) {
                 rnode.push_back((int)es[q].node);
                 rcomp.push_back(es[q].comp);
                 rptr.push_back((int)ent.size());
