@@ -153,6 +153,23 @@ typedef struct {
 } sgpu_nodal_desc;
 sgpu_status sgpu_add_nodal(sgpu_ctx* ctx, const sgpu_nodal_desc* d);
 
+/* Borders other than CPML.  Face order back, front, left, right, down, up
+ * (sgg%Border, fdetypes.F90:468-497).  A PEC face needs no call: it is medium
+ * 0 in the media matrices (healer.F90:1442-1617).
+ *   pmc[f], periodic[f]: InitOtherBorders (bordersother.F90:36-58); the H
+ *     outside the face is cloned by sgpu_advance_pmc_h / _periodic_h.
+ *   mur[f]: InitMURBorders (bordersmur.F90:79-314) -- a Mur face, or a CPML
+ *     face under -mur1/-mur2; mur_cab1[f] is CAB1 of calc_murconstants
+ *     (bordersmur.F90:316-363), num_media+1 values.  The Past_ layers start
+ *     at zero (a fresh start). */
+typedef struct {
+    int pmc[6];
+    int periodic[6];
+    int mur[6];
+    const float* mur_cab1[6];
+} sgpu_border_desc;
+sgpu_status sgpu_init_borders(sgpu_ctx* ctx, const sgpu_border_desc* d);
+
 /* crea_timevector (timestepping.F90:3230-3240): tiempo(n0 .. n0+count-1). */
 sgpu_status sgpu_set_time(sgpu_ctx* ctx, int n0, int count, const double* tiempo);
 
@@ -165,7 +182,10 @@ sgpu_status sgpu_set_probes(sgpu_ctx* ctx, int nprobes, const int* comp_ijk, int
  * *first_n the step index n of the first row. */
 sgpu_status sgpu_read_probes(sgpu_ctx* ctx, float* out, int max_steps, int* nsteps, int* first_n);
 
-/* One call per reference routine, in the order of timestepping.F90:1286-1742. */
+/* One call per reference routine, in the order of timestepping.F90:1286-1742
+ * (the border calls: after the magnetic CPML and again after the H sources
+ * for PMC/periodic, timestepping.F90:1568-1573 and :1636-1641; Mur before the
+ * observation, :1711-1712). */
 sgpu_status sgpu_advance_ex(sgpu_ctx* ctx);                 /* Advance_Ex :2165 */
 sgpu_status sgpu_advance_ey(sgpu_ctx* ctx);                 /* Advance_Ey :2206 */
 sgpu_status sgpu_advance_ez(sgpu_ctx* ctx);                 /* Advance_Ez :2250 */
@@ -179,10 +199,15 @@ sgpu_status sgpu_advance_hz(sgpu_ctx* ctx);                 /* Advance_Hz :2374 
 sgpu_status sgpu_advance_magnetic_cpml(sgpu_ctx* ctx);      /* borderscpml.F90:881 */
 sgpu_status sgpu_advance_planewave_h(sgpu_ctx* ctx, int n); /* planewaves.F90:1180 */
 sgpu_status sgpu_advance_nodal_h(sgpu_ctx* ctx, int n);     /* nodalsources.F90:584 */
+sgpu_status sgpu_advance_pmc_h(sgpu_ctx* ctx);              /* MinusCloneMagneticPMC, bordersother.F90:65 */
+sgpu_status sgpu_advance_periodic_h(sgpu_ctx* ctx);         /* CloneMagneticPeriodic, bordersother.F90:146 */
+sgpu_status sgpu_advance_magnetic_mur(sgpu_ctx* ctx);       /* AdvanceMagneticMUR, bordersmur.F90:502 */
 sgpu_status sgpu_update_observation(sgpu_ctx* ctx, int n);  /* observation.F90:2540 */
 
 /* Fused forms, same results bit for bit: the E half step (curl + CPML +
- * ADE + TF/SF + nodal), the H half step (curl + CPML + TF/SF + nodal), and
+ * ADE + TF/SF + nodal), the H half step (curl + CPML + TF/SF + nodal +
+ * PMC/periodic clones + Mur; the clones before the H sources are left out
+ * because nothing between the two clone calls reads the cloned layers), and
  * `count` whole steps n0 .. n0+count-1 including the probe gather, captured
  * into a CUDA graph and replayed. */
 sgpu_status sgpu_advance_e(sgpu_ctx* ctx, int n);
@@ -205,7 +230,7 @@ sgpu_status sgpu_check_finite(sgpu_ctx* ctx);
 sgpu_status sgpu_elapsed_steps(sgpu_ctx* ctx, int n0, int count, float* ms);
 /* `count` steps launched directly with CUDA events between the phases;
  * ms6 accumulates the device time of: E curl+CPML, ADE, E sources,
- * H curl+CPML, H sources, probe gather. */
+ * H curl+CPML, H sources and borders (clones, Mur), probe gather. */
 sgpu_status sgpu_profile_steps(sgpu_ctx* ctx, int n0, int count, float* ms6);
 /* Algorithmic bytes of one launch of each phase of sgpu_profile_steps:
  * compulsory field/media/psi/ADE-state traffic, without neighbour re-reads
@@ -285,7 +310,7 @@ typedef struct {
     double dt;          /* general%dt */
     int forcecfl;       /* the -cfl switch */
     float cfl;
-    int pml_layers[6];  /* back, front, left, right, down, up; all >= 1 */
+    int pml_layers[6];  /* back, front, left, right, down, up; >= 1 on CPML faces */
     float pml_order[6];
     float pml_refl[6];
     float alphamax, alphaorder, kappamax;   /* -pmlalpha, -pmlkappa */
@@ -298,6 +323,11 @@ typedef struct {
     int nprobes;
     const int* probes;  /* 4*nprobes: comp, i, j, k */
     int probe_capacity; /* rows of the device probe ring */
+    /* Border kind per face, the tipofrontera codes of nfde_types.F90:67-71:
+     * 1 PEC, 2 PMC, 4 periodic, 7 first-order Mur, 9 CPML; 0 reads as 9.
+     * Only CPML faces have layers (pml_* of other faces are ignored). */
+    int border[6];
+    int mur_after_pml;  /* -mur1 / -mur2: first-order Mur on every CPML face too */
 } sgpu_problem;
 
 /* Restated set-up of semba_fdtd.F90:1197-1300 and timestepping.F90:305-1014
@@ -320,6 +350,9 @@ sgpu_status sgpu_host_get_g(const sgpu_ctx* ctx, float* g1, float* g2, float* gm
 /* which as for the oracle: 0..5 Idxe..Idzh, 6..17 P_be, P_ce, P_bm, P_cm. */
 sgpu_status sgpu_host_get_metric(const sgpu_ctx* ctx, int which, float* out, int* lo, int* hi);
 sgpu_status sgpu_host_get_media(const sgpu_ctx* ctx, int comp, int16_t* out);
+/* CAB1 of calc_murconstants for face f (back, front, left, right, down, up),
+ * num_media+1 values; SGPU_ERR_ARG when the face has no Mur condition. */
+sgpu_status sgpu_host_get_mur_cab1(const sgpu_ctx* ctx, int face, float* out);
 
 /* ------------------------------------------------------------------------
  * Batched form (no counterpart in the reference, which runs one problem per
@@ -378,7 +411,8 @@ sgpu_status sgpu_batch_get_tuning(const sgpu_batch* b, int* chunk3, int* ctas_pe
  * present) and keeps the fastest.  The trials advance the instances. */
 sgpu_status sgpu_batch_autotune(sgpu_batch* b, int steps_per_trial, int* chunk3, int* ctas_per_sm);
 /* Device time of each phase summed over nsteps real steps launched one by
- * one: E field + CPML, ADE, E sources, H field + CPML, H sources, probes. */
+ * one: E field + CPML, ADE, E sources, H field + CPML, H sources and
+ * borders, probes. */
 sgpu_status sgpu_batch_profile_steps(sgpu_batch* b, int nsteps, float* ms6);
 /* The batch step counter (steps queued so far). */
 sgpu_status sgpu_batch_steps(const sgpu_batch* b, int* counter);

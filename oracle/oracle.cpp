@@ -156,6 +156,16 @@ template <class R> struct Sim {
     A1<R> P_ce_x, P_ce_y, P_ce_z, P_be_x, P_be_y, P_be_z, P_cm_x, P_cm_y, P_cm_z, P_bm_x, P_bm_y, P_bm_z;
     // psi arrays: [region][which] where which is the reference's member order
     A3<R> psiLR[2][4], psiDU[2][4], psiBF[2][4];
+    // border kinds per [axis][side] (sgg%Border, fdetypes.F90:468-497)
+    bool isPML[3][2] = {}, isPEC[3][2] = {}, isPMC[3][2] = {}, isPer[3][2] = {}, isMur[3][2] = {};
+    // Mur (bordersmur.F90:36-70): MURc limits per H component and region,
+    // the Past_ layers of regLR (Hx, Hz), regDU (Hy, Hx), regBF (Hz, Hy) and
+    // CAB1 per region and medium.  PastPast_ is read only by the second-order
+    // branch, which stops with an error (bordersmur.F90:525), so it is not kept.
+    bool anyMur = false;
+    Lim MURc[6][6];
+    A3<R> pastLR[2][2], pastDU[2][2], pastBF[2][2];
+    std::vector<R> CAB1[6];
     // ADE
     std::vector<EDispMedium<R>> dut;
     // plane waves
@@ -184,11 +194,20 @@ template <class R> void setup_grid(Sim<R>& s, const orc_problem* p) {
     // face order back, front, left, right, down, up -> [axis][side]
     const int fa[6] = {0, 0, 1, 1, 2, 2}, fs[6] = {0, 1, 0, 1, 0, 1};
     for (int f = 0; f < 6; ++f) {
-        s.L[fa[f]][fs[f]] = p->pml_layers[f];
-        float rf = p->pml_refl[f];
+        // preprocess_geom.F90:5398-5600: the border flags; only CPML faces
+        // carry layers, order and reflection (sgg%PML starts zeroed)
+        const int kind = p->border[f] == 0 ? 9 : p->border[f];
+        const int a = fa[f], sd = fs[f];
+        s.isPML[a][sd] = kind == 9;
+        s.isPEC[a][sd] = kind == 1;
+        s.isPMC[a][sd] = kind == 2;
+        s.isPer[a][sd] = kind == 4;
+        s.isMur[a][sd] = kind == 7 || (kind == 9 && p->mur_after_pml);
+        s.L[a][sd] = s.isPML[a][sd] ? p->pml_layers[f] : 0;
+        float rf = s.isPML[a][sd] ? p->pml_refl[f] : 0.0f;
         if (rf >= 1.0f) rf = (float)0.99999;  // preprocess_geom.F90:5447
-        s.refl[fa[f]][fs[f]] = (R)rf;
-        s.order[fa[f]][fs[f]] = (R)p->pml_order[f];
+        s.refl[a][sd] = (R)rf;
+        s.order[a][sd] = s.isPML[a][sd] ? (R)p->pml_order[f] : (R)0;
     }
     s.alphamax = (R)p->alphamax; s.alphaorder = (R)p->alphaorder; s.kappamax = (R)p->kappamax;
     int mx2 = s.nx, my2 = s.ny, mz2 = s.nz;
@@ -352,6 +371,21 @@ template <class R> void create_pml_matrix(Sim<R>& s) {
                     }
                 }
     s.NumMedia = nuevo;
+    // PEC borders, healer.F90:1442-1617: medium 0 on the boundary plane of
+    // the components tangential to it (E) and normal to it (H)
+    for (int f = 0; f < 6; ++f) {
+        const bool elec = f < 3;
+        const int ca = f % 3;  // the component's own axis
+        for (int a = 0; a < 3; ++a)
+            for (int sd = 0; sd < 2; ++sd) {
+                if (!s.isPEC[a][sd] || (elec ? a == ca : a != ca)) continue;
+                int lo[3] = {XIP[f], YIP[f], ZIP[f]}, hi[3] = {XEP[f], YEP[f], ZEP[f]};
+                lo[a] = hi[a] = sd == 0 ? lo[a] : hi[a];
+                for (int k = lo[2]; k <= hi[2]; ++k)
+                    for (int j = lo[1]; j <= hi[1]; ++j)
+                        for (int i = lo[0]; i <= hi[0]; ++i) s.mi[f](i, j, k) = 0;
+            }
+    }
 }
 
 // Media table and matrices of read_geomData (preprocess_geom.F90:421-760,
@@ -513,9 +547,15 @@ template <class R> void setup_cpml(Sim<R>& s) {
             }
         }
     };
-    depth(s.ce_x, s.Ice_x, s.cm_x, s.Icm_x, s.Alloc[iHx].XI, s.Alloc[iHx].XE, s.SINPML[iHx].XI, s.SINPML[iHx].XE, s.L[0][0], s.L[0][1]);
-    depth(s.ce_y, s.Ice_y, s.cm_y, s.Icm_y, s.Alloc[iHy].YI, s.Alloc[iHy].YE, s.SINPML[iHy].YI, s.SINPML[iHy].YE, s.L[1][0], s.L[1][1]);
-    depth(s.ce_z, s.Ice_z, s.cm_z, s.Icm_z, s.Alloc[iHz].ZI, s.Alloc[iHz].ZE, s.SINPML[iHz].ZI, s.SINPML[iHz].ZE, s.L[2][0], s.L[2][1]);
+    // without a CPML face InitCPMLBorders returns before the depth vectors
+    // and calc_cpmlconstants (borderscpml.F90:140-143)
+    bool anyPML = false;
+    for (int a = 0; a < 3; ++a) anyPML = anyPML || s.isPML[a][0] || s.isPML[a][1];
+    if (anyPML) {
+        depth(s.ce_x, s.Ice_x, s.cm_x, s.Icm_x, s.Alloc[iHx].XI, s.Alloc[iHx].XE, s.SINPML[iHx].XI, s.SINPML[iHx].XE, s.L[0][0], s.L[0][1]);
+        depth(s.ce_y, s.Ice_y, s.cm_y, s.Icm_y, s.Alloc[iHy].YI, s.Alloc[iHy].YE, s.SINPML[iHy].YI, s.SINPML[iHy].YE, s.L[1][0], s.L[1][1]);
+        depth(s.ce_z, s.Ice_z, s.cm_z, s.Icm_z, s.Alloc[iHz].ZI, s.Alloc[iHz].ZE, s.SINPML[iHz].ZI, s.SINPML[iHz].ZE, s.L[2][0], s.L[2][1]);
+    }
 
     // calc_cpmlconstants
     R sig_max[3][2], aPar_max[3][2], kPar_max[3][2];
@@ -569,6 +609,9 @@ template <class R> void setup_cpml(Sim<R>& s) {
         Pce = (sigmae * (Pbe - (R)1.0) / (sigmae + kpare * apare) / kpare) / dh;
         Id = (R)1.0 / (kpare * dh);
     };
+    // faces without CPML keep order 0 and kPar_max 1, so the inverse steps of
+    // their outer nodes come out unchanged (their P_b/P_c are never read)
+    if (anyPML) {
     for (int i = s.Alloc[iEx].XI; i <= s.Alloc[iEx].XE; ++i) {
         if (i <= s.SINPML[iHx].XI - 1) eco(0, 0, s.ce_x(i), s.Ice_x(i), s.dxh(i), s.P_be_x(i), s.P_ce_x(i), s.Idxh(i));
         else if (i >= s.SINPML[iHx].XE + 1) eco(0, 1, s.ce_x(i), s.Ice_x(i), s.dxh(i), s.P_be_x(i), s.P_ce_x(i), s.Idxh(i));
@@ -594,6 +637,7 @@ template <class R> void setup_cpml(Sim<R>& s) {
         if (k <= s.SINPML[iHz].ZI - 1) eco(2, 0, s.cm_z(k), s.Icm_z(k), s.dze(k), s.P_bm_z(k), s.P_cm_z(k), s.Idze(k));
         else if (k >= s.SINPML[iHz].ZE) eco(2, 1, s.cm_z(k), s.Icm_z(k), s.dze(k), s.P_bm_z(k), s.P_cm_z(k), s.Idze(k));
     }
+    }  // anyPML
     // absent faces are faked empty (borderscpml.F90:307-314); every face is a
     // PML face here only when its layer count is non-zero.
     const int face_axis_side[6][2] = {{2, 0}, {2, 1}, {1, 0}, {1, 1}, {0, 0}, {0, 1}};
@@ -611,6 +655,46 @@ template <class R> void setup_cpml(Sim<R>& s) {
         reg = Back + r;
         s.psiBF[r][0].alloc(box(iEz, reg), 0); s.psiBF[r][1].alloc(box(iEy, reg), 0);
         s.psiBF[r][2].alloc(box(iHz, reg), 0); s.psiBF[r][3].alloc(box(iHy, reg), 0);
+    }
+}
+
+// Region (Down..Front) -> [axis][side].
+const int kRegAxis[6] = {2, 2, 1, 1, 0, 0}, kRegSide[6] = {0, 1, 0, 1, 0, 1};
+
+// InitMURBorders and calc_murconstants, bordersmur.F90:79-363 (fresh start:
+// the Past_ layers start at zero).
+template <class R> void setup_mur(Sim<R>& s) {
+    s.anyMur = false;
+    for (int a = 0; a < 3; ++a) s.anyMur = s.anyMur || s.isMur[a][0] || s.isMur[a][1];
+    if (!s.anyMur) return;
+    // two planes per region: the outer H layer and the first swept one
+    for (int f = iHx; f <= iHz; ++f) {
+        const Lim& w = s.Sweep[f];
+        s.MURc[f][Down] = Lim{w.XI, w.XE, w.YI, w.YE, w.ZI - 1, w.ZI};
+        s.MURc[f][Up] = Lim{w.XI, w.XE, w.YI, w.YE, w.ZE, w.ZE + 1};
+        s.MURc[f][Left] = Lim{w.XI, w.XE, w.YI - 1, w.YI, w.ZI, w.ZE};
+        s.MURc[f][Right] = Lim{w.XI, w.XE, w.YE, w.YE + 1, w.ZI, w.ZE};
+        s.MURc[f][Back] = Lim{w.XI - 1, w.XI, w.YI, w.YE, w.ZI, w.ZE};
+        s.MURc[f][Front] = Lim{w.XE, w.XE + 1, w.YI, w.YE, w.ZI, w.ZE};
+        for (int r = 0; r < 6; ++r)  // bordersmur.F90:163-170
+            if (!s.isMur[kRegAxis[r]][kRegSide[r]]) s.MURc[f][r].ZI = s.MURc[f][r].ZE + 100;
+    }
+    for (int r = 0; r < 2; ++r) {
+        s.pastLR[r][0].alloc(s.MURc[iHx][Left + r], (R)0); s.pastLR[r][1].alloc(s.MURc[iHz][Left + r], (R)0);
+        s.pastDU[r][0].alloc(s.MURc[iHy][Down + r], (R)0); s.pastDU[r][1].alloc(s.MURc[iHx][Down + r], (R)0);
+        s.pastBF[r][0].alloc(s.MURc[iHz][Back + r], (R)0); s.pastBF[r][1].alloc(s.MURc[iHy][Back + r], (R)0);
+    }
+    // cnum = (1/Id(outer node)) / (dt * cluz / sqrt(Epr*Mur)): RKIND operands,
+    // the real(8) dt promotes the denominator, the quotient is stored in RKIND
+    const R idh[6] = {s.Idzh(s.Alloc[iEz].ZI), s.Idzh(s.Alloc[iEz].ZE), s.Idyh(s.Alloc[iEy].YI),
+                      s.Idyh(s.Alloc[iEy].YE), s.Idxh(s.Alloc[iEx].XI), s.Idxh(s.Alloc[iEx].XE)};
+    for (int r = 0; r < 6; ++r) {
+        s.CAB1[r].assign(s.NumMedia + 1, (R)0);
+        for (int m = 0; m <= s.NumMedia; ++m) {
+            const R den = std::sqrt(s.med[m].Epr * s.med[m].Mur);
+            const R cnum = (R)((double)((R)1.0 / idh[r]) / ((s.dt * (double)s.cluz) / (double)den));
+            s.CAB1[r][m] = ((R)1.0 - cnum) / ((R)1.0 + cnum);
+        }
     }
 }
 
@@ -1211,6 +1295,92 @@ template <class R> void advance_nodal(Sim<R>& s, int n, bool elec) {
     }
 }
 
+// One whole-plane assignment F(plane dst) = +-F(plane src) along `axis`,
+// over the full Alloc extent of the other two axes.
+template <class R> void plane_copy(A3<R>& F, int axis, int dst, int src, bool negate) {
+    const Lim& b = F.b;
+    int lo[3] = {b.XI, b.YI, b.ZI}, hi[3] = {b.XE, b.YE, b.ZE};
+    lo[axis] = hi[axis] = dst;
+    const int sh = src - dst;
+    for (int k = lo[2]; k <= hi[2]; ++k)
+        for (int j = lo[1]; j <= hi[1]; ++j)
+            for (int i = lo[0]; i <= hi[0]; ++i) {
+                const R v = F(i + (axis == 0 ? sh : 0), j + (axis == 1 ? sh : 0), k + (axis == 2 ? sh : 0));
+                F(i, j, k) = negate ? -v : v;
+            }
+}
+
+// The twelve (component, face) assignments of MinusCloneMagneticPMC and
+// CloneMagneticPeriodic in their order: Hx down/up/left/right, Hy back/front/
+// down/up, Hz back/front/left/right (bordersother.F90:82-135, 157-189).
+const int kCloneOps[12][3] = {{iHx, 2, 0}, {iHx, 2, 1}, {iHx, 1, 0}, {iHx, 1, 1}, {iHy, 0, 0}, {iHy, 0, 1},
+                              {iHy, 2, 0}, {iHy, 2, 1}, {iHz, 0, 0}, {iHz, 0, 1}, {iHz, 1, 0}, {iHz, 1, 1}};
+
+// MinusCloneMagneticPMC, bordersother.F90:65-140: the H outside a PMC face
+// is minus the first swept H (image theory); one layout, so the z faces
+// always apply.
+template <class R> void clone_pmc(Sim<R>& s) {
+    for (const auto& op : kCloneOps) {
+        const int f = op[0], a = op[1], sd = op[2];
+        if (!s.isPMC[a][sd]) continue;
+        const Lim& c = s.Sweep[f];
+        const int lo = a == 0 ? c.XI : (a == 1 ? c.YI : c.ZI), hi = a == 0 ? c.XE : (a == 1 ? c.YE : c.ZE);
+        if (sd == 0) plane_copy(s.F[f], a, lo - 1, lo, true);
+        else plane_copy(s.F[f], a, hi + 1, hi, true);
+    }
+}
+
+// CloneMagneticPeriodic, bordersother.F90:146-190: the H outside a periodic
+// face is the swept H at the opposite end.
+template <class R> void clone_periodic(Sim<R>& s) {
+    for (const auto& op : kCloneOps) {
+        const int f = op[0], a = op[1], sd = op[2];
+        if (!s.isPer[a][sd]) continue;
+        const Lim& c = s.Sweep[f];
+        const int lo = a == 0 ? c.XI : (a == 1 ? c.YI : c.ZI), hi = a == 0 ? c.XE : (a == 1 ? c.YE : c.ZE);
+        if (sd == 0) plane_copy(s.F[f], a, lo - 1, hi, false);
+        else plane_copy(s.F[f], a, hi + 1, lo, false);
+    }
+}
+
+// AdvanceMagneticMUR, first order (bordersmur.F90:1129-1383), then the
+// storage of the Past_ layers (:1396-1650):
+//   H(outer) = Past(inner) + CAB1(medium of the inner node) * (H(inner) - Past(outer))
+template <class R> void advance_mur(Sim<R>& s) {
+    if (!s.anyMur) return;
+    struct Part { int reg, comp; A3<R>* past; };
+    const Part parts[12] = {{Left, iHx, &s.pastLR[0][0]},  {Left, iHz, &s.pastLR[0][1]},  {Right, iHx, &s.pastLR[1][0]},
+                            {Right, iHz, &s.pastLR[1][1]}, {Down, iHy, &s.pastDU[0][0]},  {Down, iHx, &s.pastDU[0][1]},
+                            {Up, iHy, &s.pastDU[1][0]},    {Up, iHx, &s.pastDU[1][1]},    {Back, iHz, &s.pastBF[0][0]},
+                            {Back, iHy, &s.pastBF[0][1]},  {Front, iHz, &s.pastBF[1][0]}, {Front, iHy, &s.pastBF[1][1]}};
+    for (const Part& p : parts) {
+        const int a = kRegAxis[p.reg], side = kRegSide[p.reg];
+        if (!s.isMur[a][side]) continue;
+        const Lim& b = s.MURc[p.comp][p.reg];
+        int lo[3] = {b.XI, b.YI, b.ZI}, hi[3] = {b.XE, b.YE, b.ZE};
+        const int outer = side == 0 ? lo[a] : hi[a], d = side == 0 ? 1 : -1;
+        lo[a] = hi[a] = outer;
+        A3<R>& H = s.F[p.comp];
+        A3<R>& P = *p.past;
+        const std::vector<R>& cab = s.CAB1[p.reg];
+        for (int k = lo[2]; k <= hi[2]; ++k)
+            for (int j = lo[1]; j <= hi[1]; ++j)
+                for (int i = lo[0]; i <= hi[0]; ++i) {
+                    const int ii = i + (a == 0 ? d : 0), jj = j + (a == 1 ? d : 0), kk = k + (a == 2 ? d : 0);
+                    const int medio = s.mi[p.comp](ii, jj, kk);
+                    H(i, j, k) = P(ii, jj, kk) + cab[medio] * (H(ii, jj, kk) - P(i, j, k));
+                }
+    }
+    for (const Part& p : parts) {
+        if (!s.isMur[kRegAxis[p.reg]][kRegSide[p.reg]]) continue;
+        const Lim& b = s.MURc[p.comp][p.reg];
+        for (int k = b.ZI; k <= b.ZE; ++k)
+            for (int j = b.YI; j <= b.YE; ++j)
+                for (int i = b.XI; i <= b.XE; ++i) (*p.past)(i, j, k) = s.F[p.comp](i, j, k);
+    }
+}
+
+// The loop body of timestepping.F90:1286-1712 for the routines of this path.
 template <class R> void one_step(Sim<R>& s, int n) {
     advance_e(s);
     advance_cpml_e(s);
@@ -1219,15 +1389,23 @@ template <class R> void one_step(Sim<R>& s, int n) {
     advance_nodal(s, n, true);
     advance_h(s);
     advance_cpml_h(s);
+    clone_pmc(s);
+    clone_periodic(s);
     advance_pw_h(s, n);
     advance_nodal(s, n, false);
+    clone_pmc(s);
+    clone_periodic(s);
+    advance_mur(s);
 }
 
 template <class R> int create(const orc_problem* p, Sim<R>** out) {
     Sim<R>* s = new (std::nothrow) Sim<R>();
     if (!s) return 2;
-    for (int f = 0; f < 6; ++f)
-        if (p->pml_layers[f] < 1) { delete s; return 3; }
+    for (int f = 0; f < 6; ++f) {
+        const int kind = p->border[f] == 0 ? 9 : p->border[f];
+        if (kind != 1 && kind != 2 && kind != 4 && kind != 7 && kind != 9) { delete s; return 3; }
+        if (kind == 9 && p->pml_layers[f] < 1) { delete s; return 3; }
+    }
     setup_grid(*s, p);
     setup_dt(*s, p);
     setup_media(*s, p);
@@ -1235,6 +1413,7 @@ template <class R> int create(const orc_problem* p, Sim<R>** out) {
     for (int f = 0; f < 6; ++f) s->F[f].alloc(s->Alloc[f], (R)0);
     setup_metrics(*s);
     setup_cpml(*s);
+    setup_mur(*s);
     setup_edisp(*s, p);
     setup_planewave(*s, p);
     setup_nodal(*s, p);
@@ -1422,6 +1601,20 @@ int orc_get_metric(void* hv, int which, float* out) {
         std::memcpy(out, a->v.data(), a->v.size() * sizeof(float));
     }
     return 0;
+}
+
+int orc_get_mur_cab1(void* hv, int face, float* out) {
+    Handle* h = (Handle*)hv;
+    if (face < 0 || face > 5) return 1;
+    // face order back, front, left, right, down, up -> region Back..Up
+    const int reg[6] = {Back, Front, Left, Right, Down, Up};
+    auto get = [&](auto& s) {
+        const int r = reg[face];
+        if (!s.isMur[kRegAxis[r]][kRegSide[r]]) return 1;
+        for (size_t m = 0; m < s.CAB1[r].size(); ++m) out[m] = (float)s.CAB1[r][m];
+        return 0;
+    };
+    return h->fp64 ? get(*h->sd) : get(*h->sf);
 }
 
 int orc_get_edisp(void* hv, int m, int* medium_index, int* npoles, double* kappa, double* beta, double* g3) {

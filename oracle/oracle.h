@@ -16,6 +16,9 @@
  *   - metric arrays                             (timestepping.F90:314-370)
  *   - CPML                                      (borderscpml.F90:90-473, 584-1176,
  *                                                1465-1733)
+ *   - PEC, PMC, periodic and first-order Mur    (healer.F90:1442-1617,
+ *     borders                                    bordersother.F90:65-190,
+ *                                                bordersmur.F90:79-363, 502-1653)
  *   - electric pole-residue ADE                 (electricdispersive.F90:77-362)
  *   - plane-wave TF/SF                          (planewaves.F90:72-853, 878-1510)
  *   - nodal sources                             (nodalsources.F90:76-583)
@@ -77,7 +80,8 @@ typedef struct {
     int forcecfl;                    /* -cfl switch given             */
     float cfl;
     /* face order of the reference: back(x-), front(x+), left(y-), right(y+),
-     * down(z-), up(z+).  All faces are CPML; layers must be >= 1. */
+     * down(z-), up(z+).  Layers of a CPML face must be >= 1; other faces have
+     * none and their pml_* entries are ignored. */
     int pml_layers[6];
     float pml_order[6];
     float pml_refl[6];
@@ -90,6 +94,10 @@ typedef struct {
     const orc_nodal* nodal;
     int nprobes;
     const int* probes;               /* 4*nprobes: comp(0..5 = Ex..Hz), i, j, k */
+    /* Border kind per face, the tipofrontera codes of nfde_types.F90:67-71:
+     * 1 PEC, 2 PMC, 4 periodic, 7 first-order Mur, 9 CPML (0 reads as 9). */
+    int border[6];
+    int mur_after_pml;               /* -mur1/-mur2: Mur also on every CPML face */
 } orc_problem;
 
 /* Extents of one component (sgg%Alloc, sgg%Sweep) in the reference's
@@ -127,6 +135,10 @@ int orc_get_metric_range(void* h, int which, int* lo, int* hi);
 int orc_get_edisp(void* h, int m, int* medium_index, int* npoles, double* kappa,
                   double* beta, double* g3);
 double orc_get_time(void* h, int n);
+/* CAB1 of calc_murconstants (bordersmur.F90:316-363) for face f (back, front,
+ * left, right, down, up), num_media+1 values; returns 1 when the face has no
+ * Mur condition. */
+int orc_get_mur_cab1(void* h, int face, float* out);
 
 #ifdef __cplusplus
 }

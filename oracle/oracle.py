@@ -51,7 +51,8 @@ class OrcProblem(C.Structure):
                 ("nregions", C.c_int), ("regions", C.POINTER(OrcRegion)),
                 ("npw", C.c_int), ("pw", C.POINTER(OrcPW)),
                 ("nnodal", C.c_int), ("nodal", C.POINTER(OrcNodal)),
-                ("nprobes", C.c_int), ("probes", C.POINTER(C.c_int))]
+                ("nprobes", C.c_int), ("probes", C.POINTER(C.c_int)),
+                ("border", C.c_int * 6), ("mur_after_pml", C.c_int)]
 
 
 _lib = None
@@ -90,6 +91,7 @@ def load():
         lib.orc_get_metric.argtypes = [vp, C.c_int, C.POINTER(C.c_float)]
         lib.orc_get_metric_range.argtypes = [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         lib.orc_get_edisp.argtypes = [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)] + [C.POINTER(C.c_double)] * 3
+        lib.orc_get_mur_cab1.argtypes = [vp, C.c_int, C.POINTER(C.c_float)]
         _lib = lib
     return _lib
 
@@ -146,6 +148,9 @@ def _problem(pb):
     p.nnodal, p.nodal = len(pb.nodals), nds
     p.nprobes = len(pb.probes)
     p.probes = i32(np.asarray(pb.probes).reshape(-1))
+    for f, code in enumerate(pb.border_codes):
+        p.border[f] = code
+    p.mur_after_pml = int(pb.mur_after_pml)
     return p, keep
 
 
@@ -228,3 +233,10 @@ class Oracle:
 
     def time(self, n: int) -> float:
         return self.lib.orc_get_time(self._h, n)
+
+    def mur_cab1(self, face: int):
+        """CAB1 per medium of a Mur face (back, front, left, right, down, up),
+        or None when the face has no Mur condition."""
+        out = np.empty(self.num_media + 1, np.float32)
+        rc = self.lib.orc_get_mur_cab1(self._h, face, out.ctypes.data_as(C.POINTER(C.c_float)))
+        return None if rc else out

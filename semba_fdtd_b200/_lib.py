@@ -51,7 +51,8 @@ class ProblemDesc(C.Structure):
                 ("nregions", C.c_int), ("regions", C.POINTER(Region)),
                 ("npw", C.c_int), ("pw", C.POINTER(PlaneWaveSrc)),
                 ("nnodal", C.c_int), ("nodal", C.POINTER(NodalSrc)),
-                ("nprobes", C.c_int), ("probes", c_int_p), ("probe_capacity", C.c_int)]
+                ("nprobes", C.c_int), ("probes", c_int_p), ("probe_capacity", C.c_int),
+                ("border", C.c_int * 6), ("mur_after_pml", C.c_int)]
 
 
 class GridDesc(C.Structure):
@@ -124,6 +125,7 @@ def _declare(lib: C.CDLL) -> None:
         "sgpu_host_get_g": ([vp, c_float_p, c_float_p, c_float_p, c_float_p], C.c_int),
         "sgpu_host_get_metric": ([vp, C.c_int, c_float_p, c_int_p, c_int_p], C.c_int),
         "sgpu_host_get_media": ([vp, C.c_int, C.POINTER(C.c_int16)], C.c_int),
+        "sgpu_host_get_mur_cab1": ([vp, C.c_int, c_float_p], C.c_int),
         "sgpu_batch_create": ([C.c_uint64, C.c_int, C.POINTER(vp)], C.c_int),
         "sgpu_batch_destroy": ([vp], None),
         "sgpu_batch_last_error": ([vp], C.c_char_p),
@@ -150,7 +152,8 @@ def _declare(lib: C.CDLL) -> None:
         f.restype = res
     for name in ["sgpu_advance_ex", "sgpu_advance_ey", "sgpu_advance_ez", "sgpu_advance_electric_cpml",
                  "sgpu_advance_edispersive_e", "sgpu_advance_hx", "sgpu_advance_hy", "sgpu_advance_hz",
-                 "sgpu_advance_magnetic_cpml"]:
+                 "sgpu_advance_magnetic_cpml", "sgpu_advance_pmc_h", "sgpu_advance_periodic_h",
+                 "sgpu_advance_magnetic_mur"]:
         f = getattr(lib, name)
         f.argtypes = [vp]
         f.restype = C.c_int

@@ -193,7 +193,7 @@ class Batch:
 
     def profile(self, nsteps: int) -> list[float]:
         """Device ms per phase summed over nsteps real steps (E field, ADE,
-        E sources, H field, H sources, probes)."""
+        E sources, H field, H sources and borders, probes)."""
         ms = (C.c_float * 6)()
         self._check(self.lib.sgpu_batch_profile_steps(self._h, int(nsteps), ms), "sgpu_batch_profile_steps")
         return list(ms)

@@ -33,6 +33,9 @@ import numpy as np
 
 from . import _lib
 
+# tipofrontera codes of nfde_types.F90:67-71 and the smbjson labels of
+# src_json_parser/labels_mod.F90:108-112
+BORDER_CODES = {"pec": 1, "pmc": 2, "periodic": 4, "mur": 7, "pml": 9}
 EPS0 = np.float32(8.8541878176203898505365630317107502606083701665994498081024171524053950954599821142852891607182008932e-12)
 MU0 = np.float32(1.2566370614359172953850573533118011536788677597500423283899778369231265625144835994512139301368468271e-6)
 COMP = {"Ex": 0, "Ey": 1, "Ez": 2, "Hx": 3, "Hy": 4, "Hz": 5}
@@ -102,11 +105,24 @@ class Problem:
     origin: tuple = (0.0, 0.0, 0.0)
     name: str = "case"
     boundary: str = "pml"
+    # per face (back, front, left, right, down, up): "pml", "pec", "pmc",
+    # "periodic" or "mur"; only "pml" faces carry layers
+    borders: tuple = ("pml",) * 6
+    mur_after_pml: bool = False  # the -mur1 / -mur2 switch
+
+    @property
+    def border_codes(self) -> tuple:
+        return tuple(BORDER_CODES[b] for b in self.borders)
+
+    @property
+    def layers(self) -> tuple:
+        """CPML layers per face (0 on faces of other kinds)."""
+        return tuple(int(L) if b == "pml" else 0 for L, b in zip(self.pml_layers, self.borders))
 
     @property
     def swept_cells(self) -> int:
         """Cells per E+H update, PML included (the Mcells of errorreport.F90:530)."""
-        L = self.pml_layers
+        L = self.layers
         return (self.nx + L[0] + L[1]) * (self.ny + L[2] + L[3]) * (self.nz + L[4] + L[5])
 
     # -- C description ---------------------------------------------------
@@ -174,6 +190,9 @@ class Problem:
         d.nprobes = len(self.probes)
         d.probes = ip(np.asarray(self.probes, np.int32).reshape(-1))
         d.probe_capacity = probe_capacity
+        for f, code in enumerate(self.border_codes):
+            d.border[f] = code
+        d.mur_after_pml = int(self.mur_after_pml)
         return d, keep
 
 
@@ -245,7 +264,10 @@ def read_case(path: str | Path, search: tuple = ()) -> Problem:
     gen = js.get("general", {})
     bnd = js.get("boundary", {}).get("all", {})
     btype = bnd.get("type", "pml")
-    # other boundary kinds are read (layers 0) and refused by the solver
+    if btype not in BORDER_CODES:
+        raise ValueError(f"boundary type {btype!r} is not one of {sorted(BORDER_CODES)}")
+    # readBoundary (smbjson.F90:329-370): one kind for all six faces; CPML
+    # properties only when that kind is "pml"
     L = int(bnd.get("layers", 8)) if btype == "pml" else 0
     order = float(bnd.get("order", 2.0))
     refl = float(bnd.get("reflection", 0.001))
@@ -254,7 +276,8 @@ def read_case(path: str | Path, search: tuple = ()) -> Problem:
                  forcecfl="cfl" in gen, cfl=float(gen.get("cfl", 1.0)),
                  pml_layers=(L,) * 6, pml_order=(order,) * 6, pml_refl=(refl,) * 6,
                  alphamax=float(bnd.get("pmlAlpha", 0.0)), alphaorder=float(bnd.get("pmlAlphaOrder", 1.0)),
-                 kappamax=float(bnd.get("pmlKappa", 1.0)), name=path.name.split(".")[0], boundary=btype)
+                 kappamax=float(bnd.get("pmlKappa", 1.0)), name=path.name.split(".")[0], boundary=btype,
+                 borders=(btype,) * 6)
     coords = {c["id"]: c["relativePosition"] for c in js["mesh"].get("coordinates", [])}
     elems = {e["id"]: e for e in js["mesh"].get("elements", [])}
     mats = {m["id"]: m for m in js.get("materials", [])}

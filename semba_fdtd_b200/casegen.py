@@ -52,10 +52,12 @@ def gaussian_derivative(ds: float, sigma: float, t0: float, duration: float) -> 
 
 
 class _Builder:
-    def __init__(self, n, steps, layers, order=3.0, refl=1e-6, cfl=0.8):
+    def __init__(self, n, steps, layers, order=3.0, refl=1e-6, cfl=0.8, boundary="pml"):
+        bnd = {"type": "pml", "layers": int(layers), "order": order, "reflection": refl} if boundary == "pml" \
+            else {"type": boundary}
         self.js = {"format": "FDTD Input file",
                    "general": {"timeStep": 0.0, "numberOfSteps": int(steps), "cfl": cfl},
-                   "boundary": {"all": {"type": "pml", "layers": int(layers), "order": order, "reflection": refl}},
+                   "boundary": {"all": bnd},
                    "mesh": {"grid": {"numberOfCells": [int(v) for v in n], "steps": {}}, "coordinates": [], "elements": []},
                    "materials": [], "materialAssociations": [], "sources": [], "probes": []}
         self._eid = 0
@@ -195,6 +197,32 @@ def plain_mid(outdir, n=256, steps=4000, inset=15, radius=60, nblocks=20, nprobe
         comp = int(rng.integers(0, 6))
         b.probe(f"p{q}", "electric" if comp < 3 else "magnetic", pos, "xyz"[comp % 3])
     return b.write(outdir, f"plain_mid_{n}")
+
+
+def bordered(outdir, n=(20, 23, 18), steps=160, boundary="mur", layers=4, seed=7) -> Path:
+    """Border test case: a TF/SF plane wave, a soft Ez dipole two cells from
+    a corner (so the borders see strong oblique fields early), a PEC block
+    and a dielectric block, and probes on and next to the boundary planes."""
+    nx, ny, nz = n
+    rng = np.random.default_rng(seed)
+    b = _Builder((nx, ny, nz), steps, layers, boundary=boundary)
+    dx = 0.004
+    b.steps([dx], [dx], [dx])
+    ds = courant_dt(dx) / 4
+    th, ph, al, be = _tem_angles(rng)
+    b.planewave((3, 3, 3), (nx - 3, ny - 3, nz - 3), th, ph, al, be, "gauss.exc", ds,
+                gaussian(ds, 40e-12, 160e-12, 0.5e-9))
+    b.nodal((2, 2, 2), (2, 2, 3), "dipole.exc", ds, gaussian_derivative(ds, 15e-12, 90e-12, 0.3e-9), hard=False)
+    pec = b.material({"type": "pec"})
+    b.bulk(pec, [(nx // 2, nx // 2 + 2, ny // 2, ny // 2 + 3, 4, 6)])
+    die = b.material({"type": "simple", "relativePermittivity": 3.5, "electricConductivity": 0.02})
+    b.bulk(die, [(5, 8, ny - 8, ny - 5, nz // 2, nz // 2 + 3)])
+    spots = [(0, 0, 0), (nx, ny // 2, nz // 2), (nx // 2, 0, nz // 2), (nx // 2, ny, nz - 1), (1, 1, nz),
+             (nx - 1, ny - 1, 1), (2, 2, 2), (nx // 2, ny // 2, nz // 2)]
+    for q, pos in enumerate(spots):
+        b.probe(f"e{q}", "electric", pos, "xyz")
+        b.probe(f"h{q}", "magnetic", pos, "xyz")
+    return b.write(outdir, f"bordered_{boundary}_{nx}x{ny}x{nz}")
 
 
 def graded_steps(n, rng, dmin=1e-3, dmax=3e-3):

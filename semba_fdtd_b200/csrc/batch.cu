@@ -114,6 +114,7 @@ struct InstDesc {
     KDisp d;
     KSrc src[2];
     KProbes pr;
+    KBorder bd;
     const double* tiempo;
     double dt;
     int step_off;  // instance step n = batch counter + step_off
@@ -128,10 +129,11 @@ struct RangeItem {
     long long q0, q1;  // node / row / probe range
 };
 
-enum : int { kCntE = 0, kCntH, kCntNode, kCntSrcE, kCntSrcH, kCntProbe, kNumCounts };
+enum : int { kCntE = 0, kCntH, kCntNode, kCntSrcE, kCntSrcH, kCntProbe, kCntClone, kCntMur, kNumCounts };
 
 constexpr int kNodeChunk = 2048;  // ADE nodes per work item
 constexpr int kRowChunk = 128;    // source rows / probes per work item
+constexpr int kBorderChunk = 1024;  // clone / Mur cells per work item
 constexpr int kPhaseThreads = 256;
 
 __device__ __forceinline__ int inst_step(const InstDesc& D, const int* G, bool* on) {
@@ -305,6 +307,25 @@ __global__ void __launch_bounds__(kPhaseThreads)
     }
 }
 
+// The H-side borders after the H sources: PMC / periodic clones (which 0),
+// then Mur (which 1), each over cell ranges of every active instance.
+__global__ void __launch_bounds__(kPhaseThreads)
+    k_batch_borders(const InstDesc* __restrict__ descs, const RangeItem* __restrict__ items, const int* counts, const int* G,
+                    int which) {
+    const int n_items = counts[which == 0 ? kCntClone : kCntMur];
+    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+        const RangeItem w = items[it];
+        const InstDesc& D = descs[w.slot];
+        bool on;
+        inst_step(D, G, &on);
+        if (!on) continue;
+        for (long long q = w.q0 + threadIdx.x; q < w.q1; q += blockDim.x) {
+            if (which == 0) clone_cell(D.g, D.bd, 6, q);
+            else mur_cell(D.g, D.bd, q);
+        }
+    }
+}
+
 // The batch counter moves on by one step.
 __global__ void k_batch_tick(int* G) { *G += 1; }
 
@@ -350,7 +371,9 @@ struct sgpu_batch {
     RangeItem* d_node = nullptr;
     RangeItem* d_src[2] = {};
     RangeItem* d_probe = nullptr;
-    size_t cap_field[2] = {}, cap_node = 0, cap_src[2] = {}, cap_probe = 0;
+    RangeItem* d_border[2] = {};  // clone cells, Mur cells
+    size_t cap_field[2] = {}, cap_node = 0, cap_src[2] = {}, cap_probe = 0, cap_border[2] = {};
+    bool any_border[2] = {};      // some listed instance has clone / Mur cells
     int family = 1;  // 1: TMA-pipelined field kernels, 0: register-marching
     std::vector<char> has_maps;
     bool dirty = true;         // work lists must be rebuilt before the next step
@@ -363,7 +386,7 @@ struct sgpu_batch {
     // graph of kGraphSteps steps
     cudaGraphExec_t graph = nullptr;
     int graph_nu = 0, graph_ctas = 0;
-    bool graph_tma = false;
+    bool graph_tma = false, graph_border[2] = {};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
@@ -395,6 +418,7 @@ InstDesc make_desc(const Slot& s, bool active) {
     D.src[0] = c->src[0];
     D.src[1] = c->src[1];
     D.pr = c->probes;
+    D.bd = c->border;
     D.tiempo = c->d_tiempo;
     D.dt = c->dt;
     D.step_off = -s.start;
@@ -430,7 +454,7 @@ bool running(const Slot& s, int G) { return s.ctx && G - s.start <= s.nsteps; }
 // Rebuild the flattened work lists from the instances that still run.
 sgpu_status rebuild(sgpu_batch* b) {
     std::vector<FieldItem> fi[2];
-    std::vector<RangeItem> node, src[2], probe;
+    std::vector<RangeItem> node, src[2], probe, border[2];
     int nu = 1;
     b->listed.assign(b->slots.size(), 0);
     for (int sl = 0; sl < (int)b->slots.size(); ++sl) {
@@ -468,6 +492,10 @@ sgpu_status rebuild(sgpu_batch* b) {
                 src[side].push_back(RangeItem{sl, side, r, std::min<long long>(r + kRowChunk, c->src[side].nrows)});
         for (long long q = 0; q < c->probes.n; q += kRowChunk)
             probe.push_back(RangeItem{sl, 0, q, std::min<long long>(q + kRowChunk, c->probes.n)});
+        const long long bcells[2] = {c->border.cl_cells, c->border.mur_cells};
+        for (int w = 0; w < 2; ++w)
+            for (long long q = 0; q < bcells[w]; q += kBorderChunk)
+                border[w].push_back(RangeItem{sl, w, q, std::min<long long>(q + kBorderChunk, bcells[w])});
     }
     sgpu_status s;
     for (int side = 0; side < 2; ++side) {
@@ -476,6 +504,11 @@ sgpu_status rebuild(sgpu_batch* b) {
     }
     if ((s = ensure(b, &b->d_node, &b->cap_node, node.size())) || (s = ensure(b, &b->d_probe, &b->cap_probe, probe.size())))
         return s;
+    for (int w = 0; w < 2; ++w) {
+        if ((s = ensure(b, &b->d_border[w], &b->cap_border[w], border[w].size()))) return s;
+        if ((s = upload(b, b->d_border[w], border[w]))) return s;
+        b->any_border[w] = !border[w].empty();
+    }
     if ((s = upload(b, b->d_field[0], fi[0])) || (s = upload(b, b->d_field[1], fi[1])) || (s = upload(b, b->d_node, node)) ||
         (s = upload(b, b->d_src[0], src[0])) || (s = upload(b, b->d_src[1], src[1])) || (s = upload(b, b->d_probe, probe)))
         return s;
@@ -486,6 +519,8 @@ sgpu_status rebuild(sgpu_batch* b) {
     counts[kCntSrcE] = (int)src[0].size();
     counts[kCntSrcH] = (int)src[1].size();
     counts[kCntProbe] = (int)probe.size();
+    counts[kCntClone] = (int)border[0].size();
+    counts[kCntMur] = (int)border[1].size();
     if ((s = upload(b, b->d_counts, counts))) return s;
     if (nu > b->nu_max) b->nu_max = nu;
     // the copies read the host vectors; wait before they go out of scope
@@ -521,7 +556,7 @@ template <int NU> void edisp_batch(sgpu_batch* b, int grid) {
 }
 
 // One whole step of every instance in the order of timestepping.F90 (E curl +
-// CPML, ADE, E sources, H curl + CPML, H sources, probes).  With `marks`, an
+// CPML, ADE, E sources, H curl + CPML, H sources and borders, probes).  With `marks`, an
 // event is recorded after each of the six phases.
 sgpu_status enqueue_step(sgpu_batch* b, cudaEvent_t* marks = nullptr) {
     const int grid = b->num_sms * b->ctas_per_sm;
@@ -554,6 +589,9 @@ sgpu_status enqueue_step(sgpu_batch* b, cudaEvent_t* marks = nullptr) {
         k_batch_field<1><<<grid, blk, 0, b->stream>>>(b->d_desc, b->d_field[1], b->d_counts, b->d_G);
     mark(3);
     k_batch_sources<<<grid, kPhaseThreads, 0, b->stream>>>(b->d_desc, b->d_src[1], b->d_counts, b->d_G, 1);
+    for (int w = 0; w < 2; ++w)
+        if (b->any_border[w])
+            k_batch_borders<<<grid, kPhaseThreads, 0, b->stream>>>(b->d_desc, b->d_border[w], b->d_counts, b->d_G, w);
     mark(4);
     k_batch_probes<<<grid, kPhaseThreads, 0, b->stream>>>(b->d_desc, b->d_probe, b->d_counts, b->d_G);
     k_batch_tick<<<1, 1, 0, b->stream>>>(b->d_G);
@@ -564,7 +602,9 @@ sgpu_status enqueue_step(sgpu_batch* b, cudaEvent_t* marks = nullptr) {
 }
 
 sgpu_status ensure_graph(sgpu_batch* b) {
-    if (b->graph && b->graph_nu == b->nu_max && b->graph_ctas == b->ctas_per_sm && b->graph_tma == use_tma(b)) return SGPU_OK;
+    if (b->graph && b->graph_nu == b->nu_max && b->graph_ctas == b->ctas_per_sm && b->graph_tma == use_tma(b) &&
+        b->graph_border[0] == b->any_border[0] && b->graph_border[1] == b->any_border[1])
+        return SGPU_OK;
     if (b->graph) {
         cudaGraphExecDestroy(b->graph);
         b->graph = nullptr;
@@ -588,6 +628,8 @@ sgpu_status ensure_graph(sgpu_batch* b) {
     b->graph_nu = b->nu_max;
     b->graph_ctas = b->ctas_per_sm;
     b->graph_tma = use_tma(b);
+    b->graph_border[0] = b->any_border[0];
+    b->graph_border[1] = b->any_border[1];
     return SGPU_OK;
 }
 
@@ -680,6 +722,8 @@ void sgpu_batch_destroy(sgpu_batch* b) {
     }
     cudaFree(b->d_node);
     cudaFree(b->d_probe);
+    cudaFree(b->d_border[0]);
+    cudaFree(b->d_border[1]);
     if (b->arena.base) cudaFree(b->arena.base);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
@@ -892,7 +936,7 @@ sgpu_status sgpu_batch_autotune(sgpu_batch* b, int steps_per_trial, int* chunk3,
 }
 
 // Device time of each phase summed over nsteps steps launched one by one
-// (ms6: E field, ADE, E sources, H field, H sources, probes + counter).
+// (ms6: E field, ADE, E sources, H field, H sources + borders, probes + counter).
 // The steps are real steps of the live instances.
 sgpu_status sgpu_batch_profile_steps(sgpu_batch* b, int nsteps, float* ms6) {
     if (!b || !ms6 || nsteps < 0) return SGPU_ERR_ARG;

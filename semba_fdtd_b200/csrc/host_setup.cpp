@@ -75,6 +75,10 @@ Cx cx_div(Cx a, Cx b) {
 
 struct HostState {
     Box sinpml[6], full[6], alloc[6], sweep[6];
+    // border kind per [axis][side] (tipofrontera codes) and the Mur flags
+    int kind[3][2];
+    bool mur[3][2];
+    std::vector<float> cab1[6];  // calc_murconstants, face order back..up
     int layers[3][2];
     float order[3][2], refl[3][2];
     Vec dx, dy, dz, lx, ly, lz;
@@ -110,13 +114,19 @@ sgpu_lim to_lim(const Box& b) { return sgpu_lim{b.x0, b.x1, b.y0, b.y1, b.z0, b.
 // read_limits_nogeom (preprocess_geom.F90:5266-5737) and the Alloc/Sweep
 // rule of NFDE2sgg for a single layout (semba_fdtd.F90:1285-1300).
 void limits(HostState& h, const sgpu_problem* p) {
-    // reference face order back, front, left, right, down, up
+    // reference face order back, front, left, right, down, up; only CPML
+    // faces carry layers, order and reflection (sgg%PML starts zeroed,
+    // preprocess_geom.F90:5398-5600)
     for (int f = 0; f < 6; ++f) {
         int ax = f / 2, sd = f % 2;
-        h.layers[ax][sd] = p->pml_layers[f];
-        float r = p->pml_refl[f];
+        const int kind = p->border[f] == 0 ? 9 : p->border[f];
+        const bool pml = kind == 9;
+        h.kind[ax][sd] = kind;
+        h.mur[ax][sd] = kind == 7 || (pml && p->mur_after_pml);
+        h.layers[ax][sd] = pml ? p->pml_layers[f] : 0;
+        float r = pml ? p->pml_refl[f] : 0.0f;
         h.refl[ax][sd] = r >= 1.0f ? (float)0.99999 : r;
-        h.order[ax][sd] = p->pml_order[f];
+        h.order[ax][sd] = pml ? p->pml_order[f] : 0.0f;
     }
     const int N[3] = {p->nx, p->ny, p->nz};
     // components whose SINPML range is one node shorter along an axis
@@ -283,6 +293,23 @@ void pml_media(HostState& h) {
             }
         });
     h.num_media = next;
+    // PEC borders (healer.F90:1442-1617): medium 0 on the boundary plane of
+    // the E components tangential to the face and the H component normal to it
+    for (int f = 0; f < 6; ++f) {
+        const bool elec = f < 3;
+        const int own = f % 3;
+        for (int a = 0; a < 3; ++a)
+            for (int sd = 0; sd < 2; ++sd) {
+                if (h.kind[a][sd] != 1 || (elec ? a == own : a != own)) continue;
+                const Box& r = reach[f];
+                int lo[3] = {r.x0, r.y0, r.z0}, hi[3] = {r.x1, r.y1, r.z1};
+                lo[a] = hi[a] = sd == 0 ? lo[a] : hi[a];
+                MediaMat& m = h.mm[f];
+                for (int k = lo[2]; k <= hi[2]; ++k)
+                    for (int j = lo[1]; j <= hi[1]; ++j)
+                        for (int i = lo[0]; i <= hi[0]; ++i) m.at(i, j, k) = 0;
+            }
+    }
 }
 
 // Media table and matrices of read_geomData (preprocess_geom.F90:421-760,
@@ -446,6 +473,12 @@ void cpml(HostState& h, const sgpu_problem* p, sgpu_cpml_desc& d) {
         lo = a == 0 ? b->x0 : (a == 1 ? b->y0 : b->z0);
         hi = a == 0 ? b->x1 : (a == 1 ? b->y1 : b->z1);
     };
+    // without a CPML face InitCPMLBorders returns before calc_cpmlconstants
+    // (borderscpml.F90:140-143): the inverse steps stay as they are; faces
+    // without CPML keep order 0 and kPar_max 1, which leaves their outer
+    // inverse steps unchanged too (their P_b/P_c are never read)
+    bool any_pml = false;
+    for (int a = 0; a < 3; ++a) any_pml = any_pml || h.layers[a][0] > 0 || h.layers[a][1] > 0;
     for (int a = 0; a < 3; ++a) {
         int lo, hi, alo, ahi, slo, shi;
         lohi(AH[a], a, lo, hi);
@@ -486,11 +519,11 @@ void cpml(HostState& h, const sgpu_problem* p, sgpu_cpml_desc& d) {
             inv = 1.0f / (kap * step);
         };
         lohi(AE[a], a, alo, ahi);
-        for (int i = alo; i <= ahi; ++i) {
+        for (int i = alo; i <= ahi && any_pml; ++i) {
             if (i <= slo - 1) coef(0, ce[i], ice[i], (*dhv[a])[i], h.pbe[a][i], h.pce[a][i], (*ihv[a])[i]);
             else if (i >= shi + 1) coef(1, ce[i], ice[i], (*dhv[a])[i], h.pbe[a][i], h.pce[a][i], (*ihv[a])[i]);
         }
-        for (int i = lo; i <= hi; ++i) {
+        for (int i = lo; i <= hi && any_pml; ++i) {
             if (i <= slo - 1) coef(0, cm[i], icm[i], (*dev[a])[i], h.pbm[a][i], h.pcm[a][i], (*iev[a])[i]);
             else if (i >= shi) coef(1, cm[i], icm[i], (*dev[a])[i], h.pbm[a][i], h.pcm[a][i], (*iev[a])[i]);
         }
@@ -498,6 +531,25 @@ void cpml(HostState& h, const sgpu_problem* p, sgpu_cpml_desc& d) {
         d.p_ce[a] = h.pce[a].v.data();
         d.p_bm[a] = h.pbm[a].v.data();
         d.p_cm[a] = h.pcm[a].v.data();
+    }
+}
+
+// calc_murconstants (bordersmur.F90:316-363) for the Mur faces:
+//   cnum = (1/Id(outer node)) / (dt * cluz / sqrt(Epr*Mur)),  CAB1 = (1-cnum)/(1+cnum)
+// with FP32 operands, the FP64 dt promoting the denominator and the quotient
+// stored in FP32.  Id is taken after calc_cpmlconstants.
+void mur_constants(HostState& h) {
+    const float idh[6] = {h.idxh[h.alloc[EX].x0], h.idxh[h.alloc[EX].x1], h.idyh[h.alloc[EY].y0],
+                          h.idyh[h.alloc[EY].y1], h.idzh[h.alloc[EZ].z0], h.idzh[h.alloc[EZ].z1]};
+    for (int f = 0; f < 6; ++f) {
+        h.cab1[f].clear();
+        if (!h.mur[f / 2][f % 2]) continue;
+        h.cab1[f].resize(h.num_media + 1);
+        for (int m = 0; m <= h.num_media; ++m) {
+            const float den = std::sqrt(h.med[m].epr * h.med[m].mur);
+            const float cnum = (float)((double)(1.0f / idh[f]) / ((h.dt * (double)h.cluz) / (double)den));
+            h.cab1[f][m] = (1.0f - cnum) / (1.0f + cnum);
+        }
     }
 }
 
@@ -692,8 +744,11 @@ HostState* make_plan(const sgpu_problem* p, int max_steps, sgpu_status* rc) {
         *rc = SGPU_ERR_ARG;
         return nullptr;
     }
-    for (int f = 0; f < 6; ++f)
-        if (p->pml_layers[f] < 1) { *rc = SGPU_ERR_ARG; return nullptr; }
+    for (int f = 0; f < 6; ++f) {
+        const int kind = p->border[f] == 0 ? 9 : p->border[f];
+        if (kind != 1 && kind != 2 && kind != 4 && kind != 7 && kind != 9) { *rc = SGPU_ERR_ARG; return nullptr; }
+        if (kind == 9 && p->pml_layers[f] < 1) { *rc = SGPU_ERR_ARG; return nullptr; }
+    }
     for (int r = 0; r < p->nregions; ++r)
         if (p->regions[r].kind < 0 || p->regions[r].kind > 2 || (p->regions[r].nboxes > 0 && !p->regions[r].boxes)) {
             *rc = SGPU_ERR_ARG;
@@ -709,6 +764,7 @@ HostState* make_plan(const sgpu_problem* p, int max_steps, sgpu_status* rc) {
         coefficients(*h);
         metrics(*h);
         cpml(*h, p, h->cd);
+        mur_constants(*h);
         edisp(*h, p, h->didx, h->dnp, h->dK, h->dB, h->dG);
         h->pec.resize(h->num_media + 1);
         for (int m = 0; m <= h->num_media; ++m) h->pec[m] = h->med[m].pec ? 1 : 0;
@@ -723,6 +779,22 @@ HostState* make_plan(const sgpu_problem* p, int max_steps, sgpu_status* rc) {
     h->probe_cap = p->probe_capacity > 0 ? p->probe_capacity : 1024;  // BuffObse, fdetypes.F90:97
     h->max_steps = max_steps;
     return h;
+}
+
+// Device buffers sgpu_init_borders allocates for the Mur faces: the CAB1
+// table per face and Past_ (two layers) per (face, tangential H component).
+template <class Fn> void mur_buffers(const HostState& h, Fn&& fn) {
+    const int comps[6][2] = {{HZ, HY}, {HZ, HY}, {HX, HZ}, {HX, HZ}, {HY, HX}, {HY, HX}};
+    for (int f = 0; f < 6; ++f) {
+        if (!h.mur[f / 2][f % 2]) continue;
+        fn((uint64_t)(h.num_media + 1) * 4);
+        const int a = f / 2;
+        for (int comp : comps[f]) {
+            const Box& w = h.sweep[comp];
+            const uint64_t n[3] = {(uint64_t)(w.x1 - w.x0 + 1), (uint64_t)(w.y1 - w.y0 + 1), (uint64_t)(w.z1 - w.z0 + 1)};
+            fn(2 * 4 * (a == 0 ? n[1] * n[2] : (a == 1 ? n[0] * n[2] : n[0] * n[1])));
+        }
+    }
 }
 
 // Hand the plan to the level-1 entry points.
@@ -749,6 +821,17 @@ sgpu_status realize(HostState* h, sgpu::Arena* arena, cudaStream_t stream, sgpu_
         std::vector<int16_t>().swap(h->mm[f].v);  // released once on the device
     }
     if ((s = sgpu_init_cpml(c, &h->cd))) return s;
+    sgpu_border_desc bd{};
+    bool borders = false;
+    for (int f = 0; f < 6; ++f) {
+        const int a = f / 2, sd = f % 2;
+        bd.pmc[f] = h->kind[a][sd] == 2;
+        bd.periodic[f] = h->kind[a][sd] == 4;
+        bd.mur[f] = h->mur[a][sd];
+        bd.mur_cab1[f] = h->cab1[f].empty() ? nullptr : h->cab1[f].data();
+        borders = borders || bd.pmc[f] || bd.periodic[f] || bd.mur[f];
+    }
+    if (borders && (s = sgpu_init_borders(c, &bd))) return s;
     sgpu_edisp_desc ed{(int)h->didx.size(), h->didx.data(), h->dnp.data(), h->dK.data(), h->dB.data(), h->dG.data()};
     if ((s = sgpu_init_edisp(c, &ed))) return s;
     for (const sgpu_planewave_desc& d : h->pw)
@@ -839,6 +922,7 @@ sgpu_status sgpu_host_footprint(const sgpu_ctx* c, uint64_t* bytes) {
         if (!have) nodes = (uint64_t)vol * 3;  // upper bound once the host copy is released
         b += nodes * (4 + 1 + 4 + 16 * (uint64_t)nu);
     }
+    mur_buffers(*h, [&](uint64_t n) { b += n; });
     b += (uint64_t)h->probes.size() / 4 * h->probe_cap * 4;
     *bytes = b;
     return SGPU_OK;
@@ -931,6 +1015,7 @@ sgpu_status sgpu_batch_footprint(const sgpu_ctx* c, uint64_t* bytes, uint64_t* l
         buf((h->pw.size() + h->nodal.size()) * 16);
         buf(samples * 4);
     }
+    mur_buffers(*h, buf);
     buf((uint64_t)(h->max_steps + 3) * 8);  // time vector
     const uint64_t np = h->probes.size() / 4;
     buf(np * 4);
@@ -973,6 +1058,14 @@ sgpu_status sgpu_host_get_metric(const sgpu_ctx* c, int which, float* out, int* 
     if (lo) *lo = v->lo;
     if (hi) *hi = v->hi();
     if (out) std::memcpy(out, v->v.data(), v->v.size() * 4);
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_host_get_mur_cab1(const sgpu_ctx* c, int face, float* out) {
+    if (!c || !c->host || face < 0 || face > 5 || !out) return SGPU_ERR_ARG;
+    const HostState* h = (const HostState*)c->host;
+    if (h->cab1[face].empty()) return SGPU_ERR_ARG;
+    std::memcpy(out, h->cab1[face].data(), h->cab1[face].size() * sizeof(float));
     return SGPU_OK;
 }
 

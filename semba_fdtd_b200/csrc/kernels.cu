@@ -213,6 +213,13 @@ __global__ void k_probes(KGrid g, KProbes p, StepRef sr, int first_n) {
     if (q < p.n) probe_one(g, p, step_of(sr), first_n, q);
 }
 
+// MinusCloneMagneticPMC / CloneMagneticPeriodic (bordersother.F90:65-190)
+// for the face kinds in `mask`, and AdvanceMagneticMUR (bordersmur.F90:502).
+__global__ void k_clone_h(KGrid g, KBorder b, int mask) {
+    clone_cell(g, b, mask, blockIdx.x * (long long)blockDim.x + threadIdx.x);
+}
+__global__ void k_mur_h(KGrid g, KBorder b) { mur_cell(g, b, blockIdx.x * (long long)blockDim.x + threadIdx.x); }
+
 __global__ void k_set_step(int* d, int v) { *d = v; }
 __global__ void k_add_step(int* d, int v) { *d += v; }
 
@@ -438,6 +445,35 @@ sgpu_status launch_probes(sgpu_ctx* c, StepRef sr) {
     return check_launch(c, "k_probes");
 }
 
+bool has_clone(const sgpu_ctx* c, int mask) {
+    for (int a = 0; a < 3; ++a)
+        for (int sd = 0; sd < 2; ++sd)
+            if (c->border.face_kind[a][sd] & mask) return true;
+    return false;
+}
+
+sgpu_status launch_clone(sgpu_ctx* c, int mask) {
+    if (c->border.cl_cells == 0 || !has_clone(c, mask)) return SGPU_OK;
+    const unsigned blocks = (unsigned)((c->border.cl_cells + 255) / 256);
+    k_clone_h<<<blocks, 256, 0, c->stream>>>(kgrid(c), c->border, mask);
+    return check_launch(c, "k_clone_h");
+}
+
+sgpu_status launch_mur(sgpu_ctx* c) {
+    if (c->border.mur_cells == 0) return SGPU_OK;
+    const unsigned blocks = (unsigned)((c->border.mur_cells + 255) / 256);
+    k_mur_h<<<blocks, 256, 0, c->stream>>>(kgrid(c), c->border);
+    return check_launch(c, "k_mur_h");
+}
+
+// The H-side borders after the H sources: both clone kinds in one launch
+// (PMC, then periodic, composed per cell), then Mur.
+sgpu_status launch_borders_h(sgpu_ctx* c) {
+    sgpu_status s = launch_clone(c, 6);
+    if (s) return s;
+    return launch_mur(c);
+}
+
 sgpu_status field_e(sgpu_ctx* c) {
     if (c->family == 1 && c->tma_ready) return launch_tma(c, false);
     return c->cpml.on ? launch_e<kBulk | kCpml | kAll>(c) : launch_e<kBulk | kAll>(c);
@@ -458,7 +494,8 @@ sgpu_status half_e(sgpu_ctx* c, StepRef sr) {
 sgpu_status half_h(sgpu_ctx* c, StepRef sr) {
     sgpu_status s = field_h(c);
     if (s) return s;
-    return launch_sources(c, 1, sr);
+    if ((s = launch_sources(c, 1, sr))) return s;
+    return launch_borders_h(c);
 }
 
 sgpu_status whole_step(sgpu_ctx* c, StepRef sr) {
@@ -638,6 +675,7 @@ void sgpu_destroy(sgpu_ctx* c) {
     dev_free(c, c->idxh); dev_free(c, c->idyh); dev_free(c, c->idzh);
     dev_free(c, c->d_tiempo); dev_free(c, c->d_step); dev_free(c, c->d_flag); dev_free(c, c->d_err);
     free_list(c, c->cpml_allocs);
+    free_list(c, c->border_allocs);
     free_list(c, c->disp_allocs);
     free_list(c, c->src_allocs[0]);
     free_list(c, c->src_allocs[1]);
@@ -771,6 +809,87 @@ sgpu_status sgpu_init_cpml(sgpu_ctx* c, const sgpu_cpml_desc* d) {
             }
     k.on = any ? 1 : 0;
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_init_borders(sgpu_ctx* c, const sgpu_border_desc* d) {
+    if (!c || !d) return set_error(c, SGPU_ERR_ARG, "null border descriptor");
+    free_list(c, c->border_allocs);
+    KBorder& b = c->border;
+    b = KBorder{};
+    for (int f = 0; f < 6; ++f) {
+        const int kinds = (d->pmc[f] != 0) + (d->periodic[f] != 0) + (d->mur[f] != 0);
+        if (kinds > 1) return set_error(c, SGPU_ERR_ARG, "a face has more than one border kind");
+        if (d->mur[f] && !d->mur_cab1[f]) return set_error(c, SGPU_ERR_ARG, "Mur face without CAB1 table");
+        b.face_kind[f / 2][f % 2] = d->pmc[f] ? 2 : (d->periodic[f] ? 4 : 0);
+    }
+    const int org[3] = {c->ox, c->oy, c->oz};
+    for (int q = 0; q < 3; ++q) {
+        const sgpu_lim& w = c->sweep[3 + q];
+        const sgpu_lim& al = c->alloc[3 + q];
+        const int wl[3] = {w.xi, w.yi, w.zi}, wh[3] = {w.xe, w.ye, w.ze};
+        const int al0[3] = {al.xi, al.yi, al.zi}, al1[3] = {al.xe, al.ye, al.ze};
+        for (int a = 0; a < 3; ++a) {
+            b.slo[q][a] = wl[a] - org[a];
+            b.shi[q][a] = wh[a] - org[a];
+            b.glo[q][a] = b.slo[q][a] - 1;  // inside Alloc: the sweep lies strictly inside it
+            b.ghi[q][a] = b.shi[q][a] + 1;
+            b.alo[q][a] = al0[a] - org[a];
+            b.ahi[q][a] = al1[a] - org[a];
+        }
+    }
+    // clone parts in the order of the reference's assignments
+    const int ops[12][3] = {{0, 2, 0}, {0, 2, 1}, {0, 1, 0}, {0, 1, 1}, {1, 0, 0}, {1, 0, 1},
+                            {1, 2, 0}, {1, 2, 1}, {2, 0, 0}, {2, 0, 1}, {2, 1, 0}, {2, 1, 1}};
+    long long tot = 0;
+    for (const auto& op : ops) {
+        const int q = op[0], a = op[1], sd = op[2];
+        if (!b.face_kind[a][sd]) continue;
+        const int ua = a == 0 ? 1 : 0, va = a == 2 ? 1 : 2;
+        b.cl[b.ncl++] = ClonePart{q, a, sd, tot};
+        tot += (long long)(b.ahi[q][ua] - b.alo[q][ua] + 1) * (b.ahi[q][va] - b.alo[q][va] + 1);
+    }
+    b.cl_cells = tot;
+    // Mur parts: regions left, right, down, up, back, front with the
+    // components of regLR (Hx, Hz), regDU (Hy, Hx), regBF (Hz, Hy)
+    const int regs[6][3] = {{2, 3, 5}, {3, 3, 5}, {4, 4, 3}, {5, 4, 3}, {0, 5, 4}, {1, 5, 4}};  // face, comps
+    const int n1 = c->num_media + 1;
+    sgpu_status s;
+    tot = 0;
+    for (const auto& rg : regs) {
+        const int f = rg[0];
+        if (!d->mur[f]) continue;
+        float* cab;
+        if ((s = dalloc(c, &cab, n1, &c->border_allocs))) return s;
+        if ((s = h2d(c, cab, d->mur_cab1[f], n1))) return s;
+        const int a = f / 2, sd = f % 2;
+        for (int t = 1; t <= 2; ++t) {
+            const int comp = rg[t], q = comp - 3;
+            const int ua = a == 0 ? 1 : 0, va = a == 2 ? 1 : 2;
+            MurPart m{};
+            m.comp = comp;
+            m.axis = a;
+            m.inner = sd ? b.shi[q][a] : b.slo[q][a];
+            m.outer = sd ? b.ghi[q][a] : b.glo[q][a];
+            m.u0 = b.slo[q][ua];
+            m.nu = b.shi[q][ua] - b.slo[q][ua] + 1;
+            m.v0 = b.slo[q][va];
+            m.nv = b.shi[q][va] - b.slo[q][va] + 1;
+            const size_t cells = (size_t)m.nu * m.nv;
+            if ((s = dalloc(c, &m.past, 2 * cells, &c->border_allocs))) return s;
+            CUDA_TRY(c, cudaMemsetAsync(m.past, 0, 2 * cells * sizeof(float), c->stream));
+            m.cab1 = cab;
+            m.first = tot;
+            tot += (long long)cells;
+            b.mur[b.nmur++] = m;
+        }
+    }
+    b.mur_cells = tot;
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    if (c->graph) {
+        cudaGraphExecDestroy(c->graph);
+        c->graph = nullptr;
+    }
     return SGPU_OK;
 }
 
@@ -1191,6 +1310,9 @@ sgpu_status sgpu_advance_nodal_h(sgpu_ctx* c, int n) {
     SGPU_READY(c);
     return launch_sources(c, 1, StepRef{nullptr, n}, kMaskNodal);
 }
+sgpu_status sgpu_advance_pmc_h(sgpu_ctx* c) { SGPU_READY(c); return launch_clone(c, 2); }
+sgpu_status sgpu_advance_periodic_h(sgpu_ctx* c) { SGPU_READY(c); return launch_clone(c, 4); }
+sgpu_status sgpu_advance_magnetic_mur(sgpu_ctx* c) { SGPU_READY(c); return launch_mur(c); }
 sgpu_status sgpu_update_observation(sgpu_ctx* c, int n) {
     SGPU_READY(c);
     sgpu_status s = note_probe_rows(c, n, 1);
@@ -1284,6 +1406,7 @@ sgpu_status sgpu_profile_steps(sgpu_ctx* c, int n0, int count, float* ms6) {
         if (!s) s = field_h(c);
         cudaEventRecord(ev[4], c->stream);
         if (!s) s = launch_sources(c, 1, sr);
+        if (!s) s = launch_borders_h(c);
         cudaEventRecord(ev[5], c->stream);
         if (!s) s = launch_probes(c, sr);
         cudaEventRecord(ev[6], c->stream);
@@ -1327,7 +1450,10 @@ sgpu_status sgpu_algorithmic_bytes(const sgpu_ctx* c, double* b6) {
     b6[1] = c->disp_on ? nodes * (21.0 + 32.0 * c->disp.nu_max) : 0.0;
     b6[2] = 0;
     b6[3] = h + psi_bytes(3);
-    b6[4] = 0;
+    // H sources (not counted) and borders: a clone cell reads and writes 4 B
+    // each; a Mur cell reads H, its medium and both Past_ values and writes H
+    // and both Past_ values (26 B)
+    b6[4] = 8.0 * (double)c->border.cl_cells + 26.0 * (double)c->border.mur_cells;
     b6[5] = 8.0 * c->probes.n;
     return SGPU_OK;
 }
@@ -1343,6 +1469,8 @@ sgpu_status sgpu_kernels_per_step(const sgpu_ctx* c, int* n) {
     k += c->src[0].nrows > 0;
     k += c->src[1].nrows > 0;
     k += c->probes.n > 0;
+    k += c->border.cl_cells > 0;
+    k += c->border.mur_cells > 0;
     *n = k;
     return SGPU_OK;
 }
@@ -1491,6 +1619,7 @@ sgpu_status sgpu_device_bytes(const sgpu_ctx* c, uint64_t* bytes) {
             }
     for (int comp = 0; comp < 3; ++comp)
         b += (uint64_t)c->disp.n[comp] * (4 + 1 + 4 + 16 * (uint64_t)std::max(1, c->disp.nu_max));
+    b += (uint64_t)c->border.mur_cells * 2 * sizeof(float);
     *bytes = b;
     return SGPU_OK;
 }

@@ -94,6 +94,38 @@ struct KSrc {
     const float* samples;
 };
 
+// Borders of the H field outside the swept box (local coordinates).
+// One Mur part is one (face, tangential H component) pair: its outer layer
+// and first swept layer, over the component's sweep range of the other two
+// axes (u the lower axis, v the higher), with Past_ of both layers.
+struct MurPart {
+    int comp;              // 3..5
+    int axis;              // face normal
+    int outer, inner;      // layer indices along the normal
+    int u0, nu, v0, nv;
+    float* past;           // [2][nv][nu]: outer layer, then inner layer
+    const float* cab1;     // num_media + 1
+    long long first;       // first cell in the flattened list
+};
+// One clone part is one (tangential H component, PMC or periodic face): the
+// plane outside the face over the component's whole Alloc extent.
+struct ClonePart {
+    int comp;              // 0..2 for Hx..Hz
+    int axis, side;
+    long long first;
+};
+struct KBorder {
+    int face_kind[3][2];   // [axis][side]: 2 PMC, 4 periodic, else 0
+    // per H component (0..2) and axis: outer layers and swept ends
+    int glo[3][3], ghi[3][3], slo[3][3], shi[3][3], alo[3][3], ahi[3][3];
+    int ncl;
+    ClonePart cl[12];
+    long long cl_cells;
+    int nmur;
+    MurPart mur[12];
+    long long mur_cells;
+};
+
 struct KProbes {
     int n;
     const int* comp;
@@ -150,6 +182,9 @@ struct sgpu_ctx {
     bool disp_on = false;
     sgpu::KDisp disp{};
     std::vector<void*> disp_allocs;
+    // borders (PMC / periodic clones, Mur)
+    sgpu::KBorder border{};
+    std::vector<void*> border_allocs;
     // sources
     struct HostSrcTable {
         std::vector<float> samples;

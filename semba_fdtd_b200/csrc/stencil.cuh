@@ -391,5 +391,86 @@ __device__ __forceinline__ void probe_one(const KGrid& g, const KProbes& p, int 
     p.ring[row * p.n + q] = g.F[p.comp[q]][p.idx[q]];
 }
 
+// Cell q of the flattened clone planes, for the face kinds in `mask` (2 PMC,
+// 4 periodic, 6 both).  MinusCloneMagneticPMC and CloneMagneticPeriodic
+// (bordersother.F90:65-190) assign whole planes one face after another, each
+// spanning the component's Alloc extent, so a cell outside two or three such
+// faces ends up with the composition of their maps (the later assignment
+// reads the value the earlier one wrote in the same call).  Each cell here
+// computes that composition directly from swept cells -- a PMC face maps the
+// outer layer to the first swept one with a sign flip, a periodic face to the
+// swept layer at the other end -- so no cell reads a cell another thread of
+// the launch writes, and each cell is written once (by the first of its
+// faces in part order).
+__device__ __forceinline__ void clone_cell(const KGrid& g, const KBorder& b, int mask, long long q) {
+    if (q >= b.cl_cells) return;
+    int p = 0;
+    while (p + 1 < b.ncl && q >= b.cl[p + 1].first) ++p;
+    const ClonePart& cp = b.cl[p];
+    if (!(b.face_kind[cp.axis][cp.side] & mask)) return;
+    const int c = cp.comp;
+    const int ua = cp.axis == 0 ? 1 : 0, va = cp.axis == 2 ? 1 : 2;
+    const long long r = q - cp.first;
+    const int nu = b.ahi[c][ua] - b.alo[c][ua] + 1;
+    int pos[3];
+    pos[cp.axis] = cp.side ? b.ghi[c][cp.axis] : b.glo[c][cp.axis];
+    pos[ua] = b.alo[c][ua] + (int)(r % nu);
+    pos[va] = b.alo[c][va] + (int)(r / nu);
+    for (int e = 0; e < p; ++e) {
+        const ClonePart& o = b.cl[e];
+        if (o.comp == c && (b.face_kind[o.axis][o.side] & mask) &&
+            pos[o.axis] == (o.side ? b.ghi[c][o.axis] : b.glo[c][o.axis]))
+            return;
+    }
+    int src[3] = {pos[0], pos[1], pos[2]};
+    bool neg = false;
+    for (int a = 0; a < 3; ++a) {
+        if (a == c) continue;  // only the faces tangential to the component
+        for (int sd = 0; sd < 2; ++sd) {
+            const int k = b.face_kind[a][sd];
+            if (!(k & mask) || pos[a] != (sd ? b.ghi[c][a] : b.glo[c][a])) continue;
+            if (k == 2) {
+                src[a] = sd ? b.shi[c][a] : b.slo[c][a];
+                neg = !neg;
+            } else {
+                src[a] = sd ? b.slo[c][a] : b.shi[c][a];
+            }
+        }
+    }
+    float* F = g.F[3 + c];
+    const float v = F[src[0] + (long long)g.pitch * src[1] + g.plane * src[2]];
+    F[pos[0] + (long long)g.pitch * pos[1] + g.plane * pos[2]] = neg ? -v : v;
+}
+
+// Cell q of the flattened Mur layers: AdvanceMagneticMUR, first order
+// (bordersmur.F90:1129-1383), and the storage of Past_ (:1396-1650):
+//   H(outer) = Past(inner) + CAB1(medium of the inner node) * (H(inner) - Past(outer))
+//   Past(outer) = H(outer), Past(inner) = H(inner)
+// A part reads its inner layer, which no part writes, so the store can
+// follow the update in the same thread.
+__device__ __forceinline__ void mur_cell(const KGrid& g, const KBorder& b, long long q) {
+    if (q >= b.mur_cells) return;
+    int p = 0;
+    while (p + 1 < b.nmur && q >= b.mur[p + 1].first) ++p;
+    const MurPart& m = b.mur[p];
+    const long long r = q - m.first;
+    const int ua = m.axis == 0 ? 1 : 0, va = m.axis == 2 ? 1 : 2;
+    int pos[3];
+    pos[ua] = m.u0 + (int)(r % m.nu);
+    pos[va] = m.v0 + (int)(r / m.nu);
+    pos[m.axis] = m.outer;
+    const long long no = pos[0] + (long long)g.pitch * pos[1] + g.plane * pos[2];
+    pos[m.axis] = m.inner;
+    const long long ni = pos[0] + (long long)g.pitch * pos[1] + g.plane * pos[2];
+    float* F = g.F[m.comp];
+    const long long layer = (long long)m.nu * m.nv;
+    const float past_outer = m.past[r], past_inner = m.past[layer + r];
+    const float h_inner = F[ni];
+    const float h = past_inner + m.cab1[g.M[m.comp][ni]] * (h_inner - past_outer);
+    F[no] = h;
+    m.past[r] = h;
+    m.past[layer + r] = h_inner;
+}
+
 }  // namespace dev
 }  // namespace sgpu

@@ -9,7 +9,9 @@ Three ways to advance, all bit-identical:
 * ``mode="routines"`` -- one call per reference routine, in the order of
   timestepping.F90:1286-1742 (Advance_Ex, Ey, Ez, AdvanceelectricCPML,
   AdvanceEDispersiveE, AdvancePlaneWaveE, AdvanceNodalE, Advance_Hx, Hy, Hz,
-  AdvanceMagneticCPML, AdvancePlaneWaveH, AdvanceNodalH, UpdateObservation).
+  AdvanceMagneticCPML, MinusCloneMagneticPMC, CloneMagneticPeriodic,
+  AdvancePlaneWaveH, AdvanceNodalH, MinusCloneMagneticPMC,
+  CloneMagneticPeriodic, AdvanceMagneticMUR, UpdateObservation).
 """
 from __future__ import annotations
 
@@ -108,10 +110,12 @@ class Solver:
                     self._check(lib.sgpu_advance_planewave_e(h, n))
                     self._check(lib.sgpu_advance_nodal_e(h, n))
                     for f in (lib.sgpu_advance_hx, lib.sgpu_advance_hy, lib.sgpu_advance_hz,
-                              lib.sgpu_advance_magnetic_cpml):
+                              lib.sgpu_advance_magnetic_cpml, lib.sgpu_advance_pmc_h, lib.sgpu_advance_periodic_h):
                         self._check(f(h))
                     self._check(lib.sgpu_advance_planewave_h(h, n))
                     self._check(lib.sgpu_advance_nodal_h(h, n))
+                    for f in (lib.sgpu_advance_pmc_h, lib.sgpu_advance_periodic_h, lib.sgpu_advance_magnetic_mur):
+                        self._check(f(h))
                     self._check(lib.sgpu_update_observation(h, n))
             else:
                 raise ValueError(mode)
@@ -181,6 +185,13 @@ class Solver:
         out = np.empty(hi.value - lo.value + 1, np.float32)
         self._check(self.lib.sgpu_host_get_metric(self._h, which, out.ctypes.data_as(_lib.c_float_p), None, None))
         return lo.value, out
+
+    def mur_cab1(self, face: int):
+        """CAB1 per medium of a Mur face (back, front, left, right, down, up),
+        or None when the face has no Mur condition."""
+        out = np.empty(self.num_media + 1, np.float32)
+        rc = self.lib.sgpu_host_get_mur_cab1(self._h, int(face), out.ctypes.data_as(_lib.c_float_p))
+        return None if rc else out
 
     def check_finite(self) -> bool:
         rc = self.lib.sgpu_check_finite(self._h)

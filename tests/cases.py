@@ -1,4 +1,5 @@
 """Scaled variants of the benchmark configurations for parity tests."""
+from dataclasses import replace
 from functools import lru_cache
 from pathlib import Path
 import tempfile
@@ -28,4 +29,26 @@ def disp(n=32, steps=120, layers=5):
                                               edge=(4, max(5, n // 3)), nprobes=6))
 
 
-ALL = {"small": small, "mid": mid, "disp": disp}
+@lru_cache(maxsize=None)
+def mur(steps=160):
+    """First-order Mur on all six faces (the reference's default border)."""
+    return read_case(casegen.bordered(_DIR / "mur", steps=steps, boundary="mur"))
+
+
+@lru_cache(maxsize=None)
+def mixed(steps=160):
+    """One border kind per face: CPML with Mur behind it (-mur1) at x-, Mur at
+    x+, PEC at y-, PMC at y+, periodic along z."""
+    pb = read_case(casegen.bordered(_DIR / "mixed", steps=steps, boundary="pml", layers=4))
+    return replace(pb, borders=("pml", "mur", "pec", "pmc", "periodic", "periodic"), mur_after_pml=True)
+
+
+@lru_cache(maxsize=None)
+def closed(steps=160):
+    """PMC along x, periodic along y, PEC below and Mur above: PMC and
+    periodic clones meet on the Hz edges."""
+    pb = read_case(casegen.bordered(_DIR / "closed", steps=steps, boundary="pec"))
+    return replace(pb, borders=("pmc", "pmc", "periodic", "periodic", "pec", "mur"))
+
+
+ALL = {"small": small, "mid": mid, "disp": disp, "mur": mur, "mixed": mixed, "closed": closed}

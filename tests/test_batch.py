@@ -98,3 +98,20 @@ def test_arena_too_small_is_refused_cleanly():
             b.add(pbs[2])
         assert b.memory()[1] == 0
     plan.close()
+
+
+@pytest.mark.parametrize("family", [1, 0], ids=["tma", "regs"])
+def test_batch_with_every_border_kind(family):
+    """Mur, PEC, PMC, periodic and CPML(+Mur) instances next to a CPML one:
+    the clone and Mur phases run over the instances that have them."""
+    from cases import closed, mixed, mur
+    pbs = [mur(), mixed(), closed(), _instances()[1]]
+    with Batch(1 << 30, 8, kernel_family=family) as b:
+        slots = [b.add(pb) for pb in pbs]
+        b.run_all()
+        for s, pb in zip(slots, pbs):
+            o = oracle.Oracle(pb)
+            tr = o.step(pb.nsteps + 1)
+            np.testing.assert_array_equal(b.probes(s), tr, err_msg=pb.name)
+            for c in range(6):
+                np.testing.assert_array_equal(b.field(s, c), o.field(c), err_msg=f"{pb.name} component {c}")

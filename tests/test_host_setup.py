@@ -56,6 +56,14 @@ def test_host_plan_matches_oracle_setup(name):
             olo, oarr = o.metric(w)
             assert olo == lo.value
             np.testing.assert_array_equal(arr, oarr)
+        # calc_murconstants per Mur face
+        for f in range(6):
+            oc = o.mur_cab1(f)
+            hc = np.empty(n1, np.float32)
+            rc = lib.sgpu_host_get_mur_cab1(h, f, hc.ctypes.data_as(_lib.c_float_p))
+            assert (rc == 0) == (oc is not None)
+            if oc is not None:
+                np.testing.assert_array_equal(hc, oc)
         for c in range(6):
             xi, xe, yi, ye, zi, ze = a6[c].tuple()
             m = np.empty((ze - zi + 1, ye - yi + 1, xe - xi + 1), np.int16)
@@ -88,3 +96,12 @@ def test_plan_rejects_bad_problems():
     d, keep = pb.to_desc()
     d.nx = 1
     assert lib.sgpu_host_plan(C.byref(d), 10, C.byref(h)) == 1
+    # a border code outside nfde_types.F90:67-71
+    d, keep = pb.to_desc()
+    d.border[3] = 3
+    assert lib.sgpu_host_plan(C.byref(d), 10, C.byref(h)) == 1
+    # a non-CPML face needs no layers
+    d, keep = pb.to_desc()
+    d.border[0], d.pml_layers[0] = 7, 0
+    assert lib.sgpu_host_plan(C.byref(d), 10, C.byref(h)) == 0
+    lib.sgpu_destroy(h)

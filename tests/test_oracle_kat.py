@@ -13,6 +13,14 @@ reference's own parser fixture:
 * Debye relaxation of a uniform field in a single-real-pole medium converges
   to the analytic solution (electricdispersive.F90:77-362);
 * FP32 against FP64 oracle per probe;
+* borders (healer.F90:1442-1617, bordersother.F90:65-190,
+  bordersmur.F90:1129-1650): a PEC box keeps tangential E and normal H at
+  zero on its faces; PMC faces hold the odd image of the first swept H
+  (edges the product of two images); a plane wave in a box periodic across
+  its wavefront stays uniform over every periodic plane, bit for bit; Mur
+  faces absorb a normally incident pulse that PEC faces reflect whole, and
+  the first step after a field is planted outside a Mur face follows the
+  update formula exactly;
 * the reference's parser fixture test/smbjson/test_read_planewave.F90 on
   testData/cases/planewave.fdtd.json (skipped where that tree is absent).
 """
@@ -173,3 +181,143 @@ def test_reader_matches_reference_parser_fixture():
     assert tuple(int(v) for v in w.coor1) == (1, 1, 1) and tuple(int(v) for v in w.coor2) == (8, 8, 8)
     assert (w.theta, w.phi, w.beta) == (0.0, 0.0, 0.0) and w.alpha == pytest.approx(1.5708)
     np.testing.assert_array_equal(pb.probes, [[0, 4, 4, 4], [1, 4, 4, 4], [2, 4, 4, 4]])
+
+
+# ---------------------------------------------------------------------------
+# borders
+
+
+def _bordered(n, steps, borders, layers=4):
+    pb = _box(n, steps, layers)
+    return _with(pb, borders)
+
+
+def _with(pb, borders):
+    from dataclasses import replace
+    return replace(pb, borders=tuple(borders))
+
+
+def _soft_dipole(pb, c, dt, sig):
+    ds = dt / 4
+    t = np.arange(int(pb.nsteps * dt / ds) + 2) * ds
+    x = (t - 4 * sig) / sig
+    w = Waveform((-x * np.exp(-0.5 * x * x)).astype(np.float32), np.float32(ds))
+    pb.nodals = [NodalSource(True, False, np.array([list(c[:1]) * 2 + list(c[1:2]) * 2 + list(c[2:]) * 2], np.int32),
+                             np.array([[1, 1, 1]], np.float32), w)]
+    return pb
+
+
+def _planes(o, comp, axis, idx):
+    """The plane(s) `idx` (absolute) of a component along `axis`."""
+    f = o.field(comp)
+    lo = o.alloc[comp][2 * axis]
+    return np.take(f, [i - lo for i in idx], axis=axis)
+
+
+def test_pec_faces_keep_tangential_e_and_normal_h_zero():
+    n, steps = 12, 60
+    dt = _dt()
+    pb = _soft_dipole(_bordered(n, steps, ["pec"] * 6), (3, 4, 5), dt, 6 * dt)
+    o = oracle.Oracle(pb)
+    o.step(steps)
+    assert np.abs(o.field(0)).max() > 0
+    # E tangential to a face sits on its plane (Ex on y = 0, n and z = 0, n ...)
+    for comp in range(3):
+        for axis in range(3):
+            if axis != comp:
+                assert not np.any(_planes(o, comp, axis, [0, n])), (comp, axis)
+    # H normal to a face (Hx on x = 0, n ...)
+    for comp in range(3):
+        assert not np.any(_planes(o, 3 + comp, comp, [0, n]))
+
+
+def test_pmc_faces_hold_the_odd_image():
+    n, steps = 12, 40
+    dt = _dt()
+    pb = _soft_dipole(_bordered(n, steps, ["pmc"] * 6), (3, 4, 5), dt, 6 * dt)
+    o = oracle.Oracle(pb)
+    o.step(steps)
+    hx = o.field(3)  # Alloc x -1..n+1, y -1..n, z -1..n: index = coordinate + 1
+    assert np.abs(hx).max() > 0
+    # outside y = 0 and y = n-1 (the swept ends of Hx), all x and z
+    np.testing.assert_array_equal(hx[:, 0, 1:-1], -hx[:, 1, 1:-1])
+    np.testing.assert_array_equal(hx[:, -1, 1:-1], -hx[:, -2, 1:-1])
+    np.testing.assert_array_equal(hx[:, 1:-1, 0], -hx[:, 1:-1, 1])
+    # an edge outside two PMC faces carries the product of both images
+    np.testing.assert_array_equal(hx[:, 0, 0], hx[:, 1, 1])
+    np.testing.assert_array_equal(hx[:, -1, -1], hx[:, -2, -2])
+
+
+def test_periodic_box_keeps_a_normal_plane_wave_uniform():
+    """A +z plane wave in a box periodic along x and y, its TF/SF box spanning
+    the whole x-y extent (those faces are inactive): every Ex, Hy plane is
+    uniform, bit for bit, and the centre sees the unit incident field."""
+    n, steps, sig = 10, 200, 150e-12
+    pb = _bordered(n, steps, ["periodic"] * 4 + ["pml"] * 2, layers=8)
+    pb.nz = 40
+    pb.desz = np.full(40, np.float32(0.01))
+    pb.planewaves = [PlaneWave((0, 0, 8), (n, n, 32), 0.0, 0.0, float(np.float32(np.pi / 2)), 0.0,
+                               _gauss(_dt(), steps, sig, 4 * sig))]
+    pb.probes = np.array([[0, 5, 5, 20]], np.int32)
+    o = oracle.Oracle(pb)
+    tr = [o.step(steps // 2)[:, 0]]
+    for comp in (0, 4):
+        f = o.field(comp)
+        sw = o.sweep[comp]
+        al = o.alloc[comp]
+        core = f[sw[0] - al[0]:sw[1] - al[0] + 1, sw[2] - al[2]:sw[3] - al[2] + 1, :]
+        assert np.abs(core).max() > 1e-3
+        assert np.all(core == core[:1, :1, :]), comp
+    assert not np.any(o.field(1)) and not np.any(o.field(2))
+    tr.append(o.step(steps - steps // 2)[:, 0])
+    assert abs(np.abs(np.concatenate(tr)).max() - 1.0) < 0.02
+
+
+def _sheet_run(borders, n=6, nz=60, steps=320):
+    """A soft Ex current sheet across a box periodic in x and y: two plane
+    pulses leave it along -z and +z towards the z faces."""
+    dt = _dt()
+    pb = _bordered(n, steps, ["periodic"] * 4 + borders)
+    pb.nz = nz
+    pb.desz = np.full(nz, np.float32(0.01))
+    ds = dt / 4
+    sig = 10 * dt
+    t = np.arange(int(steps * dt / ds) + 2) * ds
+    w = Waveform(np.exp(-((t - 4 * sig) ** 2) / (2 * sig * sig)).astype(np.float32), np.float32(ds))
+    pb.nodals = [NodalSource(True, False, np.array([[0, n - 1, 0, n, nz // 2, nz // 2]], np.int32),
+                             np.array([[1, 0, 0]], np.float32), w)]
+    pb.probes = np.array([[0, 2, 2, nz // 2 + 10]], np.int32)
+    o = oracle.Oracle(pb, fp64=True)
+    tr = o.step(steps)[:, 0]
+    return np.abs(tr[: steps // 3]).max(), np.abs(o.field(0)).max()
+
+
+def test_mur_faces_absorb_a_normal_pulse():
+    peak, left_mur = _sheet_run(["mur", "mur"])
+    _, left_pec = _sheet_run(["pec", "pec"])
+    assert peak > 0
+    assert left_pec > 0.5 * peak          # PEC faces send the pulses back
+    assert left_mur < 0.02 * peak         # Mur faces let them out
+
+
+def test_mur_update_formula_on_a_planted_field():
+    """Hx planted on the first swept layer above the z- face (Mur): after one
+    step without sources the outer layer holds Past(inner) + CAB1 * (H(inner)
+    - Past(outer)) with Past = 0 (fresh start), i.e. CAB1 * H(inner)."""
+    n = 8
+    pb = _bordered(n, 1, ["pec"] * 4 + ["mur", "pec"])
+    o = oracle.Oracle(pb)
+    xi, xe, yi, ye, zi, ze = o.alloc[3]
+    hx = np.zeros((xe - xi + 1, ye - yi + 1, ze - zi + 1), np.float32)
+    rng = np.random.default_rng(3)
+    hx[:, :, 0 - zi] = rng.uniform(-1, 1, size=hx[:, :, 0].shape).astype(np.float32)
+    o.set_field(3, hx)
+    o.step(1)
+    cab = o.mur_cab1(4)
+    after = o.field(3)
+    inner, outer = after[:, :, 0 - zi], after[:, :, -1 - zi]
+    m = o.media(3)[:, :, 0 - zi]
+    sw = o.sweep[3]
+    sl = (slice(sw[0] - xi, sw[1] - xi + 1), slice(sw[2] - yi, sw[3] - yi + 1))
+    want = (np.float32(0) + cab[m[sl]] * (inner[sl] - np.float32(0))).astype(np.float32)
+    np.testing.assert_array_equal(outer[sl], want)
