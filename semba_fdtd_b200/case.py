@@ -262,22 +262,37 @@ def read_case(path: str | Path, search: tuple = ()) -> Problem:
         return np.full(n, v[0], np.float32) if len(v) == 1 else v.astype(np.float32)
 
     gen = js.get("general", {})
-    bnd = js.get("boundary", {}).get("all", {})
-    btype = bnd.get("type", "pml")
-    if btype not in BORDER_CODES:
-        raise ValueError(f"boundary type {btype!r} is not one of {sorted(BORDER_CODES)}")
-    # readBoundary (smbjson.F90:329-370): one kind for all six faces; CPML
-    # properties only when that kind is "pml"
-    L = int(bnd.get("layers", 8)) if btype == "pml" else 0
-    order = float(bnd.get("order", 2.0))
-    refl = float(bnd.get("reflection", 0.001))
+    # readBoundary (smbjson.F90:329-370) reads "all": one kind for the six
+    # faces, CPML properties (defaults 8 layers, order 2, R 0.001) only for
+    # "pml".  The format's documentation (doc/smbjson.md:72-100) also names
+    # per-face labels and a Mur default when "boundary" is absent; both are
+    # read here too.
+    faces = ("xLower", "xUpper", "yLower", "yUpper", "zLower", "zUpper")
+    bjs = js.get("boundary")
+    if bjs is None:
+        per = [{"type": "mur"}] * 6
+    elif "all" in bjs:
+        per = [bjs["all"]] * 6
+    else:
+        missing = [f for f in faces if f not in bjs]
+        if missing:
+            raise ValueError(f"boundary: no entry for {missing}")
+        per = [bjs[f] for f in faces]
+    kinds = tuple(str(b.get("type", "pml")) for b in per)
+    for k in kinds:
+        if k not in BORDER_CODES:
+            raise ValueError(f"boundary type {k!r} is not one of {sorted(BORDER_CODES)}")
+    layers = tuple(int(b.get("layers", 8)) if k == "pml" else 0 for b, k in zip(per, kinds))
+    orders = tuple(float(b.get("order", 2.0)) for b in per)
+    refls = tuple(float(b.get("reflection", 0.001)) for b in per)
+    first = per[0]
     pb = Problem(nx=nx, ny=ny, nz=nz, desx=des("x", nx), desy=des("y", ny), desz=des("z", nz),
                  nsteps=int(gen.get("numberOfSteps", 0)), dt=float(gen.get("timeStep", 0.0)),
                  forcecfl="cfl" in gen, cfl=float(gen.get("cfl", 1.0)),
-                 pml_layers=(L,) * 6, pml_order=(order,) * 6, pml_refl=(refl,) * 6,
-                 alphamax=float(bnd.get("pmlAlpha", 0.0)), alphaorder=float(bnd.get("pmlAlphaOrder", 1.0)),
-                 kappamax=float(bnd.get("pmlKappa", 1.0)), name=path.name.split(".")[0], boundary=btype,
-                 borders=(btype,) * 6)
+                 pml_layers=layers, pml_order=orders, pml_refl=refls,
+                 alphamax=float(first.get("pmlAlpha", 0.0)), alphaorder=float(first.get("pmlAlphaOrder", 1.0)),
+                 kappamax=float(first.get("pmlKappa", 1.0)), name=path.name.split(".")[0],
+                 boundary=kinds[0] if len(set(kinds)) == 1 else "mixed", borders=kinds)
     coords = {c["id"]: c["relativePosition"] for c in js["mesh"].get("coordinates", [])}
     elems = {e["id"]: e for e in js["mesh"].get("elements", [])}
     mats = {m["id"]: m for m in js.get("materials", [])}

@@ -3,6 +3,7 @@ loads and exports every entry point of include/semba_gpu.h, and the level-2
 set-up (sgpu_host_plan) produces exactly the oracle's dt, coefficient tables,
 metric/CPML vectors and media matrices."""
 import ctypes as C
+from pathlib import Path
 
 import numpy as np
 import pytest
@@ -105,3 +106,30 @@ def test_plan_rejects_bad_problems():
     d.border[0], d.pml_layers[0] = 7, 0
     assert lib.sgpu_host_plan(C.byref(d), 10, C.byref(h)) == 0
     lib.sgpu_destroy(h)
+
+
+REF_CASE = Path("/root/reference/testData/cases/planewave.fdtd.json")
+
+
+@pytest.mark.skipif(not REF_CASE.exists(), reason="reference tree absent")
+def test_reference_mur_case_plan_matches_oracle():
+    """The reference's own Mur case (testData/cases/planewave.fdtd.json): the
+    library's set-up equals the oracle's, including CAB1 of every face."""
+    from semba_fdtd_b200 import read_case
+    pb = read_case(REF_CASE, search=(REF_CASE.parents[1] / "excitations",))
+    assert pb.borders == ("mur",) * 6
+    lib, h = _plan(pb)
+    try:
+        o = oracle.Oracle(pb)
+        n1 = o.num_media + 1
+        for f in range(6):
+            hc = np.empty(n1, np.float32)
+            assert lib.sgpu_host_get_mur_cab1(h, f, hc.ctypes.data_as(_lib.c_float_p)) == 0
+            np.testing.assert_array_equal(hc, o.mur_cab1(f))
+        for c in range(6):
+            xi, xe, yi, ye, zi, ze = o.alloc[c]
+            m = np.empty((ze - zi + 1, ye - yi + 1, xe - xi + 1), np.int16)
+            lib.sgpu_host_get_media(h, c, m.ctypes.data_as(C.POINTER(C.c_int16)))
+            np.testing.assert_array_equal(m, o.media(c).transpose(2, 1, 0))
+    finally:
+        lib.sgpu_destroy(h)
