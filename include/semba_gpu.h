@@ -117,6 +117,10 @@ typedef struct {
     const double* g3;
 } sgpu_edisp_desc;
 sgpu_status sgpu_init_edisp(sgpu_ctx* ctx, const sgpu_edisp_desc* d);
+/* InitMdispersives (magneticdispersive.F90:79-289): the same description for
+ * the magnetic pole-residue media (Kappa, Beta, GM3); the node lists are the
+ * swept H nodes of those media. */
+sgpu_status sgpu_init_mdisp(sgpu_ctx* ctx, const sgpu_edisp_desc* d);
 
 /* InitPlaneWave (planewaves.F90:72-770) + calc_planewaveconstants
  * (:1494-1510) for one plane wave (one mode).  face[] holds, per face
@@ -185,7 +189,7 @@ sgpu_status sgpu_read_probes(sgpu_ctx* ctx, float* out, int max_steps, int* nste
 /* One call per reference routine, in the order of timestepping.F90:1286-1742
  * (the border calls: after the magnetic CPML and again after the H sources
  * for PMC/periodic, timestepping.F90:1568-1573 and :1636-1641; Mur before the
- * observation, :1711-1712). */
+ * observation, :1711-1712; the magnetic ADE after the first clones, :1582). */
 sgpu_status sgpu_advance_ex(sgpu_ctx* ctx);                 /* Advance_Ex :2165 */
 sgpu_status sgpu_advance_ey(sgpu_ctx* ctx);                 /* Advance_Ey :2206 */
 sgpu_status sgpu_advance_ez(sgpu_ctx* ctx);                 /* Advance_Ez :2250 */
@@ -199,14 +203,15 @@ sgpu_status sgpu_advance_hz(sgpu_ctx* ctx);                 /* Advance_Hz :2374 
 sgpu_status sgpu_advance_magnetic_cpml(sgpu_ctx* ctx);      /* borderscpml.F90:881 */
 sgpu_status sgpu_advance_planewave_h(sgpu_ctx* ctx, int n); /* planewaves.F90:1180 */
 sgpu_status sgpu_advance_nodal_h(sgpu_ctx* ctx, int n);     /* nodalsources.F90:584 */
+sgpu_status sgpu_advance_mdispersive_h(sgpu_ctx* ctx);      /* AdvanceMdispersiveH, magneticdispersive.F90:298 */
 sgpu_status sgpu_advance_pmc_h(sgpu_ctx* ctx);              /* MinusCloneMagneticPMC, bordersother.F90:65 */
 sgpu_status sgpu_advance_periodic_h(sgpu_ctx* ctx);         /* CloneMagneticPeriodic, bordersother.F90:146 */
 sgpu_status sgpu_advance_magnetic_mur(sgpu_ctx* ctx);       /* AdvanceMagneticMUR, bordersmur.F90:502 */
 sgpu_status sgpu_update_observation(sgpu_ctx* ctx, int n);  /* observation.F90:2540 */
 
 /* Fused forms, same results bit for bit: the E half step (curl + CPML +
- * ADE + TF/SF + nodal), the H half step (curl + CPML + TF/SF + nodal +
- * PMC/periodic clones + Mur; the clones before the H sources are left out
+ * ADE + TF/SF + nodal), the H half step (curl + CPML + magnetic ADE + TF/SF +
+ * nodal + PMC/periodic clones + Mur; the clones before the H sources are left out
  * because nothing between the two clone calls reads the cloned layers), and
  * `count` whole steps n0 .. n0+count-1 including the probe gather, captured
  * into a CUDA graph and replayed. */
@@ -230,7 +235,7 @@ sgpu_status sgpu_check_finite(sgpu_ctx* ctx);
 sgpu_status sgpu_elapsed_steps(sgpu_ctx* ctx, int n0, int count, float* ms);
 /* `count` steps launched directly with CUDA events between the phases;
  * ms6 accumulates the device time of: E curl+CPML, ADE, E sources,
- * H curl+CPML, H sources and borders (clones, Mur), probe gather. */
+ * H curl+CPML, magnetic ADE + H sources + borders (clones, Mur), probe gather. */
 sgpu_status sgpu_profile_steps(sgpu_ctx* ctx, int n0, int count, float* ms6);
 /* Algorithmic bytes of one launch of each phase of sgpu_profile_steps:
  * compulsory field/media/psi/ADE-state traffic, without neighbour re-reads
@@ -271,7 +276,7 @@ sgpu_status sgpu_device_bytes(const sgpu_ctx* ctx, uint64_t* bytes);
 /* ======================================================================== */
 
 /* A material region in NFDE terms: kind 0 = PEC volume, 1 = isotropic
- * dielectric volume, 2 = electric pole-residue volume.  eps/mu absolute
+ * dielectric volume, 2 = pole-residue volume.  eps/mu absolute
  * (for a pole-residue region eps is the high-frequency permittivity).
  * Poles: the complex64 residues a11 and b11 = minus the pole, as in
  * preprocess_geom.F90:5196-5199. */
@@ -283,6 +288,12 @@ typedef struct {
     const float* bpoles;     /* 2*npoles */
     int nboxes;
     const int* boxes;        /* 6*nboxes: XI XE YI YE ZI ZE inclusive */
+    /* kind 2: magnetic poles (aM11 residues, bM11 = minus the pole,
+     * preprocess_geom.F90:5223-5226); mu is then the high-frequency
+     * permeability and sigmam its conductivity.  Either set may be empty. */
+    int mpoles;
+    const float* mresidues;  /* 2*mpoles */
+    const float* mbpoles;    /* 2*mpoles */
 } sgpu_region;
 
 typedef struct {

@@ -84,7 +84,7 @@ inline C8 cdiv(C8 a, C8 b) {
 template <class R> struct Medium {
     R Epr = 1, Sigma = 0, Mur = 1, SigmaM = 0;
     int prio = prior_BV;
-    bool pec = false, edisp = false, yee_dummy = false;
+    bool pec = false, edisp = false, mdisp = false, yee_dummy = false;
     int region = -1;  // source region (dispersive data)
 };
 
@@ -166,8 +166,8 @@ template <class R> struct Sim {
     Lim MURc[6][6];
     A3<R> pastLR[2][2], pastDU[2][2], pastBF[2][2];
     std::vector<R> CAB1[6];
-    // ADE
-    std::vector<EDispMedium<R>> dut;
+    // ADE: electric (Dutton) and magnetic (MDutton) media
+    std::vector<EDispMedium<R>> dut, mdut;
     // plane waves
     std::vector<PlaneWave<R>> pws;
     std::vector<R> phys[6][3];
@@ -439,6 +439,7 @@ template <class R> void setup_media(Sim<R>& s, const orc_problem* p) {
         m.Mur = (R)g.mu / s.mu0;
         m.SigmaM = (R)g.sigmam;
         m.edisp = g.npoles != 0;
+        m.mdisp = g.mpoles != 0;
         m.region = r;
         s.med.push_back(m);
         ++contamedia;
@@ -465,14 +466,7 @@ template <class R> void calc_g(Sim<R>& s) {
                 s.GM2[r] = ((R)1.0 - s.GM1[r]) / Sigmam;
             }
         };
-        if (m.yee_dummy) {
-            s.G1[r] = 1; s.G2[r] = 0; s.GM1[r] = 1; s.GM2[r] = 0;
-        } else if (m.pec || r == 0) {
-            s.G1[r] = 0; s.G2[r] = 0; s.GM1[r] = 0; s.GM2[r] = 0;
-        } else if (m.edisp) {
-            s.G1[r] = 0; s.G2[r] = 0;
-            magnetic();
-        } else {
+        auto electric = [&]() {
             double a = ((double)Sigma * dt) / (double)((R)2.0 * Epsilon);
             s.G1[r] = (R)((1.0 - a) / (1.0 + a));
             s.G2[r] = (R)((dt / (double)Epsilon) / (1.0 + a));
@@ -480,6 +474,21 @@ template <class R> void calc_g(Sim<R>& s) {
                 s.G1[r] = (R)std::exp(-(((double)Sigma * dt) / (double)Epsilon));
                 s.G2[r] = ((R)1.0 - s.G1[r]) / Sigma;
             }
+        };
+        if (m.yee_dummy) {
+            s.G1[r] = 1; s.G2[r] = 0; s.GM1[r] = 1; s.GM2[r] = 0;
+        } else if (m.pec || r == 0) {
+            s.G1[r] = 0; s.G2[r] = 0; s.GM1[r] = 0; s.GM2[r] = 0;
+        } else if (m.edisp && !m.mdisp) {
+            s.G1[r] = 0; s.G2[r] = 0;  // InitEDispersives sets them
+            magnetic();
+        } else if (m.mdisp && !m.edisp) {
+            electric();
+            s.GM1[r] = 0; s.GM2[r] = 0;  // InitMdispersives sets them
+        } else {
+            // also a medium with both kinds of poles: both Init routines
+            // overwrite these values
+            electric();
             magnetic();
         }
     }
@@ -698,50 +707,60 @@ template <class R> void setup_mur(Sim<R>& s) {
     }
 }
 
-// InitEDispersives, electricdispersive.F90:77-298.
-template <class R> void setup_edisp(Sim<R>& s, const orc_problem* p) {
-    s.dut.clear();
+// InitEDispersives (electricdispersive.F90:77-298) and, with mag,
+// InitMdispersives (magneticdispersive.F90:79-289): the same construction
+// with the magnetic poles, mu11 and sigmam11 of the medium, writing GM1/GM2
+// and listing the swept H nodes.
+template <class R> void setup_disp(Sim<R>& s, const orc_problem* p, bool mag) {
+    std::vector<EDispMedium<R>>& list = mag ? s.mdut : s.dut;
+    list.clear();
     const double dt = s.dt;
     for (int jmed = 1; jmed <= s.NumMedia; ++jmed) {
-        if (!s.med[jmed].edisp) continue;
+        if (!(mag ? s.med[jmed].mdisp : s.med[jmed].edisp)) continue;
         const orc_region& g = p->regions[s.med[jmed].region];
+        const int np = mag ? g.mpoles : g.npoles;
+        const float* res = mag ? g.mresidues : g.residues;
+        const float* bp = mag ? g.mbpoles : g.bpoles;
         EDispMedium<R> d;
         d.indexmed = jmed;
-        d.np = g.npoles;
-        for (int q = 0; q < g.npoles; ++q) {
+        d.np = np;
+        for (int q = 0; q < np; ++q) {
             // complex64 inputs promoted to complex(8); a11 = -b11
-            // (preprocess_geom.F90:5196-5199)
-            C8 C{(double)g.residues[2 * q], (double)g.residues[2 * q + 1]};
-            C8 a{(double)(-g.bpoles[2 * q]), (double)(-g.bpoles[2 * q + 1])};
+            // (preprocess_geom.F90:5196-5199, 5223-5226 for the magnetic ones)
+            C8 C{(double)res[2 * q], (double)res[2 * q + 1]};
+            C8 a{(double)(-bp[2 * q]), (double)(-bp[2 * q + 1])};
             C8 adt2{(a.re * dt) / 2.0, (a.im * dt) / 2.0};
             C8 num{1.0 + adt2.re, adt2.im};
             C8 den{1.0 - adt2.re, -adt2.im};
             d.kappa.push_back(cdiv(num, den));
             d.beta.push_back(cdiv(C8{C.re * dt, C.im * dt}, den));
         }
-        s.dut.push_back(d);
+        list.push_back(d);
     }
-    for (EDispMedium<R>& d : s.dut) {
+    std::vector<R>& C1 = mag ? s.GM1 : s.G1;
+    std::vector<R>& C2 = mag ? s.GM2 : s.G2;
+    for (EDispMedium<R>& d : list) {
         const orc_region& g = p->regions[s.med[d.indexmed].region];
         R tempo = 0;
         for (int q = 0; q < d.np; ++q) tempo = (R)((double)tempo + d.beta[q].re);
-        R eps11 = (R)g.eps, sig11 = (R)g.sigma;
-        double den = (double)((R)2.0 * eps11 + tempo) + (double)sig11 * dt;
-        s.G1[d.indexmed] = (R)(((double)((R)2.0 * eps11 + tempo) - (double)sig11 * dt) / den);
-        s.G2[d.indexmed] = (R)(((double)(R)2.0 * dt) / den);
+        // eps11 / sigma11 (electric), mu11 / sigmam11 (magnetic)
+        R v11 = mag ? (R)g.mu : (R)g.eps, sig11 = mag ? (R)g.sigmam : (R)g.sigma;
+        double den = (double)((R)2.0 * v11 + tempo) + (double)sig11 * dt;
+        C1[d.indexmed] = (R)(((double)((R)2.0 * v11 + tempo) - (double)sig11 * dt) / den);
+        C2[d.indexmed] = (R)(((double)(R)2.0 * dt) / den);
         for (int q = 0; q < d.np; ++q) {
-            double gh = (double)(s.G2[d.indexmed] / (R)2.0);
+            double gh = (double)(C2[d.indexmed] / (R)2.0);
             d.g3.push_back(C8{gh * (1.0 + d.kappa[q].re), gh * d.kappa[q].im});
         }
     }
-    for (EDispMedium<R>& d : s.dut) {
+    const int c0 = mag ? 3 : 0;
+    for (EDispMedium<R>& d : list) {
         for (int c = 0; c < 3; ++c) {
-            const Lim& w = s.Sweep[c];
-            (void)w;
+            const Lim& w = s.Sweep[c0 + c];
             for (int k = w.ZI; k <= w.ZE; ++k)
                 for (int j = w.YI; j <= w.YE; ++j)
                     for (int i = w.XI; i <= w.XE; ++i)
-                        if (s.mi[c](i, j, k) == d.indexmed) {
+                        if (s.mi[c0 + c](i, j, k) == d.indexmed) {
                             DNode<R> n;
                             n.i = i; n.j = j; n.k = k;
                             n.prev = 0;
@@ -1095,6 +1114,40 @@ template <class R> void advance_edisp(Sim<R>& s) {
     }
 }
 
+// AdvanceMdispersiveH, magneticdispersive.F90:298-360: as the electric
+// update on the H nodes, except that the current takes (Beta/dt)*(H-Hprev),
+// dividing before the product.
+template <class R> void advance_mdisp(Sim<R>& s) {
+    const double dt = s.dt;
+    for (EDispMedium<R>& d : s.mdut) {
+        const int np = d.np;
+        for (int c = 0; c < 3; ++c) {
+            std::vector<DNode<R>>& nodes = d.nodes[c];
+            A3<R>& H = s.F[3 + c];
+            const long nn = (long)nodes.size();
+#pragma omp parallel for schedule(static)
+            for (long q = 0; q < nn; ++q) {
+                DNode<R>& n = nodes[q];
+                R& H0 = H(n.i, n.j, n.k);
+                C8* Jn = &d.J[c][q * np];
+                for (int p = 0; p < np; ++p) {
+                    double re = d.g3[p].re * Jn[p].re - d.g3[p].im * Jn[p].im;
+                    H0 = (R)((double)H0 - re);
+                }
+                R diff = H0 - n.prev;
+                for (int p = 0; p < np; ++p) {
+                    C8 kj = cmul(d.kappa[p], Jn[p]);
+                    C8 bd{d.beta[p].re / dt, d.beta[p].im / dt};
+                    bd.re = bd.re * (double)diff;
+                    bd.im = bd.im * (double)diff;
+                    Jn[p] = C8{kj.re + bd.re, kj.im + bd.im};
+                }
+                n.prev = H0;
+            }
+        }
+    }
+}
+
 // AdvancePlaneWaveE, planewaves.F90:878-1174.
 template <class R> void advance_pw_e(Sim<R>& s, int n) {
     R timei = (R)s.time(n);
@@ -1391,6 +1444,7 @@ template <class R> void one_step(Sim<R>& s, int n) {
     advance_cpml_h(s);
     clone_pmc(s);
     clone_periodic(s);
+    advance_mdisp(s);
     advance_pw_h(s, n);
     advance_nodal(s, n, false);
     clone_pmc(s);
@@ -1414,7 +1468,8 @@ template <class R> int create(const orc_problem* p, Sim<R>** out) {
     setup_metrics(*s);
     setup_cpml(*s);
     setup_mur(*s);
-    setup_edisp(*s, p);
+    setup_disp(*s, p, false);
+    setup_disp(*s, p, true);
     setup_planewave(*s, p);
     setup_nodal(*s, p);
     s->probes.assign(p->probes, p->probes + 4 * p->nprobes);
@@ -1617,11 +1672,12 @@ int orc_get_mur_cab1(void* hv, int face, float* out) {
     return h->fp64 ? get(*h->sd) : get(*h->sf);
 }
 
-int orc_get_edisp(void* hv, int m, int* medium_index, int* npoles, double* kappa, double* beta, double* g3) {
+static int get_disp(void* hv, bool mag, int m, int* medium_index, int* npoles, double* kappa, double* beta, double* g3) {
     Handle* h = (Handle*)hv;
     auto fill = [&](auto& s) {
-        if (m < 0 || m >= (int)s.dut.size()) return 1;
-        auto& d = s.dut[m];
+        auto& list = mag ? s.mdut : s.dut;
+        if (m < 0 || m >= (int)list.size()) return 1;
+        auto& d = list[m];
         *medium_index = d.indexmed;
         *npoles = d.np;
         for (int q = 0; q < d.np; ++q) {
@@ -1632,6 +1688,14 @@ int orc_get_edisp(void* hv, int m, int* medium_index, int* npoles, double* kappa
         return 0;
     };
     return h->fp64 ? fill(*h->sd) : fill(*h->sf);
+}
+
+int orc_get_edisp(void* hv, int m, int* medium_index, int* npoles, double* kappa, double* beta, double* g3) {
+    return get_disp(hv, false, m, medium_index, npoles, kappa, beta, g3);
+}
+
+int orc_get_mdisp(void* hv, int m, int* medium_index, int* npoles, double* kappa, double* beta, double* g3) {
+    return get_disp(hv, true, m, medium_index, npoles, kappa, beta, g3);
 }
 
 }  // extern "C"

@@ -20,6 +20,7 @@
  *     borders                                    bordersother.F90:65-190,
  *                                                bordersmur.F90:79-363, 502-1653)
  *   - electric pole-residue ADE                 (electricdispersive.F90:77-362)
+ *   - magnetic pole-residue ADE                 (magneticdispersive.F90:79-360)
  *   - plane-wave TF/SF                          (planewaves.F90:72-853, 878-1510)
  *   - nodal sources                             (nodalsources.F90:76-583)
  *   - point probes                              (observation.F90:2633-2668)
@@ -41,7 +42,8 @@ extern "C" {
 #endif
 
 /* A material region in NFDE terms (nfde_types.F90).  kind: 0 = PEC volume,
- * 1 = isotropic dielectric volume, 2 = electric pole-residue volume.
+ * 1 = isotropic dielectric volume, 2 = pole-residue volume (electric and/or
+ * magnetic poles).
  * eps/mu are absolute (F/m, H/m) as stored by the NFDE structures; for a
  * dispersive region eps is eps11 (the high-frequency permittivity). */
 typedef struct {
@@ -52,6 +54,11 @@ typedef struct {
     const float* bpoles;   /* 2*npoles: complex64 b11 = minus the pole (re, im) */
     int nboxes;
     const int* boxes;      /* 6*nboxes: XI XE YI YE ZI ZE, inclusive cell coords */
+    /* kind 2 only: magnetic poles (aM11 residues, bM11 = minus the pole),
+     * with mu the high-frequency permeability and sigmam its conductivity */
+    int mpoles;
+    const float* mresidues; /* 2*mpoles */
+    const float* mbpoles;   /* 2*mpoles */
 } orc_region;
 
 typedef struct {
@@ -131,8 +138,11 @@ int orc_get_g(void* h, float* g1, float* g2, float* gm1, float* gm2);
 int orc_get_metric(void* h, int which, float* out);
 int orc_get_metric_range(void* h, int which, int* lo, int* hi);
 /* Per dispersive medium m (0-based in creation order): numpoles, kappa,
- * beta, g3 as interleaved doubles (re, im). */
+ * beta, g3 as interleaved doubles (re, im).  orc_get_mdisp: the same for
+ * the magnetic media (GM3 in g3). */
 int orc_get_edisp(void* h, int m, int* medium_index, int* npoles, double* kappa,
+                  double* beta, double* g3);
+int orc_get_mdisp(void* h, int m, int* medium_index, int* npoles, double* kappa,
                   double* beta, double* g3);
 double orc_get_time(void* h, int n);
 /* CAB1 of calc_murconstants (bordersmur.F90:316-363) for face f (back, front,

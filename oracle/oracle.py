@@ -26,7 +26,8 @@ class OrcLim(C.Structure):
 class OrcRegion(C.Structure):
     _fields_ = [("kind", C.c_int), ("eps", C.c_float), ("sigma", C.c_float), ("mu", C.c_float), ("sigmam", C.c_float),
                 ("npoles", C.c_int), ("residues", C.POINTER(C.c_float)), ("bpoles", C.POINTER(C.c_float)),
-                ("nboxes", C.c_int), ("boxes", C.POINTER(C.c_int))]
+                ("nboxes", C.c_int), ("boxes", C.POINTER(C.c_int)),
+                ("mpoles", C.c_int), ("mresidues", C.POINTER(C.c_float)), ("mbpoles", C.POINTER(C.c_float))]
 
 
 class OrcPW(C.Structure):
@@ -92,6 +93,7 @@ def load():
         lib.orc_get_metric_range.argtypes = [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         lib.orc_get_edisp.argtypes = [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)] + [C.POINTER(C.c_double)] * 3
         lib.orc_get_mur_cab1.argtypes = [vp, C.c_int, C.POINTER(C.c_float)]
+        lib.orc_get_mdisp.argtypes = lib.orc_get_edisp.argtypes
         _lib = lib
     return _lib
 
@@ -127,6 +129,9 @@ def _problem(pb):
         g.bpoles = f32(np.asarray(r.bpoles, np.complex64).view(np.float32))
         g.nboxes = len(r.boxes)
         g.boxes = i32(np.asarray(r.boxes).reshape(-1))
+        g.mpoles = len(r.mresidues)
+        g.mresidues = f32(np.asarray(r.mresidues, np.complex64).view(np.float32))
+        g.mbpoles = f32(np.asarray(r.mbpoles, np.complex64).view(np.float32))
     keep.append(regs)
     p.nregions, p.regions = len(pb.regions), regs
     pws = (OrcPW * max(1, len(pb.planewaves)))()

@@ -27,7 +27,7 @@ class Lim(C.Structure):
 class Region(C.Structure):
     _fields_ = [("kind", C.c_int), ("eps", C.c_float), ("sigma", C.c_float), ("mu", C.c_float), ("sigmam", C.c_float),
                 ("npoles", C.c_int), ("residues", c_float_p), ("bpoles", c_float_p), ("nboxes", C.c_int),
-                ("boxes", c_int_p)]
+                ("boxes", c_int_p), ("mpoles", C.c_int), ("mresidues", c_float_p), ("mbpoles", c_float_p)]
 
 
 class PlaneWaveSrc(C.Structure):
@@ -153,7 +153,7 @@ def _declare(lib: C.CDLL) -> None:
     for name in ["sgpu_advance_ex", "sgpu_advance_ey", "sgpu_advance_ez", "sgpu_advance_electric_cpml",
                  "sgpu_advance_edispersive_e", "sgpu_advance_hx", "sgpu_advance_hy", "sgpu_advance_hz",
                  "sgpu_advance_magnetic_cpml", "sgpu_advance_pmc_h", "sgpu_advance_periodic_h",
-                 "sgpu_advance_magnetic_mur"]:
+                 "sgpu_advance_magnetic_mur", "sgpu_advance_mdispersive_h"]:
         f = getattr(lib, name)
         f.argtypes = [vp]
         f.restype = C.c_int

@@ -13,9 +13,11 @@ reference parser does not read:
   -- an isotropic dielectric volume (the NFDE dielectric regions of
   ``preprocess_geom.F90:686-760``), eps stored as ``eps_r * eps0`` in FP32;
 * material ``"type": "poleResidue"`` with ``epsilonInfinity``,
-  ``electricConductivity``, ``poles`` and ``residues`` (lists of [re, im]) --
-  the NFDE frequency-dependent volumes (``preprocess_geom.F90:5055-5248``); the
-  NFDE stores minus the pole, ``b11 = -pole``, in complex64;
+  ``electricConductivity``, ``poles`` and ``residues`` (lists of [re, im]),
+  and for magnetic dispersion ``muInfinity``, ``magneticConductivity``,
+  ``magneticPoles`` and ``magneticResidues`` -- the NFDE frequency-dependent
+  volumes (``preprocess_geom.F90:5055-5248``); the NFDE stores minus the pole,
+  ``b11 = -pole`` (``bM11`` for the magnetic ones), in complex64;
 * nodal sources may set ``"hard": false`` for a soft (current-like) source;
   the reference's JSON path only builds hard ones (``isField``,
   ``preprocess_geom.F90:2913``).
@@ -51,6 +53,9 @@ class Region:
     sigmam: float = 0.0
     residues: np.ndarray = field(default_factory=lambda: np.zeros(0, np.complex64))
     bpoles: np.ndarray = field(default_factory=lambda: np.zeros(0, np.complex64))
+    # magnetic poles of a pole-residue region (aM11 residues, bM11 = -pole)
+    mresidues: np.ndarray = field(default_factory=lambda: np.zeros(0, np.complex64))
+    mbpoles: np.ndarray = field(default_factory=lambda: np.zeros(0, np.complex64))
 
 
 @dataclass
@@ -162,6 +167,9 @@ class Problem:
             g.bpoles = fp(np.asarray(r.bpoles, np.complex64).view(np.float32))
             g.nboxes = len(r.boxes)
             g.boxes = ip(np.asarray(r.boxes, np.int32).reshape(-1))
+            g.mpoles = len(r.mresidues)
+            g.mresidues = fp(np.asarray(r.mresidues, np.complex64).view(np.float32))
+            g.mbpoles = fp(np.asarray(r.mbpoles, np.complex64).view(np.float32))
         keep.append(regs)
         d.nregions, d.regions = len(self.regions), regs
         pws = (_lib.PlaneWaveSrc * max(1, len(self.planewaves)))()
@@ -320,10 +328,15 @@ def read_case(path: str | Path, search: tuple = ()) -> Problem:
                                mu=float(mr * MU0), sigmam=float(m.get("magneticConductivity", 0.0))))
         elif t == "poleResidue":
             einf = np.float32(m.get("epsilonInfinity", 1.0))
-            poles = np.array([complex(p[0], p[1]) for p in m["poles"]], np.complex64)
-            res = np.array([complex(p[0], p[1]) for p in m["residues"]], np.complex64)
+            muinf = np.float32(m.get("muInfinity", 1.0))
+            poles = np.array([complex(p[0], p[1]) for p in m.get("poles", [])], np.complex64)
+            res = np.array([complex(p[0], p[1]) for p in m.get("residues", [])], np.complex64)
+            mpoles = np.array([complex(p[0], p[1]) for p in m.get("magneticPoles", [])], np.complex64)
+            mres = np.array([complex(p[0], p[1]) for p in m.get("magneticResidues", [])], np.complex64)
             disp.append(Region(kind=2, boxes=boxes, eps=float(einf * EPS0), sigma=float(m.get("electricConductivity", 0.0)),
-                               mu=float(MU0), residues=res, bpoles=(-poles).astype(np.complex64)))
+                               mu=float(muinf * MU0), sigmam=float(m.get("magneticConductivity", 0.0)),
+                               residues=res, bpoles=(-poles).astype(np.complex64),
+                               mresidues=mres, mbpoles=(-mpoles).astype(np.complex64)))
         else:
             raise ValueError(f"material type {t!r} is outside this path")
     pb.regions = pec + diel + disp

@@ -141,6 +141,55 @@ def _pole_pair_material(rng, eps_inf=1.0):
             "poles": poles, "residues": res}
 
 
+def _magnetic_pole_pair(rng):
+    """One conjugate pole pair in the permeability, f0 in 2-15 GHz, damping
+    0.1-0.4, residue scaled so the static mu_r lies in 1.5-4."""
+    from .case import MU0
+    mu_s = rng.uniform(1.5, 4.0)
+    f0 = rng.uniform(2e9, 15e9)
+    z = rng.uniform(0.1, 0.4)
+    w0 = 2 * math.pi * f0
+    a = complex(-z * w0, w0 * math.sqrt(1 - z * z))
+    r = -(mu_s - 1.0) / 2.0 * float(MU0) * a
+    poles, res = [], []
+    for pa, pr in ((a, r), (a.conjugate(), r.conjugate())):
+        poles.append([_f32(pa.real), _f32(pa.imag)])
+        res.append([_f32(pr.real), _f32(pr.imag)])
+    return poles, res
+
+
+def magnetic_dispersive(outdir, n=(26, 24, 22), steps=140, layers=5, seed=9) -> Path:
+    """Pole-residue blocks with magnetic poles only, electric poles only, and
+    both, next to a TF/SF plane wave and a soft dipole."""
+    nx, ny, nz = n
+    rng = np.random.default_rng(seed)
+    b = _Builder((nx, ny, nz), steps, layers)
+    dx = 0.003
+    b.steps([dx], [dx], [dx])
+    ds = courant_dt(dx) / 4
+    th, ph, al, be = _tem_angles(rng)
+    b.planewave((3, 3, 3), (nx - 3, ny - 3, nz - 3), th, ph, al, be, "gauss.exc", ds,
+                gaussian(ds, 30e-12, 120e-12, 0.4e-9))
+    b.nodal((nx // 2, ny // 2, nz // 2), (nx // 2, ny // 2, nz // 2 + 1), "dipole.exc", ds,
+            gaussian_derivative(ds, 12e-12, 72e-12, 0.25e-9), hard=False)
+    mp, mr = _magnetic_pole_pair(rng)
+    mag = b.material({"type": "poleResidue", "epsilonInfinity": 2.0, "muInfinity": 1.2,
+                      "magneticConductivity": _f32(rng.uniform(0, 50.0)), "magneticPoles": mp, "magneticResidues": mr})
+    b.bulk(mag, [(5, 10, 5, 9, 5, 9)])
+    both = dict(_pole_pair_material(rng))
+    mp2, mr2 = _magnetic_pole_pair(rng)
+    both.update({"muInfinity": 1.5, "magneticPoles": mp2, "magneticResidues": mr2})
+    mid = b.material(both)
+    b.bulk(mid, [(nx - 11, nx - 6, ny - 10, ny - 6, nz - 10, nz - 6)])
+    ele = b.material(_pole_pair_material(rng))
+    b.bulk(ele, [(5, 9, ny - 10, ny - 6, 6, 10)])
+    spots = [(7, 7, 7), (nx - 8, ny - 8, nz - 8), (7, ny - 8, 8), (nx // 2, ny // 2 + 3, nz // 2)]
+    for q, pos in enumerate(spots):
+        b.probe(f"e{q}", "electric", pos, "xyz")
+        b.probe(f"h{q}", "magnetic", pos, "xyz")
+    return b.write(outdir, f"magnetic_dispersive_{nx}x{ny}x{nz}")
+
+
 def plain_small(outdir, n=64, steps=1000, inset=15, nprobes=8, seed=1, layers=10, dx=0.01) -> Path:
     rng = np.random.default_rng(seed)
     b = _Builder((n, n, n), steps, layers)

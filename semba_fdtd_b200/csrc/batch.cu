@@ -111,7 +111,7 @@ size_t arena_largest(Arena* a) {
 struct InstDesc {
     KGrid g;
     KCpml cp;
-    KDisp d;
+    KDisp d, md;  // electric and magnetic pole-residue media
     KSrc src[2];
     KProbes pr;
     KBorder bd;
@@ -129,7 +129,7 @@ struct RangeItem {
     long long q0, q1;  // node / row / probe range
 };
 
-enum : int { kCntE = 0, kCntH, kCntNode, kCntSrcE, kCntSrcH, kCntProbe, kCntClone, kCntMur, kNumCounts };
+enum : int { kCntE = 0, kCntH, kCntNode, kCntSrcE, kCntSrcH, kCntProbe, kCntClone, kCntMur, kCntMNode, kNumCounts };
 
 constexpr int kNodeChunk = 2048;  // ADE nodes per work item
 constexpr int kRowChunk = 128;    // source rows / probes per work item
@@ -258,18 +258,19 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
     if (producer && t.lane == 0) tma_drain(t, gp, err, 15);
 }
 
-// AdvanceEDispersiveE over node ranges of every active instance.
-template <int NU>
+// AdvanceEDispersiveE (MAG false) or AdvanceMdispersiveH (MAG true) over
+// node ranges of every active instance.
+template <int NU, bool MAG>
 __global__ void __launch_bounds__(kPhaseThreads)
-    k_batch_edisp(const InstDesc* __restrict__ descs, const RangeItem* __restrict__ items, const int* counts, const int* G) {
-    const int n_items = counts[kCntNode];
+    k_batch_ade(const InstDesc* __restrict__ descs, const RangeItem* __restrict__ items, const int* counts, const int* G) {
+    const int n_items = counts[MAG ? kCntMNode : kCntNode];
     for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
         const RangeItem w = items[it];
         const InstDesc& D = descs[w.slot];
         bool on;
         inst_step(D, G, &on);
         if (!on) continue;
-        for (long long q = w.q0 + threadIdx.x; q < w.q1; q += blockDim.x) edisp_node<NU>(D.g, D.d, w.sub, q);
+        for (long long q = w.q0 + threadIdx.x; q < w.q1; q += blockDim.x) ade_node<NU, MAG>(D.g, MAG ? D.md : D.d, w.sub, q);
     }
 }
 
@@ -369,6 +370,9 @@ struct sgpu_batch {
     int* d_G = nullptr;
     FieldItem* d_field[2] = {};
     RangeItem* d_node = nullptr;
+    RangeItem* d_mnode = nullptr;  // magnetic ADE node ranges
+    size_t cap_mnode = 0;
+    bool any_mnode = false;
     RangeItem* d_src[2] = {};
     RangeItem* d_probe = nullptr;
     RangeItem* d_border[2] = {};  // clone cells, Mur cells
@@ -386,7 +390,7 @@ struct sgpu_batch {
     // graph of kGraphSteps steps
     cudaGraphExec_t graph = nullptr;
     int graph_nu = 0, graph_ctas = 0;
-    bool graph_tma = false, graph_border[2] = {};
+    bool graph_tma = false, graph_border[2] = {}, graph_mnode = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
@@ -415,6 +419,8 @@ InstDesc make_desc(const Slot& s, bool active) {
     D.cp = c->cpml;
     D.d = c->disp;
     if (!c->disp_on) D.d.n[0] = D.d.n[1] = D.d.n[2] = 0;
+    D.md = c->mdisp;
+    if (!c->mdisp_on) D.md.n[0] = D.md.n[1] = D.md.n[2] = 0;
     D.src[0] = c->src[0];
     D.src[1] = c->src[1];
     D.pr = c->probes;
@@ -454,7 +460,7 @@ bool running(const Slot& s, int G) { return s.ctx && G - s.start <= s.nsteps; }
 // Rebuild the flattened work lists from the instances that still run.
 sgpu_status rebuild(sgpu_batch* b) {
     std::vector<FieldItem> fi[2];
-    std::vector<RangeItem> node, src[2], probe, border[2];
+    std::vector<RangeItem> node, mnode, src[2], probe, border[2];
     int nu = 1;
     b->listed.assign(b->slots.size(), 0);
     for (int sl = 0; sl < (int)b->slots.size(); ++sl) {
@@ -487,6 +493,12 @@ sgpu_status rebuild(sgpu_batch* b) {
                 for (long long q = 0; q < c->disp.n[comp]; q += kNodeChunk)
                     node.push_back(RangeItem{sl, comp, q, std::min<long long>(q + kNodeChunk, c->disp.n[comp])});
         }
+        if (c->mdisp_on) {
+            nu = std::max(nu, c->mdisp.nu_max);
+            for (int comp = 0; comp < 3; ++comp)
+                for (long long q = 0; q < c->mdisp.n[comp]; q += kNodeChunk)
+                    mnode.push_back(RangeItem{sl, comp, q, std::min<long long>(q + kNodeChunk, c->mdisp.n[comp])});
+        }
         for (int side = 0; side < 2; ++side)
             for (long long r = 0; r < c->src[side].nrows; r += kRowChunk)
                 src[side].push_back(RangeItem{sl, side, r, std::min<long long>(r + kRowChunk, c->src[side].nrows)});
@@ -504,6 +516,8 @@ sgpu_status rebuild(sgpu_batch* b) {
     }
     if ((s = ensure(b, &b->d_node, &b->cap_node, node.size())) || (s = ensure(b, &b->d_probe, &b->cap_probe, probe.size())))
         return s;
+    if ((s = ensure(b, &b->d_mnode, &b->cap_mnode, mnode.size())) || (s = upload(b, b->d_mnode, mnode))) return s;
+    b->any_mnode = !mnode.empty();
     for (int w = 0; w < 2; ++w) {
         if ((s = ensure(b, &b->d_border[w], &b->cap_border[w], border[w].size()))) return s;
         if ((s = upload(b, b->d_border[w], border[w]))) return s;
@@ -521,6 +535,7 @@ sgpu_status rebuild(sgpu_batch* b) {
     counts[kCntProbe] = (int)probe.size();
     counts[kCntClone] = (int)border[0].size();
     counts[kCntMur] = (int)border[1].size();
+    counts[kCntMNode] = (int)mnode.size();
     if ((s = upload(b, b->d_counts, counts))) return s;
     if (nu > b->nu_max) b->nu_max = nu;
     // the copies read the host vectors; wait before they go out of scope
@@ -551,12 +566,22 @@ bool use_tma(const sgpu_batch* b) {
     return true;
 }
 
-template <int NU> void edisp_batch(sgpu_batch* b, int grid) {
-    k_batch_edisp<NU><<<grid, kPhaseThreads, 0, b->stream>>>(b->d_desc, b->d_node, b->d_counts, b->d_G);
+template <int NU, bool MAG> void ade_batch(sgpu_batch* b, int grid) {
+    k_batch_ade<NU, MAG><<<grid, kPhaseThreads, 0, b->stream>>>(b->d_desc, MAG ? b->d_mnode : b->d_node, b->d_counts, b->d_G);
+}
+
+template <bool MAG> void ade_phase(sgpu_batch* b, int grid) {
+    switch (b->nu_max) {
+        case 1: ade_batch<1, MAG>(b, grid); break;
+        case 2: ade_batch<2, MAG>(b, grid); break;
+        case 3: ade_batch<3, MAG>(b, grid); break;
+        case 4: ade_batch<4, MAG>(b, grid); break;
+        default: ade_batch<kMaxPolesPerMedium, MAG>(b, grid); break;
+    }
 }
 
 // One whole step of every instance in the order of timestepping.F90 (E curl +
-// CPML, ADE, E sources, H curl + CPML, H sources and borders, probes).  With `marks`, an
+// CPML, ADE, E sources, H curl + CPML, magnetic ADE + H sources + borders, probes).  With `marks`, an
 // event is recorded after each of the six phases.
 sgpu_status enqueue_step(sgpu_batch* b, cudaEvent_t* marks = nullptr) {
     const int grid = b->num_sms * b->ctas_per_sm;
@@ -572,13 +597,7 @@ sgpu_status enqueue_step(sgpu_batch* b, cudaEvent_t* marks = nullptr) {
     else
         k_batch_field<0><<<grid, blk, 0, b->stream>>>(b->d_desc, b->d_field[0], b->d_counts, b->d_G);
     mark(0);
-    switch (b->nu_max) {
-        case 1: edisp_batch<1>(b, grid); break;
-        case 2: edisp_batch<2>(b, grid); break;
-        case 3: edisp_batch<3>(b, grid); break;
-        case 4: edisp_batch<4>(b, grid); break;
-        default: edisp_batch<kMaxPolesPerMedium>(b, grid); break;
-    }
+    ade_phase<false>(b, grid);
     mark(1);
     k_batch_sources<<<grid, kPhaseThreads, 0, b->stream>>>(b->d_desc, b->d_src[0], b->d_counts, b->d_G, 0);
     mark(2);
@@ -588,6 +607,7 @@ sgpu_status enqueue_step(sgpu_batch* b, cudaEvent_t* marks = nullptr) {
     else
         k_batch_field<1><<<grid, blk, 0, b->stream>>>(b->d_desc, b->d_field[1], b->d_counts, b->d_G);
     mark(3);
+    if (b->any_mnode) ade_phase<true>(b, grid);
     k_batch_sources<<<grid, kPhaseThreads, 0, b->stream>>>(b->d_desc, b->d_src[1], b->d_counts, b->d_G, 1);
     for (int w = 0; w < 2; ++w)
         if (b->any_border[w])
@@ -603,7 +623,8 @@ sgpu_status enqueue_step(sgpu_batch* b, cudaEvent_t* marks = nullptr) {
 
 sgpu_status ensure_graph(sgpu_batch* b) {
     if (b->graph && b->graph_nu == b->nu_max && b->graph_ctas == b->ctas_per_sm && b->graph_tma == use_tma(b) &&
-        b->graph_border[0] == b->any_border[0] && b->graph_border[1] == b->any_border[1])
+        b->graph_border[0] == b->any_border[0] && b->graph_border[1] == b->any_border[1] &&
+        b->graph_mnode == b->any_mnode)
         return SGPU_OK;
     if (b->graph) {
         cudaGraphExecDestroy(b->graph);
@@ -630,6 +651,7 @@ sgpu_status ensure_graph(sgpu_batch* b) {
     b->graph_tma = use_tma(b);
     b->graph_border[0] = b->any_border[0];
     b->graph_border[1] = b->any_border[1];
+    b->graph_mnode = b->any_mnode;
     return SGPU_OK;
 }
 
@@ -721,6 +743,7 @@ void sgpu_batch_destroy(sgpu_batch* b) {
         cudaFree(b->d_src[s]);
     }
     cudaFree(b->d_node);
+    cudaFree(b->d_mnode);
     cudaFree(b->d_probe);
     cudaFree(b->d_border[0]);
     cudaFree(b->d_border[1]);

@@ -57,7 +57,7 @@ struct MediaMat {
 struct Med {
     float epr = 1, sigma = 0, mur = 1, sigmam = 0;
     int prio = kPrioBackground;
-    bool pec = false, disp = false, inert = false;
+    bool pec = false, disp = false, mdisp = false, inert = false;
     int region = -1;
 };
 
@@ -93,8 +93,8 @@ struct HostState {
     Vec pbe[3], pce[3], pbm[3], pcm[3];
     // descriptors for the level-1 calls (pointers refer to the vectors here)
     sgpu_cpml_desc cd{};
-    std::vector<int> didx, dnp;
-    std::vector<double> dK, dB, dG;
+    std::vector<int> didx, dnp, mdidx, mdnp;      // electric / magnetic pole-residue media
+    std::vector<double> dK, dB, dG, mdK, mdB, mdG;
     std::vector<uint8_t> pec;
     std::vector<float> phys[6][3];
     int phys_lo[6][3];
@@ -358,6 +358,7 @@ void media(HostState& h, const sgpu_problem* p) {
         m.mur = g.mu / h.mu0;
         m.sigmam = g.sigmam;
         m.disp = g.npoles != 0;
+        m.mdisp = g.mpoles != 0;
         m.region = r;
         h.med.push_back(m);
         paint_all(g, ++n);
@@ -387,9 +388,13 @@ void coefficients(HostState& h) {
             h.g1[r] = 1; h.g2[r] = 0; h.gm1[r] = 1; h.gm2[r] = 0;
         } else if (m.pec || r == 0) {
             h.g1[r] = h.g2[r] = h.gm1[r] = h.gm2[r] = 0;
-        } else if (m.disp) {
-            lossy(m.sigmam, mu, h.gm1[r], h.gm2[r]);  // G1/G2 come from the ADE set-up
+        } else if (m.disp && !m.mdisp) {
+            lossy(m.sigmam, mu, h.gm1[r], h.gm2[r]);  // G1/G2 come from the electric ADE set-up
+        } else if (m.mdisp && !m.disp) {
+            lossy(m.sigma, eps, h.g1[r], h.g2[r]);    // GM1/GM2 come from the magnetic ADE set-up
         } else {
+            // also a medium with both kinds of poles: both ADE set-ups
+            // overwrite these values
             lossy(m.sigma, eps, h.g1[r], h.g2[r]);
             lossy(m.sigmam, mu, h.gm1[r], h.gm2[r]);
         }
@@ -553,32 +558,40 @@ void mur_constants(HostState& h) {
     }
 }
 
-// InitEDispersives coefficients (electricdispersive.F90:77-149).
-void edisp(HostState& h, const sgpu_problem* p, std::vector<int>& idx, std::vector<int>& np, std::vector<double>& K,
-           std::vector<double>& B, std::vector<double>& G) {
+// InitEDispersives coefficients (electricdispersive.F90:77-149) and, with
+// mag, those of InitMdispersives (magneticdispersive.F90:79-142): the same
+// construction from the magnetic poles, mu11 and sigmam11, writing GM1/GM2.
+void pole_residue(HostState& h, const sgpu_problem* p, bool mag, std::vector<int>& idx, std::vector<int>& np,
+                  std::vector<double>& K, std::vector<double>& B, std::vector<double>& G) {
     const double dt = h.dt;
+    std::vector<float>& c1 = mag ? h.gm1 : h.g1;
+    std::vector<float>& c2 = mag ? h.gm2 : h.g2;
     for (int m = 1; m <= h.num_media; ++m) {
-        if (!h.med[m].disp) continue;
+        if (!(mag ? h.med[m].mdisp : h.med[m].disp)) continue;
         const sgpu_region& g = p->regions[h.med[m].region];
+        const int npoles = mag ? g.mpoles : g.npoles;
+        const float* res = mag ? g.mresidues : g.residues;
+        const float* bp = mag ? g.mbpoles : g.bpoles;
         std::vector<Cx> kap, bet;
         float tempo = 0.0f;
-        for (int q = 0; q < g.npoles; ++q) {
-            Cx C{(double)g.residues[2 * q], (double)g.residues[2 * q + 1]};
-            Cx a{(double)(-g.bpoles[2 * q]), (double)(-g.bpoles[2 * q + 1])};
+        for (int q = 0; q < npoles; ++q) {
+            Cx C{(double)res[2 * q], (double)res[2 * q + 1]};
+            Cx a{(double)(-bp[2 * q]), (double)(-bp[2 * q + 1])};
             Cx half{(a.r * dt) / 2.0, (a.i * dt) / 2.0};
             Cx den{1.0 - half.r, -half.i};
             kap.push_back(cx_div(Cx{1.0 + half.r, half.i}, den));
             bet.push_back(cx_div(Cx{C.r * dt, C.i * dt}, den));
             tempo = (float)((double)tempo + bet.back().r);
         }
-        const double lo = (double)(2.0f * g.eps + tempo);
-        const double sd = (double)g.sigma * dt;
-        h.g1[m] = (float)((lo - sd) / (lo + sd));
-        h.g2[m] = (float)(((double)2.0f * dt) / (lo + sd));
-        const double half_g2 = (double)(h.g2[m] / 2.0f);
+        const float v11 = mag ? g.mu : g.eps, s11 = mag ? g.sigmam : g.sigma;
+        const double lo = (double)(2.0f * v11 + tempo);
+        const double sd = (double)s11 * dt;
+        c1[m] = (float)((lo - sd) / (lo + sd));
+        c2[m] = (float)(((double)2.0f * dt) / (lo + sd));
+        const double half_g2 = (double)(c2[m] / 2.0f);
         idx.push_back(m);
-        np.push_back(g.npoles);
-        for (int q = 0; q < g.npoles; ++q) {
+        np.push_back(npoles);
+        for (int q = 0; q < npoles; ++q) {
             K.push_back(kap[q].r); K.push_back(kap[q].i);
             B.push_back(bet[q].r); B.push_back(bet[q].i);
             G.push_back(half_g2 * (1.0 + kap[q].r)); G.push_back(half_g2 * kap[q].i);
@@ -750,7 +763,10 @@ HostState* make_plan(const sgpu_problem* p, int max_steps, sgpu_status* rc) {
         if (kind == 9 && p->pml_layers[f] < 1) { *rc = SGPU_ERR_ARG; return nullptr; }
     }
     for (int r = 0; r < p->nregions; ++r)
-        if (p->regions[r].kind < 0 || p->regions[r].kind > 2 || (p->regions[r].nboxes > 0 && !p->regions[r].boxes)) {
+        if (p->regions[r].kind < 0 || p->regions[r].kind > 2 || (p->regions[r].nboxes > 0 && !p->regions[r].boxes) ||
+            p->regions[r].npoles < 0 || p->regions[r].mpoles < 0 ||
+            (p->regions[r].kind == 2 && p->regions[r].npoles > 0 && (!p->regions[r].residues || !p->regions[r].bpoles)) ||
+            (p->regions[r].kind == 2 && p->regions[r].mpoles > 0 && (!p->regions[r].mresidues || !p->regions[r].mbpoles))) {
             *rc = SGPU_ERR_ARG;
             return nullptr;
         }
@@ -765,7 +781,8 @@ HostState* make_plan(const sgpu_problem* p, int max_steps, sgpu_status* rc) {
         metrics(*h);
         cpml(*h, p, h->cd);
         mur_constants(*h);
-        edisp(*h, p, h->didx, h->dnp, h->dK, h->dB, h->dG);
+        pole_residue(*h, p, false, h->didx, h->dnp, h->dK, h->dB, h->dG);
+        pole_residue(*h, p, true, h->mdidx, h->mdnp, h->mdK, h->mdB, h->mdG);
         h->pec.resize(h->num_media + 1);
         for (int m = 0; m <= h->num_media; ++m) h->pec[m] = h->med[m].pec ? 1 : 0;
         planewaves(*h, p);
@@ -834,6 +851,10 @@ sgpu_status realize(HostState* h, sgpu::Arena* arena, cudaStream_t stream, sgpu_
     if (borders && (s = sgpu_init_borders(c, &bd))) return s;
     sgpu_edisp_desc ed{(int)h->didx.size(), h->didx.data(), h->dnp.data(), h->dK.data(), h->dB.data(), h->dG.data()};
     if ((s = sgpu_init_edisp(c, &ed))) return s;
+    if (!h->mdidx.empty()) {
+        sgpu_edisp_desc md{(int)h->mdidx.size(), h->mdidx.data(), h->mdnp.data(), h->mdK.data(), h->mdB.data(), h->mdG.data()};
+        if ((s = sgpu_init_mdisp(c, &md))) return s;
+    }
     for (const sgpu_planewave_desc& d : h->pw)
         if ((s = sgpu_add_planewave(c, &d))) return s;
     for (const sgpu_nodal_desc& d : h->nodal)
@@ -901,17 +922,20 @@ sgpu_status sgpu_host_footprint(const sgpu_ctx* c, uint64_t* bytes) {
             if (l.xe >= l.xi && l.ye >= l.yi && l.ze >= l.zi)
                 b += (uint64_t)(l.xe - l.xi + 1) * (l.ye - l.yi + 1) * (l.ze - l.zi + 1) * 4;
         }
-    // ADE state: swept E nodes of dispersive media
-    if (!h->didx.empty()) {
+    // ADE state: swept E (H) nodes of electric (magnetic) pole-residue media
+    for (int side = 0; side < 2; ++side) {
+        const std::vector<int>& idx = side ? h->mdidx : h->didx;
+        const std::vector<int>& np = side ? h->mdnp : h->dnp;
+        if (idx.empty()) continue;
         std::vector<char> disp(h->num_media + 1, 0);
         int nu = 0;
-        for (size_t m = 0; m < h->didx.size(); ++m) {
-            disp[h->didx[m]] = 1;
-            nu = std::max(nu, h->dnp[m]);
+        for (size_t m = 0; m < idx.size(); ++m) {
+            disp[idx[m]] = 1;
+            nu = std::max(nu, np[m]);
         }
         uint64_t nodes = 0;
         bool have = true;
-        for (int f = 0; f < 3; ++f) {
+        for (int f = 3 * side; f < 3 * side + 3; ++f) {
             if (h->mm[f].v.empty()) { have = false; break; }
             const Box& w = h->sweep[f];
             MediaMat& m = const_cast<MediaMat&>(h->mm[f]);
@@ -964,16 +988,19 @@ sgpu_status sgpu_batch_footprint(const sgpu_ctx* c, uint64_t* bytes, uint64_t* l
         }
     // ADE: per component node list, slot, previous field and state; the
     // per-row count/offset scratch of the set-up is live at the same time
-    if (!h->didx.empty()) {
+    for (int side = 0; side < 2; ++side) {
+        const std::vector<int>& idx = side ? h->mdidx : h->didx;
+        const std::vector<int>& np = side ? h->mdnp : h->dnp;
+        if (idx.empty()) continue;
         std::vector<char> disp(h->num_media + 1, 0);
         int nu = 0;
-        for (size_t m = 0; m < h->didx.size(); ++m) {
-            disp[h->didx[m]] = 1;
-            nu = std::max(nu, h->dnp[m]);
+        for (size_t m = 0; m < idx.size(); ++m) {
+            disp[idx[m]] = 1;
+            nu = std::max(nu, np[m]);
         }
-        buf(h->didx.size() * 512 + 64);  // medium table
-        buf(n1 * 2);                      // slot of medium
-        for (int f = 0; f < 3; ++f) {
+        buf(idx.size() * sizeof(sgpu::DispMedium) + 64);  // medium table
+        buf(n1 * 2);                                      // slot of medium
+        for (int f = 3 * side; f < 3 * side + 3; ++f) {
             uint64_t nodes = 0;
             const Box& w = h->sweep[f];
             if (h->mm[f].v.empty()) {

@@ -192,10 +192,10 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
     else h_consume<false>(t, 0, g, cp, t1, t2, err, false);
 }
 
-template <int NU>
-__global__ void __launch_bounds__(256) k_edisp(KGrid g, KDisp d, int comp) {
+template <int NU, bool MAG>
+__global__ void __launch_bounds__(256) k_ade(KGrid g, KDisp d, int comp) {
     const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (q < d.n[comp]) edisp_node<NU>(g, d, comp, q);
+    if (q < d.n[comp]) ade_node<NU, MAG>(g, d, comp, q);
 }
 
 
@@ -395,28 +395,32 @@ bool ready(sgpu_ctx* c) {
 
 sgpu_status build_sources(sgpu_ctx* c);
 
-template <int NU> void edisp_launch(sgpu_ctx* c, int comp, unsigned blocks) {
-    k_edisp<NU><<<blocks, 256, 0, c->stream>>>(kgrid(c), c->disp, comp);
+template <int NU, bool MAG> void ade_launch(sgpu_ctx* c, int comp, unsigned blocks) {
+    k_ade<NU, MAG><<<blocks, 256, 0, c->stream>>>(kgrid(c), MAG ? c->mdisp : c->disp, comp);
 }
 
-sgpu_status launch_edisp(sgpu_ctx* c) {
-    if (!c->disp_on) return SGPU_OK;
+template <bool MAG> sgpu_status launch_ade_side(sgpu_ctx* c) {
+    const KDisp& d = MAG ? c->mdisp : c->disp;
+    if (!(MAG ? c->mdisp_on : c->disp_on)) return SGPU_OK;
     for (int comp = 0; comp < 3; ++comp) {
-        long long n = c->disp.n[comp];
+        long long n = d.n[comp];
         if (n == 0) continue;
         const unsigned blocks = (unsigned)((n + 255) / 256);
-        switch (c->disp.nu_max) {
-            case 1: edisp_launch<1>(c, comp, blocks); break;
-            case 2: edisp_launch<2>(c, comp, blocks); break;
-            case 3: edisp_launch<3>(c, comp, blocks); break;
-            case 4: edisp_launch<4>(c, comp, blocks); break;
-            default: edisp_launch<kMaxPolesPerMedium>(c, comp, blocks); break;
+        switch (d.nu_max) {
+            case 1: ade_launch<1, MAG>(c, comp, blocks); break;
+            case 2: ade_launch<2, MAG>(c, comp, blocks); break;
+            case 3: ade_launch<3, MAG>(c, comp, blocks); break;
+            case 4: ade_launch<4, MAG>(c, comp, blocks); break;
+            default: ade_launch<kMaxPolesPerMedium, MAG>(c, comp, blocks); break;
         }
-        sgpu_status s = check_launch(c, "k_edisp");
+        sgpu_status s = check_launch(c, "k_ade");
         if (s) return s;
     }
     return SGPU_OK;
 }
+
+sgpu_status launch_edisp(sgpu_ctx* c) { return launch_ade_side<false>(c); }
+sgpu_status launch_mdisp(sgpu_ctx* c) { return launch_ade_side<true>(c); }
 
 constexpr int kMaskPW = 1 << kSrcPlaneWave, kMaskNodal = (1 << kSrcNodalSoft) | (1 << kSrcNodalHard),
               kMaskAll = kMaskPW | kMaskNodal;
@@ -494,6 +498,7 @@ sgpu_status half_e(sgpu_ctx* c, StepRef sr) {
 sgpu_status half_h(sgpu_ctx* c, StepRef sr) {
     sgpu_status s = field_h(c);
     if (s) return s;
+    if ((s = launch_mdisp(c))) return s;
     if ((s = launch_sources(c, 1, sr))) return s;
     return launch_borders_h(c);
 }
@@ -677,6 +682,7 @@ void sgpu_destroy(sgpu_ctx* c) {
     free_list(c, c->cpml_allocs);
     free_list(c, c->border_allocs);
     free_list(c, c->disp_allocs);
+    free_list(c, c->mdisp_allocs);
     free_list(c, c->src_allocs[0]);
     free_list(c, c->src_allocs[1]);
     free_list(c, c->probe_allocs);
@@ -893,12 +899,21 @@ sgpu_status sgpu_init_borders(sgpu_ctx* c, const sgpu_border_desc* d) {
     return SGPU_OK;
 }
 
-sgpu_status sgpu_init_edisp(sgpu_ctx* c, const sgpu_edisp_desc* d) {
-    if (!c || !d) return set_error(c, SGPU_ERR_ARG, "null edisp descriptor");
-    if (!ready(c)) return set_error(c, SGPU_ERR_STATE, "upload the media matrices before sgpu_init_edisp");
-    free_list(c, c->disp_allocs);
-    c->disp = KDisp{};
-    c->disp_on = false;
+}  // extern "C"
+
+namespace {
+// InitEDispersives / InitMdispersives on the device: the media table, and
+// per E (H) component the node list of every swept node whose medium is in
+// the table, in k, j, i order, with zero state.
+sgpu_status init_ade(sgpu_ctx* c, const sgpu_edisp_desc* d, bool mag) {
+    if (!c || !d) return set_error(c, SGPU_ERR_ARG, "null pole-residue descriptor");
+    if (!ready(c)) return set_error(c, SGPU_ERR_STATE, "upload the media matrices before the pole-residue set-up");
+    std::vector<void*>& allocs = mag ? c->mdisp_allocs : c->disp_allocs;
+    bool& on = mag ? c->mdisp_on : c->disp_on;
+    const int c0 = mag ? 3 : 0;
+    free_list(c, allocs);
+    (mag ? c->mdisp : c->disp) = KDisp{};
+    on = false;
     if (d->nmedia <= 0) return SGPU_OK;
     if (d->nmedia > 255) return set_error(c, SGPU_ERR_UNSUPPORTED, "more than 255 dispersive media");
     std::vector<DispMedium> media(d->nmedia);
@@ -940,23 +955,24 @@ sgpu_status sgpu_init_edisp(sgpu_ctx* c, const sgpu_edisp_desc* d) {
     sgpu_status s;
     DispMedium* dmedia;
     int16_t* dslot;
-    if ((s = dalloc(c, &dmedia, media.size(), &c->disp_allocs))) return s;
+    if ((s = dalloc(c, &dmedia, media.size(), &allocs))) return s;
     if ((s = h2d(c, dmedia, media.data(), media.size()))) return s;
-    if ((s = dalloc(c, &dslot, slot.size(), &c->disp_allocs))) return s;
+    if ((s = dalloc(c, &dslot, slot.size(), &allocs))) return s;
     if ((s = h2d(c, dslot, slot.data(), slot.size()))) return s;
-    KDisp& k = c->disp;
+    KDisp& k = mag ? c->mdisp : c->disp;
     k.media = dmedia;
     k.slot_of_medium = dslot;
     k.nu_max = nu_max;
     k.dt = c->dt;
     for (int comp = 0; comp < 3; ++comp) {
-        int x0 = c->sweep[comp].xi - c->ox, x1 = c->sweep[comp].xe - c->ox;
-        int y0 = c->sweep[comp].yi - c->oy, y1 = c->sweep[comp].ye - c->oy;
-        int z0 = c->sweep[comp].zi - c->oz, z1 = c->sweep[comp].ze - c->oz;
+        const sgpu_lim& w = c->sweep[c0 + comp];
+        int x0 = w.xi - c->ox, x1 = w.xe - c->ox;
+        int y0 = w.yi - c->oy, y1 = w.ye - c->oy;
+        int z0 = w.zi - c->oz, z1 = w.ze - c->oz;
         long long rows = (long long)(y1 - y0 + 1) * (z1 - z0 + 1);
         int* dcount;
         if ((s = dalloc(c, &dcount, rows))) return s;
-        k_count_disp<<<(unsigned)((rows + 255) / 256), 256, 0, c->stream>>>(c->M[comp], dslot, c->pitch, c->plane, x0, x1,
+        k_count_disp<<<(unsigned)((rows + 255) / 256), 256, 0, c->stream>>>(c->M[c0 + comp], dslot, c->pitch, c->plane, x0, x1,
                                                                             y0, y1, z0, z1, dcount);
         if ((s = check_launch(c, "k_count_disp"))) { dev_free(c, dcount); return s; }
         std::vector<int> cnt(rows);
@@ -976,12 +992,12 @@ sgpu_status sgpu_init_edisp(sgpu_ctx* c, const sgpu_edisp_desc* d) {
         uint8_t* med;
         float* prev;
         double2* J;
-        if ((s = dalloc(c, &node, tot, &c->disp_allocs)) || (s = dalloc(c, &med, tot, &c->disp_allocs)) ||
-            (s = dalloc(c, &prev, tot, &c->disp_allocs)) || (s = dalloc(c, &J, (size_t)tot * std::max(1, nu_max), &c->disp_allocs))) {
+        if ((s = dalloc(c, &node, tot, &allocs)) || (s = dalloc(c, &med, tot, &allocs)) ||
+            (s = dalloc(c, &prev, tot, &allocs)) || (s = dalloc(c, &J, (size_t)tot * std::max(1, nu_max), &allocs))) {
             dev_free(c, doffs);
             return s;
         }
-        k_fill_disp<<<(unsigned)((rows + 255) / 256), 256, 0, c->stream>>>(c->M[comp], dslot, c->pitch, c->plane, x0, x1, y0,
+        k_fill_disp<<<(unsigned)((rows + 255) / 256), 256, 0, c->stream>>>(c->M[c0 + comp], dslot, c->pitch, c->plane, x0, x1, y0,
                                                                            y1, z0, z1, doffs, node, med);
         if ((s = check_launch(c, "k_fill_disp"))) { dev_free(c, doffs); return s; }
         CUDA_TRY(c, cudaMemsetAsync(prev, 0, tot * sizeof(float), c->stream));
@@ -993,9 +1009,15 @@ sgpu_status sgpu_init_edisp(sgpu_ctx* c, const sgpu_edisp_desc* d) {
         k.prev[comp] = prev;
         k.J[comp] = J;
     }
-    c->disp_on = (k.n[0] + k.n[1] + k.n[2]) > 0;
+    on = (k.n[0] + k.n[1] + k.n[2]) > 0;
     return SGPU_OK;
 }
+}  // namespace
+
+extern "C" {
+
+sgpu_status sgpu_init_edisp(sgpu_ctx* c, const sgpu_edisp_desc* d) { return init_ade(c, d, false); }
+sgpu_status sgpu_init_mdisp(sgpu_ctx* c, const sgpu_edisp_desc* d) { return init_ade(c, d, true); }
 
 }  // extern "C"
 
@@ -1287,6 +1309,7 @@ sgpu_status sgpu_advance_electric_cpml(sgpu_ctx* c) {
     return c->cpml.on ? launch_e<kCpml | kAll>(c) : SGPU_OK;
 }
 sgpu_status sgpu_advance_edispersive_e(sgpu_ctx* c) { SGPU_READY(c); return launch_edisp(c); }
+sgpu_status sgpu_advance_mdispersive_h(sgpu_ctx* c) { SGPU_READY(c); return launch_mdisp(c); }
 sgpu_status sgpu_advance_planewave_e(sgpu_ctx* c, int n) {
     SGPU_READY(c);
     return launch_sources(c, 0, StepRef{nullptr, n}, kMaskPW);
@@ -1405,6 +1428,7 @@ sgpu_status sgpu_profile_steps(sgpu_ctx* c, int n0, int count, float* ms6) {
         cudaEventRecord(ev[3], c->stream);
         if (!s) s = field_h(c);
         cudaEventRecord(ev[4], c->stream);
+        if (!s) s = launch_mdisp(c);
         if (!s) s = launch_sources(c, 1, sr);
         if (!s) s = launch_borders_h(c);
         cudaEventRecord(ev[5], c->stream);
@@ -1445,15 +1469,17 @@ sgpu_status sgpu_algorithmic_bytes(const sgpu_ctx* c, double* b6) {
     for (int f = 3; f < 6; ++f) h += cells(c->sweep[f]) * 10.0 + cells(c->sweep[f - 3]) * 4.0;
     b6[0] = e + psi_bytes(0);
     // ADE node: index 4 + medium slot 1 + E 8 + previous E 8 + 32 per state slot
-    double nodes = 0;
+    double nodes = 0, mnodes = 0;
     for (int comp = 0; comp < 3; ++comp) nodes += (double)c->disp.n[comp];
+    for (int comp = 0; comp < 3; ++comp) mnodes += (double)c->mdisp.n[comp];
     b6[1] = c->disp_on ? nodes * (21.0 + 32.0 * c->disp.nu_max) : 0.0;
     b6[2] = 0;
     b6[3] = h + psi_bytes(3);
     // H sources (not counted) and borders: a clone cell reads and writes 4 B
     // each; a Mur cell reads H, its medium and both Past_ values and writes H
     // and both Past_ values (26 B)
-    b6[4] = 8.0 * (double)c->border.cl_cells + 26.0 * (double)c->border.mur_cells;
+    b6[4] = 8.0 * (double)c->border.cl_cells + 26.0 * (double)c->border.mur_cells +
+            (c->mdisp_on ? mnodes * (21.0 + 32.0 * c->mdisp.nu_max) : 0.0);
     b6[5] = 8.0 * c->probes.n;
     return SGPU_OK;
 }
@@ -1466,6 +1492,7 @@ sgpu_status sgpu_kernels_per_step(const sgpu_ctx* c, int* n) {
     if (!c || !n) return SGPU_ERR_ARG;
     int k = 2;  // E and H field kernels
     for (int comp = 0; comp < 3; ++comp) k += c->disp_on && c->disp.n[comp] > 0;
+    for (int comp = 0; comp < 3; ++comp) k += c->mdisp_on && c->mdisp.n[comp] > 0;
     k += c->src[0].nrows > 0;
     k += c->src[1].nrows > 0;
     k += c->probes.n > 0;
@@ -1617,8 +1644,10 @@ sgpu_status sgpu_device_bytes(const sgpu_ctx* c, uint64_t* bytes) {
                 const Slab& sl = c->cpml.s[f][w][s];
                 if (sl.psi) b += (uint64_t)(sl.xhi - sl.xlo + 1) * (sl.yhi - sl.ylo + 1) * (sl.zhi - sl.zlo + 1) * 4;
             }
-    for (int comp = 0; comp < 3; ++comp)
+    for (int comp = 0; comp < 3; ++comp) {
         b += (uint64_t)c->disp.n[comp] * (4 + 1 + 4 + 16 * (uint64_t)std::max(1, c->disp.nu_max));
+        b += (uint64_t)c->mdisp.n[comp] * (4 + 1 + 4 + 16 * (uint64_t)std::max(1, c->mdisp.nu_max));
+    }
     b += (uint64_t)c->border.mur_cells * 2 * sizeof(float);
     *bytes = b;
     return SGPU_OK;

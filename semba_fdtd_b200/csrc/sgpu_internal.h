@@ -49,7 +49,8 @@ struct KCpml {
     int on;
 };
 
-// Electric pole-residue media (folded conjugate pairs share one state).
+// Pole-residue media, electric or magnetic (folded conjugate pairs share one
+// state).
 struct DispMedium {
     int np;                       // poles of the reference
     int nu;                       // unique poles carrying state
@@ -178,10 +179,10 @@ struct sgpu_ctx {
     // CPML
     sgpu::KCpml cpml{};
     std::vector<void*> cpml_allocs;
-    // ADE
-    bool disp_on = false;
-    sgpu::KDisp disp{};
-    std::vector<void*> disp_allocs;
+    // ADE: electric (disp) and magnetic (mdisp) pole-residue media
+    bool disp_on = false, mdisp_on = false;
+    sgpu::KDisp disp{}, mdisp{};
+    std::vector<void*> disp_allocs, mdisp_allocs;
     // borders (PMC / periodic clones, Mur)
     sgpu::KBorder border{};
     std::vector<void*> border_allocs;

@@ -304,17 +304,20 @@ __device__ __forceinline__ void hfield_column(const KGrid& g, const KCpml& cp, c
 }
 
 
-// AdvanceEDispersiveE (electricdispersive.F90:304-362): one thread per node.
+// AdvanceEDispersiveE (electricdispersive.F90:304-362) and, with MAG,
+// AdvanceMdispersiveH (magneticdispersive.F90:298-360): one thread per node.
 // Conjugate poles share one state slot; the subtraction still runs once
 // per pole of the reference, in its order, and Re(conj(g)*conj(J)) equals
-// Re(g*J) exactly.  NU (the largest number of state slots of any medium) is
-// a template parameter so the states stay in registers.
-template <int NU>
-__device__ __forceinline__ void edisp_node(const KGrid& g, const KDisp& d, int comp, long long q) {
+// Re(g*J) exactly.  The electric current takes (Beta*(E-Eprev))/dt, the
+// magnetic one (Beta/dt)*(H-Hprev), as the two routines are written.  NU
+// (the largest number of state slots of any medium) is a template parameter
+// so the states stay in registers.
+template <int NU, bool MAG>
+__device__ __forceinline__ void ade_node(const KGrid& g, const KDisp& d, int comp, long long q) {
     const long long n = d.n[comp];
     const int idx = d.node[comp][q];
     const DispMedium* __restrict__ md = d.media + d.med[comp][q];
-    float* F = g.F[comp];
+    float* F = g.F[MAG ? 3 + comp : comp];
     double2* J = d.J[comp];
     const int nu = md->nu;
     double2 st[NU];
@@ -338,8 +341,8 @@ __device__ __forceinline__ void edisp_node(const KGrid& g, const KDisp& d, int c
             const double2 kp = md->kappa[u], bt = md->beta[u];
             const double kr = kp.x * st[u].x - kp.y * st[u].y;
             const double ki = kp.x * st[u].y + kp.y * st[u].x;
-            const double br = (bt.x * dd) / d.dt;
-            const double bi = (bt.y * dd) / d.dt;
+            const double br = MAG ? (bt.x / d.dt) * dd : (bt.x * dd) / d.dt;
+            const double bi = MAG ? (bt.y / d.dt) * dd : (bt.y * dd) / d.dt;
             J[u * n + q] = make_double2(kr + br, ki + bi);
         }
     }

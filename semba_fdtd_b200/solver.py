@@ -10,7 +10,7 @@ Three ways to advance, all bit-identical:
   timestepping.F90:1286-1742 (Advance_Ex, Ey, Ez, AdvanceelectricCPML,
   AdvanceEDispersiveE, AdvancePlaneWaveE, AdvanceNodalE, Advance_Hx, Hy, Hz,
   AdvanceMagneticCPML, MinusCloneMagneticPMC, CloneMagneticPeriodic,
-  AdvancePlaneWaveH, AdvanceNodalH, MinusCloneMagneticPMC,
+  AdvanceMdispersiveH, AdvancePlaneWaveH, AdvanceNodalH, MinusCloneMagneticPMC,
   CloneMagneticPeriodic, AdvanceMagneticMUR, UpdateObservation).
 """
 from __future__ import annotations
@@ -110,7 +110,8 @@ class Solver:
                     self._check(lib.sgpu_advance_planewave_e(h, n))
                     self._check(lib.sgpu_advance_nodal_e(h, n))
                     for f in (lib.sgpu_advance_hx, lib.sgpu_advance_hy, lib.sgpu_advance_hz,
-                              lib.sgpu_advance_magnetic_cpml, lib.sgpu_advance_pmc_h, lib.sgpu_advance_periodic_h):
+                              lib.sgpu_advance_magnetic_cpml, lib.sgpu_advance_pmc_h, lib.sgpu_advance_periodic_h,
+                              lib.sgpu_advance_mdispersive_h):
                         self._check(f(h))
                     self._check(lib.sgpu_advance_planewave_h(h, n))
                     self._check(lib.sgpu_advance_nodal_h(h, n))

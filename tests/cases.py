@@ -51,4 +51,11 @@ def closed(steps=160):
     return replace(pb, borders=("pmc", "pmc", "periodic", "periodic", "pec", "mur"))
 
 
-ALL = {"small": small, "mid": mid, "disp": disp, "mur": mur, "mixed": mixed, "closed": closed}
+@lru_cache(maxsize=None)
+def mdisp(steps=140):
+    """Magnetic pole-residue blocks (alone and with electric poles) and an
+    electric one."""
+    return read_case(casegen.magnetic_dispersive(_DIR / "mdisp", steps=steps))
+
+
+ALL = {"small": small, "mid": mid, "disp": disp, "mur": mur, "mixed": mixed, "closed": closed, "mdisp": mdisp}

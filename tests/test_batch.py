@@ -101,11 +101,12 @@ def test_arena_too_small_is_refused_cleanly():
 
 
 @pytest.mark.parametrize("family", [1, 0], ids=["tma", "regs"])
-def test_batch_with_every_border_kind(family):
-    """Mur, PEC, PMC, periodic and CPML(+Mur) instances next to a CPML one:
-    the clone and Mur phases run over the instances that have them."""
-    from cases import closed, mixed, mur
-    pbs = [mur(), mixed(), closed(), _instances()[1]]
+def test_batch_with_every_border_kind_and_magnetic_ade(family):
+    """Mur, PEC, PMC, periodic and CPML(+Mur) instances and one with magnetic
+    pole-residue media next to a CPML one: the clone, Mur and magnetic ADE
+    phases run over the instances that have them."""
+    from cases import closed, mdisp, mixed, mur
+    pbs = [mur(), mixed(), closed(), mdisp(), _instances()[1]]
     with Batch(1 << 30, 8, kernel_family=family) as b:
         slots = [b.add(pb) for pb in pbs]
         b.run_all()

@@ -11,7 +11,8 @@ reference's own parser fixture:
 * CPML reflection against a domain large enough to have none in the window
   (borderscpml.F90:584-1176, 1465-1733);
 * Debye relaxation of a uniform field in a single-real-pole medium converges
-  to the analytic solution (electricdispersive.F90:77-362);
+  to the analytic solution (electricdispersive.F90:77-362), and its magnetic
+  dual (magneticdispersive.F90:79-360);
 * FP32 against FP64 oracle per probe;
 * borders (healer.F90:1442-1617, bordersother.F90:65-190,
   bordersmur.F90:1129-1650): a PEC box keeps tangential E and normal H at
@@ -141,6 +142,41 @@ def _debye_error(m, n=40, steps=18):
     t = np.arange(steps) * dt
     exact = eps_inf / eps_s + (1 - eps_inf / eps_s) * np.exp(-t / tau_e)
     return np.abs(tr - exact).max()
+
+
+def _magnetic_debye_error(m, n=40, steps=18):
+    """The dual of _debye_error: a uniform H = 1 in a single-real-pole
+    magnetic medium (mu_inf 2, mu_s 6) relaxes as
+    H(t) = mu_inf/mu_s + (1 - mu_inf/mu_s) exp(-t/tau_H)."""
+    from semba_fdtd_b200.case import MU0
+    pb = _box(n, steps, 4)
+    dt = oracle.Oracle(pb, fp64=True).dt
+    mu_inf, mu_s = 2.0, 6.0
+    tau_h = m * dt
+    tau = tau_h * mu_s / mu_inf
+    a = -1.0 / tau
+    r = (mu_s - mu_inf) * float(MU0) / tau
+    pb.regions = [Region(kind=2, boxes=np.array([[0, n - 1] * 3], np.int32), eps=float(EPS0),
+                         mu=float(np.float32(mu_inf) * MU0),
+                         mresidues=np.array([r], np.complex64), mbpoles=np.array([-a], np.complex64))]
+    pb.probes = np.array([[3, n // 2, n // 2, n // 2]], np.int32)
+    o = oracle.Oracle(pb, fp64=True)
+    for c in range(3, 6):
+        _fill(o, c, lambda i, j, k: np.ones(i.shape))
+    tr = o.step(steps)[:, 0].astype(np.float64)
+    t = np.arange(steps) * dt
+    exact = mu_inf / mu_s + (1 - mu_inf / mu_s) * np.exp(-t / tau_h)
+    return np.abs(tr - exact).max(), tr
+
+
+def test_magnetic_debye_relaxation_converges_to_analytic():
+    """AdvanceMdispersiveH (magneticdispersive.F90:298-360) by duality with
+    the electric test: second-order convergence of the relaxation."""
+    e12, tr = _magnetic_debye_error(12)
+    e24, _ = _magnetic_debye_error(24)
+    assert tr[0] == 1.0 and np.all(np.diff(tr) < 0)  # the state starts at zero
+    assert e24 < 5e-3
+    assert e12 / e24 > 2.0
 
 
 def test_debye_relaxation_converges_to_analytic():
