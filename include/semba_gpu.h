@@ -412,8 +412,8 @@ sgpu_status sgpu_batch_footprint(const sgpu_ctx* plan, uint64_t* bytes, uint64_t
  * kernels (each instance's tensor maps in global memory), 0 the
  * register-marching kernels.  Both give identical results. */
 sgpu_status sgpu_batch_set_kernel_family(sgpu_batch* b, int family);
-/* Launch shape: z-chunk length of the field work items for the three size
- * classes (Alloc z extent <= 80, <= 160, larger) and persistent CTAs per SM.
+/* Launch shape: z-chunk length (1..64) of the field work items for the three
+ * size classes (Alloc z extent <= 80, <= 160, larger) and persistent CTAs per SM.
  * Either may be NULL / 0 to keep the current value. */
 sgpu_status sgpu_batch_set_tuning(sgpu_batch* b, const int* chunk3, int ctas_per_sm);
 sgpu_status sgpu_batch_get_tuning(const sgpu_batch* b, int* chunk3, int* ctas_per_sm);

@@ -211,6 +211,7 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
                       const int* counts, const int* G, int* err) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ WarpView views[kConsumerWarps];
+    __shared__ ProdTable tb;
     TmaCta t = tma_cta_setup(smem, 0, 0, 0, 1);
     const int n_items = counts[SIDE == 0 ? kCntE : kCntH];
     const bool producer = t.warp == kConsumerWarps;
@@ -227,30 +228,42 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
         t.kb = w.kb;
         t.ke = w.ke;
         const int np = w.ke - w.kb + 2;  // the item's planes, edge plane included
+        const int c0 = SIDE == 0 ? 0 : 3;
         if (producer) {
+            // CPML items stage their psi tiles through the ring when the tile
+            // has at most kPsiSlots slabs (the consumers derive the same mask)
+            const int p0 = SIDE == 0 ? w.kb - 1 : w.kb, p1 = SIDE == 0 ? w.ke : w.ke + 1;
+            const int edge = SIDE == 0 ? w.kb - 1 : w.ke + 1;
+            const unsigned tmask = w.cp ? cpml_tile_mask(D.cp, c0, w.ib, w.ib + kTX - 1, w.jb, w.jb + kTY - 1) : 0u;
+            const unsigned smask = __popc(tmask) <= kPsiSlots ? tmask : 0u;
+            prod_prepare(&tb, t, p0, p1, edge, SIDE != 0, D.g, D.cp, tmask);
+            int got = np;
             if (t.lane == 0) {
                 const CUtensorMap* m = maps[2 * w.slot + SIDE].m;
                 if (fenced != w.slot) {
-                    for (int q = 0; q < 9; ++q) tensormap_acquire(&m[q]);
+                    for (int q = 0; q < kPsiMap0 + 12; ++q) tensormap_acquire(&m[q]);
                     fenced = w.slot;
                 }
-                const int got = SIDE == 0 ? tma_issue(t, m, gp, w.kb - 1, w.ke, w.kb - 1, false, err)
-                                          : tma_issue(t, m, gp, w.kb, w.ke + 1, w.ke + 1, true, err);
-                if (got < np) {
-                    tma_drain(t, gp + (unsigned)got, err, 15);
-                    return;
-                }
+                got = tma_issue(t, m, gp, p0, p1, edge, SIDE != 0, err, &tb, smask);
+            }
+            got = __shfl_sync(0xffffffffu, got, 0);
+            if (got < np) {
+                if (t.lane == 0) tma_drain(t, gp + (unsigned)got, err, 15);
+                return;
             }
         } else {
             const WarpView& V = stage_view(&views[t.warp], D, w.cp != 0, t.lane);
             const KGrid& g = V.g;
+            const unsigned smask = w.cp ? staged_mask(V.cp, c0, w.ib, w.jb) : 0u;
             bool ok;
             if (SIDE == 0)
-                ok = w.cp ? e_consume<true>(t, gp, g, V.cp, g.g1, g.g2, err, true)
-                          : e_consume<false>(t, gp, g, V.cp, g.g1, g.g2, err, true);
+                ok = smask  ? e_consume<2>(t, gp, g, V.cp, g.g1, g.g2, err, true)
+                     : w.cp ? e_consume<1>(t, gp, g, V.cp, g.g1, g.g2, err, true)
+                            : e_consume<0>(t, gp, g, V.cp, g.g1, g.g2, err, true);
             else
-                ok = w.cp ? h_consume<true>(t, gp, g, V.cp, g.gm1, g.gm2, err, true)
-                          : h_consume<false>(t, gp, g, V.cp, g.gm1, g.gm2, err, true);
+                ok = smask  ? h_consume<2>(t, gp, g, V.cp, g.gm1, g.gm2, err, true)
+                     : w.cp ? h_consume<1>(t, gp, g, V.cp, g.gm1, g.gm2, err, true)
+                            : h_consume<0>(t, gp, g, V.cp, g.gm1, g.gm2, err, true);
             if (!ok) return;
         }
         gp += (unsigned)np;
@@ -392,6 +405,10 @@ struct sgpu_batch {
     int graph_nu = 0, graph_ctas = 0;
     bool graph_tma = false, graph_border[2] = {}, graph_mnode = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // instances are set up on their own stream, so host set-up and uploads
+    // overlap the steps already queued; the batch stream waits on setup_done
+    cudaStream_t setup = nullptr;
+    cudaEvent_t setup_done = nullptr;
 };
 
 namespace sgpu {
@@ -538,8 +555,9 @@ sgpu_status rebuild(sgpu_batch* b) {
     counts[kCntMNode] = (int)mnode.size();
     if ((s = upload(b, b->d_counts, counts))) return s;
     if (nu > b->nu_max) b->nu_max = nu;
-    // the copies read the host vectors; wait before they go out of scope
-    BTRY(b, cudaStreamSynchronize(b->stream));
+    // no wait: an asynchronous copy from pageable host memory has staged the
+    // data by the time it returns, so the vectors may go out of scope, and
+    // the steps already queued keep running meanwhile
     b->dirty = false;
     return SGPU_OK;
 }
@@ -699,6 +717,8 @@ sgpu_status sgpu_batch_create(uint64_t arena_bytes, int max_instances, sgpu_batc
     BTRY(b, cudaGetDevice(&b->device));
     cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, b->device);
     BTRY(b, cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    BTRY(b, cudaStreamCreateWithFlags(&b->setup, cudaStreamNonBlocking));
+    BTRY(b, cudaEventCreateWithFlags(&b->setup_done, cudaEventDisableTiming));
     void* base = nullptr;
     if (cudaMalloc(&base, arena_bytes) != cudaSuccess) {
         cudaGetLastError();
@@ -723,12 +743,16 @@ sgpu_status sgpu_batch_create(uint64_t arena_bytes, int max_instances, sgpu_batc
     BTRY(b, cudaMemcpyAsync(b->d_desc, off.data(), sizeof(InstDesc) * max_instances, cudaMemcpyHostToDevice, b->stream));
     BTRY(b, cudaEventCreate(&b->ev0));
     BTRY(b, cudaEventCreate(&b->ev1));
+    // the TMA ring (with its psi slots) is above the default dynamic limit
+    BTRY(b, cudaFuncSetAttribute(k_batch_tma_field<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTmaSmem));
+    BTRY(b, cudaFuncSetAttribute(k_batch_tma_field<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTmaSmem));
     BTRY(b, cudaStreamSynchronize(b->stream));
     return SGPU_OK;
 }
 
 void sgpu_batch_destroy(sgpu_batch* b) {
     if (!b) return;
+    if (b->setup) cudaStreamSynchronize(b->setup);
     if (b->stream) cudaStreamSynchronize(b->stream);
     for (Slot& s : b->slots)
         if (s.ctx) sgpu_destroy(s.ctx);
@@ -751,6 +775,8 @@ void sgpu_batch_destroy(sgpu_batch* b) {
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->stream) cudaStreamDestroy(b->stream);
+    if (b->setup) cudaStreamDestroy(b->setup);
+    if (b->setup_done) cudaEventDestroy(b->setup_done);
     delete b;
 }
 
@@ -766,16 +792,20 @@ sgpu_status sgpu_batch_add(sgpu_batch* b, const sgpu_problem* p, sgpu_ctx* plan,
             break;
         }
     if (sl < 0) return berr(b, SGPU_ERR_OOM, "no free instance slot");
-    // everything in flight finishes before set-up work joins the stream
-    BTRY(b, cudaStreamSynchronize(b->stream));
+    // set-up on the set-up stream: it touches only the new instance's arena
+    // memory, so the steps queued on the batch stream keep running; the
+    // batch stream then waits for it before anything reads the instance
     sgpu_ctx* c = nullptr;
-    sgpu_status s = host_create_in(p, plan, nsteps, &b->arena, b->stream, &c);
+    sgpu_status s = host_create_in(p, plan, nsteps, &b->arena, b->setup, &c);
     if (!s) s = rebuild_sources(c);
     if (s) {
         b->err = c ? c->err : "instance set-up failed";
         if (c) sgpu_destroy(c);
         return s;
     }
+    BTRY(b, cudaEventRecord(b->setup_done, b->setup));
+    BTRY(b, cudaStreamWaitEvent(b->stream, b->setup_done, 0));
+    c->stream = b->stream;
     Slot& S = b->slots[sl];
     S.ctx = c;
     S.start = b->G;
@@ -786,7 +816,6 @@ sgpu_status sgpu_batch_add(sgpu_batch* b, const sgpu_problem* p, sgpu_ctx* plan,
     b->has_maps[sl] = c->tma_ready ? 1 : 0;
     TMaps m2[2] = {c->tme, c->tmh};
     if (c->tma_ready) BTRY(b, cudaMemcpyAsync(b->d_maps + 2 * sl, m2, sizeof(m2), cudaMemcpyHostToDevice, b->stream));
-    BTRY(b, cudaStreamSynchronize(b->stream));
     b->dirty = true;
     *slot = sl;
     return SGPU_OK;
@@ -882,7 +911,7 @@ sgpu_status sgpu_batch_set_tuning(sgpu_batch* b, const int* chunk3, int ctas_per
     if (!b) return SGPU_ERR_ARG;
     if (chunk3)
         for (int q = 0; q < kNumClasses; ++q) {
-            if (chunk3[q] < 1 || chunk3[q] > 1024) return berr(b, SGPU_ERR_ARG, "z chunk out of range");
+            if (chunk3[q] < 1 || chunk3[q] > kMaxItemPlanes - 8) return berr(b, SGPU_ERR_ARG, "z chunk out of range (1..64)");
             if (b->chunk[q] != chunk3[q]) b->dirty = true;
             b->chunk[q] = chunk3[q];
         }

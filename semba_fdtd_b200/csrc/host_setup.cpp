@@ -798,6 +798,16 @@ HostState* make_plan(const sgpu_problem* p, int max_steps, sgpu_status* rc) {
     return h;
 }
 
+// Floats of the psi array sgpu_init_cpml allocates for a slab box: rows
+// start at the local x rounded down to a multiple of 4 and are padded to a
+// multiple of 4 floats.
+uint64_t psi_floats(const HostState& h, const sgpu_lim& l) {
+    if (l.xe < l.xi || l.ye < l.yi || l.ze < l.zi) return 0;
+    const int x0 = l.xi - h.alloc[0].x0, x1 = l.xe - h.alloc[0].x0;
+    const int xb = x0 & ~3, px = (x1 - xb + 1 + 3) & ~3;
+    return (uint64_t)px * (l.ye - l.yi + 1) * (l.ze - l.zi + 1);
+}
+
 // Device buffers sgpu_init_borders allocates for the Mur faces: the CAB1
 // table per face and Past_ (two layers) per (face, tangential H component).
 template <class Fn> void mur_buffers(const HostState& h, Fn&& fn) {
@@ -917,11 +927,7 @@ sgpu_status sgpu_host_footprint(const sgpu_ctx* c, uint64_t* bytes) {
     uint64_t b = (uint64_t)vol * 6 * (sizeof(float) + sizeof(int16_t));
     // psi slabs
     for (int f = 0; f < 6; ++f)
-        for (int reg = 0; reg < 6; ++reg) {
-            const sgpu_lim& l = h->cd.pmlc[f][reg];
-            if (l.xe >= l.xi && l.ye >= l.yi && l.ze >= l.zi)
-                b += (uint64_t)(l.xe - l.xi + 1) * (l.ye - l.yi + 1) * (l.ze - l.zi + 1) * 4;
-        }
+        for (int reg = 0; reg < 6; ++reg) b += psi_floats(*h, h->cd.pmlc[f][reg]) * 4;
     // ADE state: swept E (H) nodes of electric (magnetic) pole-residue media
     for (int side = 0; side < 2; ++side) {
         const std::vector<int>& idx = side ? h->mdidx : h->didx;
@@ -981,11 +987,7 @@ sgpu_status sgpu_batch_footprint(const sgpu_ctx* c, uint64_t* bytes, uint64_t* l
     for (int a = 0; a < 3; ++a)
         for (const Vec* v : {&h->pbe[a], &h->pce[a], &h->pbm[a], &h->pcm[a]}) buf((uint64_t)v->v.size() * 4 + 64);
     for (int f = 0; f < 6; ++f)
-        for (int reg = 0; reg < 6; ++reg) {
-            const sgpu_lim& l = h->cd.pmlc[f][reg];
-            if (l.xe >= l.xi && l.ye >= l.yi && l.ze >= l.zi)
-                buf((uint64_t)(l.xe - l.xi + 1) * (l.ye - l.yi + 1) * (l.ze - l.zi + 1) * 4);
-        }
+        for (int reg = 0; reg < 6; ++reg) buf(psi_floats(*h, h->cd.pmlc[f][reg]) * 4);
     // ADE: per component node list, slot, previous field and state; the
     // per-row count/offset scratch of the set-up is live at the same time
     for (int side = 0; side < 2; ++side) {

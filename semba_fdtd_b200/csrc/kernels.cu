@@ -155,20 +155,25 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
     extern __shared__ __align__(128) unsigned char smem[];
     const float* tab = tma_tables(smem, g.g1, g.g2, g.nmed1);
     const TmaCta t = tma_cta_setup(smem, y0, z0, z1, zchunk);
-    if (t.warp == kConsumerWarps) {
-        if (t.lane == 0) tma_drain(t, (unsigned)tma_issue(t, tm.m, 0, t.kb - 1, t.ke, t.kb - 1, false, err), err, 12);
-        return;
-    }
-    const float* t1 = tab ? tab : g.g1;
-    const float* t2 = tab ? tab + g.nmed1 : g.g2;
     bool cpml_block = false;
     if (cp.on)
         for (int f = 0; f < 3; ++f)
             for (int w = 0; w < 2; ++w)
                 for (int sd = 0; sd < 2; ++sd)
                     cpml_block |= slab_touches(cp.s[f][w][sd], t.ib, t.ib + kTX - 1, t.jb, t.jb + kTY - 1, t.kb, t.ke);
-    if (cpml_block) e_consume<true>(t, 0, g, cp, t1, t2, err, false);
-    else e_consume<false>(t, 0, g, cp, t1, t2, err, false);
+    const unsigned tmask = cpml_block ? cpml_tile_mask(cp, 0, t.ib, t.ib + kTX - 1, t.jb, t.jb + kTY - 1) : 0u;
+    const unsigned smask = cpml_block ? staged_mask(cp, 0, t.ib, t.jb) : 0u;
+    if (t.warp == kConsumerWarps) {
+        __shared__ ProdTable tb;
+        prod_prepare(&tb, t, t.kb - 1, t.ke, t.kb - 1, false, g, cp, tmask);
+        if (t.lane == 0) tma_drain(t, (unsigned)tma_issue(t, tm.m, 0, t.kb - 1, t.ke, t.kb - 1, false, err, &tb, smask), err, 12);
+        return;
+    }
+    const float* t1 = tab ? tab : g.g1;
+    const float* t2 = tab ? tab + g.nmed1 : g.g2;
+    if (smask) e_consume<2>(t, 0, g, cp, t1, t2, err, false);
+    else if (cpml_block) e_consume<1>(t, 0, g, cp, t1, t2, err, false);
+    else e_consume<0>(t, 0, g, cp, t1, t2, err, false);
 }
 
 __global__ void __launch_bounds__(kTmaThreads, 3)
@@ -176,20 +181,25 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
     extern __shared__ __align__(128) unsigned char smem[];
     const float* tab = tma_tables(smem, g.gm1, g.gm2, g.nmed1);
     const TmaCta t = tma_cta_setup(smem, y0, z0, z1, zchunk);
-    if (t.warp == kConsumerWarps) {
-        if (t.lane == 0) tma_drain(t, (unsigned)tma_issue(t, tm.m, 0, t.kb, t.ke + 1, t.ke + 1, true, err), err, 14);
-        return;
-    }
-    const float* t1 = tab ? tab : g.gm1;
-    const float* t2 = tab ? tab + g.nmed1 : g.gm2;
     bool cpml_block = false;
     if (cp.on)
         for (int f = 3; f < 6; ++f)
             for (int w = 0; w < 2; ++w)
                 for (int sd = 0; sd < 2; ++sd)
                     cpml_block |= slab_touches(cp.s[f][w][sd], t.ib, t.ib + kTX - 1, t.jb, t.jb + kTY - 1, t.kb, t.ke);
-    if (cpml_block) h_consume<true>(t, 0, g, cp, t1, t2, err, false);
-    else h_consume<false>(t, 0, g, cp, t1, t2, err, false);
+    const unsigned tmask = cpml_block ? cpml_tile_mask(cp, 3, t.ib, t.ib + kTX - 1, t.jb, t.jb + kTY - 1) : 0u;
+    const unsigned smask = cpml_block ? staged_mask(cp, 3, t.ib, t.jb) : 0u;
+    if (t.warp == kConsumerWarps) {
+        __shared__ ProdTable tb;
+        prod_prepare(&tb, t, t.kb, t.ke + 1, t.ke + 1, true, g, cp, tmask);
+        if (t.lane == 0) tma_drain(t, (unsigned)tma_issue(t, tm.m, 0, t.kb, t.ke + 1, t.ke + 1, true, err, &tb, smask), err, 14);
+        return;
+    }
+    const float* t1 = tab ? tab : g.gm1;
+    const float* t2 = tab ? tab + g.nmed1 : g.gm2;
+    if (smask) h_consume<2>(t, 0, g, cp, t1, t2, err, false);
+    else if (cpml_block) h_consume<1>(t, 0, g, cp, t1, t2, err, false);
+    else h_consume<0>(t, 0, g, cp, t1, t2, err, false);
 }
 
 template <int NU, bool MAG>
@@ -366,6 +376,19 @@ bool encode_map(const sgpu_ctx* c, CUtensorMap* m, void* base, bool int16, int b
     return fn(m, int16 ? CU_TENSOR_MAP_DATA_TYPE_UINT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, es,
               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// A psi slab as a 3-D tiled map with a 32 x 8 x 1 box (rows of px floats).
+bool encode_psi_map(CUtensorMap* m, const Slab& sl) {
+    EncodeTiled fn = encoder();
+    if (!fn) return false;
+    const cuuint64_t ny = (cuuint64_t)(sl.yhi - sl.ylo + 1), nz = (cuuint64_t)(sl.zhi - sl.zlo + 1);
+    const cuuint64_t dims[3] = {(cuuint64_t)sl.px, ny, nz};
+    const cuuint64_t strides[2] = {(cuuint64_t)sl.px * 4, (cuuint64_t)sl.px * ny * 4};
+    const cuuint32_t box[3] = {(cuuint32_t)kTX, (cuuint32_t)kTY, 1};
+    const cuuint32_t es[3] = {1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, sl.psi, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 bool build_tensor_maps(sgpu_ctx* c) {
@@ -803,17 +826,32 @@ sgpu_status sgpu_init_cpml(sgpu_ctx* c, const sgpu_cpml_desc* d) {
             for (int side = 0; side < 2; ++side) {
                 const sgpu_lim& b = d->pmlc[f][pairs[f][w] + side];
                 Slab& sl = k.s[f][w][side];
-                sl = Slab{b.xi - c->ox, b.xe - c->ox, b.yi - c->oy, b.ye - c->oy, b.zi - c->oz, b.ze - c->oz, nullptr};
+                sl = Slab{b.xi - c->ox, b.xe - c->ox, b.yi - c->oy, b.ye - c->oy, b.zi - c->oz, b.ze - c->oz, nullptr, 0, 0};
                 if (b.xe < b.xi || b.ye < b.yi || b.ze < b.zi) {
-                    sl = Slab{1, 0, 1, 0, 1, 0, nullptr};
+                    sl = Slab{1, 0, 1, 0, 1, 0, nullptr, 0, 0};
                     continue;
                 }
-                size_t n = (size_t)(b.xe - b.xi + 1) * (b.ye - b.yi + 1) * (b.ze - b.zi + 1);
+                sl.xb = sl.xlo & ~3;
+                sl.px = (sl.xhi - sl.xb + 1 + 3) & ~3;
+                size_t n = (size_t)sl.px * (b.ye - b.yi + 1) * (b.ze - b.zi + 1);
                 if ((s = dalloc(c, &sl.psi, n, &c->cpml_allocs))) return s;
                 CUDA_TRY(c, cudaMemsetAsync(sl.psi, 0, n * sizeof(float), c->stream));
                 any = true;
             }
     k.on = any ? 1 : 0;
+    // psi tensor maps of the TMA kernels: map 9+n of a side is slab bit n
+    if (c->tma_ready)
+        for (int side = 0; side < 2; ++side)
+            for (int n = 0; n < 12; ++n) {
+                const Slab& sl = k.s[3 * side + (n >> 2)][(n >> 1) & 1][n & 1];
+                CUtensorMap* m = &(side ? c->tmh : c->tme).m[kPsiMap0 + n];
+                *m = CUtensorMap{};
+                if (sl.psi && !encode_psi_map(m, sl)) c->tma_ready = false;
+            }
+    if (c->graph) {
+        cudaGraphExecDestroy(c->graph);
+        c->graph = nullptr;
+    }
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     return SGPU_OK;
 }
@@ -1642,7 +1680,7 @@ sgpu_status sgpu_device_bytes(const sgpu_ctx* c, uint64_t* bytes) {
         for (int w = 0; w < 2; ++w)
             for (int s = 0; s < 2; ++s) {
                 const Slab& sl = c->cpml.s[f][w][s];
-                if (sl.psi) b += (uint64_t)(sl.xhi - sl.xlo + 1) * (sl.yhi - sl.ylo + 1) * (sl.zhi - sl.zlo + 1) * 4;
+                if (sl.psi) b += (uint64_t)sl.px * (sl.yhi - sl.ylo + 1) * (sl.zhi - sl.zlo + 1) * 4;
             }
     for (int comp = 0; comp < 3; ++comp) {
         b += (uint64_t)c->disp.n[comp] * (4 + 1 + 4 + 16 * (uint64_t)std::max(1, c->disp.nu_max));

@@ -20,11 +20,14 @@ namespace sgpu {
 
 constexpr int kMaxPolesPerMedium = 8;
 
-// A CPML slab in local coordinates with its psi array (dense over the box,
-// x fastest).
+// A CPML slab in local coordinates with its psi array: x fastest, rows from
+// xb (xlo rounded down to a multiple of 4) with a pitch px (a multiple of 4
+// floats), so a TMA box of the slab starts on a 16-byte boundary whenever
+// the tile's x origin does.
 struct Slab {
     int xlo, xhi, ylo, yhi, zlo, zhi;
     float* psi;
+    int xb, px;
 };
 
 // Kernel view of the grid: fields, media, coefficient tables, metrics and
@@ -137,7 +140,7 @@ struct KProbes {
 
 // Tensor maps of one fused TMA kernel (see tma_fields.cuh for the order).
 struct alignas(64) TMaps {
-    CUtensorMap m[9];
+    CUtensorMap m[21];  // 9 field / media maps, then the 12 psi slabs of the side
 };
 
 struct StepRef {

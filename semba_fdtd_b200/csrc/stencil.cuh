@@ -12,10 +12,12 @@ namespace dev {
 enum : int { kBulk = 1, kCpml = 2, kCx = 4, kCy = 8, kCz = 16, kAll = kCx | kCy | kCz };
 constexpr int kShTable = 4096;  // media entries held in shared memory
 
+__device__ __forceinline__ long long slab_index(const Slab& s, int i, int j, int k) {
+    return (i - s.xb) + (long long)s.px * ((j - s.ylo) + (long long)(s.yhi - s.ylo + 1) * (k - s.zlo));
+}
 __device__ __forceinline__ float* slab_ptr(const Slab& s, int i, int j, int k) {
     if (i < s.xlo || i > s.xhi || j < s.ylo || j > s.yhi || k < s.zlo || k > s.zhi) return nullptr;
-    long long nx = s.xhi - s.xlo + 1, ny = s.yhi - s.ylo + 1;
-    return s.psi + ((i - s.xlo) + nx * ((j - s.ylo) + ny * (long long)(k - s.zlo)));
+    return s.psi + slab_index(s, i, j, k);
 }
 
 // True when the (x, y) column range [x0,x1]x[y0,y1] or the z range [z0,z1]
@@ -105,14 +107,33 @@ __device__ __forceinline__ float cpml_pair(const Slab (&s)[2], unsigned live2, i
     if (live2) {
         const bool a = live2 & 1;
         float* const psi = a ? s[0].psi : s[1].psi;
-        const int xlo = a ? s[0].xlo : s[1].xlo, xhi = a ? s[0].xhi : s[1].xhi;
+        const int xb = a ? s[0].xb : s[1].xb, px = a ? s[0].px : s[1].px;
         const int ylo = a ? s[0].ylo : s[1].ylo, yhi = a ? s[0].yhi : s[1].yhi;
         const int zlo = a ? s[0].zlo : s[1].zlo;
-        float* p = psi + ((i - xlo) + (long long)(xhi - xlo + 1) * ((j - ylo) + (long long)(yhi - ylo + 1) * (k - zlo)));
+        float* p = psi + ((i - xb) + (long long)px * ((j - ylo) + (long long)(yhi - ylo + 1) * (k - zlo)));
         const float ps = pb * (*p) + diff * pc;
         *p = ps;
         v = ADD ? v + g * ps : v - g * ps;
         touched = true;
+    }
+    return v;
+}
+
+// The same correction with the old psi value taken from a shared-memory
+// tile staged by TMA (slab number nbase + side within the side's 12, slot =
+// its rank among the tile's slabs `smask`, cell offset o in the 32 x 8 tile);
+// the new value goes to global memory with a plain store.
+template <bool ADD>
+__device__ __forceinline__ float cpml_pair_staged(const Slab (&s)[2], unsigned live2, int nbase, unsigned smask,
+                                                  const float* slots, int slot_floats, int o, int i, int j, int k, float pb,
+                                                  float pc, float diff, float g, float v) {
+    if (live2) {
+        const int sd = (live2 & 1) ? 0 : 1;
+        const int slot = __popc(smask & ((1u << (nbase + sd)) - 1u));
+        const float ps = pb * slots[slot * slot_floats + o] + diff * pc;
+        const Slab& q = s[sd];
+        q.psi[(i - q.xb) + (long long)q.px * ((j - q.ylo) + (long long)(q.yhi - q.ylo + 1) * (k - q.zlo))] = ps;
+        v = ADD ? v + g * ps : v - g * ps;
     }
     return v;
 }

@@ -35,13 +35,19 @@ constexpr int kBoxB = kHaloW * kTY * 4;         // 36 x 8 floats
 constexpr int kBoxC = kHaloW * (kTY + 1) * 4;   // 36 x 9 floats
 constexpr int kBoxF = kTX * kTY * 4;            // 32 x 8 floats
 constexpr int kBoxM = kTX * kTY * 2;            // 32 x 8 int16
+constexpr int kBoxP = kTX * kTY * 4;            // 32 x 8 floats of one psi slab
+constexpr int kPsiSlots = 6;                    // psi tiles staged per plane
 __host__ __device__ constexpr int align128(int b) { return (b + 127) / 128 * 128; }
 constexpr int kOffA = 0;
 constexpr int kOffB = kOffA + align128(kBoxA);
 constexpr int kOffC = kOffB + align128(kBoxB);
 constexpr int kOffF = kOffC + align128(kBoxC);
 constexpr int kOffM = kOffF + 3 * align128(kBoxF);
-constexpr int kStageBytes = kOffM + 3 * align128(kBoxM);
+constexpr int kOffP = kOffM + 3 * align128(kBoxM);
+constexpr int kOffW = kOffP + kPsiSlots * align128(kBoxP);
+constexpr int kStageBytes = kOffW + 128;
+constexpr int kPsiSlotFloats = align128(kBoxP) / 4;
+constexpr int kPsiMap0 = 9;  // first psi map in TMaps
 constexpr int kTmaSmem = kStages * kStageBytes + 2 * kStages * 8;
 constexpr unsigned kTxFull = kBoxA + kBoxB + kBoxC + 3 * kBoxF + 3 * kBoxM;
 constexpr unsigned kTxEdge = kBoxA + kBoxB;  // the extra plane: two arrays only
@@ -49,6 +55,21 @@ constexpr unsigned kTxEdge = kBoxA + kBoxB;  // the extra plane: two arrays only
 // TMaps holds the tensor maps in the order the kernels use them:
 //   E kernel: Hx(32x9) Hy(36x8) Hz(36x9) Ex Ey Ez (32x8) Mx My Mz (32x8 int16)
 //   H kernel: Ex(32x9) Ey(36x8) Ez(36x9) Hx Hy Hz (32x8) Mx My Mz (32x8 int16)
+// then the psi slabs of the side (32x8), map 9+n for slab bit n of the
+// CPML masks (cp.s[c0 + n/4][(n/2)%2][n%2]).
+//
+// Each full plane also carries four words the producer lane writes before
+// it arrives on the stage's barrier: the slabs of the tile that hold the
+// plane, the plane's inverse z step and its z-indexed P_b / P_c pair, so the
+// consumers make no global load in the plane loop.
+//
+// CPML tiles whose slabs (cpml_tile_mask) number at most kPsiSlots also get
+// their psi tiles through the ring: a stage carries, after the media, one
+// 32x8 psi tile per slab that holds the plane, in the slot given by the
+// slab's rank in the tile mask.  The consumers read the old psi from there
+// and store the new value with a plain store.  Tiles with more slabs (narrow
+// grids where both sides of an axis fall in one tile) read psi from global
+// memory.
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -88,6 +109,12 @@ __device__ __forceinline__ void tma_load3(unsigned dst, const CUtensorMap* map, 
         : "memory");
 }
 
+struct PlaneWords {
+    unsigned live;  // bits of the tile mask whose slab holds the plane
+    float idz;      // Idzh(k) (E side) or Idze(k) (H side)
+    float bz, cz;   // P_be/P_ce (E) or P_bm/P_cm (H) at k, when a z slab holds it
+};
+
 // Shared set-up of the two kernels: barriers, coefficient tables, geometry.
 struct TmaCta {
     unsigned char* ring;
@@ -120,6 +147,43 @@ __device__ __forceinline__ TmaCta tma_cta_setup(unsigned char* smem, int y0, int
     return t;
 }
 
+// The producer's per-item table: the four plane words of every plane of the
+// item and the psi TMA coordinates of every slab of the tile, prepared by the
+// whole producer warp before lane 0 issues the item, so lane 0's plane loop
+// makes no global (or parameter) load between two barrier operations.
+constexpr int kMaxItemPlanes = 72;  // z chunk + 1; chunks are at most 64 planes
+struct ProdTable {
+    PlaneWords w[kMaxItemPlanes];
+    int4 psi[12];  // per slab bit: x origin (ib - xb), y origin (jb - ylo), zlo
+};
+
+// Producer warp, all lanes: planes p0 .. p1 (edge excluded) of one item.
+// `tmask` is the CPML tile's slab mask (0 for a bulk tile).
+__device__ __forceinline__ void prod_prepare(ProdTable* tb, const TmaCta& t, int p0, int p1, int edge, bool hside,
+                                             const KGrid& g, const KCpml& cp, unsigned tmask) {
+    const int c0 = hside ? 3 : 0;
+    const float* idz = hside ? g.idze : g.idzh;
+    const float* pb = hside ? cp.pbm[2] : cp.pbe[2];
+    const float* pc = hside ? cp.pcm[2] : cp.pce[2];
+    for (int p = p0 + t.lane; p <= p1; p += 32) {
+        PlaneWords w{0u, 0.0f, 0.0f, 0.0f};
+        if (p != edge) {
+            w.live = tmask ? cpml_plane_mask(cp, c0, tmask, p) : 0u;
+            w.idz = idz[p];
+            if (w.live & kCpmlZ) {
+                w.bz = pb[p];
+                w.cz = pc[p];
+            }
+        }
+        tb->w[p - p0] = w;
+    }
+    if (t.lane < 12 && ((tmask >> t.lane) & 1u)) {
+        const Slab& sl = cp.s[c0 + (t.lane >> 2)][(t.lane >> 1) & 1][t.lane & 1];
+        tb->psi[t.lane] = make_int4(t.ib - sl.xb, t.jb - sl.ylo, sl.zlo, 0);
+    }
+    __syncwarp();
+}
+
 // Producer (lane 0 of the producer warp): planes p0 .. p1 of one work item
 // into the ring; the item's first plane has the running plane number G0 (a
 // plane lands in stage G % kStages; its n-th use of that stage is phase n).
@@ -128,15 +192,22 @@ __device__ __forceinline__ TmaCta tma_cta_setup(unsigned char* smem, int y0, int
 // Hy (ib-4, jb), Hz (ib-4, jb-1), own fields and media (ib, jb); H side all
 // at (ib, jb).  Returns the number of planes issued: fewer than p1-p0+1 when
 // a bounded wait ran out.
+//
+// `smask` is the staged slab mask (the tile mask or 0): every full plane
+// brings the psi tile of each slab of smask that holds it.  The plane words
+// and psi coordinates come from the table prod_prepare filled.
 __device__ __forceinline__ int tma_issue(const TmaCta& t, const CUtensorMap* maps, unsigned G0, int p0, int p1, int edge,
-                                         bool hside, int* err) {
+                                         bool hside, int* err, const ProdTable* tb, unsigned smask) {
     for (int p = p0; p <= p1; ++p) {
         const unsigned G = G0 + (unsigned)(p - p0), s = G % kStages, u = G / kStages;
+        const PlaneWords w = tb->w[p - p0];
         if (u >= 1 && !mbar_wait(t.empty0 + 8 * s, (u - 1) & 1, err, hside ? 13 : 11)) return p - p0;
         const unsigned bar = t.full0 + 8 * s;
         unsigned char* st = t.ring + s * kStageBytes;
         const bool part = p == edge;
-        mbar_expect_tx(bar, part ? kTxEdge : kTxFull);
+        unsigned live = w.live & smask;
+        if (!part) *(PlaneWords*)(st + kOffW) = w;
+        mbar_expect_tx(bar, (part ? kTxEdge : kTxFull) + (unsigned)__popc(live) * (unsigned)kBoxP);
         const int xh = hside ? t.ib : t.ib - 4, ya = hside ? t.jb : t.jb - 1;
         tma_load3(smem_u32(st + kOffA), &maps[0], t.ib, ya, p, bar);  // first array (halo in y)
         tma_load3(smem_u32(st + kOffB), &maps[1], xh, t.jb, p, bar);  // second (halo in x)
@@ -145,8 +216,31 @@ __device__ __forceinline__ int tma_issue(const TmaCta& t, const CUtensorMap* map
             for (int q = 0; q < 3; ++q) tma_load3(smem_u32(st + kOffF + q * align128(kBoxF)), &maps[3 + q], t.ib, t.jb, p, bar);
             for (int q = 0; q < 3; ++q) tma_load3(smem_u32(st + kOffM + q * align128(kBoxM)), &maps[6 + q], t.ib, t.jb, p, bar);
         }
+        while (live) {
+            const int n = __ffs(live) - 1;
+            live &= live - 1u;
+            const int4 c = tb->psi[n];
+            const int slot = __popc(smask & ((1u << n) - 1u));
+            tma_load3(smem_u32(st + kOffP + slot * align128(kBoxP)), &maps[kPsiMap0 + n], c.x, c.y, p - c.z, bar);
+        }
     }
     return p1 - p0 + 1;
+}
+
+// The slab mask whose psi tiles a CPML tile stages (0: psi from global memory).
+__device__ __forceinline__ unsigned staged_mask(const KCpml& cp, int c0, int ib, int jb) {
+    const unsigned m = cpml_tile_mask(cp, c0, ib, ib + kTX - 1, jb, jb + kTY - 1);
+    return __popc(m) <= kPsiSlots ? m : 0u;
+}
+
+// One CPML correction of a consumer: CP 2 takes the old psi from the staged
+// tile, CP 1 from global memory.
+template <int CP, bool ADD>
+__device__ __forceinline__ float cpml_corr(const Slab (&s)[2], unsigned live2, int nbase, unsigned smask, const float* slots,
+                                           int o, int i, int j, int k, float pb, float pc, float diff, float g, float v,
+                                           bool& st) {
+    if (CP == 2) return cpml_pair_staged<ADD>(s, live2, nbase, smask, slots, kPsiSlotFloats, o, i, j, k, pb, pc, diff, g, v);
+    return cpml_pair<ADD>(s, live2, i, j, k, pb, pc, diff, g, v, st);
 }
 
 // Nothing may be in flight into the CTA's shared memory when it exits: wait
@@ -173,7 +267,7 @@ __device__ __forceinline__ void warp_release(const TmaCta& t, unsigned G) {
 // G0 (k = kb-1, edge) and G0+1+(k-kb).  Plane k-1 is released once plane k is
 // done; with `release_last` the item's last plane is released too (a
 // persistent CTA goes on to another item).  False on a timeout.
-template <bool CP>
+template <int CP>
 __device__ __forceinline__ bool e_consume(const TmaCta& t, unsigned G0, const KGrid& g, const KCpml& cp, const float* t1,
                                           const float* t2, int* err, bool release_last) {
     const int w = t.warp, l = t.lane;
@@ -183,20 +277,19 @@ __device__ __forceinline__ bool e_consume(const TmaCta& t, unsigned G0, const KG
     const float idyh = g.idyh[min(j, nya - 1)], idxh = g.idxh[i];
     const long long pitch = g.pitch, plane = g.plane;
     const unsigned tmask = CP ? cpml_tile_mask(cp, 0, t.ib, t.ib + kTX - 1, t.jb, t.jb + kTY - 1) : 0u;
+    const unsigned smask = CP == 2 ? tmask : 0u;
     const CpmlCol cc = CP ? cpml_col(cp, 0, tmask, i, j, t.kb, t.ke) : CpmlCol{};
     for (int k = t.kb; k <= t.ke; ++k) {
         const unsigned Gk = G0 + 1 + (unsigned)(k - t.kb), Gp = Gk - 1;
         const unsigned s = Gk % kStages, sp = Gp % kStages;
-        // slabs holding cell (i, j, k), and the P_b / P_c pair indexed by k
-        const unsigned pm = CP ? cc.live(cp, 0, k) : 0u;
-        float bz = 0.0f, cz = 0.0f;
-        if (CP && (pm & kCpmlZ)) {
-            bz = cp.pbe[2][k];
-            cz = cp.pce[2][k];
-        }
         if (k == t.kb && !warp_wait(t.full0 + 8 * sp, (Gp / kStages) & 1, err, 2)) return false;
         if (!warp_wait(t.full0 + 8 * s, (Gk / kStages) & 1, err, 1)) return false;
         const unsigned char* st = t.ring + s * kStageBytes;
+        // slabs holding cell (i, j, k): the column's slabs that hold plane k;
+        // the plane's Idzh and z-indexed P_b / P_c come with the plane
+        const PlaneWords pw = *(const PlaneWords*)(st + kOffW);
+        const unsigned pm = CP ? (cc.col & pw.live) : 0u;
+        const float bz = pw.bz, cz = pw.cz;
         const unsigned char* pv = t.ring + sp * kStageBytes;
         const float* HX = (const float*)(st + kOffA);
         const float* HY = (const float*)(st + kOffB);
@@ -205,11 +298,12 @@ __device__ __forceinline__ bool e_consume(const TmaCta& t, unsigned G0, const KG
         const float* HYp = (const float*)(pv + kOffB);
         const float* EF = (const float*)(st + kOffF);
         const int16_t* MF = (const int16_t*)(st + kOffM);
+        const float* PS = (const float*)(st + kOffP);
         constexpr int fs = align128(kBoxF) / 4, ms = align128(kBoxM) / 2;
         const float hx = HX[(w + 1) * kTX + l], hx_jm = HX[w * kTX + l], hx_km = HXp[(w + 1) * kTX + l];
         const float hy = HY[w * kHaloW + l + 4], hy_im = HY[w * kHaloW + l + 3], hy_km = HYp[w * kHaloW + l + 4];
         const float hz = HZ[(w + 1) * kHaloW + l + 4], hz_jm = HZ[w * kHaloW + l + 4], hz_im = HZ[(w + 1) * kHaloW + l + 3];
-        const float idzh = g.idzh[k];
+        const float idzh = pw.idz;
         const long long c = i + pitch * j + plane * k;
         const int o = w * kTX + l;
         bool st_ = true;
@@ -219,8 +313,8 @@ __device__ __forceinline__ bool e_consume(const TmaCta& t, unsigned G0, const KG
             const float dy = hz - hz_jm, dz = hy - hy_km;
             e = t1[m] * e + t2[m] * (dy * idyh - dz * idzh);
             if (CP && pm) {
-                e = cpml_pair<true>(cp.s[0][0], pm & 3, i, j, k, cc.by, cc.cy, dy, t2[m], e, st_);
-                e = cpml_pair<false>(cp.s[0][1], (pm >> 2) & 3, i, j, k, bz, cz, dz, t2[m], e, st_);
+                e = cpml_corr<CP, true>(cp.s[0][0], pm & 3, 0, smask, PS, o, i, j, k, cc.by, cc.cy, dy, t2[m], e, st_);
+                e = cpml_corr<CP, false>(cp.s[0][1], (pm >> 2) & 3, 2, smask, PS, o, i, j, k, bz, cz, dz, t2[m], e, st_);
             }
             g.F[0][c] = e;
         }
@@ -230,8 +324,8 @@ __device__ __forceinline__ bool e_consume(const TmaCta& t, unsigned G0, const KG
             const float dz = hx - hx_km, dx = hz - hz_im;
             e = t1[m] * e + t2[m] * (dz * idzh - dx * idxh);
             if (CP && pm) {
-                e = cpml_pair<true>(cp.s[1][0], (pm >> 4) & 3, i, j, k, bz, cz, dz, t2[m], e, st_);
-                e = cpml_pair<false>(cp.s[1][1], (pm >> 6) & 3, i, j, k, cc.bx, cc.cx, dx, t2[m], e, st_);
+                e = cpml_corr<CP, true>(cp.s[1][0], (pm >> 4) & 3, 4, smask, PS, o, i, j, k, bz, cz, dz, t2[m], e, st_);
+                e = cpml_corr<CP, false>(cp.s[1][1], (pm >> 6) & 3, 6, smask, PS, o, i, j, k, cc.bx, cc.cx, dx, t2[m], e, st_);
             }
             g.F[1][c] = e;
         }
@@ -241,8 +335,8 @@ __device__ __forceinline__ bool e_consume(const TmaCta& t, unsigned G0, const KG
             const float dx = hy - hy_im, dy = hx - hx_jm;
             e = t1[m] * e + t2[m] * (dx * idxh - dy * idyh);
             if (CP && pm) {
-                e = cpml_pair<false>(cp.s[2][0], (pm >> 8) & 3, i, j, k, cc.by, cc.cy, dy, t2[m], e, st_);
-                e = cpml_pair<true>(cp.s[2][1], (pm >> 10) & 3, i, j, k, cc.bx, cc.cx, dx, t2[m], e, st_);
+                e = cpml_corr<CP, false>(cp.s[2][0], (pm >> 8) & 3, 8, smask, PS, o, i, j, k, cc.by, cc.cy, dy, t2[m], e, st_);
+                e = cpml_corr<CP, true>(cp.s[2][1], (pm >> 10) & 3, 10, smask, PS, o, i, j, k, cc.bx, cc.cx, dx, t2[m], e, st_);
             }
             g.F[2][c] = e;
         }
@@ -255,7 +349,7 @@ __device__ __forceinline__ bool e_consume(const TmaCta& t, unsigned G0, const KG
 // Consumers of the H side: Advance_Hx/Hy/Hz + AdvanceMagneticCPML from the
 // ring (hfield_column's arithmetic).  The item's planes are G0+(k-kb) for
 // k = kb..ke+1 (ke+1 the edge); plane k is released once it is done.
-template <bool CP>
+template <int CP>
 __device__ __forceinline__ bool h_consume(const TmaCta& t, unsigned G0, const KGrid& g, const KCpml& cp, const float* t1,
                                           const float* t2, int* err, bool release_last) {
     const int w = t.warp, l = t.lane;
@@ -265,20 +359,18 @@ __device__ __forceinline__ bool h_consume(const TmaCta& t, unsigned G0, const KG
     const float idye = g.idye[min(j, nya - 1)], idxe = g.idxe[i];
     const long long pitch = g.pitch, plane = g.plane;
     const unsigned tmask = CP ? cpml_tile_mask(cp, 3, t.ib, t.ib + kTX - 1, t.jb, t.jb + kTY - 1) : 0u;
+    const unsigned smask = CP == 2 ? tmask : 0u;
     const CpmlCol cc = CP ? cpml_col(cp, 3, tmask, i, j, t.kb, t.ke) : CpmlCol{};
     for (int k = t.kb; k <= t.ke; ++k) {
         const unsigned Gk = G0 + (unsigned)(k - t.kb), Gn = Gk + 1;
         const unsigned s = Gk % kStages, sn = Gn % kStages;
-        // slabs holding cell (i, j, k), and the P_b / P_c pair indexed by k
-        const unsigned pm = CP ? cc.live(cp, 3, k) : 0u;
-        float bz = 0.0f, cz = 0.0f;
-        if (CP && (pm & kCpmlZ)) {
-            bz = cp.pbm[2][k];
-            cz = cp.pcm[2][k];
-        }
         if (!warp_wait(t.full0 + 8 * s, (Gk / kStages) & 1, err, 3)) return false;
         if (!warp_wait(t.full0 + 8 * sn, (Gn / kStages) & 1, err, 4)) return false;
         const unsigned char* st = t.ring + s * kStageBytes;
+        // slabs holding cell (i, j, k), the plane's Idze and P_b / P_c pair
+        const PlaneWords pw = *(const PlaneWords*)(st + kOffW);
+        const unsigned pm = CP ? (cc.col & pw.live) : 0u;
+        const float bz = pw.bz, cz = pw.cz;
         const unsigned char* nx = t.ring + sn * kStageBytes;
         const float* EX = (const float*)(st + kOffA);
         const float* EY = (const float*)(st + kOffB);
@@ -287,11 +379,12 @@ __device__ __forceinline__ bool h_consume(const TmaCta& t, unsigned G0, const KG
         const float* EYn = (const float*)(nx + kOffB);
         const float* HF = (const float*)(st + kOffF);
         const int16_t* MF = (const int16_t*)(st + kOffM);
+        const float* PS = (const float*)(st + kOffP);
         constexpr int fs = align128(kBoxF) / 4, ms = align128(kBoxM) / 2;
         const float ex = EX[w * kTX + l], ex_jp = EX[(w + 1) * kTX + l], ex_kp = EXn[w * kTX + l];
         const float ey = EY[w * kHaloW + l], ey_ip = EY[w * kHaloW + l + 1], ey_kp = EYn[w * kHaloW + l];
         const float ez = EZ[w * kHaloW + l], ez_ip = EZ[w * kHaloW + l + 1], ez_jp = EZ[(w + 1) * kHaloW + l];
-        const float idze = g.idze[k];
+        const float idze = pw.idz;
         const long long c = i + pitch * j + plane * k;
         const int o = w * kTX + l;
         bool st_ = true;
@@ -301,8 +394,8 @@ __device__ __forceinline__ bool h_consume(const TmaCta& t, unsigned G0, const KG
             const float dz = ey_kp - ey, dy = ez_jp - ez;
             h = t1[m] * h + t2[m] * (dz * idze - dy * idye);
             if (CP && pm) {
-                h = cpml_pair<false>(cp.s[3][0], pm & 3, i, j, k, cc.by, cc.cy, dy, t2[m], h, st_);
-                h = cpml_pair<true>(cp.s[3][1], (pm >> 2) & 3, i, j, k, bz, cz, dz, t2[m], h, st_);
+                h = cpml_corr<CP, false>(cp.s[3][0], pm & 3, 0, smask, PS, o, i, j, k, cc.by, cc.cy, dy, t2[m], h, st_);
+                h = cpml_corr<CP, true>(cp.s[3][1], (pm >> 2) & 3, 2, smask, PS, o, i, j, k, bz, cz, dz, t2[m], h, st_);
             }
             g.F[3][c] = h;
         }
@@ -312,8 +405,8 @@ __device__ __forceinline__ bool h_consume(const TmaCta& t, unsigned G0, const KG
             const float dx = ez_ip - ez, dz = ex_kp - ex;
             h = t1[m] * h + t2[m] * (dx * idxe - dz * idze);
             if (CP && pm) {
-                h = cpml_pair<false>(cp.s[4][0], (pm >> 4) & 3, i, j, k, bz, cz, dz, t2[m], h, st_);
-                h = cpml_pair<true>(cp.s[4][1], (pm >> 6) & 3, i, j, k, cc.bx, cc.cx, dx, t2[m], h, st_);
+                h = cpml_corr<CP, false>(cp.s[4][0], (pm >> 4) & 3, 4, smask, PS, o, i, j, k, bz, cz, dz, t2[m], h, st_);
+                h = cpml_corr<CP, true>(cp.s[4][1], (pm >> 6) & 3, 6, smask, PS, o, i, j, k, cc.bx, cc.cx, dx, t2[m], h, st_);
             }
             g.F[4][c] = h;
         }
@@ -323,8 +416,8 @@ __device__ __forceinline__ bool h_consume(const TmaCta& t, unsigned G0, const KG
             const float dy = ex_jp - ex, dx = ey_ip - ey;
             h = t1[m] * h + t2[m] * (dy * idye - dx * idxe);
             if (CP && pm) {
-                h = cpml_pair<true>(cp.s[5][0], (pm >> 8) & 3, i, j, k, cc.by, cc.cy, dy, t2[m], h, st_);
-                h = cpml_pair<false>(cp.s[5][1], (pm >> 10) & 3, i, j, k, cc.bx, cc.cx, dx, t2[m], h, st_);
+                h = cpml_corr<CP, true>(cp.s[5][0], (pm >> 8) & 3, 8, smask, PS, o, i, j, k, cc.by, cc.cy, dy, t2[m], h, st_);
+                h = cpml_corr<CP, false>(cp.s[5][1], (pm >> 10) & 3, 10, smask, PS, o, i, j, k, cc.bx, cc.cx, dx, t2[m], h, st_);
             }
             g.F[5][c] = h;
         }

@@ -131,6 +131,16 @@ class Server:
                     waiting.append(pending.popleft())
                 submit_plans()
                 collect_plans()
+                # the next chunk is queued first: the set-up of the requests
+                # admitted below overlaps it on the device's set-up stream
+                launched = False
+                if active:
+                    if not tuned and len(active) >= 4:
+                        b.autotune(2)
+                        tuned = True
+                    b.advance(self.chunk)
+                    st.chunks += 1
+                    launched = True
                 # admission: first come first served with bounded look-ahead
                 k = 0
                 while k < min(len(waiting), self.backfill) and len(active) < self.max_instances:
@@ -152,20 +162,16 @@ class Server:
                 submit_plans()
                 st.peak_resident = max(st.peak_resident, len(active))
                 st.peak_bytes = max(st.peak_bytes, b.memory()[1])
-                if not active:
-                    planned = [r for r in waiting[: self.backfill] if r.plan is not None]
-                    if waiting and not pending and len(planned) == len(waiting[: self.backfill]):
-                        raise _lib.SembaGpuError(f"request {waiting[0].rid} needs {waiting[0].plan.footprint} "
-                                                 f"bytes; the arena holds {b.memory()[0]}")
-                    # nothing to step: wait for a plan or the next arrival
-                    nxt = pending[0].arrival - now() if pending else 0.05
-                    wait(list(futures.values()), timeout=max(0.0, min(nxt, 0.05)), return_when=FIRST_COMPLETED)
+                if not launched:
+                    if not active:
+                        planned = [r for r in waiting[: self.backfill] if r.plan is not None]
+                        if waiting and not pending and len(planned) == len(waiting[: self.backfill]):
+                            raise _lib.SembaGpuError(f"request {waiting[0].rid} needs {waiting[0].plan.footprint} "
+                                                     f"bytes; the arena holds {b.memory()[0]}")
+                        # nothing to step: wait for a plan or the next arrival
+                        nxt = pending[0].arrival - now() if pending else 0.05
+                        wait(list(futures.values()), timeout=max(0.0, min(nxt, 0.05)), return_when=FIRST_COMPLETED)
                     continue
-                if not tuned and len(active) >= 4:
-                    b.autotune(2)
-                    tuned = True
-                b.advance(self.chunk)  # queued; the planner threads keep working meanwhile
-                st.chunks += 1
                 b.synchronize()
                 t = now()
                 for slot in [s for s in active if b.done(s)]:
