@@ -1658,6 +1658,25 @@ int orc_get_metric(void* hv, int which, float* out) {
     return 0;
 }
 
+long orc_check_div_dt(double dt, long n, unsigned long long seed) {
+    const double y = 1.0 / dt;
+    unsigned long long x = seed ? seed : 0x9E3779B97F4A7C15ull;
+    long bad = 0;
+    for (long i = 0; i < n; ++i) {
+        // xorshift64*: sign, a mantissa and an exponent keeping a/dt normal
+        x ^= x >> 12; x ^= x << 25; x ^= x >> 27;
+        const unsigned long long r = x * 2685821657736338717ull;
+        const int e = (int)((r >> 52) % 1200) - 600;
+        double a = std::ldexp(1.0 + (double)(r & ((1ull << 52) - 1)) / 4503599627370496.0, e);
+        if (r & (1ull << 63)) a = -a;
+        const double q0 = a * y;
+        const double rr = std::fma(-q0, dt, a);
+        const double q = std::fma(rr, y, q0);
+        if (q != a / dt) ++bad;
+    }
+    return bad;
+}
+
 int orc_get_mur_cab1(void* hv, int face, float* out) {
     Handle* h = (Handle*)hv;
     if (face < 0 || face > 5) return 1;

@@ -149,6 +149,11 @@ double orc_get_time(void* h, int n);
  * left, right, down, up), num_media+1 values; returns 1 when the face has no
  * Mur condition. */
 int orc_get_mur_cab1(void* h, int face, float* out);
+/* Checks the library's quotient by dt, RN(q + (a - dt*q)*y) with y = RN(1/dt)
+ * and q = RN(a*y) (two FMAs), against IEEE division a/dt for n operands
+ * drawn from `seed` over the whole finite exponent range that does not
+ * underflow; returns the number of differing results. */
+long orc_check_div_dt(double dt, long n, unsigned long long seed);
 
 #ifdef __cplusplus
 }

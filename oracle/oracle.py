@@ -94,6 +94,8 @@ def load():
         lib.orc_get_edisp.argtypes = [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)] + [C.POINTER(C.c_double)] * 3
         lib.orc_get_mur_cab1.argtypes = [vp, C.c_int, C.POINTER(C.c_float)]
         lib.orc_get_mdisp.argtypes = lib.orc_get_edisp.argtypes
+        lib.orc_check_div_dt.argtypes = [C.c_double, C.c_long, C.c_ulonglong]
+        lib.orc_check_div_dt.restype = C.c_long
         _lib = lib
     return _lib
 

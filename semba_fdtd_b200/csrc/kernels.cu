@@ -983,6 +983,7 @@ sgpu_status init_ade(sgpu_ctx* c, const sgpu_edisp_desc* d, bool mag) {
             } else {
                 dm.kappa[dm.nu] = make_double2(K[0], K[1]);
                 dm.beta[dm.nu] = make_double2(B[0], B[1]);
+                dm.beta_dt[dm.nu] = make_double2(B[0] / c->dt, B[1] / c->dt);
                 dm.g3[dm.nu] = make_double2(G[0], G[1]);
                 dm.map[p] = dm.nu++;
             }
@@ -1002,6 +1003,7 @@ sgpu_status init_ade(sgpu_ctx* c, const sgpu_edisp_desc* d, bool mag) {
     k.slot_of_medium = dslot;
     k.nu_max = nu_max;
     k.dt = c->dt;
+    k.inv_dt = 1.0 / c->dt;
     for (int comp = 0; comp < 3; ++comp) {
         const sgpu_lim& w = c->sweep[c0 + comp];
         int x0 = w.xi - c->ox, x1 = w.xe - c->ox;

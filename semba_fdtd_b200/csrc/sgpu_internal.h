@@ -59,6 +59,7 @@ struct DispMedium {
     int nu;                       // unique poles carrying state
     int map[kMaxPolesPerMedium];  // pole -> unique state slot
     double2 kappa[kMaxPolesPerMedium], beta[kMaxPolesPerMedium], g3[kMaxPolesPerMedium];
+    double2 beta_dt[kMaxPolesPerMedium];  // Beta / dt, componentwise (the magnetic current's factor)
 };
 
 struct KDisp {
@@ -71,6 +72,7 @@ struct KDisp {
     const int16_t* slot_of_medium;  // media index -> slot (-1 none)
     int nu_max;
     double dt;
+    double inv_dt;  // RN(1/dt), for the corrected quotient by dt
 };
 
 // One source contribution applied after the curl/CPML/ADE work of a half

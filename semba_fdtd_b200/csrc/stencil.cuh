@@ -325,6 +325,19 @@ __device__ __forceinline__ void hfield_column(const KGrid& g, const KCpml& cp, c
 }
 
 
+// a / dt, correctly rounded, from y = RN(1/dt): q = RN(a*y), the exact
+// residual r = a - dt*q by FMA, then RN(q + r*y) -- Markstein's correction,
+// which returns RN(a/dt) whenever y is the correctly rounded reciprocal and
+// no intermediate underflows (P. Markstein, IBM J. Res. Dev. 34(1), 1990;
+// J.-M. Muller et al., Handbook of Floating-Point Arithmetic, section 4.7).
+// Two FMAs and a multiply replace the IEEE division sequence; the oracle's
+// tests check it against IEEE division on random operands.
+__device__ __forceinline__ double div_dt(double a, double dt, double inv_dt) {
+    const double q = a * inv_dt;
+    const double r = fma(-q, dt, a);
+    return fma(r, inv_dt, q);
+}
+
 // AdvanceEDispersiveE (electricdispersive.F90:304-362) and, with MAG,
 // AdvanceMdispersiveH (magneticdispersive.F90:298-360): one thread per node.
 // Conjugate poles share one state slot; the subtraction still runs once
@@ -362,8 +375,17 @@ __device__ __forceinline__ void ade_node(const KGrid& g, const KDisp& d, int com
             const double2 kp = md->kappa[u], bt = md->beta[u];
             const double kr = kp.x * st[u].x - kp.y * st[u].y;
             const double ki = kp.x * st[u].y + kp.y * st[u].x;
-            const double br = MAG ? (bt.x / d.dt) * dd : (bt.x * dd) / d.dt;
-            const double bi = MAG ? (bt.y / d.dt) * dd : (bt.y * dd) / d.dt;
+            double br, bi;
+            if (MAG) {
+                // (Beta/dt)*(H - Hprev): Beta/dt is the same quotient for every
+                // node, formed once on the host
+                const double2 bd = md->beta_dt[u];
+                br = bd.x * dd;
+                bi = bd.y * dd;
+            } else {
+                br = div_dt(bt.x * dd, d.dt, d.inv_dt);
+                bi = div_dt(bt.y * dd, d.dt, d.inv_dt);
+            }
             J[u * n + q] = make_double2(kr + br, ki + bi);
         }
     }

@@ -357,3 +357,17 @@ def test_mur_update_formula_on_a_planted_field():
     sl = (slice(sw[0] - xi, sw[1] - xi + 1), slice(sw[2] - yi, sw[3] - yi + 1))
     want = (np.float32(0) + cab[m[sl]] * (inner[sl] - np.float32(0))).astype(np.float32)
     np.testing.assert_array_equal(outer[sl], want)
+
+
+def test_corrected_quotient_by_dt_matches_ieee_division():
+    """The ADE kernels divide by dt as RN(q + (a - dt*q)*y), y = RN(1/dt),
+    q = RN(a*y) (Markstein's correction); it must equal IEEE a/dt.  Checked
+    for the time steps of the parity cases and of random grids on 2e6
+    operands each, spanning the exponent range."""
+    from cases import ALL
+    lib = oracle.load()
+    dts = {oracle.Oracle(ALL[name]()).dt for name in ("disp", "mdisp", "small")}
+    rng = np.random.default_rng(5)
+    dts |= {float(v) for v in rng.uniform(1e-13, 1e-10, size=5)}
+    for q, dt in enumerate(sorted(dts)):
+        assert lib.orc_check_div_dt(dt, 2_000_000, 1234 + q) == 0, dt
