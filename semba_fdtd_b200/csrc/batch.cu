@@ -145,9 +145,11 @@ __device__ __forceinline__ int inst_step(const InstDesc& D, const int* G, bool* 
 // Per-warp copy of an instance's grid (and CPML) view into shared memory:
 // the field kernels then read slab bounds, pointers and sweep limits with
 // shared loads instead of global ones, and no warp waits for another.
+constexpr int kWarpTab = 32;  // media per coefficient table held in a warp's view
 struct WarpView {
     KGrid g;
     KCpml cp;
+    float tab[2 * kWarpTab];  // the side's two coefficient tables, when nmed1 <= kWarpTab
 };
 template <class T> __device__ __forceinline__ void warp_copy(T* dst, const T* src, int lane) {
     static_assert(sizeof(T) % 4 == 0, "word copy");
@@ -155,10 +157,17 @@ template <class T> __device__ __forceinline__ void warp_copy(T* dst, const T* sr
     int* d = (int*)dst;
     for (int q = lane; q < (int)(sizeof(T) / 4); q += 32) d[q] = s[q];
 }
-__device__ __forceinline__ const WarpView& stage_view(WarpView* slot, const InstDesc& D, bool cpml, int lane) {
+// side < 0: no tables; 0: G1 / G2; 1: GM1 / GM2 (when the instance has at
+// most kWarpTab media, else the consumers read the tables from global memory).
+__device__ __forceinline__ const WarpView& stage_view(WarpView* slot, const InstDesc& D, bool cpml, int lane,
+                                                      int side = -1) {
     __syncwarp();  // the warp is done with the previous item's view
     warp_copy(&slot->g, &D.g, lane);
     if (cpml) warp_copy(&slot->cp, &D.cp, lane);
+    if (side >= 0 && lane < D.g.nmed1 && D.g.nmed1 <= kWarpTab) {
+        slot->tab[lane] = (side ? D.g.gm1 : D.g.g1)[lane];
+        slot->tab[kWarpTab + lane] = (side ? D.g.gm2 : D.g.g2)[lane];
+    }
     __syncwarp();
     return *slot;
 }
@@ -212,11 +221,13 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ WarpView views[kConsumerWarps];
     __shared__ ProdTable tb;
+    __shared__ PsiRow rows[kConsumerWarps][12];
     TmaCta t = tma_cta_setup(smem, 0, 0, 0, 1);
     const int n_items = counts[SIDE == 0 ? kCntE : kCntH];
     const bool producer = t.warp == kConsumerWarps;
     unsigned gp = 0;  // running plane number of the ring
-    int fenced = -1;
+    int fenced = -1;  // the instance whose tensor maps the producer has acquired
+    int viewed = -1;  // ... whose view the consumer warp holds
     for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
         const FieldItem w = items[it];
         const InstDesc& D = descs[w.slot];
@@ -230,12 +241,12 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
         const int np = w.ke - w.kb + 2;  // the item's planes, edge plane included
         const int c0 = SIDE == 0 ? 0 : 3;
         if (producer) {
-            // CPML items stage their psi tiles through the ring when the tile
-            // has at most kPsiSlots slabs (the consumers derive the same mask)
+            // CPML items stage their psi tiles through the ring when the tile's
+            // slabs fit the kPsiSlots slots (the consumers derive the same mask)
             const int p0 = SIDE == 0 ? w.kb - 1 : w.kb, p1 = SIDE == 0 ? w.ke : w.ke + 1;
             const int edge = SIDE == 0 ? w.kb - 1 : w.ke + 1;
             const unsigned tmask = w.cp ? cpml_tile_mask(D.cp, c0, w.ib, w.ib + kTX - 1, w.jb, w.jb + kTY - 1) : 0u;
-            const unsigned smask = __popc(tmask) <= kPsiSlots ? tmask : 0u;
+            const unsigned smask = w.cp ? staged_mask(D.cp, c0, w.ib, w.jb) : 0u;
             prod_prepare(&tb, t, p0, p1, edge, SIDE != 0, D.g, D.cp, tmask);
             int got = np;
             if (t.lane == 0) {
@@ -252,18 +263,25 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
                 return;
             }
         } else {
-            const WarpView& V = stage_view(&views[t.warp], D, w.cp != 0, t.lane);
+            if (w.slot != viewed) {
+                stage_view(&views[t.warp], D, true, t.lane, SIDE);
+                viewed = w.slot;
+            }
+            const WarpView& V = views[t.warp];
             const KGrid& g = V.g;
             const unsigned smask = w.cp ? staged_mask(V.cp, c0, w.ib, w.jb) : 0u;
+            const bool local = g.nmed1 <= kWarpTab;
+            const float* t1 = local ? V.tab : SIDE == 0 ? g.g1 : g.gm1;
+            const float* t2 = local ? V.tab + kWarpTab : SIDE == 0 ? g.g2 : g.gm2;
             bool ok;
             if (SIDE == 0)
-                ok = smask  ? e_consume<2>(t, gp, g, V.cp, g.g1, g.g2, err, true)
-                     : w.cp ? e_consume<1>(t, gp, g, V.cp, g.g1, g.g2, err, true)
-                            : e_consume<0>(t, gp, g, V.cp, g.g1, g.g2, err, true);
+                ok = smask  ? e_consume<2>(t, gp, g, V.cp, t1, t2, err, true, rows[t.warp])
+                     : w.cp ? e_consume<1>(t, gp, g, V.cp, t1, t2, err, true, rows[t.warp])
+                            : e_consume<0>(t, gp, g, V.cp, t1, t2, err, true, rows[t.warp]);
             else
-                ok = smask  ? h_consume<2>(t, gp, g, V.cp, g.gm1, g.gm2, err, true)
-                     : w.cp ? h_consume<1>(t, gp, g, V.cp, g.gm1, g.gm2, err, true)
-                            : h_consume<0>(t, gp, g, V.cp, g.gm1, g.gm2, err, true);
+                ok = smask  ? h_consume<2>(t, gp, g, V.cp, t1, t2, err, true, rows[t.warp])
+                     : w.cp ? h_consume<1>(t, gp, g, V.cp, t1, t2, err, true, rows[t.warp])
+                            : h_consume<0>(t, gp, g, V.cp, t1, t2, err, true, rows[t.warp]);
             if (!ok) return;
         }
         gp += (unsigned)np;

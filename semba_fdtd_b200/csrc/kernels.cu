@@ -171,9 +171,10 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
     }
     const float* t1 = tab ? tab : g.g1;
     const float* t2 = tab ? tab + g.nmed1 : g.g2;
-    if (smask) e_consume<2>(t, 0, g, cp, t1, t2, err, false);
-    else if (cpml_block) e_consume<1>(t, 0, g, cp, t1, t2, err, false);
-    else e_consume<0>(t, 0, g, cp, t1, t2, err, false);
+    __shared__ PsiRow rows[kConsumerWarps][12];
+    if (smask) e_consume<2>(t, 0, g, cp, t1, t2, err, false, rows[t.warp]);
+    else if (cpml_block) e_consume<1>(t, 0, g, cp, t1, t2, err, false, rows[t.warp]);
+    else e_consume<0>(t, 0, g, cp, t1, t2, err, false, rows[t.warp]);
 }
 
 __global__ void __launch_bounds__(kTmaThreads, 3)
@@ -197,9 +198,10 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
     }
     const float* t1 = tab ? tab : g.gm1;
     const float* t2 = tab ? tab + g.nmed1 : g.gm2;
-    if (smask) h_consume<2>(t, 0, g, cp, t1, t2, err, false);
-    else if (cpml_block) h_consume<1>(t, 0, g, cp, t1, t2, err, false);
-    else h_consume<0>(t, 0, g, cp, t1, t2, err, false);
+    __shared__ PsiRow rows[kConsumerWarps][12];
+    if (smask) h_consume<2>(t, 0, g, cp, t1, t2, err, false, rows[t.warp]);
+    else if (cpml_block) h_consume<1>(t, 0, g, cp, t1, t2, err, false, rows[t.warp]);
+    else h_consume<0>(t, 0, g, cp, t1, t2, err, false, rows[t.warp]);
 }
 
 template <int NU, bool MAG>

@@ -119,20 +119,52 @@ __device__ __forceinline__ float cpml_pair(const Slab (&s)[2], unsigned live2, i
     return v;
 }
 
+// Staged psi slots: a tile's slabs take slots in bit order, except that the
+// two sides of the z-normal slab pairs (bits 2/3 and 4/5, the z kinds of the
+// side's first two components) share one slot, since a plane lies in at most
+// one of them.
+__device__ __forceinline__ unsigned psi_slot_groups(unsigned m) { return (m & ~0x28u) | ((m >> 1) & 0x14u); }
+__device__ __forceinline__ int psi_slot(unsigned m, int n) {
+    const int b = (n == 3 || n == 5) ? n - 1 : n;
+    return __popc(psi_slot_groups(m) & ((1u << b) - 1u));
+}
+
+// A staged tile's psi rows, per consumer warp and slab bit n: the psi address
+// of the warp's first column (ib, row j) at plane 0, the plane stride (a cell's
+// psi is base + lane + k * stride) and the first float of the slab's staged
+// slot (psi_slot of the tile's slabs `tmask`).  Bits outside tmask get a
+// null row at slot 0.
+struct PsiRow {
+    float* base;
+    int stride;
+    int slot;
+};
+__device__ __forceinline__ void psi_rows_fill(PsiRow* rows, const KCpml& cp, int c0, unsigned tmask, int slot_floats,
+                                              int ib, int j, int lane) {
+    if (lane < 12) {
+        PsiRow r{nullptr, 0, 0};
+        if ((tmask >> lane) & 1u) {
+            const Slab& sl = cp.s[c0 + (lane >> 2)][(lane >> 1) & 1][lane & 1];
+            r.stride = sl.px * (sl.yhi - sl.ylo + 1);
+            r.base = sl.psi + ((ib - sl.xb) + (long long)sl.px * (j - sl.ylo) - (long long)r.stride * sl.zlo);
+            r.slot = psi_slot(tmask, lane) * slot_floats;
+        }
+        rows[lane] = r;
+    }
+    __syncwarp();
+}
+
 // The same correction with the old psi value taken from a shared-memory
-// tile staged by TMA (slab number nbase + side within the side's 12, slot =
-// its rank among the tile's slabs `smask`, cell offset o in the 32 x 8 tile);
-// the new value goes to global memory with a plain store.
+// tile staged by TMA (slab number nbase + side within the side's 12, cell
+// offset o in the 32 x 8 tile); the new value goes to global memory with a
+// plain store through the warp's psi row table.
 template <bool ADD>
-__device__ __forceinline__ float cpml_pair_staged(const Slab (&s)[2], unsigned live2, int nbase, unsigned smask,
-                                                  const float* slots, int slot_floats, int o, int i, int j, int k, float pb,
-                                                  float pc, float diff, float g, float v) {
+__device__ __forceinline__ float cpml_pair_staged(unsigned live2, int nbase, const float* slots, int o, const PsiRow* rows,
+                                                  int lane, int k, float pb, float pc, float diff, float g, float v) {
     if (live2) {
-        const int sd = (live2 & 1) ? 0 : 1;
-        const int slot = __popc(smask & ((1u << (nbase + sd)) - 1u));
-        const float ps = pb * slots[slot * slot_floats + o] + diff * pc;
-        const Slab& q = s[sd];
-        q.psi[(i - q.xb) + (long long)q.px * ((j - q.ylo) + (long long)(q.yhi - q.ylo + 1) * (k - q.zlo))] = ps;
+        const PsiRow r = rows[nbase + ((live2 & 1) ? 0 : 1)];
+        const float ps = pb * slots[r.slot + o] + diff * pc;
+        r.base[lane + (long long)k * r.stride] = ps;
         v = ADD ? v + g * ps : v - g * ps;
     }
     return v;

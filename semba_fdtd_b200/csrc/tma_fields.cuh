@@ -220,26 +220,30 @@ __device__ __forceinline__ int tma_issue(const TmaCta& t, const CUtensorMap* map
             const int n = __ffs(live) - 1;
             live &= live - 1u;
             const int4 c = tb->psi[n];
-            const int slot = __popc(smask & ((1u << n) - 1u));
+            const int slot = psi_slot(smask, n);
             tma_load3(smem_u32(st + kOffP + slot * align128(kBoxP)), &maps[kPsiMap0 + n], c.x, c.y, p - c.z, bar);
         }
     }
     return p1 - p0 + 1;
 }
 
-// The slab mask whose psi tiles a CPML tile stages (0: psi from global memory).
+// The slab mask whose psi tiles a CPML tile stages (0: psi from global
+// memory): the tile's slabs when they need at most kPsiSlots slots and the
+// two sides of each z pair they hold are apart in z (so they can share).
 __device__ __forceinline__ unsigned staged_mask(const KCpml& cp, int c0, int ib, int jb) {
     const unsigned m = cpml_tile_mask(cp, c0, ib, ib + kTX - 1, jb, jb + kTY - 1);
-    return __popc(m) <= kPsiSlots ? m : 0u;
+    const bool apart = ((m & 0x0Cu) != 0x0Cu || cp.s[c0][1][0].zhi < cp.s[c0][1][1].zlo) &&
+                       ((m & 0x30u) != 0x30u || cp.s[c0 + 1][0][0].zhi < cp.s[c0 + 1][0][1].zlo);
+    return apart && __popc(psi_slot_groups(m)) <= kPsiSlots ? m : 0u;
 }
 
 // One CPML correction of a consumer: CP 2 takes the old psi from the staged
 // tile, CP 1 from global memory.
 template <int CP, bool ADD>
-__device__ __forceinline__ float cpml_corr(const Slab (&s)[2], unsigned live2, int nbase, unsigned smask, const float* slots,
-                                           int o, int i, int j, int k, float pb, float pc, float diff, float g, float v,
-                                           bool& st) {
-    if (CP == 2) return cpml_pair_staged<ADD>(s, live2, nbase, smask, slots, kPsiSlotFloats, o, i, j, k, pb, pc, diff, g, v);
+__device__ __forceinline__ float cpml_corr(const Slab (&s)[2], unsigned live2, int nbase, const float* slots,
+                                           int o, const PsiRow* rows, int i, int j, int k, float pb, float pc, float diff,
+                                           float g, float v, bool& st) {
+    if (CP == 2) return cpml_pair_staged<ADD>(live2, nbase, slots, o, rows, o & 31, k, pb, pc, diff, g, v);
     return cpml_pair<ADD>(s, live2, i, j, k, pb, pc, diff, g, v, st);
 }
 
@@ -269,7 +273,7 @@ __device__ __forceinline__ void warp_release(const TmaCta& t, unsigned G) {
 // persistent CTA goes on to another item).  False on a timeout.
 template <int CP>
 __device__ __forceinline__ bool e_consume(const TmaCta& t, unsigned G0, const KGrid& g, const KCpml& cp, const float* t1,
-                                          const float* t2, int* err, bool release_last) {
+                                          const float* t2, int* err, bool release_last, PsiRow* rows) {
     const int w = t.warp, l = t.lane;
     const int i = t.ib + l, j = t.jb + w;
     const int nya = (int)(g.plane / g.pitch);
@@ -277,8 +281,8 @@ __device__ __forceinline__ bool e_consume(const TmaCta& t, unsigned G0, const KG
     const float idyh = g.idyh[min(j, nya - 1)], idxh = g.idxh[i];
     const long long pitch = g.pitch, plane = g.plane;
     const unsigned tmask = CP ? cpml_tile_mask(cp, 0, t.ib, t.ib + kTX - 1, t.jb, t.jb + kTY - 1) : 0u;
-    const unsigned smask = CP == 2 ? tmask : 0u;
     const CpmlCol cc = CP ? cpml_col(cp, 0, tmask, i, j, t.kb, t.ke) : CpmlCol{};
+    if (CP == 2) psi_rows_fill(rows, cp, 0, tmask, kPsiSlotFloats, t.ib, j, l);
     for (int k = t.kb; k <= t.ke; ++k) {
         const unsigned Gk = G0 + 1 + (unsigned)(k - t.kb), Gp = Gk - 1;
         const unsigned s = Gk % kStages, sp = Gp % kStages;
@@ -313,8 +317,8 @@ __device__ __forceinline__ bool e_consume(const TmaCta& t, unsigned G0, const KG
             const float dy = hz - hz_jm, dz = hy - hy_km;
             e = t1[m] * e + t2[m] * (dy * idyh - dz * idzh);
             if (CP && pm) {
-                e = cpml_corr<CP, true>(cp.s[0][0], pm & 3, 0, smask, PS, o, i, j, k, cc.by, cc.cy, dy, t2[m], e, st_);
-                e = cpml_corr<CP, false>(cp.s[0][1], (pm >> 2) & 3, 2, smask, PS, o, i, j, k, bz, cz, dz, t2[m], e, st_);
+                e = cpml_corr<CP, true>(cp.s[0][0], pm & 3, 0, PS, o, rows, i, j, k, cc.by, cc.cy, dy, t2[m], e, st_);
+                e = cpml_corr<CP, false>(cp.s[0][1], (pm >> 2) & 3, 2, PS, o, rows, i, j, k, bz, cz, dz, t2[m], e, st_);
             }
             g.F[0][c] = e;
         }
@@ -324,8 +328,8 @@ __device__ __forceinline__ bool e_consume(const TmaCta& t, unsigned G0, const KG
             const float dz = hx - hx_km, dx = hz - hz_im;
             e = t1[m] * e + t2[m] * (dz * idzh - dx * idxh);
             if (CP && pm) {
-                e = cpml_corr<CP, true>(cp.s[1][0], (pm >> 4) & 3, 4, smask, PS, o, i, j, k, bz, cz, dz, t2[m], e, st_);
-                e = cpml_corr<CP, false>(cp.s[1][1], (pm >> 6) & 3, 6, smask, PS, o, i, j, k, cc.bx, cc.cx, dx, t2[m], e, st_);
+                e = cpml_corr<CP, true>(cp.s[1][0], (pm >> 4) & 3, 4, PS, o, rows, i, j, k, bz, cz, dz, t2[m], e, st_);
+                e = cpml_corr<CP, false>(cp.s[1][1], (pm >> 6) & 3, 6, PS, o, rows, i, j, k, cc.bx, cc.cx, dx, t2[m], e, st_);
             }
             g.F[1][c] = e;
         }
@@ -335,8 +339,8 @@ __device__ __forceinline__ bool e_consume(const TmaCta& t, unsigned G0, const KG
             const float dx = hy - hy_im, dy = hx - hx_jm;
             e = t1[m] * e + t2[m] * (dx * idxh - dy * idyh);
             if (CP && pm) {
-                e = cpml_corr<CP, false>(cp.s[2][0], (pm >> 8) & 3, 8, smask, PS, o, i, j, k, cc.by, cc.cy, dy, t2[m], e, st_);
-                e = cpml_corr<CP, true>(cp.s[2][1], (pm >> 10) & 3, 10, smask, PS, o, i, j, k, cc.bx, cc.cx, dx, t2[m], e, st_);
+                e = cpml_corr<CP, false>(cp.s[2][0], (pm >> 8) & 3, 8, PS, o, rows, i, j, k, cc.by, cc.cy, dy, t2[m], e, st_);
+                e = cpml_corr<CP, true>(cp.s[2][1], (pm >> 10) & 3, 10, PS, o, rows, i, j, k, cc.bx, cc.cx, dx, t2[m], e, st_);
             }
             g.F[2][c] = e;
         }
@@ -351,7 +355,7 @@ __device__ __forceinline__ bool e_consume(const TmaCta& t, unsigned G0, const KG
 // k = kb..ke+1 (ke+1 the edge); plane k is released once it is done.
 template <int CP>
 __device__ __forceinline__ bool h_consume(const TmaCta& t, unsigned G0, const KGrid& g, const KCpml& cp, const float* t1,
-                                          const float* t2, int* err, bool release_last) {
+                                          const float* t2, int* err, bool release_last, PsiRow* rows) {
     const int w = t.warp, l = t.lane;
     const int i = t.ib + l, j = t.jb + w;
     const int nya = (int)(g.plane / g.pitch);
@@ -359,8 +363,8 @@ __device__ __forceinline__ bool h_consume(const TmaCta& t, unsigned G0, const KG
     const float idye = g.idye[min(j, nya - 1)], idxe = g.idxe[i];
     const long long pitch = g.pitch, plane = g.plane;
     const unsigned tmask = CP ? cpml_tile_mask(cp, 3, t.ib, t.ib + kTX - 1, t.jb, t.jb + kTY - 1) : 0u;
-    const unsigned smask = CP == 2 ? tmask : 0u;
     const CpmlCol cc = CP ? cpml_col(cp, 3, tmask, i, j, t.kb, t.ke) : CpmlCol{};
+    if (CP == 2) psi_rows_fill(rows, cp, 3, tmask, kPsiSlotFloats, t.ib, j, l);
     for (int k = t.kb; k <= t.ke; ++k) {
         const unsigned Gk = G0 + (unsigned)(k - t.kb), Gn = Gk + 1;
         const unsigned s = Gk % kStages, sn = Gn % kStages;
@@ -394,8 +398,8 @@ __device__ __forceinline__ bool h_consume(const TmaCta& t, unsigned G0, const KG
             const float dz = ey_kp - ey, dy = ez_jp - ez;
             h = t1[m] * h + t2[m] * (dz * idze - dy * idye);
             if (CP && pm) {
-                h = cpml_corr<CP, false>(cp.s[3][0], pm & 3, 0, smask, PS, o, i, j, k, cc.by, cc.cy, dy, t2[m], h, st_);
-                h = cpml_corr<CP, true>(cp.s[3][1], (pm >> 2) & 3, 2, smask, PS, o, i, j, k, bz, cz, dz, t2[m], h, st_);
+                h = cpml_corr<CP, false>(cp.s[3][0], pm & 3, 0, PS, o, rows, i, j, k, cc.by, cc.cy, dy, t2[m], h, st_);
+                h = cpml_corr<CP, true>(cp.s[3][1], (pm >> 2) & 3, 2, PS, o, rows, i, j, k, bz, cz, dz, t2[m], h, st_);
             }
             g.F[3][c] = h;
         }
@@ -405,8 +409,8 @@ __device__ __forceinline__ bool h_consume(const TmaCta& t, unsigned G0, const KG
             const float dx = ez_ip - ez, dz = ex_kp - ex;
             h = t1[m] * h + t2[m] * (dx * idxe - dz * idze);
             if (CP && pm) {
-                h = cpml_corr<CP, false>(cp.s[4][0], (pm >> 4) & 3, 4, smask, PS, o, i, j, k, bz, cz, dz, t2[m], h, st_);
-                h = cpml_corr<CP, true>(cp.s[4][1], (pm >> 6) & 3, 6, smask, PS, o, i, j, k, cc.bx, cc.cx, dx, t2[m], h, st_);
+                h = cpml_corr<CP, false>(cp.s[4][0], (pm >> 4) & 3, 4, PS, o, rows, i, j, k, bz, cz, dz, t2[m], h, st_);
+                h = cpml_corr<CP, true>(cp.s[4][1], (pm >> 6) & 3, 6, PS, o, rows, i, j, k, cc.bx, cc.cx, dx, t2[m], h, st_);
             }
             g.F[4][c] = h;
         }
@@ -416,8 +420,8 @@ __device__ __forceinline__ bool h_consume(const TmaCta& t, unsigned G0, const KG
             const float dy = ex_jp - ex, dx = ey_ip - ey;
             h = t1[m] * h + t2[m] * (dy * idye - dx * idxe);
             if (CP && pm) {
-                h = cpml_corr<CP, true>(cp.s[5][0], (pm >> 8) & 3, 8, smask, PS, o, i, j, k, cc.by, cc.cy, dy, t2[m], h, st_);
-                h = cpml_corr<CP, false>(cp.s[5][1], (pm >> 10) & 3, 10, smask, PS, o, i, j, k, cc.bx, cc.cx, dx, t2[m], h, st_);
+                h = cpml_corr<CP, true>(cp.s[5][0], (pm >> 8) & 3, 8, PS, o, rows, i, j, k, cc.by, cc.cy, dy, t2[m], h, st_);
+                h = cpml_corr<CP, false>(cp.s[5][1], (pm >> 10) & 3, 10, PS, o, rows, i, j, k, cc.bx, cc.cx, dx, t2[m], h, st_);
             }
             g.F[5][c] = h;
         }
