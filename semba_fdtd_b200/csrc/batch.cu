@@ -132,9 +132,9 @@ struct RangeItem {
 enum : int { kCntE = 0, kCntH, kCntNode, kCntSrcE, kCntSrcH, kCntProbe, kCntClone, kCntMur, kCntMNode, kNumCounts };
 
 constexpr int kNodeChunk = 2048;  // ADE nodes per work item
-constexpr int kRowChunk = 128;    // source rows / probes per work item
-constexpr int kBorderChunk = 1024;  // clone / Mur cells per work item
 constexpr int kPhaseThreads = 256;
+constexpr int kRowChunk = kPhaseThreads;  // source rows / probes per work item (one per thread)
+constexpr int kBorderChunk = 1024;  // clone / Mur cells per work item
 
 __device__ __forceinline__ int inst_step(const InstDesc& D, const int* G, bool* on) {
     const int n = *G + D.step_off;
@@ -226,7 +226,8 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
     const int n_items = counts[SIDE == 0 ? kCntE : kCntH];
     const bool producer = t.warp == kConsumerWarps;
     unsigned gp = 0;  // running plane number of the ring
-    int fenced = -1;  // the instance whose tensor maps the producer has acquired
+    int fenced = -1;     // the instance whose tensor maps the producer has acquired
+    unsigned fmask = 0;  // ... and which of them
     int viewed = -1;  // ... whose view the consumer warp holds
     for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
         const FieldItem w = items[it];
@@ -251,10 +252,16 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
             int got = np;
             if (t.lane == 0) {
                 const CUtensorMap* m = maps[2 * w.slot + SIDE].m;
+                // acquire the maps this item loads through that this CTA has not
+                // acquired yet for the instance: the field / media maps and the
+                // staged psi maps
                 if (fenced != w.slot) {
-                    for (int q = 0; q < kPsiMap0 + 12; ++q) tensormap_acquire(&m[q]);
                     fenced = w.slot;
+                    fmask = 0;
                 }
+                const unsigned need = ((1u << kPsiMap0) - 1u) | (smask << kPsiMap0);
+                for (unsigned todo = need & ~fmask; todo; todo &= todo - 1u) tensormap_acquire(&m[__ffs(todo) - 1]);
+                fmask |= need;
                 got = tma_issue(t, m, gp, p0, p1, edge, SIDE != 0, err, &tb, smask);
             }
             got = __shfl_sync(0xffffffffu, got, 0);
