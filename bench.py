@@ -230,7 +230,7 @@ def run_ours(args):
     lib.sgpu_algorithmic_bytes(s.handle, bytes6)
     names = ["efield_curl_cpml", "edispersive_ade", "sources_e", "hfield_curl_cpml", "sources_h", "probes"]
     fe, fh = ("k_tma_efield", "k_tma_hfield") if args.family == 1 else ("k_efield", "k_hfield")
-    kern = [fe, "k_edisp", "k_sources", fh, "k_sources", "k_probes"]
+    kern = [fe, "k_ade", "k_sources", fh, "k_sources", "k_probes"]
     avg_ms = [phases[q] / K for q in range(6)]
     dom = int(np.argmax(avg_ms))
     peak, peak_kind = measured_hbm_peak()

@@ -12,6 +12,8 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <mutex>
+#include <memory>
 #include <new>
 #include <string>
 #include <vector>
@@ -40,18 +42,34 @@ struct Vec {
     float operator[](int i) const { return v[i - lo]; }
 };
 
-// int16 media matrix over one component's Alloc, column-major.
+// Planes of an nx x ny box that make about 64 Ki cells: the smallest share
+// of a plane loop one set-up thread takes.
+long long plane_grain(long long nx, long long ny) { return std::max(1LL, (1LL << 16) / std::max(1LL, nx * ny)); }
+
+// int16 media matrix over one component's Alloc, column-major (filled with
+// medium 1 by several threads on large grids).
 struct MediaMat {
     Box b;
-    long long nx, ny;
-    std::vector<int16_t> v;
+    long long nx = 0, ny = 0;
+    size_t n = 0;
+    std::unique_ptr<int16_t[]> v;
     void init(const Box& bb) {
         b = bb;
         nx = b.x1 - b.x0 + 1;
         ny = b.y1 - b.y0 + 1;
-        v.assign((size_t)nx * ny * (b.z1 - b.z0 + 1), (int16_t)1);
+        n = (size_t)nx * ny * (b.z1 - b.z0 + 1);
+        v.reset(new int16_t[n]);
+        int16_t* p = v.get();
+        sgpu::host_parallel((long long)n, [p](long long a, long long e) { std::fill(p + a, p + e, (int16_t)1); }, 1 << 20);
     }
     int16_t& at(int i, int j, int k) { return v[(i - b.x0) + nx * ((j - b.y0) + ny * (long long)(k - b.z0))]; }
+    int16_t* data() const { return v.get(); }
+    size_t size() const { return n; }
+    bool empty() const { return n == 0; }
+    void release() {
+        v.reset();
+        n = 0;
+    }
 };
 
 struct Med {
@@ -196,13 +214,17 @@ void paint(HostState& h, const Box& pt, int idx) {
     for (int f = 0; f < 6; ++f) {
         MediaMat& m = h.mm[f];
         const bool electric = f < 3;
-        for (int k = z0; k <= up[f][2]; ++k)
-            for (int j = y0; j <= up[f][1]; ++j)
-                for (int i = x0; i <= up[f][0]; ++i) {
-                    int16_t& cell = m.at(i, j, k);
-                    int cur = h.med[cell].prio;
-                    if (electric ? pr > cur : pr >= cur) cell = (int16_t)idx;
-                }
+        const int nk = up[f][2] - z0 + 1;
+        if (nk <= 0 || up[f][1] < y0 || up[f][0] < x0) continue;
+        sgpu::host_parallel(nk, [&, f](long long a, long long e) {
+            for (int k = z0 + (int)a; k < z0 + (int)e; ++k)
+                for (int j = y0; j <= up[f][1]; ++j)
+                    for (int i = x0; i <= up[f][0]; ++i) {
+                        int16_t& cell = m.at(i, j, k);
+                        const int cur = h.med[cell].prio;
+                        if (electric ? pr > cur : pr >= cur) cell = (int16_t)idx;
+                    }
+        }, plane_grain(up[f][0] - x0 + 1, up[f][1] - y0 + 1));
     }
 }
 
@@ -222,76 +244,109 @@ void pml_media(HostState& h) {
                        std::max(outer.y0, h.full[HY].y0), std::min(outer.y1 + on_hi[f][1], h.full[HY].y1),
                        std::max(outer.z0, h.full[HZ].z0), std::min(outer.z1 + on_hi[f][2], h.full[HZ].z1)};
     auto neg = [](int16_t v) { return (int16_t)(-std::abs((int)v)); };
+    // the three extrusions in order; within each, planes are independent
     for (int f = 0; f < 6; ++f) {
         MediaMat& m = h.mm[f];
         const Box& r = reach[f];
         const int lo_src[3] = {inner.x0, inner.y0, inner.z0};
         const int hi_src[3] = {inner.x1 + in_lo[f][0] - 1, inner.y1 + in_lo[f][1] - 1, inner.z1 + in_lo[f][2] - 1};
+        const long long grain = plane_grain(r.x1 - r.x0 + 1, r.y1 - r.y0 + 1);
+        auto planes = [&](int k0, int k1, auto&& fn) {
+            if (k1 >= k0) sgpu::host_parallel(k1 - k0 + 1, [&](long long a, long long e) {
+                for (int k = k0 + (int)a; k < k0 + (int)e; ++k) fn(k);
+            }, grain);
+        };
         // along x (rows are contiguous: k, then j, then the two i ranges)
-        for (int k = r.z0; k <= r.z1; ++k)
+        planes(r.z0, r.z1, [&](int k) {
             for (int j = r.y0; j <= r.y1; ++j) {
                 int16_t* row = &m.at(r.x0, j, k) - r.x0;  // row[i] is cell (i, j, k)
                 const int16_t lo = neg(row[lo_src[0]]), hi = neg(row[hi_src[0]]);
                 for (int i = r.x0; i <= inner.x0 - 1; ++i) row[i] = lo;
                 for (int i = inner.x1 + in_lo[f][0]; i <= r.x1; ++i) row[i] = hi;
             }
+        });
         // along y, over the whole x reach (edges): whole rows copied
         auto copy_row = [&](int16_t* dst, const int16_t* src) {
             for (int i = r.x0; i <= r.x1; ++i) dst[i] = neg(src[i]);
         };
-        for (int k = r.z0; k <= r.z1; ++k) {
+        planes(r.z0, r.z1, [&](int k) {
             const int16_t* slo = &m.at(r.x0, lo_src[1], k) - r.x0;
             const int16_t* shi = &m.at(r.x0, hi_src[1], k) - r.x0;
             for (int j = r.y0; j <= inner.y0 - 1; ++j) copy_row(&m.at(r.x0, j, k) - r.x0, slo);
             for (int j = inner.y1 + in_lo[f][1]; j <= r.y1; ++j) copy_row(&m.at(r.x0, j, k) - r.x0, shi);
-        }
+        });
         // along z, over the whole x and y reach (corners): whole planes copied
-        for (int k = r.z0; k <= inner.z0 - 1; ++k)
+        planes(r.z0, inner.z0 - 1, [&](int k) {
             for (int j = r.y0; j <= r.y1; ++j) copy_row(&m.at(r.x0, j, k) - r.x0, &m.at(r.x0, j, lo_src[2]) - r.x0);
-        for (int k = inner.z1 + in_lo[f][2]; k <= r.z1; ++k)
+        });
+        planes(inner.z1 + in_lo[f][2], r.z1, [&](int k) {
             for (int j = r.y0; j <= r.y1; ++j) copy_row(&m.at(r.x0, j, k) - r.x0, &m.at(r.x0, j, hi_src[2]) - r.x0);
+        });
     }
-    // Only the extruded shell can hold negative (to be copied) entries; the
-    // scans below visit it row by row in the k, j, i order of a full sweep,
-    // so copies are numbered in order of first appearance exactly as a full
-    // sweep numbers them.
-    auto shell_rows = [&](int f, auto&& fn) {
-        MediaMat& m = h.mm[f];
-        const Box& r = reach[f];
-        const int xa = inner.x0, xb = inner.x1 + in_lo[f][0] - 1;
-        const int ya = inner.y0, yb = inner.y1 + in_lo[f][1] - 1;
-        const int za = inner.z0, zb = inner.z1 + in_lo[f][2] - 1;
-        for (int k = r.z0; k <= r.z1; ++k)
-            for (int j = r.y0; j <= r.y1; ++j) {
-                int16_t* row = &m.at(r.x0, j, k) - r.x0;
-                if (k < za || k > zb || j < ya || j > yb) {
-                    fn(row, r.x0, r.x1);
-                } else {
-                    fn(row, r.x0, std::min(r.x1, xa - 1));
-                    fn(row, std::max(r.x0, xb + 1), r.x1);
-                }
-            }
+    // Only the extruded shell can hold negative (to be copied) entries.  A
+    // full sweep (components in order, then k, j, i) numbers the copies in
+    // order of first appearance; here every plane of the shell is scanned
+    // in parallel for the first position of each entry, and the copies are
+    // numbered by those positions.
+    struct Task {
+        int f, k;
     };
+    std::vector<Task> tasks;
+    for (int f = 0; f < 6; ++f)
+        for (int k = reach[f].z0; k <= reach[f].z1; ++k) tasks.push_back(Task{f, k});
+    auto shell_row_spans = [&](const Task& t, auto&& fn) {
+        MediaMat& m = h.mm[t.f];
+        const Box& r = reach[t.f];
+        const int xa = inner.x0, xb = inner.x1 + in_lo[t.f][0] - 1;
+        const int ya = inner.y0, yb = inner.y1 + in_lo[t.f][1] - 1;
+        const int za = inner.z0, zb = inner.z1 + in_lo[t.f][2] - 1;
+        for (int j = r.y0; j <= r.y1; ++j) {
+            int16_t* row = &m.at(r.x0, j, t.k) - r.x0;
+            if (t.k < za || t.k > zb || j < ya || j > yb) {
+                fn(row, j - r.y0, r.x0, r.x1, r.x0);
+            } else {
+                fn(row, j - r.y0, r.x0, std::min(r.x1, xa - 1), r.x0);
+                fn(row, j - r.y0, std::max(r.x0, xb + 1), r.x1, r.x0);
+            }
+        }
+    };
+    const long long kNone = std::numeric_limits<long long>::max();
+    std::vector<long long> first(h.num_media + 1, kNone);
+    std::mutex mu;
+    const long long row_cells = (long long)(outer.x1 - outer.x0 + 1) * (outer.y1 - outer.y0 + 1);
+    sgpu::host_parallel((long long)tasks.size(), [&](long long a, long long e) {
+        std::vector<long long> mine(h.num_media + 1, kNone);
+        for (long long q = a; q < e; ++q)
+            shell_row_spans(tasks[q], [&](const int16_t* row, int jr, int i0, int i1, int x0) {
+                for (int i = i0; i <= i1; ++i) {
+                    const int v = row[i];
+                    if (v < 0) {
+                        const long long key = (q * (outer.y1 - outer.y0 + 1) + jr) * (outer.x1 - outer.x0 + 1) + (i - x0);
+                        if (key < mine[-v]) mine[-v] = key;
+                    }
+                }
+            });
+        std::lock_guard<std::mutex> g(mu);
+        for (size_t v = 0; v < mine.size(); ++v) first[v] = std::min(first[v], mine[v]);
+    }, plane_grain(row_cells, 1));
+    std::vector<int> order;
+    for (int v = 1; v <= h.num_media; ++v)
+        if (first[v] != kNone) order.push_back(v);
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return first[a] < first[b]; });
     std::vector<int> copy_of(h.num_media + 1, 0);
     int next = h.num_media;
-    for (int f = 0; f < 6; ++f)
-        shell_rows(f, [&](int16_t* row, int i0, int i1) {
-            for (int i = i0; i <= i1; ++i) {
-                const int v = row[i];
-                if (v < 0 && copy_of[-v] == 0) copy_of[-v] = ++next;
-            }
-        });
-    h.med.resize(next + 1);
-    for (int f = 0; f < 6; ++f)
-        shell_rows(f, [&](int16_t* row, int i0, int i1) {
-            for (int i = i0; i <= i1; ++i) {
-                const int v = row[i];
-                if (v < 0) {
-                    h.med[copy_of[-v]] = h.med[-v];
-                    row[i] = (int16_t)copy_of[-v];
-                }
-            }
-        });
+    h.med.resize(h.num_media + 1 + order.size());
+    for (int v : order) {
+        copy_of[v] = ++next;
+        h.med[next] = h.med[v];
+    }
+    sgpu::host_parallel((long long)tasks.size(), [&](long long a, long long e) {
+        for (long long q = a; q < e; ++q)
+            shell_row_spans(tasks[q], [&](int16_t* row, int, int i0, int i1, int) {
+                for (int i = i0; i <= i1; ++i)
+                    if (row[i] < 0) row[i] = (int16_t)copy_of[-row[i]];
+            });
+    }, plane_grain(row_cells, 1));
     h.num_media = next;
     // PEC borders (healer.F90:1442-1617): medium 0 on the boundary plane of
     // the E components tangential to the face and the H component normal to it
@@ -844,8 +899,8 @@ sgpu_status realize(HostState* h, sgpu::Arena* arena, cudaStream_t stream, sgpu_
     c->host = h;
     c->host_free = free_host;
     for (int f = 0; f < 6; ++f) {
-        if ((s = sgpu_upload_media(c, f, h->mm[f].v.data()))) return s;
-        std::vector<int16_t>().swap(h->mm[f].v);  // released once on the device
+        if ((s = sgpu_upload_media(c, f, h->mm[f].data()))) return s;
+        h->mm[f].release();  // released once on the device
     }
     if ((s = sgpu_init_cpml(c, &h->cd))) return s;
     sgpu_border_desc bd{};
@@ -942,7 +997,7 @@ sgpu_status sgpu_host_footprint(const sgpu_ctx* c, uint64_t* bytes) {
         uint64_t nodes = 0;
         bool have = true;
         for (int f = 3 * side; f < 3 * side + 3; ++f) {
-            if (h->mm[f].v.empty()) { have = false; break; }
+            if (h->mm[f].empty()) { have = false; break; }
             const Box& w = h->sweep[f];
             MediaMat& m = const_cast<MediaMat&>(h->mm[f]);
             for (int k = w.z0; k <= w.z1; ++k)
@@ -1005,7 +1060,7 @@ sgpu_status sgpu_batch_footprint(const sgpu_ctx* c, uint64_t* bytes, uint64_t* l
         for (int f = 3 * side; f < 3 * side + 3; ++f) {
             uint64_t nodes = 0;
             const Box& w = h->sweep[f];
-            if (h->mm[f].v.empty()) {
+            if (h->mm[f].empty()) {
                 nodes = (uint64_t)vol;
             } else {
                 MediaMat& m = const_cast<MediaMat&>(h->mm[f]);
@@ -1103,7 +1158,7 @@ sgpu_status sgpu_host_get_media(const sgpu_ctx* c, int comp, int16_t* out) {
     sgpu_ctx* cc = const_cast<sgpu_ctx*>(c);
     if (c->host_only) {
         const HostState* h = (const HostState*)c->host;
-        std::memcpy(out, h->mm[comp].v.data(), h->mm[comp].v.size() * sizeof(int16_t));
+        std::memcpy(out, h->mm[comp].data(), h->mm[comp].size() * sizeof(int16_t));
         return SGPU_OK;
     }
     const sgpu_lim& a = c->alloc[comp];

@@ -232,6 +232,10 @@ __global__ void k_clone_h(KGrid g, KBorder b, int mask) {
 }
 __global__ void k_mur_h(KGrid g, KBorder b) { mur_cell(g, b, blockIdx.x * (long long)blockDim.x + threadIdx.x); }
 
+__global__ void k_fill_i16(int16_t* p, long long n, int v) {
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        p[q] = (int16_t)v;
+}
 __global__ void k_set_step(int* d, int v) { *d = v; }
 __global__ void k_add_step(int* d, int v) { *d += v; }
 
@@ -746,39 +750,35 @@ sgpu_status sgpu_upload_media(sgpu_ctx* c, int comp, const int16_t* mi) {
     const sgpu_lim& a = c->alloc[comp];
     const long long ax = a.xe - a.xi + 1, ay = a.ye - a.yi + 1, az = a.ze - a.zi + 1;
     const long long n = ax * ay * az;
+    std::mutex mu;
     int lo = 0x7fff, hi = 0;
-    for (long long q = 0; q < n; ++q) {
-        lo = std::min(lo, (int)mi[q]);
-        hi = std::max(hi, (int)mi[q]);
-    }
+    host_parallel(n, [&](long long q0, long long q1) {
+        int l = 0x7fff, h = 0;
+        for (long long q = q0; q < q1; ++q) {
+            l = std::min(l, (int)mi[q]);
+            h = std::max(h, (int)mi[q]);
+        }
+        std::lock_guard<std::mutex> g(mu);
+        lo = std::min(lo, l);
+        hi = std::max(hi, h);
+    }, 1 << 20);
     if (lo < 0 || hi > c->num_media) return set_error(c, SGPU_ERR_ARG, "media index outside 0..num_media");
-    // the padded device layout built on the host and sent in one copy; the
-    // unused padding of the common box is vacuum
-    std::vector<int16_t> buf((size_t)c->vol, (int16_t)1);
-    for (long long k = 0; k < az; ++k)
-        for (long long j = 0; j < ay; ++j)
-            std::memcpy(&buf[(size_t)(c->pitch * j + c->plane * k)], mi + ax * (j + ay * k), (size_t)ax * sizeof(int16_t));
-    CUDA_TRY(c, cudaMemcpyAsync(c->M[comp], buf.data(), buf.size() * sizeof(int16_t), cudaMemcpyHostToDevice, c->stream));
-    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    // the unused padding of the common box is vacuum
+    k_fill_i16<<<(unsigned)std::min<long long>((c->vol + 255) / 256, 65535), 256, 0, c->stream>>>(c->M[comp], c->vol, 1);
+    CUDA_TRY(c, cudaGetLastError());
+    CUDA_TRY(c, box_to_device(c->M[comp], mi, sizeof(int16_t), ax, ay, az, c->pitch, c->plane / c->pitch, c->stream));
     c->media_loaded[comp] = true;
     c->src_dirty = true;
     return SGPU_OK;
 }
 
-// Field copies go through a host image of the padded device array in one
-// contiguous transfer (a row-by-row copy of short rows is far slower).  The
-// padding outside a component's Alloc range is zero on the device and stays
-// zero.
+// The padding outside a component's Alloc range is zero on the device and
+// stays zero; only the Alloc box moves.
 sgpu_status sgpu_upload_field(sgpu_ctx* c, int comp, const float* f) {
     if (!c || !f || comp < 0 || comp > 5) return set_error(c, SGPU_ERR_ARG, "bad field upload");
     const sgpu_lim& a = c->alloc[comp];
     const long long ax = a.xe - a.xi + 1, ay = a.ye - a.yi + 1, az = a.ze - a.zi + 1;
-    std::vector<float> buf((size_t)c->vol, 0.0f);
-    for (long long k = 0; k < az; ++k)
-        for (long long j = 0; j < ay; ++j)
-            std::memcpy(&buf[(size_t)(c->pitch * j + c->plane * k)], f + ax * (j + ay * k), (size_t)ax * sizeof(float));
-    CUDA_TRY(c, cudaMemcpyAsync(c->F[comp], buf.data(), buf.size() * sizeof(float), cudaMemcpyHostToDevice, c->stream));
-    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    CUDA_TRY(c, box_to_device(c->F[comp], f, sizeof(float), ax, ay, az, c->pitch, c->plane / c->pitch, c->stream));
     return SGPU_OK;
 }
 
@@ -786,12 +786,7 @@ sgpu_status sgpu_download_field(sgpu_ctx* c, int comp, float* f) {
     if (!c || !f || comp < 0 || comp > 5) return set_error(c, SGPU_ERR_ARG, "bad field download");
     const sgpu_lim& a = c->alloc[comp];
     const long long ax = a.xe - a.xi + 1, ay = a.ye - a.yi + 1, az = a.ze - a.zi + 1;
-    std::vector<float> buf((size_t)c->vol);
-    CUDA_TRY(c, cudaMemcpyAsync(buf.data(), c->F[comp], buf.size() * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
-    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-    for (long long k = 0; k < az; ++k)
-        for (long long j = 0; j < ay; ++j)
-            std::memcpy(f + ax * (j + ay * k), &buf[(size_t)(c->pitch * j + c->plane * k)], (size_t)ax * sizeof(float));
+    CUDA_TRY(c, box_to_host(f, c->F[comp], sizeof(float), ax, ay, az, c->pitch, c->plane / c->pitch, c->stream));
     return SGPU_OK;
 }
 

@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -252,4 +253,15 @@ sgpu_status host_create_in(const sgpu_problem* p, sgpu_ctx* plan, int max_steps,
 // Source lists built on the device now (normally built lazily before the
 // first launch that needs them).
 sgpu_status rebuild_sources(sgpu_ctx* c);
+// Copies between a compact column-major box of ax x ay x az elements of es
+// bytes in host memory and the same box at the origin of a padded device
+// array (rows of `pitch` elements, `rows` rows per plane), on stream `st`,
+// through pinned staging (transfer.cu); synchronous.
+cudaError_t box_to_device(void* dev, const void* host, size_t es, long long ax, long long ay, long long az, int pitch,
+                          long long rows, cudaStream_t st);
+cudaError_t box_to_host(void* host, const void* dev, size_t es, long long ax, long long ay, long long az, int pitch,
+                        long long rows, cudaStream_t st);
+// fn(lo, hi) over [0, n) split across up to 8 host threads, each taking at
+// least `grain` units.
+void host_parallel(long long n, const std::function<void(long long, long long)>& fn, long long grain = 2048);
 }  // namespace sgpu

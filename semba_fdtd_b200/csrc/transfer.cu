@@ -1,0 +1,175 @@
+// Host <-> device copies of whole component arrays.
+//
+// The device keeps each component in the padded box of sgpu_internal.h (rows
+// of `pitch` elements, `rows` rows per plane); callers hand over the compact
+// column-major Alloc box (ax x ay x az).  A copy goes in chunks of whole
+// planes (or of rows, when one plane exceeds a chunk) through two pinned
+// staging buffers shared by the process: host threads move one chunk between
+// the caller's array and a staging buffer -- a plain contiguous copy, since a
+// chunk of the compact box is contiguous -- while the copy engine moves the
+// other between the staging buffer and the padded device array with a pitched
+// 3D copy, which does the re-layout.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "sgpu_internal.h"
+
+namespace sgpu {
+
+namespace {
+
+constexpr size_t kStageBytes = 32u << 20;
+
+struct Staging {
+    std::mutex mu;
+    void* buf[2] = {nullptr, nullptr};
+};
+
+Staging& staging() {
+    static Staging s;  // kept for the life of the process
+    return s;
+}
+
+cudaError_t staging_ready(Staging& s) {
+    for (int b = 0; b < 2; ++b)
+        if (!s.buf[b]) {
+            const cudaError_t e = cudaHostAlloc(&s.buf[b], kStageBytes, cudaHostAllocPortable);
+            if (e != cudaSuccess) {
+                s.buf[b] = nullptr;
+                return e;
+            }
+        }
+    return cudaSuccess;
+}
+
+// One chunk: planes k0 .. k0+nk-1, rows j0 .. j0+nj-1 of each (nj == ay or
+// nk == 1, so the chunk is contiguous in the compact box).
+struct Chunk {
+    long long k0, nk, j0, nj;
+};
+
+std::vector<Chunk> chunks(size_t es, long long ax, long long ay, long long az) {
+    std::vector<Chunk> v;
+    const size_t row = (size_t)ax * es, plane = row * (size_t)ay;
+    if (plane <= kStageBytes) {
+        const long long per = std::max<long long>(1, (long long)(kStageBytes / plane));
+        for (long long k = 0; k < az; k += per) v.push_back(Chunk{k, std::min(per, az - k), 0, ay});
+    } else {
+        const long long per = std::max<long long>(1, (long long)(kStageBytes / row));
+        for (long long k = 0; k < az; ++k)
+            for (long long j = 0; j < ay; j += per) v.push_back(Chunk{k, 1, j, std::min(per, ay - j)});
+    }
+    return v;
+}
+
+cudaMemcpy3DParms pitched(void* dev, int pitch, long long rows, void* stage, size_t es, long long ax, const Chunk& q,
+                          bool to_device) {
+    cudaMemcpy3DParms p{};
+    const cudaPitchedPtr d = make_cudaPitchedPtr(dev, (size_t)pitch * es, (size_t)pitch * es, (size_t)rows);
+    const cudaPitchedPtr h = make_cudaPitchedPtr(stage, (size_t)ax * es, (size_t)ax * es, (size_t)q.nj);
+    const cudaPos at = make_cudaPos(0, (size_t)q.j0, (size_t)q.k0);
+    if (to_device) {
+        p.srcPtr = h;
+        p.dstPtr = d;
+        p.dstPos = at;
+        p.kind = cudaMemcpyHostToDevice;
+    } else {
+        p.srcPtr = d;
+        p.srcPos = at;
+        p.dstPtr = h;
+        p.kind = cudaMemcpyDeviceToHost;
+    }
+    p.extent = make_cudaExtent((size_t)ax * es, (size_t)q.nj, (size_t)q.nk);
+    return p;
+}
+
+void copy_bytes(void* dst, const void* src, size_t n) {
+    host_parallel((long long)((n + 4095) / 4096), [&](long long a, long long b) {
+        const size_t lo = (size_t)a * 4096, hi = std::min(n, (size_t)b * 4096);
+        if (hi > lo) std::memcpy((char*)dst + lo, (const char*)src + lo, hi - lo);
+    });
+}
+
+}  // namespace
+
+void host_parallel(long long n, const std::function<void(long long, long long)>& fn, long long grain) {
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    const int nt = (int)std::min<long long>(std::min(8, hw), std::max<long long>(1, n / std::max(1LL, grain)));
+    if (nt <= 1) {
+        if (n > 0) fn(0, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    th.reserve(nt - 1);
+    const long long per = (n + nt - 1) / nt;
+    for (int t = 1; t < nt; ++t) {
+        const long long a = t * per, b = std::min(n, a + per);
+        if (a < b) th.emplace_back(fn, a, b);
+    }
+    fn(0, std::min(n, per));
+    for (std::thread& t : th) t.join();
+}
+
+cudaError_t box_to_device(void* dev, const void* host, size_t es, long long ax, long long ay, long long az, int pitch,
+                          long long rows, cudaStream_t st) {
+    Staging& s = staging();
+    std::lock_guard<std::mutex> lock(s.mu);
+    cudaError_t e = staging_ready(s);
+    if (e != cudaSuccess) return e;
+    cudaEvent_t done[2] = {nullptr, nullptr};
+    for (cudaEvent_t& d : done)
+        if ((e = cudaEventCreateWithFlags(&d, cudaEventDisableTiming)) != cudaSuccess) break;
+    const std::vector<Chunk> cs = e == cudaSuccess ? chunks(es, ax, ay, az) : std::vector<Chunk>();
+    for (size_t q = 0; q < cs.size() && e == cudaSuccess; ++q) {
+        const int b = (int)(q & 1);
+        if (q >= 2 && (e = cudaEventSynchronize(done[b])) != cudaSuccess) break;  // the engine is done with buffer b
+        const Chunk& c = cs[q];
+        const size_t off = ((size_t)c.k0 * ay + c.j0) * ax * es, n = (size_t)c.nk * c.nj * ax * es;
+        copy_bytes(s.buf[b], (const char*)host + off, n);
+        const cudaMemcpy3DParms p = pitched(dev, pitch, rows, s.buf[b], es, ax, c, true);
+        if ((e = cudaMemcpy3DAsync(&p, st)) != cudaSuccess) break;
+        e = cudaEventRecord(done[b], st);
+    }
+    const cudaError_t w = cudaStreamSynchronize(st);  // the staging buffers are free again
+    for (cudaEvent_t d : done)
+        if (d) cudaEventDestroy(d);
+    return e != cudaSuccess ? e : w;
+}
+
+cudaError_t box_to_host(void* host, const void* dev, size_t es, long long ax, long long ay, long long az, int pitch,
+                        long long rows, cudaStream_t st) {
+    Staging& s = staging();
+    std::lock_guard<std::mutex> lock(s.mu);
+    cudaError_t e = staging_ready(s);
+    if (e != cudaSuccess) return e;
+    cudaEvent_t done[2] = {nullptr, nullptr};
+    for (cudaEvent_t& d : done)
+        if ((e = cudaEventCreateWithFlags(&d, cudaEventDisableTiming)) != cudaSuccess) break;
+    const std::vector<Chunk> cs = e == cudaSuccess ? chunks(es, ax, ay, az) : std::vector<Chunk>();
+    auto issue = [&](size_t q) {
+        const int b = (int)(q & 1);
+        const cudaMemcpy3DParms p = pitched(const_cast<void*>(dev), pitch, rows, s.buf[b], es, ax, cs[q], false);
+        cudaError_t r = cudaMemcpy3DAsync(&p, st);
+        return r != cudaSuccess ? r : cudaEventRecord(done[b], st);
+    };
+    if (!cs.empty() && e == cudaSuccess) e = issue(0);
+    for (size_t q = 0; q < cs.size() && e == cudaSuccess; ++q) {
+        // buffer (q+1)&1 last held chunk q-1, which the host has copied out
+        if (q + 1 < cs.size() && (e = issue(q + 1)) != cudaSuccess) break;
+        if ((e = cudaEventSynchronize(done[q & 1])) != cudaSuccess) break;
+        const Chunk& c = cs[q];
+        const size_t off = ((size_t)c.k0 * ay + c.j0) * ax * es, n = (size_t)c.nk * c.nj * ax * es;
+        copy_bytes((char*)host + off, s.buf[q & 1], n);
+    }
+    const cudaError_t w = cudaStreamSynchronize(st);
+    for (cudaEvent_t d : done)
+        if (d) cudaEventDestroy(d);
+    return e != cudaSuccess ? e : w;
+}
+
+}  // namespace sgpu
