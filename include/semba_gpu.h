@@ -186,6 +186,54 @@ sgpu_status sgpu_set_probes(sgpu_ctx* ctx, int nprobes, const int* comp_ijk, int
  * *first_n the step index n of the first row. */
 sgpu_status sgpu_read_probes(sgpu_ctx* ctx, float* out, int max_steps, int* nsteps, int* first_n);
 
+/* Volume ("movie") probes of observation.F90.  A probe samples the three E
+ * (magnetic = 0) or H (magnetic = 1) components at the nodes (i, j, k) of
+ * box[6] = XI XE YI YE ZI ZE (absolute cell coordinates, inside Alloc) whose
+ * coordinates are multiples of stride[3] (the reference's X/Y/Ztrancos); the
+ * sampled node (i, j, k) has index (i/stride[0] - i0, j/stride[1] - j0,
+ * k/stride[2] - k0), i0 = XItrancos = XI/stride[0] rounded up
+ * (observation.F90:318-331).  Probes are sampled after every whole step,
+ * with the point probes.
+ *
+ * Frequency domain (observation.F90:3527-3600, 1918-1922): after step n the
+ * complex(8) accumulators take V(f, c, node) += w(f, n) * F_c(node) with
+ *   w(f, n) = dt * exp(-i * 2 pi_f * freq[f] * tiempo(n))       (E)
+ *   w(f, n) * exp(-i * 2 pi_f * freq[f] * dt / 2)               (H)
+ * pi_f the real(4) pi, each exponential the host's complex(8) exp, formed
+ * on the host from the time vector set before the call (steps outside it
+ * add nothing). */
+typedef struct {
+    int magnetic;
+    int box[6];
+    int stride[3];
+    int nfreq;
+    const float* freq; /* real(4) frequencies (observation.F90:505-536) */
+} sgpu_freq_probe_desc;
+sgpu_status sgpu_add_freq_probe(sgpu_ctx* ctx, const sgpu_freq_probe_desc* d, int* id);
+/* Time domain: all three components of the sampled box after every step n
+ * with n_first <= n < n_last and (n - n_first) % every == 0, kept in a
+ * device ring of `capacity` frames. */
+typedef struct {
+    int magnetic;
+    int box[6];
+    int stride[3];
+    int n_first, n_last, every;
+    int capacity;
+} sgpu_movie_probe_desc;
+sgpu_status sgpu_add_movie_probe(sgpu_ctx* ctx, const sgpu_movie_probe_desc* d, int* id);
+/* Sampled nodes per axis of volume probe id and the first sampled index
+ * (XItrancos, YItrancos, ZItrancos) in ijk0[3]. */
+sgpu_status sgpu_volume_probe_shape(const sgpu_ctx* ctx, int id, int* ni, int* nj, int* nk, int* ijk0);
+/* The accumulators of frequency probe id as nfreq x 3 x nk x nj x ni
+ * complex(8) values (re, im interleaved, i fastest): the order of the
+ * reference's output records (observation.F90:4013-4046). */
+sgpu_status sgpu_read_freq_probe(sgpu_ctx* ctx, int id, double* out);
+/* The frames of movie probe id recorded since the last read, at most
+ * max_frames, as [frame][3][nk][nj][ni] floats; *frames receives their
+ * number and *first_n the step of the first.  Frames older than the ring's
+ * capacity are gone: the read starts at the oldest one kept. */
+sgpu_status sgpu_read_movie_probe(sgpu_ctx* ctx, int id, float* out, int max_frames, int* frames, int* first_n);
+
 /* One call per reference routine, in the order of timestepping.F90:1286-1742
  * (the border calls: after the magnetic CPML and again after the H sources
  * for PMC/periodic, timestepping.F90:1568-1573 and :1636-1641; Mur before the

@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <complex>
 #include <cstdint>
 #include <cstring>
 #include <limits>
@@ -177,6 +178,14 @@ template <class R> struct Sim {
     std::vector<int> nodal_seq;  // unused
     // probes
     std::vector<int> probes;
+    // frequency-domain volume probes (observation.F90:318-331, 1918-1922)
+    struct FreqProbe {
+        int mag;
+        int i0, ni, j0, nj, k0, nk, tr[3];
+        std::vector<float> freq;
+        std::vector<std::complex<double>> V;  // [f][comp][k][j][i]
+    };
+    std::vector<FreqProbe> fprobes;
 
     R physc(int field, int axis, int idx) const { return phys[field][axis][idx - phys_lo[field][axis]]; }
     double time(int n) {
@@ -1484,6 +1493,31 @@ struct Handle {
     int nthreads;
 };
 
+// UpdateObservation for a frequency-domain volume probe after step n
+// (observation.F90:3527-3600): auxExp_E = dt*(1,0)*Exp(mcPI2*Freq*at),
+// auxExp_H = auxExp_E*Exp(mcPI2*Freq*dt*0.5), mcPI2 = -(0,1)*2*pi in real(4)
+// constants (fdetypes.F90:190), then V = V + auxExp*F for the three
+// components at every sampled node.  Complex times real multiplies both parts.
+template <class R> void update_freq_probe(Sim<R>& s, typename Sim<R>::FreqProbe& p, int n) {
+    const double at = s.time(n);
+    const std::complex<double> mcpi2(-0.0, -(double)(2.0f * 3.14159265358979323846f));
+    const int c0 = p.mag ? 3 : 0;
+    const long nodes = (long)p.ni * p.nj * p.nk;
+    for (size_t f = 0; f < p.freq.size(); ++f) {
+        const std::complex<double> z = mcpi2 * (double)p.freq[f];
+        std::complex<double> w = s.dt * std::exp(z * at);
+        if (p.mag) w = w * std::exp(z * s.dt * 0.5);
+        for (int c = 0; c < 3; ++c)
+            for (int kk = 0; kk < p.nk; ++kk)
+                for (int jj = 0; jj < p.nj; ++jj)
+                    for (int ii = 0; ii < p.ni; ++ii) {
+                        const double v = (double)s.F[c0 + c]((p.i0 + ii) * p.tr[0], (p.j0 + jj) * p.tr[1], (p.k0 + kk) * p.tr[2]);
+                        std::complex<double>& a = p.V[((f * 3 + c) * nodes) + ((long)kk * p.nj + jj) * p.ni + ii];
+                        a = a + w * v;
+                    }
+    }
+}
+
 template <class R> int run(Sim<R>& s, int n0, int n1, float* out) {
     const int np = (int)s.probes.size() / 4;
     for (int n = n0; n < n1; ++n) {
@@ -1495,8 +1529,34 @@ template <class R> int run(Sim<R>& s, int n0, int n1, float* out) {
                 out[(long)(n - n0) * np + q] = (float)s.F[pr[0]](pr[1], pr[2], pr[3]);
             }
         }
+        for (auto& p : s.fprobes) update_freq_probe(s, p, n);
     }
     return 0;
+}
+
+// XItrancos / XEtrancos of observation.F90:318-331 (truncating division and
+// MOD, as Fortran's INT and MOD).
+inline bool trancos(int lo, int hi, int tr, int* first, int* count) {
+    if (tr < 1 || hi < lo) return false;
+    int a = lo / tr;
+    const int b = hi / tr;
+    if (lo % tr != 0) a += 1;
+    *first = a;
+    *count = b - a + 1;
+    return *count > 0;
+}
+
+template <class R> int add_freq_probe(Sim<R>& s, int mag, const int* box, const int* stride, int nfreq, const float* freq) {
+    typename Sim<R>::FreqProbe p;
+    p.mag = mag;
+    if (!trancos(box[0], box[1], stride[0], &p.i0, &p.ni) || !trancos(box[2], box[3], stride[1], &p.j0, &p.nj) ||
+        !trancos(box[4], box[5], stride[2], &p.k0, &p.nk) || nfreq < 1)
+        return -1;
+    for (int a = 0; a < 3; ++a) p.tr[a] = stride[a];
+    p.freq.assign(freq, freq + nfreq);
+    p.V.assign((size_t)nfreq * 3 * p.ni * p.nj * p.nk, std::complex<double>(0.0, 0.0));
+    s.fprobes.push_back(std::move(p));
+    return (int)s.fprobes.size() - 1;
 }
 
 template <class R> const A1<R>* metric(Sim<R>& s, int which) {
@@ -1530,6 +1590,34 @@ void orc_destroy(void* hv) {
     delete h->sf;
     delete h->sd;
     delete h;
+}
+
+int orc_add_freq_probe(void* hv, int magnetic, const int* box, const int* stride, int nfreq, const float* freq) {
+    Handle* h = (Handle*)hv;
+    if (!h || !box || !stride || !freq || (magnetic != 0 && magnetic != 1)) return -1;
+    return h->fp64 ? add_freq_probe(*h->sd, magnetic, box, stride, nfreq, freq)
+                   : add_freq_probe(*h->sf, magnetic, box, stride, nfreq, freq);
+}
+
+int orc_read_freq_probe(void* hv, int id, int* shape4, double* out) {
+    Handle* h = (Handle*)hv;
+    auto rd = [&](auto& s) -> int {
+        if (id < 0 || id >= (int)s.fprobes.size()) return 1;
+        const auto& p = s.fprobes[id];
+        if (shape4) {
+            shape4[0] = (int)p.freq.size();
+            shape4[1] = p.nk;
+            shape4[2] = p.nj;
+            shape4[3] = p.ni;
+        }
+        if (out)
+            for (size_t q = 0; q < p.V.size(); ++q) {
+                out[2 * q] = p.V[q].real();
+                out[2 * q + 1] = p.V[q].imag();
+            }
+        return 0;
+    };
+    return h->fp64 ? rd(*h->sd) : rd(*h->sf);
 }
 
 int orc_run(void* hv, int n0, int n1, float* out) {

@@ -118,6 +118,14 @@ void orc_destroy(void* h);
  * probes after each step into rows [n - n0] of out (nprobes per row), if
  * out is non-null. */
 int orc_run(void* h, int n0, int n1, float* probe_out);
+/* Frequency-domain volume probe (observation.F90:318-331, 3527-3600) over
+ * box[6] (XI XE YI YE ZI ZE) sampled at multiples of stride[3], E (magnetic
+ * 0) or H (1), accumulated after every step that orc_run advances; returns
+ * its id or -1. */
+int orc_add_freq_probe(void* h, int magnetic, const int* box, const int* stride, int nfreq, const float* freq);
+/* shape4 = nfreq, nk, nj, ni; out = nfreq x 3 x nk x nj x ni complex(8)
+ * values (re, im interleaved). */
+int orc_read_freq_probe(void* h, int id, int* shape4, double* out);
 /* Grid description after set-up. */
 int orc_get_lims(void* h, orc_lim* alloc6, orc_lim* sweep6, orc_lim* sinpml6);
 double orc_get_dt(void* h);

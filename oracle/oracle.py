@@ -96,6 +96,11 @@ def load():
         lib.orc_get_mdisp.argtypes = lib.orc_get_edisp.argtypes
         lib.orc_check_div_dt.argtypes = [C.c_double, C.c_long, C.c_ulonglong]
         lib.orc_check_div_dt.restype = C.c_long
+        ip = C.POINTER(C.c_int)
+        lib.orc_add_freq_probe.argtypes = [vp, C.c_int, ip, ip, C.c_int, C.POINTER(C.c_float)]
+        lib.orc_add_freq_probe.restype = C.c_int
+        lib.orc_read_freq_probe.argtypes = [vp, C.c_int, ip, C.POINTER(C.c_double)]
+        lib.orc_read_freq_probe.restype = C.c_int
         _lib = lib
     return _lib
 
@@ -240,6 +245,27 @@ class Oracle:
 
     def time(self, n: int) -> float:
         return self.lib.orc_get_time(self._h, n)
+
+    def add_freq_probe(self, magnetic: bool, box, stride, freqs) -> int:
+        """Frequency-domain volume probe; accumulates after every later step."""
+        b = (C.c_int * 6)(*[int(v) for v in box])
+        st = (C.c_int * 3)(*[int(v) for v in stride])
+        fr = np.ascontiguousarray(np.asarray(freqs, np.float32))
+        pid = self.lib.orc_add_freq_probe(self._h, int(bool(magnetic)), b, st, len(fr),
+                                          fr.ctypes.data_as(C.POINTER(C.c_float)))
+        if pid < 0:
+            raise ValueError("frequency probe samples no node")
+        return pid
+
+    def freq_probe(self, pid: int) -> np.ndarray:
+        """Accumulators as complex128 [nfreq, 3, nk, nj, ni]."""
+        sh = (C.c_int * 4)()
+        if self.lib.orc_read_freq_probe(self._h, pid, sh, None):
+            raise ValueError("no frequency probe with that id")
+        nf, nk, nj, ni = list(sh)
+        out = np.empty(nf * 3 * nk * nj * ni * 2, np.float64)
+        self.lib.orc_read_freq_probe(self._h, pid, None, out.ctypes.data_as(C.POINTER(C.c_double)))
+        return out.view(np.complex128).reshape(nf, 3, nk, nj, ni)
 
     def mur_cab1(self, face: int):
         """CAB1 per medium of a Mur face (back, front, left, right, down, up),

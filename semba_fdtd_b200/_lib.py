@@ -63,6 +63,16 @@ class GridDesc(C.Structure):
                 ("idxh", c_float_p), ("idyh", c_float_p), ("idzh", c_float_p), ("dt", C.c_double)]
 
 
+class FreqProbeDesc(C.Structure):
+    _fields_ = [("magnetic", C.c_int), ("box", C.c_int * 6), ("stride", C.c_int * 3), ("nfreq", C.c_int),
+                ("freq", c_float_p)]
+
+
+class MovieProbeDesc(C.Structure):
+    _fields_ = [("magnetic", C.c_int), ("box", C.c_int * 6), ("stride", C.c_int * 3), ("n_first", C.c_int),
+                ("n_last", C.c_int), ("every", C.c_int), ("capacity", C.c_int)]
+
+
 ERRORS = {0: "ok", 1: "bad argument", 2: "out of memory", 3: "CUDA error", 4: "call out of order",
           5: "non-finite field", 6: "timeout", 7: "unsupported", 8: "size above the stated maximum"}
 
@@ -106,6 +116,11 @@ def _declare(lib: C.CDLL) -> None:
         "sgpu_set_time": ([vp, C.c_int, C.c_int, c_double_p], C.c_int),
         "sgpu_set_probes": ([vp, C.c_int, c_int_p, C.c_int], C.c_int),
         "sgpu_read_probes": ([vp, c_float_p, C.c_int, c_int_p, c_int_p], C.c_int),
+        "sgpu_add_freq_probe": ([vp, C.POINTER(FreqProbeDesc), c_int_p], C.c_int),
+        "sgpu_add_movie_probe": ([vp, C.POINTER(MovieProbeDesc), c_int_p], C.c_int),
+        "sgpu_volume_probe_shape": ([vp, C.c_int, c_int_p, c_int_p, c_int_p, c_int_p], C.c_int),
+        "sgpu_read_freq_probe": ([vp, C.c_int, C.POINTER(C.c_double)], C.c_int),
+        "sgpu_read_movie_probe": ([vp, C.c_int, c_float_p, C.c_int, c_int_p, c_int_p], C.c_int),
         "sgpu_advance_e": ([vp, C.c_int], C.c_int),
         "sgpu_advance_h": ([vp, C.c_int], C.c_int),
         "sgpu_advance_steps": ([vp, C.c_int, C.c_int], C.c_int),

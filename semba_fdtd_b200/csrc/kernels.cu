@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <complex>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -223,6 +224,41 @@ __global__ void k_sources(KGrid g, KSrc s, StepRef sr, const double* tiempo, int
 __global__ void k_probes(KGrid g, KProbes p, StepRef sr, int first_n) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q < p.n) probe_one(g, p, step_of(sr), first_n, q);
+}
+
+// Volume probes, one thread per sampled node (all three components).
+// FREQ: the frequency-domain accumulation of observation.F90:3527-3600,
+// V = V + w * F in complex(8) per frequency, component and node; else the
+// node's three values go into the frame of step n.
+template <bool FREQ>
+__global__ void k_vol_probe(KGrid g, VolProbe p, StepRef sr, int ox, int oy, int oz) {
+    const long long nodes = (long long)p.ni * p.nj * p.nk;
+    const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (q >= nodes) return;
+    const int n = step_of(sr);
+    const int ii = (int)(q % p.ni), jj = (int)((q / p.ni) % p.nj), kk = (int)(q / ((long long)p.ni * p.nj));
+    const long long c = (long long)((p.i0 + ii) * p.tr[0] - ox) + (long long)g.pitch * ((p.j0 + jj) * p.tr[1] - oy) +
+                        g.plane * (long long)((p.k0 + kk) * p.tr[2] - oz);
+    const int f0 = p.magnetic ? 3 : 0;
+    const float v[3] = {g.F[f0][c], g.F[f0 + 1][c], g.F[f0 + 2][c]};
+    if (FREQ) {
+        const int m = n - p.w_n0;
+        if (m < 0 || m >= p.w_steps) return;
+        for (int f = 0; f < p.nf; ++f) {
+            const double2 w = p.w[(long long)m * p.nf + f];
+            for (int comp = 0; comp < 3; ++comp) {
+                double2* a = p.acc + (((long long)f * 3 + comp) * nodes + q);
+                double2 x = *a;
+                x.x = x.x + w.x * (double)v[comp];
+                x.y = x.y + w.y * (double)v[comp];
+                *a = x;
+            }
+        }
+    } else {
+        if (n < p.n_first || n >= p.n_last || (n - p.n_first) % p.every) return;
+        const long long slot = (long long)((n - p.n_first) / p.every) % p.cap;
+        for (int comp = 0; comp < 3; ++comp) p.ring[(slot * 3 + comp) * nodes + q] = v[comp];
+    }
 }
 
 // MinusCloneMagneticPMC / CloneMagneticPeriodic (bordersother.F90:65-190)
@@ -471,6 +507,14 @@ sgpu_status launch_sources(sgpu_ctx* c, int side, StepRef sr, int mask = kMaskAl
 }
 
 sgpu_status launch_probes(sgpu_ctx* c, StepRef sr) {
+    for (const VolProbe& p : c->vprobes) {
+        const long long nodes = (long long)p.ni * p.nj * p.nk;
+        const unsigned blocks = (unsigned)((nodes + 255) / 256);
+        if (p.kind == 0) k_vol_probe<true><<<blocks, 256, 0, c->stream>>>(kgrid(c), p, sr, c->ox, c->oy, c->oz);
+        else k_vol_probe<false><<<blocks, 256, 0, c->stream>>>(kgrid(c), p, sr, c->ox, c->oy, c->oz);
+        sgpu_status s = check_launch(c, "k_vol_probe");
+        if (s) return s;
+    }
     if (c->probes.n == 0) return SGPU_OK;
     int threads = 128;
     int blocks = (c->probes.n + threads - 1) / threads;
@@ -715,6 +759,7 @@ void sgpu_destroy(sgpu_ctx* c) {
     free_list(c, c->src_allocs[0]);
     free_list(c, c->src_allocs[1]);
     free_list(c, c->probe_allocs);
+    free_list(c, c->vprobe_allocs);
     if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);
     if (c->host && c->host_free) c->host_free(c->host);
     delete c;
@@ -1321,6 +1366,162 @@ sgpu_status sgpu_read_probes(sgpu_ctx* c, float* out, int max_steps, int* nsteps
 }
 
 namespace {
+// The sampled index range of one axis: multiples of `tr` in [lo, hi], as
+// XItrancos / XEtrancos of observation.F90:318-331 (Fortran integer division
+// and MOD, both truncating toward zero like C++).
+bool stride_range(int lo, int hi, int tr, int* first, int* count) {
+    if (tr < 1 || hi < lo) return false;
+    int a = lo / tr, b = hi / tr;
+    if (lo % tr != 0) a += 1;
+    *first = a;
+    *count = b - a + 1;
+    return *count > 0;
+}
+
+sgpu_status add_volume_probe(sgpu_ctx* c, int kind, int magnetic, const int* box, const int* stride, VolProbe* p) {
+    if (magnetic != 0 && magnetic != 1) return set_error(c, SGPU_ERR_ARG, "volume probe: magnetic must be 0 or 1");
+    *p = VolProbe{};
+    p->kind = kind;
+    p->magnetic = magnetic;
+    for (int f = 3 * magnetic; f < 3 * magnetic + 3; ++f) {
+        const sgpu_lim& a = c->alloc[f];
+        if (box[0] < a.xi || box[1] > a.xe || box[2] < a.yi || box[3] > a.ye || box[4] < a.zi || box[5] > a.ze)
+            return set_error(c, SGPU_ERR_ARG, "volume probe box outside Alloc");
+    }
+    if (!stride_range(box[0], box[1], stride[0], &p->i0, &p->ni) || !stride_range(box[2], box[3], stride[1], &p->j0, &p->nj) ||
+        !stride_range(box[4], box[5], stride[2], &p->k0, &p->nk))
+        return set_error(c, SGPU_ERR_ARG, "volume probe samples no node");
+    for (int a = 0; a < 3; ++a) p->tr[a] = stride[a];
+    return SGPU_OK;
+}
+
+sgpu_status commit_volume_probe(sgpu_ctx* c, const VolProbe& p, int* id) {
+    c->vprobes.push_back(p);
+    c->vprobe_read.push_back(0);
+    if (id) *id = (int)c->vprobes.size() - 1;
+    if (c->graph) {  // the captured steps do not launch the new probe
+        cudaGraphExecDestroy(c->graph);
+        c->graph = nullptr;
+    }
+    return SGPU_OK;
+}
+}  // namespace
+
+sgpu_status sgpu_add_freq_probe(sgpu_ctx* c, const sgpu_freq_probe_desc* d, int* id) {
+    if (!c || !d || d->nfreq < 1 || !d->freq) return set_error(c, SGPU_ERR_ARG, "bad frequency probe");
+    if (c->h_tiempo.empty()) return set_error(c, SGPU_ERR_STATE, "set the time vector before a frequency probe");
+    VolProbe p;
+    sgpu_status s = add_volume_probe(c, 0, d->magnetic, d->box, d->stride, &p);
+    if (s) return s;
+    p.nf = d->nfreq;
+    // observation.F90:3530-3534 with mcPI2 = -(0, 1) * 2 * pi (fdetypes.F90:190),
+    // all factors real(4) so that its imaginary part is -(2 * pi_f)
+    const double mcpi2_im = -(double)(2.0f * (float)3.14159265358979323846);
+    const int steps = (int)c->h_tiempo.size();
+    std::vector<double2> w((size_t)steps * p.nf);
+    for (int f = 0; f < p.nf; ++f) {
+        const double im1 = mcpi2_im * (double)d->freq[f];  // mcPI2 * Freq
+        const double re1 = -0.0 * (double)d->freq[f];
+        std::complex<double> eh = 0.0;
+        if (d->magnetic) eh = std::exp(std::complex<double>(re1 * c->dt * 0.5, im1 * c->dt * 0.5));
+        for (int m = 0; m < steps; ++m) {
+            const double at = c->h_tiempo[m];
+            const std::complex<double> e = std::exp(std::complex<double>(re1 * at, im1 * at));
+            // dt * (1, 0) is a complex with a known zero imaginary part, so
+            // its product with e is (dt * Re e, dt * Im e)
+            double wr = c->dt * e.real();
+            double wi = c->dt * e.imag();
+            if (d->magnetic) {
+                const double hr = wr * eh.real() - wi * eh.imag();
+                const double hi = wr * eh.imag() + wi * eh.real();
+                wr = hr;
+                wi = hi;
+            }
+            w[(size_t)m * p.nf + f] = make_double2(wr, wi);
+        }
+    }
+    const long long nodes = (long long)p.ni * p.nj * p.nk;
+    double2* acc;
+    double2* dw;
+    if ((s = dalloc(c, &acc, (size_t)nodes * 3 * p.nf, &c->vprobe_allocs)) ||
+        (s = dalloc(c, &dw, w.size(), &c->vprobe_allocs)))
+        return s;
+    CUDA_TRY(c, cudaMemsetAsync(acc, 0, sizeof(double2) * (size_t)nodes * 3 * p.nf, c->stream));
+    if ((s = h2d(c, dw, w.data(), w.size()))) return s;
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    p.acc = acc;
+    p.w = dw;
+    p.w_n0 = c->t_n0;
+    p.w_steps = steps;
+    return commit_volume_probe(c, p, id);
+}
+
+sgpu_status sgpu_add_movie_probe(sgpu_ctx* c, const sgpu_movie_probe_desc* d, int* id) {
+    if (!c || !d || d->every < 1 || d->capacity < 1 || d->n_last < d->n_first)
+        return set_error(c, SGPU_ERR_ARG, "bad movie probe");
+    VolProbe p;
+    sgpu_status s = add_volume_probe(c, 1, d->magnetic, d->box, d->stride, &p);
+    if (s) return s;
+    p.n_first = d->n_first;
+    p.n_last = d->n_last;
+    p.every = d->every;
+    p.cap = d->capacity;
+    const long long nodes = (long long)p.ni * p.nj * p.nk;
+    float* ring;
+    if ((s = dalloc(c, &ring, (size_t)nodes * 3 * p.cap, &c->vprobe_allocs))) return s;
+    p.ring = ring;
+    return commit_volume_probe(c, p, id);
+}
+
+sgpu_status sgpu_volume_probe_shape(const sgpu_ctx* c, int id, int* ni, int* nj, int* nk, int* ijk0) {
+    if (!c || id < 0 || id >= (int)c->vprobes.size()) return SGPU_ERR_ARG;
+    const VolProbe& p = c->vprobes[id];
+    if (ni) *ni = p.ni;
+    if (nj) *nj = p.nj;
+    if (nk) *nk = p.nk;
+    if (ijk0) {
+        ijk0[0] = p.i0;
+        ijk0[1] = p.j0;
+        ijk0[2] = p.k0;
+    }
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_read_freq_probe(sgpu_ctx* c, int id, double* out) {
+    if (!c || !out || id < 0 || id >= (int)c->vprobes.size() || c->vprobes[id].kind != 0)
+        return set_error(c, SGPU_ERR_ARG, "no frequency probe with that id");
+    const VolProbe& p = c->vprobes[id];
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    CUDA_TRY(c, cudaMemcpy(out, p.acc, sizeof(double2) * (size_t)p.ni * p.nj * p.nk * 3 * p.nf, cudaMemcpyDeviceToHost));
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_read_movie_probe(sgpu_ctx* c, int id, float* out, int max_frames, int* frames, int* first_n) {
+    if (!c || !frames || id < 0 || id >= (int)c->vprobes.size() || c->vprobes[id].kind != 1)
+        return set_error(c, SGPU_ERR_ARG, "no movie probe with that id");
+    const VolProbe& p = c->vprobes[id];
+    *frames = 0;
+    // frames of the steps launched so far
+    const int end = std::min(p.n_last, c->steps_hi);
+    const long long total = end > p.n_first ? (end - p.n_first + p.every - 1) / p.every : 0;
+    long long& read = c->vprobe_read[id];
+    if (total - read > p.cap) read = total - p.cap;  // older frames were overwritten
+    if (first_n) *first_n = p.n_first + (int)(read * p.every);
+    const long long take = std::min<long long>(total - read, max_frames);
+    if (take <= 0) return SGPU_OK;
+    if (!out) return set_error(c, SGPU_ERR_ARG, "null output");
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    const size_t frame = (size_t)p.ni * p.nj * p.nk * 3;
+    for (long long r = 0; r < take; ++r) {
+        const long long slot = (read + r) % p.cap;
+        CUDA_TRY(c, cudaMemcpy(out + r * frame, p.ring + slot * frame, frame * sizeof(float), cudaMemcpyDeviceToHost));
+    }
+    read += take;
+    *frames = (int)take;
+    return SGPU_OK;
+}
+
+namespace {
 sgpu_status note_probe_rows(sgpu_ctx* c, int n0, int count) {
     if (c->probes.n == 0) return SGPU_OK;
     if (c->probe_first_n < 0) c->probe_first_n = n0;
@@ -1379,6 +1580,7 @@ sgpu_status sgpu_update_observation(sgpu_ctx* c, int n) {
     if (s) return s;
     s = launch_probes(c, StepRef{nullptr, n});
     if (!s && c->probes.n) c->probe_written += 1;
+    if (!s) c->steps_hi = std::max(c->steps_hi, n + 1);
     return s;
 }
 
@@ -1426,6 +1628,7 @@ sgpu_status sgpu_advance_steps(sgpu_ctx* c, int n0, int count) {
     for (; done < count; ++done)
         if ((s = whole_step(c, StepRef{nullptr, n0 + done}))) return s;
     if (c->probes.n) c->probe_written += count;
+    c->steps_hi = std::max(c->steps_hi, n0 + count);
     return SGPU_OK;
 }
 
@@ -1480,6 +1683,7 @@ sgpu_status sgpu_profile_steps(sgpu_ctx* c, int n0, int count, float* ms6) {
     }
     for (auto& e : ev) cudaEventDestroy(e);
     if (!s && c->probes.n) c->probe_written += count;
+    if (!s) c->steps_hi = std::max(c->steps_hi, n0 + count);
     return s;
 }
 
@@ -1533,6 +1737,7 @@ sgpu_status sgpu_kernels_per_step(const sgpu_ctx* c, int* n) {
     k += c->src[0].nrows > 0;
     k += c->src[1].nrows > 0;
     k += c->probes.n > 0;
+    k += (int)c->vprobes.size();
     k += c->border.cl_cells > 0;
     k += c->border.mur_cells > 0;
     *n = k;

@@ -141,6 +141,24 @@ struct KProbes {
     int cap;
 };
 
+// A volume probe: the sampled nodes (stride multiples of the box) of the
+// E or H components; kind 0 accumulates the frequency-domain transform,
+// kind 1 keeps time-domain frames in a ring.
+struct VolProbe {
+    int kind;
+    int magnetic;
+    int i0, j0, k0, ni, nj, nk;  // first sampled index and counts (stride units)
+    int tr[3];
+    // frequency domain: acc [nf][3][nk][nj][ni], weights [step - w_n0][nf]
+    int nf;
+    double2* acc;
+    const double2* w;
+    int w_n0, w_steps;
+    // time domain: ring [cap][3][nk][nj][ni]
+    int n_first, n_last, every, cap;
+    float* ring;
+};
+
 // Tensor maps of one fused TMA kernel (see tma_fields.cuh for the order).
 struct alignas(64) TMaps {
     CUtensorMap m[21];  // 9 field / media maps, then the 12 psi slabs of the side
@@ -223,6 +241,11 @@ struct sgpu_ctx {
     long long probe_written = 0;  // rows written in total
     long long probe_read = 0;
     int probe_first_n = -1;
+    // volume probes; steps_hi: one past the last step whose probes were launched
+    std::vector<sgpu::VolProbe> vprobes;
+    std::vector<long long> vprobe_read;  // movie frames read so far, per probe
+    std::vector<void*> vprobe_allocs;
+    int steps_hi = -1;
     // graph
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;

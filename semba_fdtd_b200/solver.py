@@ -155,6 +155,62 @@ class Solver:
     def synchronize(self) -> None:
         self._check(self.lib.sgpu_synchronize(self._h), "sgpu_synchronize")
 
+    # -- volume probes -----------------------------------------------------
+    def add_freq_probe(self, magnetic: bool, box, stride=(1, 1, 1), freqs=(1e9,)) -> int:
+        """Frequency-domain volume probe over box (XI XE YI YE ZI ZE) at the
+        nodes whose coordinates are multiples of stride; accumulated after
+        every later step.  Returns its id."""
+        fr = np.ascontiguousarray(np.asarray(freqs, np.float32))
+        d = _lib.FreqProbeDesc(int(bool(magnetic)), (C.c_int * 6)(*map(int, box)), (C.c_int * 3)(*map(int, stride)),
+                               len(fr), fr.ctypes.data_as(_lib.c_float_p))
+        pid = C.c_int(-1)
+        self._check(self.lib.sgpu_add_freq_probe(self._h, C.byref(d), C.byref(pid)), "sgpu_add_freq_probe")
+        return pid.value
+
+    def add_movie_probe(self, magnetic: bool, box, stride=(1, 1, 1), n_first: int = 0, n_last: int = 1 << 30,
+                        every: int = 1, capacity: int = 16) -> int:
+        """Time-domain volume probe: frames of the sampled box after steps
+        n_first <= n < n_last, every `every` steps, in a ring of `capacity`."""
+        d = _lib.MovieProbeDesc(int(bool(magnetic)), (C.c_int * 6)(*map(int, box)), (C.c_int * 3)(*map(int, stride)),
+                                int(n_first), int(n_last), int(every), int(capacity))
+        pid = C.c_int(-1)
+        self._check(self.lib.sgpu_add_movie_probe(self._h, C.byref(d), C.byref(pid)), "sgpu_add_movie_probe")
+        return pid.value
+
+    def volume_probe_shape(self, pid: int):
+        """((ni, nj, nk), (i0, j0, k0)) of a volume probe."""
+        ni, nj, nk, ijk = C.c_int(), C.c_int(), C.c_int(), (C.c_int * 3)()
+        self._check(self.lib.sgpu_volume_probe_shape(self._h, pid, C.byref(ni), C.byref(nj), C.byref(nk), ijk))
+        return (ni.value, nj.value, nk.value), tuple(ijk)
+
+    def freq_probe(self, pid: int, nfreq: int) -> np.ndarray:
+        """Accumulators of a frequency probe, complex128 [nfreq, 3, nk, nj, ni]."""
+        (ni, nj, nk), _ = self.volume_probe_shape(pid)
+        out = np.empty(nfreq * 3 * nk * nj * ni * 2, np.float64)
+        self._check(self.lib.sgpu_read_freq_probe(self._h, pid, out.ctypes.data_as(C.POINTER(C.c_double))),
+                    "sgpu_read_freq_probe")
+        return out.view(np.complex128).reshape(nfreq, 3, nk, nj, ni)
+
+    def movie_frames(self, pid: int, max_frames: int = 1 << 20):
+        """(first step, frames [F, 3, nk, nj, ni] float32) recorded since the last read."""
+        (ni, nj, nk), _ = self.volume_probe_shape(pid)
+        cap = max(1, min(max_frames, 4096))
+        frames, first = [], None
+        while True:
+            buf = np.empty((cap, 3, nk, nj, ni), np.float32)
+            got, n0 = C.c_int(), C.c_int()
+            self._check(self.lib.sgpu_read_movie_probe(self._h, pid, buf.ctypes.data_as(_lib.c_float_p), cap,
+                                                       C.byref(got), C.byref(n0)), "sgpu_read_movie_probe")
+            if first is None:
+                first = n0.value
+            if got.value == 0:
+                break
+            frames.append(buf[: got.value])
+            if got.value < cap or sum(len(f) for f in frames) >= max_frames:
+                break
+        arr = np.concatenate(frames) if frames else np.zeros((0, 3, nk, nj, ni), np.float32)
+        return first, arr
+
     def set_kernel_family(self, family: int) -> None:
         """1: TMA-pipelined fused field kernels (default); 0: register-marching."""
         self._check(self.lib.sgpu_set_kernel_family(self._h, int(family)), "sgpu_set_kernel_family")
