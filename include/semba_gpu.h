@@ -412,6 +412,26 @@ sgpu_status sgpu_host_get_media(const sgpu_ctx* ctx, int comp, int16_t* out);
 /* CAB1 of calc_murconstants for face f (back, front, left, right, down, up),
  * num_media+1 values; SGPU_ERR_ARG when the face has no Mur condition. */
 sgpu_status sgpu_host_get_mur_cab1(const sgpu_ctx* ctx, int face, float* out);
+/* eps0 and mu0 of the set-up (real(4)), as flush_and_save_resume takes them. */
+sgpu_status sgpu_host_get_constants(const sgpu_ctx* ctx, float* eps0, float* mu0);
+
+/* Restart files (resuming.F90:213-496).  sgpu_store_resume writes the
+ * records flush_and_save_resume writes, in its order: StoreFields (one
+ * record n, tiempo(n), dt, eps0, mu0; then Ex..Hz, each row of the Alloc box
+ * in records of at most 1024 values and a remainder record, empty when the
+ * row length is a multiple of 1024), StoreFieldsCPMLBorders (the psi arrays
+ * region by region, one record per row of each PMLc box), StoreFieldsMURBorders
+ * (Past_ then PastPast_ per MURc box; the first-order update leaves PastPast_
+ * at zero), StoreFieldsEDispersives and StoreFieldsMDispersives (per medium
+ * and component, each node's previous field then its current per pole,
+ * complex(8)).  Records are Fortran sequential unformatted: each framed by
+ * its byte length as a 4-byte integer.  last_step is the last executed step
+ * n, whose tiempo(n) must be in the time vector.  sgpu_load_resume reads such
+ * a file back into a context set up for the same problem (the Init*
+ * routines' resume branches, same order) and returns n in *last_step; the
+ * run goes on at n + 1. */
+sgpu_status sgpu_store_resume(sgpu_ctx* ctx, const char* path, int last_step, float eps0, float mu0);
+sgpu_status sgpu_load_resume(sgpu_ctx* ctx, const char* path, int* last_step);
 
 /* ------------------------------------------------------------------------
  * Batched form (no counterpart in the reference, which runs one problem per

@@ -13,6 +13,7 @@
 #include <cmath>
 #include <complex>
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
 #include <limits>
 #include <new>
@@ -1518,6 +1519,115 @@ template <class R> void update_freq_probe(Sim<R>& s, typename Sim<R>::FreqProbe&
     }
 }
 
+// Restart records (resuming.F90:213-496 and the Init* resume branches):
+// Fortran sequential unformatted, each record framed by its byte length.
+struct RecIO {
+    FILE* f = nullptr;
+    bool write = false, ok = true;
+    void rec(void* p, size_t n) {
+        if (!ok) return;
+        int32_t m = (int32_t)n, b = -1;
+        if (write) {
+            ok = fwrite(&m, 4, 1, f) == 1 && (!n || fwrite(p, 1, n, f) == n) && fwrite(&m, 4, 1, f) == 1;
+        } else {
+            ok = fread(&b, 4, 1, f) == 1 && b == m && (!n || fread(p, 1, n, f) == n) && fread(&b, 4, 1, f) == 1 && b == m;
+        }
+    }
+};
+
+template <class R> void resume_body(Sim<R>& s, RecIO& r) {
+    // StoreFields / ReadFields: rows of BLOCK_SIZE = 1024 values and a remainder
+    for (int f = 0; f < 6; ++f) {
+        A3<R>& a = s.F[f];
+        for (int k = a.b.ZI; k <= a.b.ZE; ++k)
+            for (int j = a.b.YI; j <= a.b.YE; ++j) {
+                R* row = &a(a.b.XI, j, k);
+                long i = 0;
+                for (; i + 1024 <= a.sx; i += 1024) r.rec(row + i, 1024 * sizeof(R));
+                r.rec(row + i, (a.sx - i) * sizeof(R));
+            }
+    }
+    auto rows = [&](A3<R>& a, bool zeros) {
+        std::vector<R> z(std::max(0L, a.sx), (R)0);
+        for (int k = a.b.ZI; k <= a.b.ZE; ++k)
+            for (int j = a.b.YI; j <= a.b.YE; ++j) {
+                if (zeros) {
+                    r.rec(z.data(), a.sx * sizeof(R));
+                    if (!r.write) std::fill(z.begin(), z.end(), (R)0);
+                } else {
+                    r.rec(&a(a.b.XI, j, k), a.sx * sizeof(R));
+                }
+            }
+    };
+    // StoreFieldsCPMLBorders (borderscpml.F90:481-558)
+    bool anyPML = false;
+    for (int a = 0; a < 3; ++a)
+        for (int sd = 0; sd < 2; ++sd) anyPML = anyPML || s.isPML[a][sd];
+    if (anyPML) {
+        for (int q = 0; q < 2; ++q)
+            for (int w = 0; w < 4; ++w) rows(s.psiLR[q][w], false);
+        for (int q = 0; q < 2; ++q)
+            for (int w = 0; w < 4; ++w) rows(s.psiDU[q][w], false);
+        for (int q = 0; q < 2; ++q)
+            for (int w = 0; w < 4; ++w) rows(s.psiBF[q][w], false);
+    }
+    // StoreFieldsMURBorders (bordersmur.F90:369-454): Past_, then PastPast_
+    // (never updated by the first-order branch: zeros of the same boxes)
+    if (s.anyMur)
+        for (int pass = 0; pass < 2; ++pass) {
+            for (int q = 0; q < 2; ++q)
+                for (int w = 0; w < 2; ++w) rows(s.pastLR[q][w], pass == 1);
+            for (int q = 0; q < 2; ++q)
+                for (int w = 0; w < 2; ++w) rows(s.pastDU[q][w], pass == 1);
+            for (int q = 0; q < 2; ++q)
+                for (int w = 0; w < 2; ++w) rows(s.pastBF[q][w], pass == 1);
+        }
+    // StoreFieldsEDispersives / StoreFieldsMDispersives
+    for (auto* list : {&s.dut, &s.mdut})
+        for (auto& m : *list)
+            for (int c = 0; c < 3; ++c)
+                for (size_t q = 0; q < m.nodes[c].size(); ++q) {
+                    r.rec(&m.nodes[c][q].prev, sizeof(R));
+                    for (int p = 0; p < m.np; ++p) {
+                        C8& j = m.J[c][q * m.np + p];
+                        double v[2] = {j.re, j.im};
+                        r.rec(v, sizeof(v));
+                        j = C8{v[0], v[1]};
+                    }
+                }
+}
+
+template <class R> int resume_io(Sim<R>& s, const char* path, bool write, int* n) {
+    RecIO r;
+    r.write = write;
+    r.f = fopen(path, write ? "wb" : "rb");
+    if (!r.f) return 2;
+    // header: n, tiempo(n), dt, eps0, mu0 in one record
+    unsigned char hd[4 + 8 + 8 + 2 * sizeof(R)];
+    if (write) {
+        const int32_t nn = *n;
+        const double t = s.time(*n), dt = s.dt;
+        std::memcpy(hd, &nn, 4);
+        std::memcpy(hd + 4, &t, 8);
+        std::memcpy(hd + 12, &dt, 8);
+        std::memcpy(hd + 20, &s.eps0, sizeof(R));
+        std::memcpy(hd + 20 + sizeof(R), &s.mu0, sizeof(R));
+    }
+    r.rec(hd, sizeof(hd));
+    if (!write && r.ok) {
+        int32_t nn;
+        double dt;
+        std::memcpy(&nn, hd, 4);
+        std::memcpy(&dt, hd + 12, 8);
+        *n = nn;
+        if (dt != s.dt) r.ok = false;
+    }
+    if (r.ok) resume_body(s, r);
+    if (!write && r.ok && fgetc(r.f) != EOF) r.ok = false;
+    fclose(r.f);
+    return r.ok ? 0 : 1;
+}
+
 template <class R> int run(Sim<R>& s, int n0, int n1, float* out) {
     const int np = (int)s.probes.size() / 4;
     for (int n = n0; n < n1; ++n) {
@@ -1618,6 +1728,20 @@ int orc_read_freq_probe(void* hv, int id, int* shape4, double* out) {
         return 0;
     };
     return h->fp64 ? rd(*h->sd) : rd(*h->sf);
+}
+
+int orc_store_resume(void* hv, const char* path, int last_step) {
+    Handle* h = (Handle*)hv;
+    int n = last_step;
+    return h->fp64 ? resume_io(*h->sd, path, true, &n) : resume_io(*h->sf, path, true, &n);
+}
+
+int orc_load_resume(void* hv, const char* path, int* last_step) {
+    Handle* h = (Handle*)hv;
+    int n = 0;
+    int rc = h->fp64 ? resume_io(*h->sd, path, false, &n) : resume_io(*h->sf, path, false, &n);
+    if (!rc && last_step) *last_step = n;
+    return rc;
 }
 
 int orc_run(void* hv, int n0, int n1, float* out) {

@@ -126,6 +126,11 @@ int orc_add_freq_probe(void* h, int magnetic, const int* box, const int* stride,
 /* shape4 = nfreq, nk, nj, ni; out = nfreq x 3 x nk x nj x ni complex(8)
  * values (re, im interleaved). */
 int orc_read_freq_probe(void* h, int id, int* shape4, double* out);
+/* Restart files in the records of resuming.F90's flush_and_save_resume
+ * (fields, CPML psi, Mur Past_/PastPast_, electric and magnetic ADE state);
+ * last_step is the last executed step n.  Load returns 0 and n on success. */
+int orc_store_resume(void* h, const char* path, int last_step);
+int orc_load_resume(void* h, const char* path, int* last_step);
 /* Grid description after set-up. */
 int orc_get_lims(void* h, orc_lim* alloc6, orc_lim* sweep6, orc_lim* sinpml6);
 double orc_get_dt(void* h);

@@ -101,6 +101,10 @@ def load():
         lib.orc_add_freq_probe.restype = C.c_int
         lib.orc_read_freq_probe.argtypes = [vp, C.c_int, ip, C.POINTER(C.c_double)]
         lib.orc_read_freq_probe.restype = C.c_int
+        lib.orc_store_resume.argtypes = [vp, C.c_char_p, C.c_int]
+        lib.orc_store_resume.restype = C.c_int
+        lib.orc_load_resume.argtypes = [vp, C.c_char_p, ip]
+        lib.orc_load_resume.restype = C.c_int
         _lib = lib
     return _lib
 
@@ -245,6 +249,19 @@ class Oracle:
 
     def time(self, n: int) -> float:
         return self.lib.orc_get_time(self._h, n)
+
+    def store_resume(self, path) -> None:
+        """Restart file of the state after the last step run (n = self.n - 1)."""
+        if self.lib.orc_store_resume(self._h, str(path).encode(), self.n - 1):
+            raise RuntimeError("orc_store_resume failed")
+
+    def load_resume(self, path) -> int:
+        """Load a restart file; the next step is n + 1.  Returns n."""
+        n = C.c_int()
+        if self.lib.orc_load_resume(self._h, str(path).encode(), C.byref(n)):
+            raise RuntimeError("orc_load_resume failed (not a restart file of this set-up)")
+        self.n = n.value + 1
+        return n.value
 
     def add_freq_probe(self, magnetic: bool, box, stride, freqs) -> int:
         """Frequency-domain volume probe; accumulates after every later step."""

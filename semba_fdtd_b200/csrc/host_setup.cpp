@@ -1145,6 +1145,14 @@ sgpu_status sgpu_host_get_metric(const sgpu_ctx* c, int which, float* out, int* 
     return SGPU_OK;
 }
 
+sgpu_status sgpu_host_get_constants(const sgpu_ctx* c, float* eps0, float* mu0) {
+    if (!c || !c->host) return SGPU_ERR_ARG;
+    const HostState* h = (const HostState*)c->host;
+    if (eps0) *eps0 = h->eps0;
+    if (mu0) *mu0 = h->mu0;
+    return SGPU_OK;
+}
+
 sgpu_status sgpu_host_get_mur_cab1(const sgpu_ctx* c, int face, float* out) {
     if (!c || !c->host || face < 0 || face > 5 || !out) return SGPU_ERR_ARG;
     const HostState* h = (const HostState*)c->host;

@@ -993,6 +993,7 @@ sgpu_status init_ade(sgpu_ctx* c, const sgpu_edisp_desc* d, bool mag) {
     const int c0 = mag ? 3 : 0;
     free_list(c, allocs);
     (mag ? c->mdisp : c->disp) = KDisp{};
+    c->h_disp_media[mag ? 1 : 0].clear();
     on = false;
     if (d->nmedia <= 0) return SGPU_OK;
     if (d->nmedia > 255) return set_error(c, SGPU_ERR_UNSUPPORTED, "more than 255 dispersive media");
@@ -1033,6 +1034,7 @@ sgpu_status init_ade(sgpu_ctx* c, const sgpu_edisp_desc* d, bool mag) {
         nu_max = std::max(nu_max, dm.nu);
         off += np;
     }
+    c->h_disp_media[mag ? 1 : 0] = media;
     sgpu_status s;
     DispMedium* dmedia;
     int16_t* dslot;

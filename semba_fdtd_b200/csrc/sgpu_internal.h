@@ -206,6 +206,7 @@ struct sgpu_ctx {
     // ADE: electric (disp) and magnetic (mdisp) pole-residue media
     bool disp_on = false, mdisp_on = false;
     sgpu::KDisp disp{}, mdisp{};
+    std::vector<sgpu::DispMedium> h_disp_media[2];  // host copies of the media tables [electric, magnetic]
     std::vector<void*> disp_allocs, mdisp_allocs;
     // borders (PMC / periodic clones, Mur)
     sgpu::KBorder border{};

@@ -126,7 +126,7 @@ class Solver:
                 self._drain()
 
     def _pending(self) -> int:
-        return self.n - sum(len(r) for r in self._probe_rows)
+        return self.n - getattr(self, "_probe_base", 0) - sum(len(r) for r in self._probe_rows)
 
     def _drain(self) -> None:
         if not self.nprobes:
@@ -154,6 +154,25 @@ class Solver:
 
     def synchronize(self) -> None:
         self._check(self.lib.sgpu_synchronize(self._h), "sgpu_synchronize")
+
+    # -- restart files -----------------------------------------------------
+    def store_resume(self, path) -> None:
+        """Write the restart file of flush_and_save_resume for the state after
+        the last step run (n = self.n - 1)."""
+        eps0, mu0 = C.c_float(), C.c_float()
+        self._check(self.lib.sgpu_host_get_constants(self._h, C.byref(eps0), C.byref(mu0)), "sgpu_host_get_constants")
+        self._check(self.lib.sgpu_store_resume(self._h, str(path).encode(), self.n - 1, eps0, mu0), "sgpu_store_resume")
+
+    def load_resume(self, path) -> int:
+        """Load a restart file written for the same problem (by this library
+        or in the reference's record layout); steps go on at n + 1.  Returns n."""
+        n = C.c_int()
+        if self.n != 0:
+            raise _lib.SembaGpuError("load a restart file into a solver that has not stepped")
+        self._check(self.lib.sgpu_load_resume(self._h, str(path).encode(), C.byref(n)), "sgpu_load_resume")
+        self.n = n.value + 1
+        self._probe_base = self.n  # probe rows start at the first step after the restart
+        return n.value
 
     # -- volume probes -----------------------------------------------------
     def add_freq_probe(self, magnetic: bool, box, stride=(1, 1, 1), freqs=(1e9,)) -> int:
