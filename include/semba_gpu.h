@@ -412,6 +412,30 @@ sgpu_status sgpu_host_get_media(const sgpu_ctx* ctx, int comp, int16_t* out);
 /* CAB1 of calc_murconstants for face f (back, front, left, right, down, up),
  * num_media+1 values; SGPU_ERR_ARG when the face has no Mur condition. */
 sgpu_status sgpu_host_get_mur_cab1(const sgpu_ctx* ctx, int face, float* out);
+/* Z-slab sub-domains: the reference's MPI decomposition along z
+ * (mpicomm.F90:122-358, 1507-1677; timestepping.F90:1453-1459, 1661-1669).
+ * sgpu_host_create_zslab sets up the problem as sgpu_host_create does and
+ * keeps the planes z0..z1 (absolute; the slabs of a decomposition tile the
+ * problem's swept z range, the first starting at or below it and the last
+ * ending at or above it): every component sweeps its owned planes, and its
+ * Alloc range reaches one plane past them on a cut side -- the halo.  After
+ * each E half step the slab above must copy Ex and Ey of its first owned
+ * plane into this slab's plane z1+1; after each H half step the slab below
+ * must copy Hx and Hy of its last owned plane into this slab's plane z0-1
+ * (those are the only values the curl of a cut plane reads across the cut).
+ * CPML, borders of the x and y faces, ADE and sources are local; z faces
+ * belong to the end slabs; point probes are recorded by the slab that owns
+ * their plane.  Periodic z faces across slabs are SGPU_ERR_UNSUPPORTED. */
+sgpu_status sgpu_host_create_zslab(const sgpu_problem* p, int max_steps, int z0, int z1, sgpu_ctx** out);
+/* Device address and byte size of plane z (absolute) of component comp: a
+ * contiguous run of the padded layout, identical in size for all slabs of
+ * one decomposition (for NCCL or peer copies). */
+sgpu_status sgpu_zplane(sgpu_ctx* ctx, int comp, int z, void** ptr, uint64_t* bytes);
+/* Copy plane z of component comp from src into dst (same x-y layout; same
+ * or peer device), after the work queued on src and before later work on
+ * dst; src's later work waits for the copy. */
+sgpu_status sgpu_copy_zplane(sgpu_ctx* dst, sgpu_ctx* src, int comp, int z);
+
 /* eps0 and mu0 of the set-up (real(4)), as flush_and_save_resume takes them. */
 sgpu_status sgpu_host_get_constants(const sgpu_ctx* ctx, float* eps0, float* mu0);
 

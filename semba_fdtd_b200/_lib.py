@@ -118,6 +118,9 @@ def _declare(lib: C.CDLL) -> None:
         "sgpu_read_probes": ([vp, c_float_p, C.c_int, c_int_p, c_int_p], C.c_int),
         "sgpu_add_freq_probe": ([vp, C.POINTER(FreqProbeDesc), c_int_p], C.c_int),
         "sgpu_store_resume": ([vp, C.c_char_p, C.c_int, C.c_float, C.c_float], C.c_int),
+        "sgpu_host_create_zslab": ([C.POINTER(ProblemDesc), C.c_int, C.c_int, C.c_int, C.POINTER(vp)], C.c_int),
+        "sgpu_zplane": ([vp, C.c_int, C.c_int, C.POINTER(vp), C.POINTER(C.c_uint64)], C.c_int),
+        "sgpu_copy_zplane": ([vp, vp, C.c_int, C.c_int], C.c_int),
         "sgpu_load_resume": ([vp, C.c_char_p, c_int_p], C.c_int),
         "sgpu_host_get_constants": ([vp, c_float_p, c_float_p], C.c_int),
         "sgpu_add_movie_probe": ([vp, C.POINTER(MovieProbeDesc), c_int_p], C.c_int),

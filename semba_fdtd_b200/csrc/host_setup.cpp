@@ -880,17 +880,46 @@ template <class Fn> void mur_buffers(const HostState& h, Fn&& fn) {
 }
 
 // Hand the plan to the level-1 entry points.
-sgpu_status realize(HostState* h, sgpu::Arena* arena, cudaStream_t stream, sgpu_ctx** out) {
+// The planes [z0, z1] of a z-slab sub-domain (the reference's MPI
+// decomposition along z, mpicomm.F90): every component's Alloc range
+// reaches one plane past the owned planes on a cut side (the halo the
+// neighbour fills) and keeps the problem's bounds on the outer sides; its
+// Sweep is the owned part of the problem's Sweep.
+struct ZWindow {
+    bool on = false, first = true, last = true;
+    int z0 = 0, z1 = 0;
+};
+
+sgpu_status realize(HostState* h, sgpu::Arena* arena, cudaStream_t stream, sgpu_ctx** out, ZWindow zw = ZWindow()) {
+    Box A[6], W[6];
+    for (int f = 0; f < 6; ++f) {
+        A[f] = h->alloc[f];
+        W[f] = h->sweep[f];
+        if (!zw.first) {
+            A[f].z0 = zw.z0 - 1;
+            W[f].z0 = std::max(W[f].z0, zw.z0);
+        }
+        if (!zw.last) {
+            A[f].z1 = zw.z1 + 1;
+            W[f].z1 = std::min(W[f].z1, zw.z1);
+        }
+        if (W[f].z1 < W[f].z0) {
+            delete h;
+            return SGPU_ERR_ARG;  // a slab must sweep at least one plane of every component
+        }
+    }
     sgpu_grid_desc g{};
     for (int f = 0; f < 6; ++f) {
-        g.alloc[f] = to_lim(h->alloc[f]);
-        g.sweep[f] = to_lim(h->sweep[f]);
+        g.alloc[f] = to_lim(A[f]);
+        g.sweep[f] = to_lim(W[f]);
     }
+    // z-indexed arrays start at the slab's lower Alloc plane
+    const long long dzh = A[HZ].z0 - h->alloc[HZ].z0, dze = A[EZ].z0 - h->alloc[EZ].z0;
     g.num_media = h->num_media;
     g.g1 = h->g1.data(); g.g2 = h->g2.data(); g.gm1 = h->gm1.data(); g.gm2 = h->gm2.data();
     g.is_pec = h->pec.data();
-    g.idxe = h->idxe.v.data(); g.idye = h->idye.v.data(); g.idze = h->idze.v.data();
-    g.idxh = h->idxh.v.data(); g.idyh = h->idyh.v.data(); g.idzh = h->idzh.v.data();
+    g.idxe = h->idxe.v.data(); g.idye = h->idye.v.data(); g.idze = h->idze.v.data() + dzh;
+    g.idxh = h->idxh.v.data(); g.idyh = h->idyh.v.data(); g.idzh = h->idzh.v.data() + dze;
     g.dt = h->dt;
     sgpu_ctx* c = nullptr;
     sgpu_status s = sgpu::create_in(&g, arena, stream, &c);
@@ -898,18 +927,37 @@ sgpu_status realize(HostState* h, sgpu::Arena* arena, cudaStream_t stream, sgpu_
     if (s) { delete h; return s; }
     c->host = h;
     c->host_free = free_host;
+    c->zslab = zw.on;
     for (int f = 0; f < 6; ++f) {
-        if ((s = sgpu_upload_media(c, f, h->mm[f].data()))) return s;
+        const size_t off = (size_t)(A[f].z0 - h->alloc[f].z0) * h->mm[f].nx * h->mm[f].ny;
+        if ((s = sgpu_upload_media(c, f, h->mm[f].data() + off))) return s;
         h->mm[f].release();  // released once on the device
     }
-    if ((s = sgpu_init_cpml(c, &h->cd))) return s;
+    sgpu_cpml_desc cd = h->cd;
+    if (zw.on) {
+        for (int f = 0; f < 6; ++f)
+            for (int r = 0; r < 6; ++r) {
+                sgpu_lim& b = cd.pmlc[f][r];
+                if (!zw.first) b.zi = std::max(b.zi, zw.z0);
+                if (!zw.last) b.ze = std::min(b.ze, zw.z1);
+            }
+        for (int w = 0; w < 4; ++w) {
+            const float** v[4] = {&cd.p_be[2], &cd.p_ce[2], &cd.p_bm[2], &cd.p_cm[2]};
+            if (*v[w]) *v[w] += dzh;
+        }
+    }
+    if ((s = sgpu_init_cpml(c, &cd))) return s;
     sgpu_border_desc bd{};
     bool borders = false;
     for (int f = 0; f < 6; ++f) {
         const int a = f / 2, sd = f % 2;
-        bd.pmc[f] = h->kind[a][sd] == 2;
-        bd.periodic[f] = h->kind[a][sd] == 4;
-        bd.mur[f] = h->mur[a][sd];
+        // z faces belong to the slabs at the ends of the problem
+        const bool here = a != 2 || (sd == 0 ? zw.first : zw.last);
+        if (a == 2 && h->kind[a][sd] == 4 && !(zw.first && zw.last))
+            return sgpu::set_error(c, SGPU_ERR_UNSUPPORTED, "periodic z faces across z-slab sub-domains");
+        bd.pmc[f] = here && h->kind[a][sd] == 2;
+        bd.periodic[f] = here && h->kind[a][sd] == 4;
+        bd.mur[f] = here && h->mur[a][sd];
         bd.mur_cab1[f] = h->cab1[f].empty() ? nullptr : h->cab1[f].data();
         borders = borders || bd.pmc[f] || bd.periodic[f] || bd.mur[f];
     }
@@ -929,8 +977,15 @@ sgpu_status realize(HostState* h, sgpu::Arena* arena, cudaStream_t stream, sgpu_
     t[0] = 0.0;
     for (size_t i = 1; i < t.size(); ++i) t[i] = t[i - 1] + h->dt;
     if ((s = sgpu_set_time(c, 0, (int)t.size(), t.data()))) return s;
-    if (!h->probes.empty())
-        if ((s = sgpu_set_probes(c, (int)h->probes.size() / 4, h->probes.data(), h->probe_cap))) return s;
+    // point probes: a slab records those on the planes it owns (the end slabs
+    // also those beyond the first and last swept planes)
+    std::vector<int> probes;
+    for (size_t q = 0; q + 3 < h->probes.size(); q += 4) {
+        const int z = h->probes[q + 3];
+        if ((zw.first || z >= zw.z0) && (zw.last || z <= zw.z1)) probes.insert(probes.end(), &h->probes[q], &h->probes[q] + 4);
+    }
+    if (!probes.empty())
+        if ((s = sgpu_set_probes(c, (int)probes.size() / 4, probes.data(), h->probe_cap))) return s;
     return SGPU_OK;
 }
 
@@ -966,6 +1021,26 @@ sgpu_status sgpu_host_create(const sgpu_problem* p, int max_steps, sgpu_ctx** ou
     HostState* h = make_plan(p, max_steps, &rc);
     if (!h) return rc;
     return realize(h, nullptr, nullptr, out);
+}
+
+sgpu_status sgpu_host_create_zslab(const sgpu_problem* p, int max_steps, int z0, int z1, sgpu_ctx** out) {
+    if (!out || z1 < z0) return SGPU_ERR_ARG;
+    *out = nullptr;
+    sgpu_status rc;
+    HostState* h = make_plan(p, max_steps, &rc);
+    if (!h) return rc;
+    int lo = h->sweep[0].z0, hi = h->sweep[0].z1;
+    for (int f = 1; f < 6; ++f) {
+        lo = std::min(lo, h->sweep[f].z0);
+        hi = std::max(hi, h->sweep[f].z1);
+    }
+    ZWindow zw;
+    zw.on = true;
+    zw.z0 = z0;
+    zw.z1 = z1;
+    zw.first = z0 <= lo;
+    zw.last = z1 >= hi;
+    return realize(h, nullptr, nullptr, out, zw);
 }
 
 sgpu_status sgpu_host_footprint(const sgpu_ctx* c, uint64_t* bytes) {
@@ -1116,9 +1191,10 @@ sgpu_status sgpu_host_info(const sgpu_ctx* c, double* dt, int* num_media, sgpu_l
     const HostState* h = (const HostState*)c->host;
     if (dt) *dt = h->dt;
     if (num_media) *num_media = h->num_media;
+    // the context's own ranges (a z-slab's differ from the problem's)
     for (int f = 0; f < 6; ++f) {
-        if (alloc6) alloc6[f] = to_lim(h->alloc[f]);
-        if (sweep6) sweep6[f] = to_lim(h->sweep[f]);
+        if (alloc6) alloc6[f] = c->alloc[f];
+        if (sweep6) sweep6[f] = c->sweep[f];
         if (sinpml6) sinpml6[f] = to_lim(h->sinpml[f]);
     }
     return SGPU_OK;

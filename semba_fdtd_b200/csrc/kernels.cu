@@ -1237,6 +1237,7 @@ sgpu_status sgpu_add_planewave(sgpu_ctx* c, const sgpu_planewave_desc* d) {
                             xyz[ax] = d->phys[fl][ax][q];
                         }
                         const float dd = (xyz[0] * d->px + xyz[1] * d->py + xyz[2] * d->pz) - d->d0;
+                        if (c->zslab && (k < c->sweep[P.comp].zi || k > c->sweep[P.comp].ze)) continue;
                         sgpu_ctx::HostEntry he;
                         he.node = lin(c, i, j, k);
                         he.comp = P.comp;
@@ -1266,6 +1267,7 @@ sgpu_status sgpu_add_nodal(sgpu_ctx* c, const sgpu_nodal_desc* d) {
     for (int k = b.zi; k <= b.ze; ++k)
         for (int j = b.yi; j <= b.ye; ++j)
             for (int i = b.xi; i <= b.xe; ++i) {
+                if (c->zslab && (k < c->sweep[d->comp].zi || k > c->sweep[d->comp].ze)) continue;
                 int16_t m;
                 long long node = lin(c, i, j, k);
                 CUDA_TRY(c, cudaMemcpy(&m, c->M[d->comp] + node, sizeof(int16_t), cudaMemcpyDeviceToHost));
@@ -1520,6 +1522,47 @@ sgpu_status sgpu_read_movie_probe(sgpu_ctx* c, int id, float* out, int max_frame
     }
     read += take;
     *frames = (int)take;
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_zplane(sgpu_ctx* c, int comp, int z, void** ptr, uint64_t* bytes) {
+    if (!c || comp < 0 || comp > 5 || !ptr) return set_error(c, SGPU_ERR_ARG, "bad plane request");
+    if (z < c->oz || z >= c->oz + c->nza) return set_error(c, SGPU_ERR_ARG, "plane outside the context's Alloc box");
+    *ptr = c->F[comp] + c->plane * (long long)(z - c->oz);
+    if (bytes) *bytes = (uint64_t)c->plane * sizeof(float);
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_copy_zplane(sgpu_ctx* dst, sgpu_ctx* src, int comp, int z) {
+    if (!dst || !src) return SGPU_ERR_ARG;
+    if (dst->pitch != src->pitch || dst->plane != src->plane || dst->ox != src->ox || dst->oy != src->oy)
+        return set_error(dst, SGPU_ERR_ARG, "the two contexts have different x-y layouts");
+    void *d, *s;
+    uint64_t n;
+    sgpu_status st;
+    if ((st = sgpu_zplane(dst, comp, z, &d, &n)) || (st = sgpu_zplane(src, comp, z, &s, nullptr))) return st;
+    // the copy waits for the work queued on src, and src's later work waits
+    // for the copy (the plane is overwritten by src's next half step)
+    // (each event is created on the device of the stream that records it)
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaEvent_t a = nullptr, b = nullptr;
+    cudaError_t e = cudaSetDevice(src->device);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&a, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(a, src->stream);
+    if (e == cudaSuccess) e = cudaSetDevice(dst->device);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(dst->stream, a, 0);
+    if (e == cudaSuccess)
+        e = dst->device == src->device ? cudaMemcpyAsync(d, s, n, cudaMemcpyDeviceToDevice, dst->stream)
+                                       : cudaMemcpyPeerAsync(d, dst->device, s, src->device, n, dst->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(b, dst->stream);
+    if (e == cudaSuccess) e = cudaSetDevice(src->device);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(src->stream, b, 0);
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    cudaSetDevice(cur);
+    if (e != cudaSuccess) return set_error(dst, SGPU_ERR_CUDA, std::string("plane copy: ") + cudaGetErrorString(e));
     return SGPU_OK;
 }
 

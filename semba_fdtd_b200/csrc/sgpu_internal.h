@@ -257,6 +257,9 @@ struct sgpu_ctx {
     bool tma_ready = false;
     int family = 1;  // 1: TMA-pipelined fused kernels when available, 0: register-marching kernels
     int* d_err = nullptr;
+    // a z-slab sub-domain (sgpu_host_create_zslab): sources are kept only on
+    // the planes this context sweeps
+    bool zslab = false;
     // level-2 host data kept for inspection; host_only contexts (from
     // sgpu_host_plan) own no device resources
     bool host_only = false;

@@ -25,7 +25,9 @@ from .case import Problem
 
 class Solver:
     def __init__(self, problem: Problem, variant: str = "exact", probe_capacity: int = 1024,
-                 max_steps: int | None = None, kernel_family: int | None = None):
+                 max_steps: int | None = None, kernel_family: int | None = None, zslab: tuple[int, int] | None = None):
+        """zslab=(z0, z1): only the z-slab sub-domain of planes z0..z1 (see
+        semba_fdtd_b200.zslab for the decomposition and its halo copies)."""
         self.problem = problem
         self.lib = _lib.load(variant)
         self.variant = variant
@@ -33,7 +35,12 @@ class Solver:
         desc, self._keep = problem.to_desc(probe_capacity)
         self.max_steps = int(max_steps if max_steps is not None else problem.nsteps)
         h = C.c_void_p()
-        rc = self.lib.sgpu_host_create(C.byref(desc), self.max_steps, C.byref(h))
+        if zslab is None:
+            rc = self.lib.sgpu_host_create(C.byref(desc), self.max_steps, C.byref(h))
+        else:
+            rc = self.lib.sgpu_host_create_zslab(C.byref(desc), self.max_steps, int(zslab[0]), int(zslab[1]),
+                                                 C.byref(h))
+        self.zslab = zslab
         self._h = h
         if rc:
             msg = self.lib.sgpu_last_error(h).decode() if h.value else ""
@@ -49,7 +56,7 @@ class Solver:
         self.alloc = [a.tuple() for a in a6]
         self.sweep = [s.tuple() for s in s6]
         self.sinpml = [q.tuple() for q in q6]
-        self.nprobes = len(problem.probes)
+        self.nprobes = len(problem.probes) if zslab is None else len(self.probe_ids())
         self._probe_rows: list[np.ndarray] = []
         if kernel_family is not None:
             self._check(self.lib.sgpu_set_kernel_family(h, int(kernel_family)), "sgpu_set_kernel_family")
@@ -154,6 +161,14 @@ class Solver:
 
     def synchronize(self) -> None:
         self._check(self.lib.sgpu_synchronize(self._h), "sgpu_synchronize")
+
+    def probe_ids(self) -> list[int]:
+        """Indices into problem.probes of the probes this solver records (a
+        z-slab records those on the planes it owns)."""
+        if self.zslab is None:
+            return list(range(len(self.problem.probes)))
+        z0, z1 = self.zslab
+        return [q for q, p in enumerate(self.problem.probes) if p[3] >= z0 and p[3] <= z1]
 
     # -- restart files -----------------------------------------------------
     def store_resume(self, path) -> None:
