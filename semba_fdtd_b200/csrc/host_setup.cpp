@@ -43,8 +43,14 @@ struct Vec {
 };
 
 // Planes of an nx x ny box that make about 64 Ki cells: the smallest share
-// of a plane loop one set-up thread takes.
-long long plane_grain(long long nx, long long ny) { return std::max(1LL, (1LL << 16) / std::max(1LL, nx * ny)); }
+// of a plane loop one set-up thread takes.  Grids under 16 Mi cells are set
+// up on the calling thread alone (their plans are usually made many at a
+// time, one per thread).
+constexpr long long kThreadedCells = 1LL << 24;
+long long plane_grain(long long grid_cells, long long nx, long long ny) {
+    if (grid_cells < kThreadedCells) return 1LL << 40;
+    return std::max(1LL, (1LL << 16) / std::max(1LL, nx * ny));
+}
 
 // int16 media matrix over one component's Alloc, column-major (filled with
 // medium 1 by several threads on large grids).
@@ -224,7 +230,7 @@ void paint(HostState& h, const Box& pt, int idx) {
                         const int cur = h.med[cell].prio;
                         if (electric ? pr > cur : pr >= cur) cell = (int16_t)idx;
                     }
-        }, plane_grain(up[f][0] - x0 + 1, up[f][1] - y0 + 1));
+        }, plane_grain(h.mm[0].size(), up[f][0] - x0 + 1, up[f][1] - y0 + 1));
     }
 }
 
@@ -250,7 +256,7 @@ void pml_media(HostState& h) {
         const Box& r = reach[f];
         const int lo_src[3] = {inner.x0, inner.y0, inner.z0};
         const int hi_src[3] = {inner.x1 + in_lo[f][0] - 1, inner.y1 + in_lo[f][1] - 1, inner.z1 + in_lo[f][2] - 1};
-        const long long grain = plane_grain(r.x1 - r.x0 + 1, r.y1 - r.y0 + 1);
+        const long long grain = plane_grain(h.mm[0].size(), r.x1 - r.x0 + 1, r.y1 - r.y0 + 1);
         auto planes = [&](int k0, int k1, auto&& fn) {
             if (k1 >= k0) sgpu::host_parallel(k1 - k0 + 1, [&](long long a, long long e) {
                 for (int k = k0 + (int)a; k < k0 + (int)e; ++k) fn(k);
@@ -328,7 +334,7 @@ void pml_media(HostState& h) {
             });
         std::lock_guard<std::mutex> g(mu);
         for (size_t v = 0; v < mine.size(); ++v) first[v] = std::min(first[v], mine[v]);
-    }, plane_grain(row_cells, 1));
+    }, plane_grain(h.mm[0].size(), row_cells, 1));
     std::vector<int> order;
     for (int v = 1; v <= h.num_media; ++v)
         if (first[v] != kNone) order.push_back(v);
@@ -346,7 +352,7 @@ void pml_media(HostState& h) {
                 for (int i = i0; i <= i1; ++i)
                     if (row[i] < 0) row[i] = (int16_t)copy_of[-row[i]];
             });
-    }, plane_grain(row_cells, 1));
+    }, plane_grain(h.mm[0].size(), row_cells, 1));
     h.num_media = next;
     // PEC borders (healer.F90:1442-1617): medium 0 on the boundary plane of
     // the E components tangential to the face and the H component normal to it
@@ -930,7 +936,7 @@ sgpu_status realize(HostState* h, sgpu::Arena* arena, cudaStream_t stream, sgpu_
     c->zslab = zw.on;
     for (int f = 0; f < 6; ++f) {
         const size_t off = (size_t)(A[f].z0 - h->alloc[f].z0) * h->mm[f].nx * h->mm[f].ny;
-        if ((s = sgpu_upload_media(c, f, h->mm[f].data() + off))) return s;
+        if ((s = sgpu::upload_media(c, f, h->mm[f].data() + off, false))) return s;  // built here: in range
         h->mm[f].release();  // released once on the device
     }
     sgpu_cpml_desc cd = h->cd;

@@ -790,13 +790,18 @@ sgpu_status sgpu_set_kernel_family(sgpu_ctx* c, int family) {
     return SGPU_OK;
 }
 
-sgpu_status sgpu_upload_media(sgpu_ctx* c, int comp, const int16_t* mi) {
+sgpu_status sgpu_upload_media(sgpu_ctx* c, int comp, const int16_t* mi) { return sgpu::upload_media(c, comp, mi, true); }
+
+}  // extern "C"
+
+sgpu_status sgpu::upload_media(sgpu_ctx* c, int comp, const int16_t* mi, bool check) {
     if (!c || !mi || comp < 0 || comp > 5) return set_error(c, SGPU_ERR_ARG, "bad media upload");
     const sgpu_lim& a = c->alloc[comp];
     const long long ax = a.xe - a.xi + 1, ay = a.ye - a.yi + 1, az = a.ze - a.zi + 1;
-    const long long n = ax * ay * az;
+    const long long n = check ? ax * ay * az : 0;
     std::mutex mu;
-    int lo = 0x7fff, hi = 0;
+    int lo = 0, hi = 0;
+    if (check) lo = 0x7fff;
     host_parallel(n, [&](long long q0, long long q1) {
         int l = 0x7fff, h = 0;
         for (long long q = q0; q < q1; ++q) {
@@ -816,6 +821,8 @@ sgpu_status sgpu_upload_media(sgpu_ctx* c, int comp, const int16_t* mi) {
     c->src_dirty = true;
     return SGPU_OK;
 }
+
+extern "C" {
 
 // The padding outside a component's Alloc range is zero on the device and
 // stays zero; only the Alloc box moves.
@@ -1131,18 +1138,27 @@ sgpu_status build_sources(sgpu_ctx* c) {
         if (es.empty()) continue;
         if (es.size() >= (1u << 30)) return set_error(c, SGPU_ERR_UNSUPPORTED, "too many source contributions");
         // group by (component, node) keeping the reference order inside a
-        // group: entries are stored in that order, so sorting the keys
-        // (component, node, position) is a stable grouping
-        std::vector<uint64_t> key(es.size());
-        for (size_t q = 0; q < es.size(); ++q)
-            key[q] = (((uint64_t)es[q].comp * (uint64_t)c->vol + (uint64_t)es[q].node) << 30) | (uint64_t)q;
-        std::sort(key.begin(), key.end());
+        // group: entries are stored in that order, so a stable sort of their
+        // positions by (component, node), an LSD radix sort of 12 bits a
+        // pass, is the grouping
+        std::vector<uint64_t> gkey(es.size());
+        for (size_t q = 0; q < es.size(); ++q) gkey[q] = (uint64_t)es[q].comp * (uint64_t)c->vol + (uint64_t)es[q].node;
+        std::vector<uint32_t> ord(es.size()), tmp(es.size());
+        for (size_t q = 0; q < es.size(); ++q) ord[q] = (uint32_t)q;
+        const uint64_t kmax = 6ull * (uint64_t)c->vol;
+        for (int shift = 0; (kmax >> shift) > 0; shift += 12) {
+            std::vector<uint32_t> cnt(4097, 0);
+            for (uint32_t q : ord) ++cnt[((gkey[q] >> shift) & 4095) + 1];
+            for (int b = 0; b < 4096; ++b) cnt[b + 1] += cnt[b];
+            for (uint32_t q : ord) tmp[cnt[(gkey[q] >> shift) & 4095]++] = q;
+            ord.swap(tmp);
+        }
         std::vector<int> rnode, rcomp, rptr;
         std::vector<SrcEntry> ent;
         ent.reserve(es.size());
-        for (size_t r = 0; r < key.size(); ++r) {
-            const size_t q = (size_t)(key[r] & ((1u << 30) - 1));
-            if (r == 0 || (key[r] >> 30) != (key[r - 1] >> 30)) {
+        for (size_t r = 0; r < ord.size(); ++r) {
+            const size_t q = ord[r];
+            if (r == 0 || gkey[q] != gkey[ord[r - 1]]) {
                 rnode.push_back((int)es[q].node);
                 rcomp.push_back(es[q].comp);
                 rptr.push_back((int)ent.size());

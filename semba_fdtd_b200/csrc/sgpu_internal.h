@@ -277,6 +277,9 @@ sgpu_status create_in(const sgpu_grid_desc* d, Arena* arena, cudaStream_t stream
 // arena every probe keeps its whole trace (nsteps + 1 rows).
 sgpu_status host_create_in(const sgpu_problem* p, sgpu_ctx* plan, int max_steps, Arena* arena, cudaStream_t stream,
                            sgpu_ctx** out);
+// sgpu_upload_media, with the range check of the indices optional (the
+// host set-up's own matrices are in range by construction).
+sgpu_status upload_media(sgpu_ctx* c, int comp, const int16_t* mi, bool check);
 // Source lists built on the device now (normally built lazily before the
 // first launch that needs them).
 sgpu_status rebuild_sources(sgpu_ctx* c);
