@@ -143,3 +143,24 @@ def test_movie_frames_equal_fields():
         assert first == kept[0] and len(fr) == 3
         for q, n in enumerate(kept):
             np.testing.assert_array_equal(fr[q], ref[n])
+
+
+@pytest.mark.gpu
+def test_volume_probe_arguments_are_checked():
+    from semba_fdtd_b200 import Solver
+    from semba_fdtd_b200._lib import SembaGpuError
+    pb = small(n=16, steps=40, layers=4)
+    with Solver(pb) as s:
+        a = s.alloc[0]
+        with pytest.raises(SembaGpuError):  # box outside Alloc
+            s.add_freq_probe(False, (a[0] - 5, a[1], a[2], a[3], a[4], a[5]), (1, 1, 1), FREQS)
+        with pytest.raises(SembaGpuError):  # stride samples no node
+            s.add_freq_probe(False, (5, 6, 5, 6, 5, 6), (7, 7, 7), FREQS)
+        with pytest.raises(SembaGpuError):  # no frequencies
+            s.add_freq_probe(False, (5, 6, 5, 6, 5, 6), (1, 1, 1), [])
+        with pytest.raises(SembaGpuError):  # bad sampling period
+            s.add_movie_probe(True, (5, 6, 5, 6, 5, 6), every=0)
+        pid = s.add_movie_probe(False, (5, 6, 5, 6, 5, 6), n_first=3, n_last=4, every=1, capacity=2)
+        s.step(6)
+        first, fr = s.movie_frames(pid)
+        assert first == 3 and len(fr) == 1  # one frame in [3, 4)

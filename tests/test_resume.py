@@ -112,3 +112,23 @@ def test_gpu_resume_rejects_other_setup(tmp_path):
     with Solver(CASES["small"]()) as s:
         with pytest.raises(SembaGpuError):
             s.load_resume(tmp_path / "o.bin")
+
+
+@pytest.mark.gpu
+def test_gpu_resume_rejects_truncated_file(tmp_path):
+    from semba_fdtd_b200 import Solver
+    from semba_fdtd_b200._lib import SembaGpuError
+    pb = CASES["disp"]()
+    o = oracle.Oracle(pb)
+    o.step(3)
+    o.store_resume(tmp_path / "o.bin")
+    data = (tmp_path / "o.bin").read_bytes()
+    (tmp_path / "cut.bin").write_bytes(data[: len(data) // 2])
+    with Solver(pb) as s:
+        with pytest.raises(SembaGpuError):
+            s.load_resume(tmp_path / "cut.bin")
+    # a file that parses is still accepted by a fresh solver after the refusal
+    with Solver(pb) as s:
+        assert s.load_resume(tmp_path / "o.bin") == 2
+        s.step(2)
+        assert s.check_finite()
