@@ -227,7 +227,7 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
     const bool producer = t.warp == kConsumerWarps;
     unsigned gp = 0;  // running plane number of the ring
     int fenced = -1;     // the instance whose tensor maps the producer has acquired
-    unsigned fmask = 0;  // ... and which of them
+    bool facq = false;   // ... and whether this lane has acquired its own map
     int viewed = -1;  // ... whose view the consumer warp holds
     for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
         const FieldItem w = items[it];
@@ -249,22 +249,19 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
             const unsigned tmask = w.cp ? cpml_tile_mask(D.cp, c0, w.ib, w.ib + kTX - 1, w.jb, w.jb + kTY - 1) : 0u;
             const unsigned smask = w.cp ? staged_mask(D.cp, c0, w.ib, w.jb) : 0u;
             prod_prepare(&tb, t, p0, p1, edge, SIDE != 0, D.g, D.cp, tmask);
-            int got = np;
-            if (t.lane == 0) {
-                const CUtensorMap* m = maps[2 * w.slot + SIDE].m;
-                // acquire the maps this item loads through that this CTA has not
-                // acquired yet for the instance: the field / media maps and the
-                // staged psi maps
-                if (fenced != w.slot) {
-                    fenced = w.slot;
-                    fmask = 0;
-                }
-                const unsigned need = ((1u << kPsiMap0) - 1u) | (smask << kPsiMap0);
-                for (unsigned todo = need & ~fmask; todo; todo &= todo - 1u) tensormap_acquire(&m[__ffs(todo) - 1]);
-                fmask |= need;
-                got = tma_issue(t, m, gp, p0, p1, edge, SIDE != 0, err, &tb, smask);
+            const CUtensorMap* m = maps[2 * w.slot + SIDE].m;
+            // each lane acquires the one map it issues through (lane q: map q),
+            // once per instance, when this item loads through it
+            if (fenced != w.slot) {
+                fenced = w.slot;
+                facq = false;
             }
-            got = __shfl_sync(0xffffffffu, got, 0);
+            const bool need = t.lane < kPsiMap0 || (t.lane < kPsiMap0 + 12 && ((smask >> (t.lane - kPsiMap0)) & 1u));
+            if (need && !facq) {
+                tensormap_acquire(&m[t.lane]);
+                facq = true;
+            }
+            const int got = tma_issue_warp(t, m, gp, p0, p1, edge, SIDE != 0, err, &tb, smask);
             if (got < np) {
                 if (t.lane == 0) tma_drain(t, gp + (unsigned)got, err, 15);
                 return;

@@ -227,6 +227,59 @@ __device__ __forceinline__ int tma_issue(const TmaCta& t, const CUtensorMap* map
     return p1 - p0 + 1;
 }
 
+// The same planes issued by the whole producer warp: lane 0 waits for the
+// stage and arms its barrier, then lane q < 9 loads the box of map q (the
+// three field arrays of the other side, the three own fields, the three
+// media) and lane 9 + n the psi box of slab bit n when the plane holds that
+// staged slab.  A lane is the only issuer of its map, so a tensor map that
+// lane acquired through the tensormap proxy needs no other thread's fence.
+// All lanes return the number of planes issued.
+__device__ __forceinline__ int tma_issue_warp(const TmaCta& t, const CUtensorMap* maps, unsigned G0, int p0, int p1,
+                                              int edge, bool hside, int* err, const ProdTable* tb, unsigned smask) {
+    const int q = t.lane;
+    const int xh = hside ? t.ib : t.ib - 4, ya = hside ? t.jb : t.jb - 1;
+    // this lane's box: shared-memory offset and x, y origin (psi: per plane below)
+    int off = 0, bx = t.ib, by = t.jb;
+    if (q == 0) { off = kOffA; by = ya; }
+    else if (q == 1) { off = kOffB; bx = xh; }
+    else if (q == 2) { off = kOffC; bx = xh; by = ya; }
+    else if (q < 6) off = kOffF + (q - 3) * align128(kBoxF);
+    else if (q < 9) off = kOffM + (q - 6) * align128(kBoxM);
+    const int n = q - kPsiMap0;
+    const bool psi_lane = n >= 0 && n < 12 && ((smask >> n) & 1u);
+    int4 pc = make_int4(0, 0, 0, 0);
+    int poff = 0;
+    if (psi_lane) {
+        pc = tb->psi[n];
+        poff = kOffP + psi_slot(smask, n) * align128(kBoxP);
+    }
+    for (int p = p0; p <= p1; ++p) {
+        const unsigned G = G0 + (unsigned)(p - p0), s = G % kStages, u = G / kStages;
+        const unsigned bar = t.full0 + 8 * s;
+        unsigned char* st = t.ring + s * kStageBytes;
+        const bool part = p == edge;
+        const PlaneWords w = tb->w[p - p0];
+        int ok = 1;
+        if (q == 0) {
+            if (u >= 1 && !mbar_wait(t.empty0 + 8 * s, (u - 1) & 1, err, hside ? 13 : 11)) {
+                ok = 0;
+            } else {
+                if (!part) *(PlaneWords*)(st + kOffW) = w;
+                mbar_expect_tx(bar, (part ? kTxEdge : kTxFull) + (unsigned)__popc(w.live & smask) * (unsigned)kBoxP);
+            }
+        }
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (!ok) return p - p0;
+        __syncwarp();  // the stage is free and armed before any lane writes into it
+        if (q < kPsiMap0) {
+            if (q < 2 || !part) tma_load3(smem_u32(st + off), &maps[q], bx, by, p, bar);
+        } else if (psi_lane && ((w.live >> n) & 1u)) {
+            tma_load3(smem_u32(st + poff), &maps[q], pc.x, pc.y, p - pc.z, bar);
+        }
+    }
+    return p1 - p0 + 1;
+}
+
 // The slab mask whose psi tiles a CPML tile stages (0: psi from global
 // memory): the tile's slabs when they need at most kPsiSlots slots and the
 // two sides of each z pair they hold are apart in z (so they can share).
