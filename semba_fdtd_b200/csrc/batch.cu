@@ -305,7 +305,20 @@ __global__ void __launch_bounds__(kPhaseThreads)
         bool on;
         inst_step(D, G, &on);
         if (!on) continue;
-        for (long long q = w.q0 + threadIdx.x; q < w.q1; q += blockDim.x) ade_node<NU, MAG>(D.g, MAG ? D.md : D.d, w.sub, q);
+        const AdeRefs r = ade_refs<MAG>(D.g, MAG ? D.md : D.d, w.sub);
+        // two nodes a thread at a time: both nodes' loads go out before
+        // either node's stores
+        for (long long q = w.q0 + threadIdx.x; q < w.q1; q += 2 * (long long)blockDim.x) {
+            const long long q2 = q + blockDim.x;
+            const bool two = q2 < w.q1;
+            AdeNode<NU> a, b;
+            ade_load<NU>(r, q, a);
+            if (two) ade_load<NU>(r, q2, b);
+            ade_update<NU, MAG>(r, a);
+            if (two) ade_update<NU, MAG>(r, b);
+            ade_store<NU>(r, q, a);
+            if (two) ade_store<NU>(r, q2, b);
+        }
     }
 }
 

@@ -378,35 +378,65 @@ __device__ __forceinline__ double div_dt(double a, double dt, double inv_dt) {
 // magnetic one (Beta/dt)*(H-Hprev), as the two routines are written.  NU
 // (the largest number of state slots of any medium) is a template parameter
 // so the states stay in registers.
-template <int NU, bool MAG>
-__device__ __forceinline__ void ade_node(const KGrid& g, const KDisp& d, int comp, long long q) {
-    const long long n = d.n[comp];
-    const int idx = d.node[comp][q];
-    const DispMedium* __restrict__ md = d.media + d.med[comp][q];
-    float* F = g.F[MAG ? 3 + comp : comp];
-    double2* J = d.J[comp];
-    const int nu = md->nu;
+// One component's node arrays and field, gathered once per launch or work
+// item so the per-node code reads no descriptor.
+struct AdeRefs {
+    const int* node;
+    const uint8_t* med;
+    float* prev;
+    double2* J;
+    long long n;
+    const DispMedium* media;
+    float* F;
+    double dt, inv_dt;
+};
+template <bool MAG> __device__ __forceinline__ AdeRefs ade_refs(const KGrid& g, const KDisp& d, int comp) {
+    return AdeRefs{d.node[comp], d.med[comp], d.prev[comp], d.J[comp], d.n[comp], d.media, g.F[MAG ? 3 + comp : comp],
+                   d.dt, d.inv_dt};
+}
+
+// The node's update in three parts (loads, arithmetic, stores), so a thread
+// can issue the loads of several nodes before any store.
+template <int NU> struct AdeNode {
+    int idx;
+    const DispMedium* md;
+    float e, prev;
     double2 st[NU];
+};
+
+template <int NU>
+__device__ __forceinline__ void ade_load(const AdeRefs& d, long long q, AdeNode<NU>& a) {
+    a.idx = d.node[q];
+    a.md = d.media + d.med[q];
+    const int nu = a.md->nu;
 #pragma unroll
-    for (int u = 0; u < NU; ++u) st[u] = u < nu ? J[u * n + q] : make_double2(0.0, 0.0);
-    float e = F[idx];
+    for (int u = 0; u < NU; ++u) a.st[u] = u < nu ? d.J[u * d.n + q] : make_double2(0.0, 0.0);
+    a.e = d.F[a.idx];
+    a.prev = d.prev[q];
+}
+
+template <int NU, bool MAG>
+__device__ __forceinline__ void ade_update(const AdeRefs& d, AdeNode<NU>& a) {
+    const DispMedium* __restrict__ md = a.md;
+    const int nu = md->nu;
+    float e = a.e;
     for (int p = 0; p < md->np; ++p) {
         const int up = md->map[p];
         double jr = 0.0, ji = 0.0;
 #pragma unroll
         for (int u = 0; u < NU; ++u)
-            if (u == up) { jr = st[u].x; ji = st[u].y; }
+            if (u == up) { jr = a.st[u].x; ji = a.st[u].y; }
         const double2 g3 = md->g3[up];
         const double re = g3.x * jr - g3.y * ji;
         e = (float)((double)e - re);
     }
-    const double dd = (double)(e - d.prev[comp][q]);
+    const double dd = (double)(e - a.prev);
 #pragma unroll
     for (int u = 0; u < NU; ++u) {
         if (u < nu) {
             const double2 kp = md->kappa[u], bt = md->beta[u];
-            const double kr = kp.x * st[u].x - kp.y * st[u].y;
-            const double ki = kp.x * st[u].y + kp.y * st[u].x;
+            const double kr = kp.x * a.st[u].x - kp.y * a.st[u].y;
+            const double ki = kp.x * a.st[u].y + kp.y * a.st[u].x;
             double br, bi;
             if (MAG) {
                 // (Beta/dt)*(H - Hprev): Beta/dt is the same quotient for every
@@ -418,11 +448,28 @@ __device__ __forceinline__ void ade_node(const KGrid& g, const KDisp& d, int com
                 br = div_dt(bt.x * dd, d.dt, d.inv_dt);
                 bi = div_dt(bt.y * dd, d.dt, d.inv_dt);
             }
-            J[u * n + q] = make_double2(kr + br, ki + bi);
+            a.st[u] = make_double2(kr + br, ki + bi);
         }
     }
-    d.prev[comp][q] = e;
-    F[idx] = e;
+    a.e = e;
+}
+
+template <int NU>
+__device__ __forceinline__ void ade_store(const AdeRefs& d, long long q, const AdeNode<NU>& a) {
+    const int nu = a.md->nu;
+#pragma unroll
+    for (int u = 0; u < NU; ++u)
+        if (u < nu) d.J[u * d.n + q] = a.st[u];
+    d.prev[q] = a.e;
+    d.F[a.idx] = a.e;
+}
+
+template <int NU, bool MAG>
+__device__ __forceinline__ void ade_node(const AdeRefs& d, long long q) {
+    AdeNode<NU> a;
+    ade_load<NU>(d, q, a);
+    ade_update<NU, MAG>(d, a);
+    ade_store<NU>(d, q, a);
 }
 
 __device__ __forceinline__ int step_of(const StepRef& s) { return (s.dev_n ? *s.dev_n : 0) + s.n; }
