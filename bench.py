@@ -362,15 +362,19 @@ def run_batched(args):
         marks["plan"] = time.perf_counter() - t0
         arena = int(sum(p.footprint for p in plans) * 1.05) + (64 << 20)
         with Batch(arena, len(pbs) + 1, kernel_family=args.batch_family) as b:
-            # a first group, tuned on, then 32-step chunks queued between the
-            # remaining set-ups: an instance is set up on its own stream while
-            # the queued steps of the others run
+            # in stream order (or longest solves first, which measured slower:
+            # the tuner then sees only the largest grids), a first group tuned
+            # on, then 32-step chunks queued between the remaining set-ups: an
+            # instance is set up on its own stream while the queued steps of
+            # the others run
+            if args.batch_order == "longest":
+                plans = sorted(plans, key=lambda p: -(p.nsteps + 1) * p.problem.swept_cells)
             first = 8
             slots = [b.add(p) for p in plans[:first]]
             chunks, ctas = b.autotune(2)
             marks["tune"] = time.perf_counter() - t0
             for q, p in enumerate(plans[first:]):
-                if q % 4 == 0:
+                if q % args.batch_advance_every == 0:
                     b.advance(32)
                 slots.append(b.add(p))
             marks["add"] = time.perf_counter() - t0
@@ -446,6 +450,10 @@ def main():
     ap.add_argument("--quick", action="store_true", help="skip the end-to-end and CPU-baseline legs (profiling runs)")
     ap.add_argument("--instances", type=int, default=64, help="batched: instances in the stream")
     ap.add_argument("--skip-plain", action="store_true", help="batched: leave out the one-at-a-time arm (profiling)")
+    ap.add_argument("--batch-order", default="stream", choices=["longest", "stream"],
+                    help="batched: order in which the instances join the batch")
+    ap.add_argument("--batch-advance-every", type=int, default=4,
+                    help="batched: a 32-step chunk is queued after this many instance set-ups")
     ap.add_argument("--batch-family", type=int, default=1, choices=[0, 1],
                     help="batched: field kernels, 1 TMA-pipelined persistent (default), 0 register-marching")
     ap.add_argument("--requests", type=int, default=160, help="served: requests in the stream")
