@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
 }
 
 template <int NU, bool MAG>
-__global__ void __launch_bounds__(256) k_ade(KGrid g, KDisp d, int comp) {
+__global__ void __launch_bounds__(256, 6) k_ade(KGrid g, KDisp d, int comp) {
     const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (q < d.n[comp]) ade_node<NU, MAG>(ade_refs<MAG>(g, d, comp), q);
 }
