@@ -520,6 +520,80 @@ sgpu_status sgpu_batch_profile_steps(sgpu_batch* b, int nsteps, float* ms6);
 /* The batch step counter (steps queued so far). */
 sgpu_status sgpu_batch_steps(const sgpu_batch* b, int* counter);
 
+/* ---- Near-to-far-field transform (farfield.F90) --------------------------
+ * InitFarField (farfield.F90:118-1158) for one closed surface.  Faces in the
+ * order Tr, Fr, Iz, De, Ab, Ar (x-, x+, y-, y+, z-, z+).  Each face carries
+ * two tangential E components, t1 / t2 = (Ez, Ey) on x faces, (Ez, Ex) on y
+ * faces, (Ey, Ex) on z faces, and for each the H component that pairs with
+ * it (Hy, Hz; Hx, Hz; Hx, Hy), sampled on two planes.
+ *   lim[face][t] = {plane, lo1, hi1, lo2, hi2}: the E plane index of
+ *     component t and the ranges of its two in-plane indices in the
+ *     reference's loop order (k then j on x faces, k then i on y faces,
+ *     j then i on z faces): TrFr%I%tra / fro, IzDe%J%izq / der,
+ *     AbAr%K%aba / arr and their com / fin limits (farfield.F90:512-580).
+ *     The H partner takes the same ranges on planes plane-1 and plane (low
+ *     faces) or plane and plane+1 (high faces).
+ *   freq[nfreq]: the frequencies, real(4) as the reference lists them.
+ *   ndecim, dtdecim: FF%NDecim and FF%dtDecim (farfield.F90:194-199);
+ *     UpdateFarField (:1163-1733) samples steps n with mod(n-1, ndecim) = 0.
+ *   cluz, zvac, cell[6] = dxe, dye, dze, dxh, dyh, dzh over cell_lo ..
+ *   cell_lo+cell_n-1 and phys[c][axis] = Punto%PhysCoor of Ex, Ey, Ez are
+ *   for the transform (FlushFarfield, :2408-3423). */
+typedef struct {
+    int active[6];
+    int lim[6][2][5];
+    int nfreq;
+    const float* freq;
+    int ndecim;
+    float dtdecim;
+    float cluz, zvac;
+    const float* cell[6];
+    int cell_lo[6];
+    int cell_n[6];
+    const float* phys[3][3];
+    int phys_lo[3][3];
+    int phys_n[3][3];
+} sgpu_farfield_desc;
+sgpu_status sgpu_add_farfield(sgpu_ctx* ctx, const sgpu_farfield_desc* d, int* id);
+/* The far-field request of the reference's input (the FarField probe of
+ * observation.F90:2050): the box esqx1, esqx2, esqy1, esqy2, esqz1, esqz2
+ * in cell indices, the faces to sample, the frequency range and the
+ * decimation switch (NF2FFDecim).  Clips the box and fills the descriptor
+ * above from the context's host set-up (sgpu_host_create), then adds it.
+ * A face on the edge of the non-CPML region is refused as the reference
+ * refuses it ("NF2FF STILL UNSUPPORTED"). */
+typedef struct {
+    int box[6];
+    int faces[6];
+    float initial_freq, final_freq, freq_step;
+    int logarithmic;
+    int decimate;
+} sgpu_farfield_spec;
+sgpu_status sgpu_host_add_farfield(sgpu_ctx* ctx, const sgpu_farfield_spec* s, int* id);
+/* Number of frequencies and surface samples (all faces, components and
+ * planes) of a far field. */
+sgpu_status sgpu_farfield_shape(const sgpu_ctx* ctx, int id, int* nfreq, int* samples);
+/* One accumulated surface array: face 0..5, slot 0 / 1 = E t1 / t2, 2 / 3 =
+ * the H partner of t1 on its first / second plane, 4 / 5 the same for t2.
+ * dims[2] = the counts of the two in-plane indices (loop order, outer
+ * first); out = complex(8) [nfreq][outer][inner]. */
+sgpu_status sgpu_read_farfield(sgpu_ctx* ctx, int id, int face, int slot, int* dims, double* out);
+/* FlushFarfield (farfield.F90:2408-3423): for every frequency and direction
+ * (theta from theta_start in theta_step up to theta_stop, the last step
+ * clamped; phi likewise), the radiation vectors L, N summed over the faces
+ * with arithmetic and geometric means of the two H planes, and from them
+ * the row  freq, theta, phi, |Etheta|, arg Etheta, |Ephi|, arg Ephi (the
+ * geometric pass), RCS (arithmetic), RCS (geometric).  incident[0..n-1]
+ * are the (time, value) pairs of the normalisation file (FileNormalize,
+ * farfield.F90:1021-1070); its DFT normalises the RCS.  Rows go to out
+ * [max_rows][9]; *rows gets the number of frequency x direction rows. */
+typedef struct {
+    float theta_start, theta_stop, theta_step;
+    float phi_start, phi_stop, phi_step;
+} sgpu_farfield_angles;
+sgpu_status sgpu_farfield_transform(sgpu_ctx* ctx, int id, const sgpu_farfield_angles* a, const float* incident,
+                                    int n_incident, double* out, int max_rows, int* rows);
+
 #ifdef __cplusplus
 }
 #endif

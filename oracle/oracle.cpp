@@ -187,6 +187,24 @@ template <class R> struct Sim {
         std::vector<std::complex<double>> V;  // [f][comp][k][j][i]
     };
     std::vector<FreqProbe> fprobes;
+    // InitFarField / UpdateFarField state (farfield.F90:64-116): per face the
+    // E arrays of its two tangential components and the H arrays of their
+    // partners on two planes, each over its accumulation range (the
+    // reference's arrays span the Alloc plane and stay zero outside it).
+    struct FarArr {
+        int comp = 0, plane = 0, lo1 = 0, hi1 = -1, lo2 = 0, hi2 = -1;
+        std::vector<std::complex<double>> v;  // [f][outer][inner]
+    };
+    struct FarOrc {
+        bool on[6] = {};
+        int lim[6][2][5] = {};
+        std::vector<R> freq;
+        int ndecim = 1;
+        R dtDecim = 0;
+        std::vector<std::complex<double>> expIwdt, auxE, auxH;
+        FarArr arr[6][6];  // [face][t1 E, t2 E, H1 plane 1, H1 plane 2, H2 plane 1, H2 plane 2]
+    };
+    std::vector<FarOrc> farfields;
 
     R physc(int field, int axis, int idx) const { return phys[field][axis][idx - phys_lo[field][axis]]; }
     double time(int n) {
@@ -1628,6 +1646,299 @@ template <class R> int resume_io(Sim<R>& s, const char* path, bool write, int* n
     return r.ok ? 0 : 1;
 }
 
+// UpdateFarField, farfield.F90:1163-1733.
+template <class R> void update_farfield(Sim<R>& s, typename Sim<R>::FarOrc& ff, int ntime) {
+    if ((ntime - 1) % ff.ndecim != 0) return;
+    const int nf = (int)ff.freq.size();
+    for (int fc = 0; fc < 6; ++fc) {
+        if (!ff.on[fc]) continue;
+        const int axis = fc / 2;
+        for (int k = 0; k < 6; ++k) {
+            auto& A = ff.arr[fc][k];
+            const int n1 = A.hi1 - A.lo1 + 1, n2 = A.hi2 - A.lo2 + 1;
+            if (n1 <= 0 || n2 <= 0) continue;
+            const auto& aux = A.comp >= 3 ? ff.auxH : ff.auxE;
+            for (int o = A.lo1; o <= A.hi1; ++o)
+                for (int u = A.lo2; u <= A.hi2; ++u) {
+                    int i, j, kk;
+                    if (axis == 0) { i = A.plane; j = u; kk = o; }
+                    else if (axis == 1) { i = u; j = A.plane; kk = o; }
+                    else { i = u; j = o; kk = A.plane; }
+                    const double v = (double)s.F[A.comp](i, j, kk);
+                    for (int f = 0; f < nf; ++f) {
+                        std::complex<double>& x = A.v[((size_t)f * n1 + (o - A.lo1)) * n2 + (u - A.lo2)];
+                        x = std::complex<double>(x.real() + aux[f].real() * v, x.imag() + aux[f].imag() * v);
+                    }
+                }
+        }
+    }
+    for (int f = 0; f < nf; ++f) {
+        const std::complex<double> a = ff.auxE[f], b = ff.auxH[f], e = ff.expIwdt[f];
+        ff.auxE[f] = {a.real() * e.real() - a.imag() * e.imag(), a.real() * e.imag() + a.imag() * e.real()};
+        ff.auxH[f] = {b.real() * e.real() - b.imag() * e.imag(), b.real() * e.imag() + b.imag() * e.real()};
+    }
+}
+
+// InitFarField, farfield.F90:118-1158, for one layout.
+template <class R> int add_farfield(Sim<R>& s, const int* box, const int* faces, float fi_, float ff_, float fs_, int logf,
+                                    int decimate) {
+    typename Sim<R>::FarOrc F;
+    const Lim &HX = s.SINPML[3], &HY = s.SINPML[4], &HZ = s.SINPML[5];
+    int e[6] = {std::max(box[0], HX.XI), std::min(box[1], HX.XE), std::max(box[2], HY.YI),
+                std::min(box[3], HY.YE), std::max(box[4], HZ.ZI), std::min(box[5], HZ.ZE)};
+    const Lim &WX = s.SINPMLSweep[3], &WY = s.SINPMLSweep[4], &WZ = s.SINPMLSweep[5];
+    const bool in[6] = {e[0] > WX.XI && e[0] <= WX.XE, e[1] < WX.XE && e[1] >= WX.XI, e[2] > WY.YI && e[2] <= WY.YE,
+                        e[3] < WY.YE && e[3] >= WY.YI, e[4] > WZ.ZI && e[4] <= WZ.ZE, e[5] < WZ.ZE && e[5] >= WZ.ZI};
+    const bool edge[6] = {e[0] <= HX.XI, e[1] >= HX.XE, e[2] <= HY.YI, e[3] >= HY.YE, e[4] <= HZ.ZI, e[5] >= HZ.ZE};
+    for (int f = 0; f < 6; ++f) {
+        const bool image = s.isPEC[f / 2][f % 2] || s.isPMC[f / 2][f % 2];
+        if (!edge[f] || !image) continue;
+        for (int g = 0; g < 6; ++g)
+            if (g != f && in[g]) return -2;  // NF2FF STILL UNSUPPORTED
+    }
+    for (int f = 0; f < 6; ++f) F.on[f] = in[f] && faces[f];
+    const Lim &Sx = s.SINPMLSweep[0], &Sy = s.SINPMLSweep[1], &Sz = s.SINPMLSweep[2];
+    for (int sd = 0; sd < 2; ++sd) {
+        const bool lo = sd == 0;
+        int* L = F.lim[sd][0];  // TrFr Ez
+        L[0] = lo ? std::max(Sz.XI, e[0]) : std::min(Sz.XE, e[1]);
+        L[1] = std::max(Sz.ZI, e[4]); L[2] = std::min(Sz.ZE, e[5] - 1); L[3] = std::max(Sz.YI, e[2]); L[4] = std::min(Sz.YE, e[3]);
+        L = F.lim[sd][1];  // TrFr Ey
+        L[0] = lo ? std::max(Sy.XI, e[0]) : std::min(Sy.XE, e[1]);
+        L[1] = std::max(Sy.ZI, e[4]); L[2] = std::min(Sy.ZE - 1, e[5]); L[3] = std::max(Sy.YI, e[2]); L[4] = std::min(Sy.YE, e[3] - 1);
+        L = F.lim[2 + sd][0];  // IzDe Ez
+        L[0] = lo ? std::max(Sz.YI, e[2]) : std::min(Sz.YE, e[3]);
+        L[1] = std::max(Sz.ZI, e[4]); L[2] = std::min(Sz.ZE, e[5] - 1); L[3] = std::max(Sz.XI, e[0]); L[4] = std::min(Sz.XE, e[1]);
+        L = F.lim[2 + sd][1];  // IzDe Ex
+        L[0] = lo ? std::max(Sx.YI, e[2]) : std::min(Sx.YE, e[3]);
+        L[1] = std::max(Sx.ZI, e[4]); L[2] = std::min(Sx.ZE - 1, e[5]); L[3] = std::max(Sx.XI, e[0]); L[4] = std::min(Sx.XE, e[1] - 1);
+        L = F.lim[4 + sd][0];  // AbAr Ey
+        L[0] = lo ? std::max(Sy.ZI, e[4]) : std::min(Sy.ZE, e[5]);
+        L[1] = std::max(Sy.YI, e[2]); L[2] = std::min(Sy.YE, e[3] - 1); L[3] = std::max(Sy.XI, e[0]); L[4] = std::min(Sy.XE, e[1]);
+        L = F.lim[4 + sd][1];  // AbAr Ex
+        L[0] = lo ? std::max(Sx.ZI, e[4]) : std::min(Sx.ZE, e[5]);
+        L[1] = std::max(Sx.YI, e[2]); L[2] = std::min(Sx.YE, e[3]); L[3] = std::max(Sx.XI, e[0]); L[4] = std::min(Sx.XE, e[1] - 1);
+    }
+    const R fi = (R)fi_, ffin = (R)ff_, fs = (R)fs_;
+    const int nf = fs != (R)0 ? (int)(std::fabs(fi - ffin) / fs) + 1 : 1;
+    if (nf < 1 || nf > 100000) return -1;
+    R init = fi, step = fs;
+    if (logf) {
+        init = std::log10(fi);
+        step = std::fabs(init - std::log10(ffin)) / (R)nf;
+    }
+    for (int q = 0; q < nf; ++q) {
+        const R x = init + (R)q * step;
+        F.freq.push_back(logf ? (R)std::pow((R)10, x) : x);
+    }
+    F.ndecim = decimate ? std::max((int)((double)((R)0.5 / ffin) / s.dt) - 1, 1) : 1;
+    F.dtDecim = (R)((double)F.ndecim * s.dt);
+    const R pi = (R)3.14159265358979323846;
+    for (int q = 0; q < nf; ++q) {
+        // Exp(-(0,1) * 2 * pi * freq * dtDecim) in complex(RKIND)
+        const std::complex<R> z4(-(R)0, ((-((R)2 * pi)) * F.freq[q]) * F.dtDecim);
+        const std::complex<R> e4 = std::exp(z4);
+        F.expIwdt.push_back(std::complex<double>((double)e4.real(), (double)e4.imag()));
+        F.auxE.push_back(std::complex<double>((double)F.dtDecim, 0.0));
+        // the half-step factor is a complex(8) exponential (sgg%dt is real(8))
+        const double x = s.dt * 0.5;
+        const std::complex<double> eh = std::exp(std::complex<double>(-0.0 * x, (double)((-((R)2 * pi)) * F.freq[q]) * x));
+        F.auxH.push_back(std::complex<double>((double)F.dtDecim * eh.real(), (double)F.dtDecim * eh.imag()));
+    }
+    const int tan[3][2] = {{2, 1}, {2, 0}, {1, 0}};
+    for (int fc = 0; fc < 6; ++fc) {
+        if (!F.on[fc]) continue;
+        const int axis = fc / 2;
+        for (int t = 0; t < 2; ++t) {
+            const int* L = F.lim[fc][t];
+            const int c = tan[axis][t], hc = 3 + (3 - axis - c);
+            const int hp = fc % 2 == 0 ? L[0] - 1 : L[0];  // TrFr%I%tra%Hy = tra%Ez - 1, fro%Hy = fro%Ez
+            const int comp[3] = {c, hc, hc}, plane[3] = {L[0], hp, hp + 1}, slot[3] = {t, 2 + 2 * t, 3 + 2 * t};
+            for (int q = 0; q < 3; ++q) {
+                auto& A = F.arr[fc][slot[q]];
+                A.comp = comp[q];
+                A.plane = plane[q];
+                A.lo1 = L[1]; A.hi1 = L[2]; A.lo2 = L[3]; A.hi2 = L[4];
+                const long n1 = std::max(0, L[2] - L[1] + 1), n2 = std::max(0, L[4] - L[3] + 1);
+                A.v.assign((size_t)nf * n1 * n2, std::complex<double>(0.0, 0.0));
+            }
+        }
+    }
+    s.farfields.push_back(std::move(F));
+    return (int)s.farfields.size() - 1;
+}
+
+// update_LN, farfield.F90:3426-3449.
+struct LN {
+    std::complex<double> Lt, Lp, Nt, Np;
+};
+template <class R> void update_ln(std::complex<double> comun, const R co[6][3], const R* t, const std::complex<double>* MJ,
+                                  LN& ln) {
+    // t: sintheta_cosphi, sintheta_sinphi, costheta, costheta_cosphi, costheta_sinphi, sintheta, sinphi, cosphi
+    std::complex<double> cm[6];
+    for (int k = 0; k < 6; ++k) {
+        const R d = co[k][0] * t[0] + co[k][1] * t[1] + co[k][2] * t[2];
+        const std::complex<double> z(comun.real() * (double)d, comun.imag() * (double)d);
+        cm[k] = std::exp(z);
+    }
+    auto sc = [](std::complex<double> a, R r) { return std::complex<double>(a.real() * (double)r, a.imag() * (double)r); };
+    ln.Lt = ln.Lt + (sc(MJ[0], t[3]) * cm[0] + sc(MJ[1], t[4]) * cm[1] - sc(MJ[2], t[5]) * cm[2]);
+    ln.Lp = ln.Lp + (sc(-MJ[0], t[6]) * cm[0] + sc(MJ[1], t[7]) * cm[1]);
+    ln.Nt = ln.Nt + (sc(MJ[3], t[3]) * cm[3] + sc(MJ[4], t[4]) * cm[4] - sc(MJ[5], t[5]) * cm[5]);
+    ln.Np = ln.Np + (sc(-MJ[3], t[6]) * cm[3] + sc(MJ[4], t[7]) * cm[4]);
+}
+
+// average(), farfield.F90:3553-3579.
+template <class R> std::complex<double> ff_average(int pasadas, std::complex<double> z1, std::complex<double> z2) {
+    const R pi = (R)3.14159265358979323846;
+    if (pasadas == 2) {
+        const R phi1 = (R)std::atan2(z1.imag(), z1.real()), phi2 = (R)std::atan2(z2.imag(), z2.real());
+        R n1 = phi1, n2 = phi2;
+        if (phi1 < -pi / (R)2 && phi2 > pi / (R)2) n1 = phi1 - (R)2 * pi;
+        if (phi2 < -pi / (R)2 && phi1 > pi / (R)2) n2 = phi2 - (R)2 * pi;
+        const std::complex<R> e = std::exp(std::complex<R>((R)0, (n1 + n2) / (R)2));
+        const std::complex<double> p(z1.real() * z2.real() - z1.imag() * z2.imag(), z1.real() * z2.imag() + z1.imag() * z2.real());
+        const double r = std::sqrt(std::abs(p));
+        return {r * (double)e.real(), r * (double)e.imag()};
+    }
+    return {(z1.real() + z2.real()) / 2.0, (z1.imag() + z2.imag()) / 2.0};
+}
+
+// FlushFarfield, farfield.F90:2408-3423 (one layout, no image faces): rows of
+// freq, theta, phi, |Etheta|, arg Etheta, |Ephi|, arg Ephi, RCS(arit), RCS(geom).
+template <class R> int farfield_transform(Sim<R>& s, int id, const float* ang, const float* inc, int ninc, double* out,
+                                          int max_rows, int* rows) {
+    if (id < 0 || id >= (int)s.farfields.size()) return 1;
+    auto& F = s.farfields[id];
+    const R pi = (R)3.14159265358979323846;
+    const R ts = (R)ang[0], tstop = (R)ang[1], tstep = (R)ang[2], ps = (R)ang[3], pstop = (R)ang[4], pstep = (R)ang[5];
+    if (!(tstep > 0) || !(pstep > 0)) return 1;
+    std::vector<R> dirs;
+    for (R theta = ts - tstep; theta < tstop;) {
+        theta = std::min(theta + tstep, tstop);
+        for (R phi = ps - pstep; phi < pstop;) {
+            phi = std::min(phi + pstep, pstop);
+            dirs.push_back(theta);
+            dirs.push_back(phi);
+        }
+    }
+    const int nd = (int)dirs.size() / 2, nf = (int)F.freq.size();
+    *rows = nd * nf;
+    if (!out) return 0;
+    if (max_rows < nd * nf || ninc < 2) return 1;
+    // dftEntrada, :1021-1070
+    std::vector<std::complex<double>> dft(nf);
+    {
+        const R dtevol = (R)inc[2] - (R)inc[0];
+        const std::complex<double> mcpi2(-0.0, -(double)((R)2 * pi));
+        for (int q = 0; q < nf; ++q) {
+            const std::complex<double> z = std::complex<double>(mcpi2.real() * (double)F.freq[q], mcpi2.imag() * (double)F.freq[q]);
+            const std::complex<double> ex = std::exp(std::complex<double>(z.real() * (double)dtevol, z.imag() * (double)dtevol));
+            std::complex<double> aux((double)dtevol, 0.0), acc(0.0, 0.0);
+            for (int m = 1; m < ninc; ++m) {
+                const double v = (double)(R)inc[2 * m + 1];
+                acc = std::complex<double>(acc.real() + v * aux.real(), acc.imag() + v * aux.imag());
+                aux = std::complex<double>(aux.real() * ex.real() - aux.imag() * ex.imag(), aux.real() * ex.imag() + aux.imag() * ex.real());
+            }
+            dft[q] = acc;
+        }
+    }
+    auto cell = [&](const A1<R>& a, int i) { return a(i); };
+    auto val = [&](const typename Sim<R>::FarArr& A, int f, int o, int u) -> std::complex<double> {
+        if (o < A.lo1 || o > A.hi1 || u < A.lo2 || u > A.hi2) return {0.0, 0.0};
+        const int n1 = A.hi1 - A.lo1 + 1, n2 = A.hi2 - A.lo2 + 1;
+        return A.v[((size_t)f * n1 + (o - A.lo1)) * n2 + (u - A.lo2)];
+    };
+    auto sc = [](std::complex<double> a, R r) { return std::complex<double>(a.real() * (double)r, a.imag() * (double)r); };
+    int row = 0;
+    for (int ii = 0; ii < nf; ++ii) {
+        const R freq = F.freq[ii];
+        const std::complex<R> c4 = std::complex<R>((R)0, (((R)2 * pi) * freq) / s.cluz);
+        const std::complex<double> comun((double)c4.real(), (double)c4.imag());
+        for (int d = 0; d < nd; ++d) {
+            const R theta = dirs[2 * d], phi = dirs[2 * d + 1];
+            double Et[3][2] = {}, Ep[3][2] = {};
+            R rcs[3] = {};
+            for (int pasadas = 2; pasadas >= 1; --pasadas) {
+                const R t[8] = {std::sin(theta) * std::cos(phi), std::sin(theta) * std::sin(phi), std::cos(theta),
+                                std::cos(theta) * std::cos(phi), std::cos(theta) * std::sin(phi), std::sin(theta),
+                                std::sin(phi), std::cos(phi)};
+                LN fin{};
+                for (int fc = 0; fc < 6; ++fc) {
+                    if (!F.on[fc]) continue;
+                    const int axis = fc / 2;
+                    const R normal = fc % 2 == 0 ? (R)-1 : (R)1;
+                    const auto* A = F.arr[fc];
+                    const int(*L)[5] = F.lim[fc];
+                    LN ln{};
+                    // co rows: Mx, My, Mz, Jx, Jy, Jz; MJ the same order
+                    if (axis == 0) {
+                        const int i = L[0][0];
+                        for (int k = L[0][1]; k <= L[1][2]; ++k)
+                            for (int j = L[0][3]; j <= L[0][4]; ++j) {
+                                std::complex<double> MJ[6] = {};
+                                if (k <= L[0][2]) MJ[1] = sc(sc(sc(-val(A[0], ii, k, j), cell(s.dyh, j)), cell(s.dze, k)), normal);
+                                if (j <= L[1][4]) MJ[2] = sc(sc(sc(val(A[1], ii, k, j), cell(s.dye, j)), cell(s.dzh, k)), normal);
+                                if (k <= L[1][2]) MJ[4] = sc(sc(sc(ff_average<R>(pasadas, val(A[4], ii, k, j), val(A[5], ii, k, j)), cell(s.dye, j)), cell(s.dzh, k)), normal);
+                                if (j <= L[0][4]) MJ[5] = sc(sc(sc(-ff_average<R>(pasadas, val(A[2], ii, k, j), val(A[3], ii, k, j)), cell(s.dyh, j)), cell(s.dze, k)), normal);
+                                R co[6][3] = {};
+                                const R pz[3] = {s.physc(2, 0, i), s.physc(2, 1, j), s.physc(2, 2, k)};
+                                const R py[3] = {s.physc(1, 0, i), s.physc(1, 1, j), s.physc(1, 2, k)};
+                                for (int a = 0; a < 3; ++a) { co[1][a] = pz[a]; co[2][a] = py[a]; co[4][a] = py[a]; co[5][a] = pz[a]; }
+                                update_ln<R>(comun, co, t, MJ, ln);
+                            }
+                    } else if (axis == 1) {
+                        const int j = L[1][0];
+                        for (int k = L[1][1]; k <= L[1][2]; ++k)
+                            for (int i = L[1][3]; i <= L[0][4]; ++i) {
+                                std::complex<double> MJ[6] = {};
+                                if (k <= L[0][2]) MJ[0] = sc(sc(sc(val(A[0], ii, k, i), cell(s.dxh, i)), cell(s.dze, k)), normal);
+                                if (i <= L[1][4]) MJ[2] = sc(sc(sc(-val(A[1], ii, k, i), cell(s.dxe, i)), cell(s.dzh, k)), normal);
+                                if (k <= L[1][2]) MJ[3] = sc(sc(sc(-ff_average<R>(pasadas, val(A[4], ii, k, i), val(A[5], ii, k, i)), cell(s.dxe, i)), cell(s.dzh, k)), normal);
+                                if (i <= L[0][4]) MJ[5] = sc(sc(sc(ff_average<R>(pasadas, val(A[2], ii, k, i), val(A[3], ii, k, i)), cell(s.dxh, i)), cell(s.dze, k)), normal);
+                                R co[6][3] = {};
+                                const R pz[3] = {s.physc(2, 0, i), s.physc(2, 1, j), s.physc(2, 2, k)};
+                                const R px[3] = {s.physc(0, 0, i), s.physc(0, 1, j), s.physc(0, 2, k)};
+                                for (int a = 0; a < 3; ++a) { co[0][a] = pz[a]; co[2][a] = px[a]; co[5][a] = pz[a]; co[3][a] = px[a]; }
+                                update_ln<R>(comun, co, t, MJ, ln);
+                            }
+                    } else {
+                        const int k = L[0][0];
+                        for (int j = L[0][1]; j <= L[1][2]; ++j)
+                            for (int i = L[0][3]; i <= L[0][4]; ++i) {
+                                std::complex<double> MJ[6] = {};
+                                if (j <= L[0][2]) MJ[0] = sc(sc(sc(-val(A[0], ii, j, i), cell(s.dxh, i)), cell(s.dye, j)), normal);
+                                if (i <= L[1][4]) MJ[1] = sc(sc(sc(val(A[1], ii, j, i), cell(s.dxe, i)), cell(s.dyh, j)), normal);
+                                if (j <= L[1][2]) MJ[3] = sc(sc(sc(ff_average<R>(pasadas, val(A[4], ii, j, i), val(A[5], ii, j, i)), cell(s.dxe, i)), cell(s.dyh, j)), normal);
+                                if (i <= L[0][4]) MJ[4] = sc(sc(sc(-ff_average<R>(pasadas, val(A[2], ii, j, i), val(A[3], ii, j, i)), cell(s.dxh, i)), cell(s.dye, j)), normal);
+                                R co[6][3] = {};
+                                const R py[3] = {s.physc(1, 0, i), s.physc(1, 1, j), s.physc(1, 2, k)};
+                                const R px[3] = {s.physc(0, 0, i), s.physc(0, 1, j), s.physc(0, 2, k)};
+                                for (int a = 0; a < 3; ++a) { co[0][a] = py[a]; co[1][a] = px[a]; co[3][a] = px[a]; co[4][a] = py[a]; }
+                                update_ln<R>(comun, co, t, MJ, ln);
+                            }
+                    }
+                    fin.Lt += ln.Lt; fin.Lp += ln.Lp; fin.Nt += ln.Nt; fin.Np += ln.Np;
+                }
+                const R be = -freq / ((R)2 * s.cluz), bp = freq / ((R)2 * s.cluz);
+                const std::complex<double> X = fin.Lp + sc(fin.Nt, s.zvac), Y = fin.Lt - sc(fin.Np, s.zvac);
+                Et[pasadas][0] = -((double)be * X.imag()); Et[pasadas][1] = (double)be * X.real();
+                Ep[pasadas][0] = -((double)bp * Y.imag()); Ep[pasadas][1] = (double)bp * Y.real();
+                const R q = (((R)2 * pi) * freq) / s.cluz;
+                const double hd = std::abs(dft[ii]), hx = std::abs(X), hy = std::abs(Y);
+                rcs[pasadas] = (R)((double)(q * q) / ((double)((R)4 * pi) * (hd * hd)) * (hx * hx + hy * hy));
+            }
+            double* r = out + (size_t)row * 9;
+            r[0] = (double)freq; r[1] = (double)theta; r[2] = (double)phi;
+            r[3] = std::hypot(Et[2][0], Et[2][1]); r[4] = std::atan2(Et[2][1], Et[2][0]);
+            r[5] = std::hypot(Ep[2][0], Ep[2][1]); r[6] = std::atan2(Ep[2][1], Ep[2][0]);
+            r[7] = (double)rcs[1]; r[8] = (double)rcs[2];
+            ++row;
+        }
+    }
+    return 0;
+}
+
 template <class R> int run(Sim<R>& s, int n0, int n1, float* out) {
     const int np = (int)s.probes.size() / 4;
     for (int n = n0; n < n1; ++n) {
@@ -1640,6 +1951,7 @@ template <class R> int run(Sim<R>& s, int n0, int n1, float* out) {
             }
         }
         for (auto& p : s.fprobes) update_freq_probe(s, p, n);
+        for (auto& ff : s.farfields) update_farfield(s, ff, n);
     }
     return 0;
 }
@@ -1728,6 +2040,38 @@ int orc_read_freq_probe(void* hv, int id, int* shape4, double* out) {
         return 0;
     };
     return h->fp64 ? rd(*h->sd) : rd(*h->sf);
+}
+
+int orc_add_farfield(void* hv, const int* box, const int* faces, float fi, float ff, float fs, int logarithmic,
+                     int decimate) {
+    Handle* h = (Handle*)hv;
+    if (!h || !box || !faces) return -1;
+    return h->fp64 ? add_farfield(*h->sd, box, faces, fi, ff, fs, logarithmic, decimate)
+                   : add_farfield(*h->sf, box, faces, fi, ff, fs, logarithmic, decimate);
+}
+
+int orc_read_farfield(void* hv, int id, int face, int slot, int* dims, double* out) {
+    Handle* h = (Handle*)hv;
+    auto rd = [&](auto& s) -> int {
+        if (id < 0 || id >= (int)s.farfields.size() || face < 0 || face > 5 || slot < 0 || slot > 5) return 1;
+        const auto& F = s.farfields[id];
+        if (!F.on[face]) { dims[0] = dims[1] = 0; return 0; }
+        const auto& A = F.arr[face][slot];
+        dims[0] = std::max(0, A.hi1 - A.lo1 + 1);
+        dims[1] = std::max(0, A.hi2 - A.lo2 + 1);
+        if (out) std::memcpy(out, A.v.data(), A.v.size() * sizeof(std::complex<double>));
+        return 0;
+    };
+    if (!h || !dims) return 1;
+    return h->fp64 ? rd(*h->sd) : rd(*h->sf);
+}
+
+int orc_farfield_transform(void* hv, int id, const float* angles, const float* incident, int n_incident, double* out,
+                           int max_rows, int* rows) {
+    Handle* h = (Handle*)hv;
+    if (!h || !angles || !rows) return 1;
+    return h->fp64 ? farfield_transform(*h->sd, id, angles, incident, n_incident, out, max_rows, rows)
+                   : farfield_transform(*h->sf, id, angles, incident, n_incident, out, max_rows, rows);
 }
 
 int orc_store_resume(void* hv, const char* path, int last_step) {

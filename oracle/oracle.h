@@ -129,6 +129,17 @@ int orc_read_freq_probe(void* h, int id, int* shape4, double* out);
 /* Restart files in the records of resuming.F90's flush_and_save_resume
  * (fields, CPML psi, Mur Past_/PastPast_, electric and magnetic ADE state);
  * last_step is the last executed step n.  Load returns 0 and n on success. */
+/* Far field (farfield.F90): InitFarField for the box esqx1..esqz2, the faces
+ * Tr, Fr, Iz, De, Ab, Ar to sample, the frequency range and NF2FFDecim
+ * (returns the id, -2 for a face on a PEC/PMC border); the accumulated
+ * arrays (face, slot 0..5 as sgpu_read_farfield); FlushFarfield's rows
+ * (angles = theta start, stop, step, phi start, stop, step; incident =
+ * (time, value) pairs). */
+int orc_add_farfield(void* h, const int* box, const int* faces, float fi, float ff, float fs, int logarithmic,
+                     int decimate);
+int orc_read_farfield(void* h, int id, int face, int slot, int* dims, double* out);
+int orc_farfield_transform(void* h, int id, const float* angles, const float* incident, int n_incident, double* out,
+                           int max_rows, int* rows);
 int orc_store_resume(void* h, const char* path, int last_step);
 int orc_load_resume(void* h, const char* path, int* last_step);
 /* Grid description after set-up. */

@@ -105,6 +105,13 @@ def load():
         lib.orc_store_resume.restype = C.c_int
         lib.orc_load_resume.argtypes = [vp, C.c_char_p, ip]
         lib.orc_load_resume.restype = C.c_int
+        fp = C.POINTER(C.c_float)
+        lib.orc_add_farfield.argtypes = [vp, ip, ip, C.c_float, C.c_float, C.c_float, C.c_int, C.c_int]
+        lib.orc_add_farfield.restype = C.c_int
+        lib.orc_read_farfield.argtypes = [vp, C.c_int, C.c_int, C.c_int, ip, C.POINTER(C.c_double)]
+        lib.orc_read_farfield.restype = C.c_int
+        lib.orc_farfield_transform.argtypes = [vp, C.c_int, fp, fp, C.c_int, C.POINTER(C.c_double), C.c_int, ip]
+        lib.orc_farfield_transform.restype = C.c_int
         _lib = lib
     return _lib
 
@@ -283,6 +290,49 @@ class Oracle:
         out = np.empty(nf * 3 * nk * nj * ni * 2, np.float64)
         self.lib.orc_read_freq_probe(self._h, pid, None, out.ctypes.data_as(C.POINTER(C.c_double)))
         return out.view(np.complex128).reshape(nf, 3, nk, nj, ni)
+
+    def add_farfield(self, box, faces=(1, 1, 1, 1, 1, 1), initial=1e8, final=1e9, step=1e8,
+                     logarithmic=False, decimate=False) -> int:
+        """InitFarField (farfield.F90:118-1158) for the box esqx1..esqz2."""
+        b = (C.c_int * 6)(*[int(v) for v in box])
+        fc = (C.c_int * 6)(*[int(bool(v)) for v in faces])
+        fid = self.lib.orc_add_farfield(self._h, b, fc, float(initial), float(final), float(step),
+                                        int(bool(logarithmic)), int(bool(decimate)))
+        if fid == -2:
+            raise ValueError("NF2FF STILL UNSUPPORTED (a face on a PEC/PMC border)")
+        if fid < 0:
+            raise ValueError("bad far-field request")
+        return fid
+
+    def farfield_array(self, fid: int, face: int, slot: int) -> np.ndarray:
+        """Accumulated array of a face and slot as complex128 [nfreq, outer, inner]."""
+        dims = (C.c_int * 2)()
+        if self.lib.orc_read_farfield(self._h, fid, face, slot, dims, None):
+            raise ValueError("no far-field array with that id, face and slot")
+        n = dims[0] * dims[1]
+        nf = self._ff_nfreq(fid)
+        out = np.zeros(max(1, nf * n * 2), np.float64)
+        self.lib.orc_read_farfield(self._h, fid, face, slot, dims, out.ctypes.data_as(C.POINTER(C.c_double)))
+        return out[:nf * n * 2].view(np.complex128).reshape(nf, dims[0], dims[1])
+
+    def _ff_nfreq(self, fid: int) -> int:
+        rows = C.c_int()
+        ang = (C.c_float * 6)(0, 0, 1, 0, 0, 1)
+        self.lib.orc_farfield_transform(self._h, fid, ang, None, 0, None, 0, C.byref(rows))
+        return rows.value
+
+    def farfield_transform(self, fid: int, angles, incident) -> np.ndarray:
+        """FlushFarfield rows [n, 9]: freq, theta, phi, |Etheta|, arg Etheta,
+        |Ephi|, arg Ephi, RCS (arithmetic), RCS (geometric)."""
+        ang = (C.c_float * 6)(*[float(v) for v in angles])
+        inc = np.ascontiguousarray(np.asarray(incident, np.float32).reshape(-1, 2))
+        rows = C.c_int()
+        self.lib.orc_farfield_transform(self._h, fid, ang, None, 0, None, 0, C.byref(rows))
+        out = np.empty((rows.value, 9), np.float64)
+        if self.lib.orc_farfield_transform(self._h, fid, ang, inc.ctypes.data_as(C.POINTER(C.c_float)), len(inc),
+                                           out.ctypes.data_as(C.POINTER(C.c_double)), rows.value, C.byref(rows)):
+            raise ValueError("far-field transform failed")
+        return out
 
     def mur_cab1(self, face: int):
         """CAB1 per medium of a Mur face (back, front, left, right, down, up),

@@ -73,6 +73,17 @@ class MovieProbeDesc(C.Structure):
                 ("n_last", C.c_int), ("every", C.c_int), ("capacity", C.c_int)]
 
 
+class FarFieldSpec(C.Structure):
+    _fields_ = [("box", C.c_int * 6), ("faces", C.c_int * 6), ("initial_freq", C.c_float),
+                ("final_freq", C.c_float), ("freq_step", C.c_float), ("logarithmic", C.c_int),
+                ("decimate", C.c_int)]
+
+
+class FarFieldAngles(C.Structure):
+    _fields_ = [("theta_start", C.c_float), ("theta_stop", C.c_float), ("theta_step", C.c_float),
+                ("phi_start", C.c_float), ("phi_stop", C.c_float), ("phi_step", C.c_float)]
+
+
 ERRORS = {0: "ok", 1: "bad argument", 2: "out of memory", 3: "CUDA error", 4: "call out of order",
           5: "non-finite field", 6: "timeout", 7: "unsupported", 8: "size above the stated maximum"}
 
@@ -127,6 +138,11 @@ def _declare(lib: C.CDLL) -> None:
         "sgpu_volume_probe_shape": ([vp, C.c_int, c_int_p, c_int_p, c_int_p, c_int_p], C.c_int),
         "sgpu_read_freq_probe": ([vp, C.c_int, C.POINTER(C.c_double)], C.c_int),
         "sgpu_read_movie_probe": ([vp, C.c_int, c_float_p, C.c_int, c_int_p, c_int_p], C.c_int),
+        "sgpu_host_add_farfield": ([vp, C.POINTER(FarFieldSpec), c_int_p], C.c_int),
+        "sgpu_farfield_shape": ([vp, C.c_int, c_int_p, c_int_p], C.c_int),
+        "sgpu_read_farfield": ([vp, C.c_int, C.c_int, C.c_int, c_int_p, C.POINTER(C.c_double)], C.c_int),
+        "sgpu_farfield_transform": ([vp, C.c_int, C.POINTER(FarFieldAngles), c_float_p, C.c_int,
+                                     C.POINTER(C.c_double), C.c_int, c_int_p], C.c_int),
         "sgpu_advance_e": ([vp, C.c_int], C.c_int),
         "sgpu_advance_h": ([vp, C.c_int], C.c_int),
         "sgpu_advance_steps": ([vp, C.c_int, C.c_int], C.c_int),

@@ -1235,6 +1235,101 @@ sgpu_status sgpu_host_get_constants(const sgpu_ctx* c, float* eps0, float* mu0) 
     return SGPU_OK;
 }
 
+// InitFarField (farfield.F90:118-1158) for the descriptor of
+// sgpu_add_farfield.  SINPMLSweep is the SINPML range of one layout.
+sgpu_status sgpu_host_add_farfield(sgpu_ctx* c, const sgpu_farfield_spec* s, int* id) {
+    if (!c || !s) return SGPU_ERR_ARG;
+    if (!c->host) return sgpu::set_error(c, SGPU_ERR_STATE, "far fields need a context from sgpu_host_create");
+    if (c->zslab) return sgpu::set_error(c, SGPU_ERR_STATE, "far fields are not split across z-slabs");
+    const HostState* h = (const HostState*)c->host;
+    const Box& SX = h->sinpml[HX];
+    const Box& SY = h->sinpml[HY];
+    const Box& SZ = h->sinpml[HZ];
+    // :179-184, the box clipped to the non-CPML H ranges
+    int e[6] = {std::max(s->box[0], SX.x0), std::min(s->box[1], SX.x1), std::max(s->box[2], SY.y0),
+                std::min(s->box[3], SY.y1), std::max(s->box[4], SZ.z0), std::min(s->box[5], SZ.z1)};
+    // :284-301, a face is sampled when it lies strictly inside that range
+    const bool in[6] = {e[0] > SX.x0 && e[0] <= SX.x1, e[1] < SX.x1 && e[1] >= SX.x0,
+                        e[2] > SY.y0 && e[2] <= SY.y1, e[3] < SY.y1 && e[3] >= SY.y0,
+                        e[4] > SZ.z0 && e[4] <= SZ.z1, e[5] < SZ.z1 && e[5] >= SZ.z0};
+    // :316-510, a side on the edge of the range with a PEC or PMC border would
+    // need image faces, which the reference refuses
+    const bool edge[6] = {e[0] <= SX.x0, e[1] >= SX.x1, e[2] <= SY.y0, e[3] >= SY.y1, e[4] <= SZ.z0, e[5] >= SZ.z1};
+    for (int f = 0; f < 6; ++f) {
+        const int kind = h->kind[f / 2][f % 2];
+        if (!edge[f] || (kind != 1 && kind != 2)) continue;
+        for (int g = 0; g < 6; ++g)
+            if (g != f && in[g]) return sgpu::set_error(c, SGPU_ERR_ARG, "NF2FF STILL UNSUPPORTED (a face on a PEC/PMC border)");
+    }
+    sgpu_farfield_desc d{};
+    for (int f = 0; f < 6; ++f) d.active[f] = in[f] && s->faces[f];
+    // :512-580 (TrFr, IzDe, AbAr limits)
+    const Box& Sx = h->sinpml[EX];
+    const Box& Sy = h->sinpml[EY];
+    const Box& Sz = h->sinpml[EZ];
+    for (int side = 0; side < 2; ++side) {
+        const bool lo = side == 0;
+        // x faces: Ez, Ey; loops k then j
+        int* L = d.lim[side][0];
+        L[0] = lo ? std::max(Sz.x0, e[0]) : std::min(Sz.x1, e[1]);
+        L[1] = std::max(Sz.z0, e[4]); L[2] = std::min(Sz.z1, e[5] - 1);
+        L[3] = std::max(Sz.y0, e[2]); L[4] = std::min(Sz.y1, e[3]);
+        L = d.lim[side][1];
+        L[0] = lo ? std::max(Sy.x0, e[0]) : std::min(Sy.x1, e[1]);
+        L[1] = std::max(Sy.z0, e[4]); L[2] = std::min(Sy.z1 - 1, e[5]);
+        L[3] = std::max(Sy.y0, e[2]); L[4] = std::min(Sy.y1, e[3] - 1);
+        // y faces: Ez, Ex; loops k then i
+        L = d.lim[2 + side][0];
+        L[0] = lo ? std::max(Sz.y0, e[2]) : std::min(Sz.y1, e[3]);
+        L[1] = std::max(Sz.z0, e[4]); L[2] = std::min(Sz.z1, e[5] - 1);
+        L[3] = std::max(Sz.x0, e[0]); L[4] = std::min(Sz.x1, e[1]);
+        L = d.lim[2 + side][1];
+        L[0] = lo ? std::max(Sx.y0, e[2]) : std::min(Sx.y1, e[3]);
+        L[1] = std::max(Sx.z0, e[4]); L[2] = std::min(Sx.z1 - 1, e[5]);
+        L[3] = std::max(Sx.x0, e[0]); L[4] = std::min(Sx.x1, e[1] - 1);
+        // z faces: Ey, Ex; loops j then i
+        L = d.lim[4 + side][0];
+        L[0] = lo ? std::max(Sy.z0, e[4]) : std::min(Sy.z1, e[5]);
+        L[1] = std::max(Sy.y0, e[2]); L[2] = std::min(Sy.y1, e[3] - 1);
+        L[3] = std::max(Sy.x0, e[0]); L[4] = std::min(Sy.x1, e[1]);
+        L = d.lim[4 + side][1];
+        L[0] = lo ? std::max(Sx.z0, e[4]) : std::min(Sx.z1, e[5]);
+        L[1] = std::max(Sx.y0, e[2]); L[2] = std::min(Sx.y1, e[3]);
+        L[3] = std::max(Sx.x0, e[0]); L[4] = std::min(Sx.x1, e[1] - 1);
+    }
+    // :947-1036, the frequency list in real(4)
+    const float fi = s->initial_freq, ff = s->final_freq, fs = s->freq_step;
+    const int n = fs != 0.0f ? (int)(std::fabs(fi - ff) / fs) + 1 : 1;
+    if (n < 1 || n > 100000) return sgpu::set_error(c, SGPU_ERR_ARG, "Freq. range for NF/FF invalid");
+    std::vector<float> freq(n);
+    if (s->logarithmic) {
+        const float li = std::log10(fi), lf = std::log10(ff), step = std::fabs(li - lf) / (float)n;
+        for (int q = 0; q < n; ++q) freq[q] = std::pow(10.0f, li + (float)q * step);
+    } else {
+        for (int q = 0; q < n; ++q) freq[q] = fi + (float)q * fs;
+    }
+    d.nfreq = n;
+    d.freq = freq.data();
+    // :194-199
+    d.ndecim = s->decimate ? std::max((int)((double)(0.5f / ff) / h->dt) - 1, 1) : 1;
+    d.dtdecim = (float)((double)d.ndecim * h->dt);
+    d.cluz = h->cluz;
+    d.zvac = h->zvac;
+    const Vec* cells[6] = {&h->dxe, &h->dye, &h->dze, &h->dxh, &h->dyh, &h->dzh};
+    for (int k = 0; k < 6; ++k) {
+        d.cell[k] = cells[k]->v.data();
+        d.cell_lo[k] = cells[k]->lo;
+        d.cell_n[k] = (int)cells[k]->v.size();
+    }
+    for (int f = 0; f < 3; ++f)
+        for (int a = 0; a < 3; ++a) {
+            d.phys[f][a] = h->phys[f][a].data();
+            d.phys_lo[f][a] = h->phys_lo[f][a];
+            d.phys_n[f][a] = (int)h->phys[f][a].size();
+        }
+    return sgpu_add_farfield(c, &d, id);
+}
+
 sgpu_status sgpu_host_get_mur_cab1(const sgpu_ctx* c, int face, float* out) {
     if (!c || !c->host || face < 0 || face > 5 || !out) return SGPU_ERR_ARG;
     const HostState* h = (const HostState*)c->host;

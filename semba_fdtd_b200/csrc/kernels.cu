@@ -507,6 +507,10 @@ sgpu_status launch_sources(sgpu_ctx* c, int side, StepRef sr, int mask = kMaskAl
 }
 
 sgpu_status launch_probes(sgpu_ctx* c, StepRef sr) {
+    if (!c->farfields.empty()) {
+        sgpu_status s = launch_farfields(c, sr);
+        if (s) return s;
+    }
     for (const VolProbe& p : c->vprobes) {
         const long long nodes = (long long)p.ni * p.nj * p.nk;
         const unsigned blocks = (unsigned)((nodes + 255) / 256);
@@ -760,6 +764,7 @@ void sgpu_destroy(sgpu_ctx* c) {
     free_list(c, c->src_allocs[1]);
     free_list(c, c->probe_allocs);
     free_list(c, c->vprobe_allocs);
+    free_farfields(c);
     if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);
     if (c->host && c->host_free) c->host_free(c->host);
     delete c;

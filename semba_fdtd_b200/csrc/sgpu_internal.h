@@ -159,6 +159,34 @@ struct VolProbe {
     float* ring;
 };
 
+// One near-to-far-field surface (farfield.cu).  A patch is one sampled
+// array of a face: a component on one plane over two in-plane ranges;
+// acc holds [nf][samples] complex(8), patch p at columns off .. off+n-1
+// (inner index fastest).  The E / H weights of the m-th sampled step are
+// wE / wH [m][nf].
+struct FarPatch {
+    int comp, axis, plane;  // sampled component, face normal axis, plane index
+    int lo1, hi1, lo2, hi2;  // outer / inner in-plane ranges
+    int off, n;
+};
+constexpr int kFarPatches = 36;  // 6 faces x 6 arrays
+struct FarField {
+    int nf = 0, ndecim = 1, npatch = 0, samples = 0, w_m = 0;
+    int face_patch[6][6];  // patch index per face and slot, -1 if the face is off
+    FarPatch patch[kFarPatches];
+    double2* acc = nullptr;
+    double2* wE = nullptr;
+    double2* wH = nullptr;
+    // transform inputs kept on the host
+    int active[6];
+    std::vector<float> freq;
+    float cluz = 0, zvac = 0;
+    std::vector<float> cell[6];
+    int cell_lo[6];
+    std::vector<float> phys[3][3];
+    int phys_lo[3][3];
+};
+
 // Tensor maps of one fused TMA kernel (see tma_fields.cuh for the order).
 struct alignas(64) TMaps {
     CUtensorMap m[21];  // 9 field / media maps, then the 12 psi slabs of the side
@@ -244,6 +272,7 @@ struct sgpu_ctx {
     int probe_first_n = -1;
     // volume probes; steps_hi: one past the last step whose probes were launched
     std::vector<sgpu::VolProbe> vprobes;
+    std::vector<sgpu::FarField> farfields;
     std::vector<long long> vprobe_read;  // movie frames read so far, per probe
     std::vector<void*> vprobe_allocs;
     int steps_hi = -1;
@@ -277,6 +306,9 @@ sgpu_status create_in(const sgpu_grid_desc* d, Arena* arena, cudaStream_t stream
 // arena every probe keeps its whole trace (nsteps + 1 rows).
 sgpu_status host_create_in(const sgpu_problem* p, sgpu_ctx* plan, int max_steps, Arena* arena, cudaStream_t stream,
                            sgpu_ctx** out);
+// UpdateFarField for every far field of the context (farfield.cu).
+sgpu_status launch_farfields(sgpu_ctx* c, StepRef sr);
+void free_farfields(sgpu_ctx* c);
 // sgpu_upload_media, with the range check of the indices optional (the
 // host set-up's own matrices are in range by construction).
 sgpu_status upload_media(sgpu_ctx* c, int comp, const int16_t* mi, bool check);

@@ -245,6 +245,50 @@ class Solver:
         arr = np.concatenate(frames) if frames else np.zeros((0, 3, nk, nj, ni), np.float32)
         return first, arr
 
+    # -- near-to-far field (farfield.F90) -----------------------------------
+    def add_farfield(self, box, faces=(1, 1, 1, 1, 1, 1), initial: float = 1e8, final: float = 1e9,
+                     step: float = 1e8, logarithmic: bool = False, decimate: bool = False) -> int:
+        """InitFarField for the box (esqx1, esqx2, esqy1, esqy2, esqz1, esqz2):
+        the faces Tr, Fr, Iz, De, Ab, Ar to sample, the frequency range and
+        NF2FFDecim.  The surface DFT then runs on the device every step."""
+        spec = _lib.FarFieldSpec()
+        spec.box[:] = [int(v) for v in box]
+        spec.faces[:] = [int(bool(v)) for v in faces]
+        spec.initial_freq, spec.final_freq, spec.freq_step = float(initial), float(final), float(step)
+        spec.logarithmic, spec.decimate = int(bool(logarithmic)), int(bool(decimate))
+        fid = C.c_int()
+        self._check(self.lib.sgpu_host_add_farfield(self._h, C.byref(spec), C.byref(fid)), "sgpu_host_add_farfield")
+        return fid.value
+
+    def farfield_array(self, fid: int, face: int, slot: int) -> np.ndarray:
+        """One accumulated surface array, complex128 [nfreq, outer, inner]
+        (slot 0/1: E t1/t2; 2/3: H partner of t1 on its two planes; 4/5: of t2)."""
+        nf, dims = C.c_int(), (C.c_int * 2)()
+        self._check(self.lib.sgpu_farfield_shape(self._h, fid, C.byref(nf), None), "sgpu_farfield_shape")
+        self._check(self.lib.sgpu_read_farfield(self._h, fid, face, slot, dims, None), "sgpu_read_farfield")
+        n = dims[0] * dims[1]
+        out = np.zeros(max(1, nf.value * n * 2), np.float64)
+        self._check(self.lib.sgpu_read_farfield(self._h, fid, face, slot, dims,
+                                                out.ctypes.data_as(C.POINTER(C.c_double))), "sgpu_read_farfield")
+        return out[:nf.value * n * 2].view(np.complex128).reshape(nf.value, dims[0], dims[1])
+
+    def farfield_transform(self, fid: int, angles, incident) -> np.ndarray:
+        """FlushFarfield on the device: rows [n, 9] of freq, theta, phi,
+        |Etheta|, arg Etheta, |Ephi|, arg Ephi, RCS (arithmetic), RCS
+        (geometric), one per frequency and direction.  angles = (theta start,
+        stop, step, phi start, stop, step) in radians; incident = the (time,
+        value) pairs of the normalisation signal."""
+        a = _lib.FarFieldAngles(*[float(v) for v in angles])
+        inc = np.ascontiguousarray(np.asarray(incident, np.float32).reshape(-1, 2))
+        rows = C.c_int()
+        self._check(self.lib.sgpu_farfield_transform(self._h, fid, C.byref(a), None, 0, None, 0, C.byref(rows)),
+                    "sgpu_farfield_transform")
+        out = np.empty((rows.value, 9), np.float64)
+        self._check(self.lib.sgpu_farfield_transform(self._h, fid, C.byref(a), inc.ctypes.data_as(_lib.c_float_p),
+                                                     len(inc), out.ctypes.data_as(C.POINTER(C.c_double)),
+                                                     rows.value, C.byref(rows)), "sgpu_farfield_transform")
+        return out
+
     def set_kernel_family(self, family: int) -> None:
         """1: TMA-pipelined fused field kernels (default); 0: register-marching."""
         self._check(self.lib.sgpu_set_kernel_family(self._h, int(family)), "sgpu_set_kernel_family")
