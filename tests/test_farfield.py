@@ -106,6 +106,16 @@ def test_oracle_transform_rows_shape_and_reciprocity():
     np.testing.assert_array_equal(rows[:, 1], np.tile(np.repeat(th, len(ph)), 3))
     np.testing.assert_array_equal(rows[:, 2], np.tile(ph, 3 * len(th)))
     assert np.all(np.isfinite(rows)) and np.all(rows[:, 7:] >= 0) and rows[:, 7].max() > 0
+    # RCS(geom) = 4 pi (|Etheta|^2 + |Ephi|^2) / |DFT(incident)|^2 with the
+    # geometric-pass fields, the DFT skipping the first sample
+    inc = _incident(o.dt).astype(np.float64)
+    dtevol = float(np.float32(inc[1, 0]) - np.float32(inc[0, 0]))
+    m = np.arange(1, len(inc))
+    for q, f in enumerate(np.float32([2e8, 4e8, 6e8])):
+        dft = np.sum(inc[1:, 1] * dtevol * np.exp(-2j * np.pi * float(f) * (m - 1) * dtevol))
+        sl = rows[rows[:, 0] == float(f)]
+        expect = 4 * np.pi * (sl[:, 3] ** 2 + sl[:, 5] ** 2) / abs(dft) ** 2
+        np.testing.assert_allclose(sl[:, 8], expect, rtol=1e-5, atol=1e-6 * expect.max())
 
 
 @pytest.mark.gpu
