@@ -13,7 +13,8 @@
  *     time loop then maps to one sgpu_advance_* call.  The field, media and
  *     coefficient arrays are passed exactly as the Fortran host holds them
  *     (column-major over sgg%Alloc, re-based to 0), so a bind(C) interface
- *     can pass them without copies.
+ *     can pass them without copies (semba_gpu_m.F90 beside this header is
+ *     that interface).
  *
  *  2. A problem-level host (sgpu_host_*) that restates, in C++, the set-up
  *     of launch_simulation from an NFDE-style problem description (grid,

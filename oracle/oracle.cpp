@@ -170,8 +170,12 @@ template <class R> struct Sim {
     std::vector<R> CAB1[6];
     // ADE: electric (Dutton) and magnetic (MDutton) media
     std::vector<EDispMedium<R>> dut, mdut;
-    // plane waves
+    // plane waves; still_planewave_time is the global switch of
+    // timestepping.F90:1219 and :1251-1267: true at the start of a run, lowered
+    // by each AdvancePlaneWaveE/H and raised again by any face node whose
+    // waveform is not over, and once it is down no plane-wave routine runs
     std::vector<PlaneWave<R>> pws;
+    bool still_planewave_time = true;
     std::vector<R> phys[6][3];
     int phys_lo[6][3];
     // nodal
@@ -918,7 +922,9 @@ template <class R> void setup_planewave(Sim<R>& s, const orc_problem* p) {
 }
 
 // Incid + evolucion, planewaves.F90:778-853 (one mode, not from observation).
-template <class R> inline R incid(const Sim<R>& s, const PlaneWave<R>& pw, int nfield, R time, int i, int j, int k) {
+// evolucion raises still_planewave_time whenever the node's retarded time
+// still lies inside the waveform table (nprev + 1 <= numus, :830-832).
+template <class R> inline R incid(Sim<R>& s, const PlaneWave<R>& pw, int nfield, R time, int i, int j, int k) {
     R xf = s.physc(nfield, 0, i), yf = s.physc(nfield, 1, j), zf = s.physc(nfield, 2, k);
     R ehi = 0;
     R d = (xf * pw.px + yf * pw.py + zf * pw.pz) - pw.d0;
@@ -926,6 +932,7 @@ template <class R> inline R incid(const Sim<R>& s, const PlaneWave<R>& pw, int n
     R arg = time - d / s.cluz;
     long long nprev = (long long)(arg / pw.deltaevol);
     if (nprev + 1 <= pw.numus) {
+        s.still_planewave_time = true;
         if (nprev > 0) {
             ev = (pw.evol[nprev + 1] - pw.evol[nprev]) / pw.deltaevol * ((time - d / s.cluz) - (R)nprev * pw.deltaevol) +
                  pw.evol[nprev];
@@ -1176,8 +1183,12 @@ template <class R> void advance_mdisp(Sim<R>& s) {
     }
 }
 
-// AdvancePlaneWaveE, planewaves.F90:878-1174.
+// AdvancePlaneWaveE, planewaves.F90:878-1174, called only while
+// still_planewave_time holds (timestepping.F90:1423-1427); the routine lowers
+// the switch before its face loops (planewaves.F90:904).
 template <class R> void advance_pw_e(Sim<R>& s, int n) {
+    if (s.pws.empty() || !s.still_planewave_time) return;
+    s.still_planewave_time = false;
     R timei = (R)s.time(n);
     R G2_1 = s.G2[1];
     A3<R>&Ex = s.F[iEx], &Ey = s.F[iEy], &Ez = s.F[iEz];
@@ -1258,8 +1269,11 @@ template <class R> void advance_pw_e(Sim<R>& s, int n) {
     }
 }
 
-// AdvancePlaneWaveH, planewaves.F90:1180-1475.
+// AdvancePlaneWaveH, planewaves.F90:1180-1475, under the same switch
+// (timestepping.F90:1596-1600, planewaves.F90:1206).
 template <class R> void advance_pw_h(Sim<R>& s, int n) {
+    if (s.pws.empty() || !s.still_planewave_time) return;
+    s.still_planewave_time = false;
     R timei = (R)(s.time(n) + (double)(R)0.5 * s.dt);
     R Gm2_1 = s.GM2[1];
     A3<R>&Hx = s.F[iHx], &Hy = s.F[iHy], &Hz = s.F[iHz];
@@ -1642,6 +1656,8 @@ template <class R> int resume_io(Sim<R>& s, const char* path, bool write, int* n
     }
     if (r.ok) resume_body(s, r);
     if (!write && r.ok && fgetc(r.f) != EOF) r.ok = false;
+    // a resumed run starts with the plane-wave switch up (timestepping.F90:1219)
+    if (!write && r.ok) s.still_planewave_time = true;
     fclose(r.f);
     return r.ok ? 0 : 1;
 }

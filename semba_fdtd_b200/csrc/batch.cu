@@ -475,6 +475,7 @@ InstDesc make_desc(const Slot& s, bool active) {
     if (!c->mdisp_on) D.md.n[0] = D.md.n[1] = D.md.n[2] = 0;
     D.src[0] = c->src[0];
     D.src[1] = c->src[1];
+    D.src[0].h_first = D.src[1].h_first = 0;  // an instance runs from step 0
     D.pr = c->probes;
     D.bd = c->border;
     D.tiempo = c->d_tiempo;

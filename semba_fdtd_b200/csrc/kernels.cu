@@ -490,11 +490,19 @@ sgpu_status launch_mdisp(sgpu_ctx* c) { return launch_ade_side<true>(c); }
 constexpr int kMaskPW = 1 << kSrcPlaneWave, kMaskNodal = (1 << kSrcNodalSoft) | (1 << kSrcNodalHard),
               kMaskAll = kMaskPW | kMaskNodal;
 
+// The first half step run fixes where the plane-wave switch starts up.
+void note_first_half(sgpu_ctx* c, int h) {
+    if (c->h_first >= 0) return;
+    c->h_first = h;
+    c->src[0].h_first = c->src[1].h_first = h;
+}
+
 sgpu_status launch_sources(sgpu_ctx* c, int side, StepRef sr, int mask = kMaskAll) {
     if (c->src_dirty) {
         sgpu_status s = build_sources(c);
         if (s) return s;
     }
+    if (!sr.dev_n) note_first_half(c, 2 * sr.n + side);
     const KSrc& k = c->src[side];
     if (k.nrows == 0) return SGPU_OK;
     if (!c->d_tiempo) return set_error(c, SGPU_ERR_STATE, "time vector not set (sgpu_set_time)");
@@ -1174,7 +1182,8 @@ sgpu_status build_sources(sgpu_ctx* c) {
         std::vector<SrcTable> tabs;
         std::vector<float> samples;
         for (const auto& t : c->src_tables) {
-            tabs.push_back(SrcTable{t.numus, t.delta, (int)samples.size(), t.is_pw});
+            tabs.push_back(SrcTable{t.numus, t.delta, (int)samples.size(), t.is_pw, {t.has[0], t.has[1]},
+                                    {t.amax[0], t.amax[1]}});
             samples.insert(samples.end(), t.samples.begin(), t.samples.end());
         }
         KSrc& k = c->src[side];
@@ -1199,6 +1208,8 @@ sgpu_status build_sources(sgpu_ctx* c) {
         k.e = de;
         k.tab = dt;
         k.samples = dsm;
+        k.ntab = (int)tabs.size();
+        k.h_first = c->h_first;
     }
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     c->src_dirty = false;
@@ -1258,6 +1269,10 @@ sgpu_status sgpu_add_planewave(sgpu_ctx* c, const sgpu_planewave_desc* d) {
                             xyz[ax] = d->phys[fl][ax][q];
                         }
                         const float dd = (xyz[0] * d->px + xyz[1] * d->py + xyz[2] * d->pz) - d->d0;
+                        const float a_node = dd / d->cluz;
+                        sgpu_ctx::HostSrcTable& T = c->src_tables[tab];
+                        T.amax[side] = T.has[side] ? std::max(T.amax[side], a_node) : a_node;
+                        T.has[side] = 1;
                         if (c->zslab && (k < c->sweep[P.comp].zi || k > c->sweep[P.comp].ze)) continue;
                         sgpu_ctx::HostEntry he;
                         he.node = lin(c, i, j, k);
@@ -1266,7 +1281,7 @@ sgpu_status sgpu_add_planewave(sgpu_ctx* c, const sgpu_planewave_desc* d) {
                         he.e.comp = P.comp;
                         he.e.type = kSrcPlaneWave;
                         he.e.table = tab;
-                        he.e.a = dd / d->cluz;
+                        he.e.a = a_node;
                         he.e.b = d->fpw[fl];
                         he.e.c = P.sign > 0 ? Id : -Id;
                         c->src_host[side].push_back(he);
@@ -1665,6 +1680,7 @@ sgpu_status sgpu_advance_steps(sgpu_ctx* c, int n0, int count) {
         return set_error(c, SGPU_ERR_ARG, "steps outside the time vector");
     sgpu_status s = note_probe_rows(c, n0, count);
     if (s) return s;
+    note_first_half(c, 2 * n0);
     const int chunk = std::min(count, 32);
     if (!c->graph || c->graph_steps != chunk) {
         if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }

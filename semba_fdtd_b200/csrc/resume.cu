@@ -267,6 +267,16 @@ sgpu_status sgpu_load_resume(sgpu_ctx* c, const char* path, int* last_step) {
     }
     fclose(r.f);
     if (!s && last_step) *last_step = hd.n;
+    if (!s) {
+        // a resumed run starts with the plane-wave switch up
+        // (timestepping.F90:1219): the next half step run is the first
+        c->h_first = -1;
+        c->src[0].h_first = c->src[1].h_first = -1;
+        if (c->graph) {
+            cudaGraphExecDestroy(c->graph);
+            c->graph = nullptr;
+        }
+    }
     return s;
 }
 

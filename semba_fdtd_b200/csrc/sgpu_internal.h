@@ -90,6 +90,11 @@ struct SrcTable {
     float delta;
     int offset;  // into the concatenated samples
     int is_pw;
+    // plane waves: per side (E, H), whether the wave has face nodes there and
+    // the largest d/c over them, taken over the whole problem (a z slab keeps
+    // only its own entries but switches off with the whole domain)
+    int has[2];
+    float amax[2];
 };
 struct KSrc {
     int nrows;
@@ -99,6 +104,8 @@ struct KSrc {
     const SrcEntry* e;
     const SrcTable* tab;
     const float* samples;
+    int ntab;
+    int h_first;           // first half step 2n + side run since the start (or a resume)
 };
 
 // Borders of the H field outside the swept box (local coordinates).
@@ -245,6 +252,8 @@ struct sgpu_ctx {
         int numus;
         float delta;
         int is_pw;
+        int has[2] = {0, 0};
+        float amax[2] = {0.0f, 0.0f};
     };
     std::vector<HostSrcTable> src_tables;
     struct HostEntry {
@@ -258,6 +267,7 @@ struct sgpu_ctx {
     std::vector<void*> src_allocs[2];
     bool src_dirty = true;
     int src_seq = 0;
+    int h_first = -1;  // first half step 2n + side launched (-1: none yet)
     // time
     std::vector<double> h_tiempo;
     int t_n0 = 0;

@@ -474,10 +474,41 @@ __device__ __forceinline__ void ade_node(const AdeRefs& d, long long q) {
 
 __device__ __forceinline__ int step_of(const StepRef& s) { return (s.dev_n ? *s.dev_n : 0) + s.n; }
 
+// Whether one half step of side `side` (0: E, evaluated at time t) keeps the
+// global plane-wave switch up: Incid raises still_planewave_time for every
+// face node whose retarded time is still inside its waveform table, nprev + 1
+// <= numus (planewaves.F90:830-832).  nprev = int((t - d/c) / delta) never
+// decreases with t and never increases with d, so some node of a wave keeps
+// the switch up exactly when its node of largest d/c does.
+__device__ __forceinline__ bool pw_side_active(const KSrc& s, int side, float t) {
+    for (int q = 0; q < s.ntab; ++q) {
+        const SrcTable tb = s.tab[q];
+        if (!tb.is_pw || !tb.has[side]) continue;
+        const long long nprev = (long long)((t - tb.amax[side]) / tb.delta);
+        if (nprev + 1 <= tb.numus) return true;
+    }
+    return false;
+}
+
+// still_planewave_time before half step h = 2n + hside (timestepping.F90:1219,
+// :1251-1267, :1423, :1596): up at the first half step run, then lowered by
+// every AdvancePlaneWaveE/H (planewaves.F90:904, :1204) and raised again by
+// its active nodes, and once down no plane-wave routine runs again.  So it is
+// up iff every half step from h_first to h - 1 kept it up; each side's
+// activity only falls as its time grows, so that is iff the last E half and
+// the last H half before h (those at or after h_first) did.
+__device__ __forceinline__ bool pw_switch_up(const KSrc& s, int n, const double* tiempo, int t_n0, double dt, int hside) {
+    const int mE = hside ? n : n - 1, mH = n - 1;
+    if (2 * mE >= s.h_first && !pw_side_active(s, 0, (float)tiempo[mE - t_n0])) return false;
+    if (2 * mH + 1 >= s.h_first && !pw_side_active(s, 1, (float)(tiempo[mH - t_n0] + (double)0.5f * dt)))
+        return false;
+    return true;
+}
+
 // AdvancePlaneWaveE/H (planewaves.F90:878-1475) with Incid/evolucion
 // (:778-853) and AdvanceNodalE/H (nodalsources.F90:310-777): source row r
 // (one touched node) applies that node's contributions in the reference
-// order.
+// order; plane-wave contributions only while the global switch is up.
 __device__ __forceinline__ void source_row(const KGrid& g, const KSrc& s, int n, const double* tiempo, int t_n0, double dt,
                                            int hside, int mask, int r) {
     const double tn = tiempo[n - t_n0];
@@ -486,12 +517,15 @@ __device__ __forceinline__ void source_row(const KGrid& g, const KSrc& s, int n,
     float* F = g.F[s.row_comp[r]];
     const int node = s.row_node[r];
     float v = F[node];
+    int pw_on = -1;  // the switch, evaluated at the row's first plane-wave entry
     for (int p = s.row_ptr[r]; p < s.row_ptr[r + 1]; ++p) {
         const SrcEntry en = s.e[p];
         if (!((1 << en.type) & mask)) continue;
         const SrcTable tb = s.tab[en.table];
         const float* ev0 = s.samples + tb.offset;
         if (en.type == kSrcPlaneWave) {
+            if (pw_on < 0) pw_on = pw_switch_up(s, n, tiempo, t_n0, dt, hside) ? 1 : 0;
+            if (!pw_on) continue;
             float ev = 0.0f;
             const long long nprev = (long long)((t - en.a) / tb.delta);
             if (nprev + 1 <= tb.numus && nprev > 0)

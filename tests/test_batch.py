@@ -5,6 +5,8 @@ import tempfile
 from pathlib import Path
 
 import numpy as np
+
+from bits import assert_bits_equal
 import pytest
 
 import oracle
@@ -44,9 +46,9 @@ def _check(b, slots, pbs):
     for i, (s, pb) in enumerate(zip(slots, pbs)):
         tr, f = _solo(i, pb)
         assert b.done(s)
-        np.testing.assert_array_equal(b.probes(s), tr, err_msg=f"instance {i}")
+        assert_bits_equal(b.probes(s), tr, err_msg=f"instance {i}")
         for c in range(6):
-            np.testing.assert_array_equal(b.field(s, c), f[c], err_msg=f"instance {i} component {c}")
+            assert_bits_equal(b.field(s, c), f[c], err_msg=f"instance {i} component {c}")
 
 
 @pytest.mark.parametrize("family", [1, 0], ids=["tma", "regs"])
@@ -113,6 +115,6 @@ def test_batch_with_every_border_kind_and_magnetic_ade(family):
         for s, pb in zip(slots, pbs):
             o = oracle.Oracle(pb)
             tr = o.step(pb.nsteps + 1)
-            np.testing.assert_array_equal(b.probes(s), tr, err_msg=pb.name)
+            assert_bits_equal(b.probes(s), tr, err_msg=pb.name)
             for c in range(6):
-                np.testing.assert_array_equal(b.field(s, c), o.field(c), err_msg=f"{pb.name} component {c}")
+                assert_bits_equal(b.field(s, c), o.field(c), err_msg=f"{pb.name} component {c}")

@@ -5,6 +5,8 @@ The oracle restates both on the CPU; the device path must give the oracle's
 surface accumulators bit for bit (-fmad=false build) and its far-field rows
 within a stated tolerance (the transform's sums run in a different order)."""
 import numpy as np
+
+from bits import assert_bits_equal
 import pytest
 
 from cases import disp, small
@@ -135,7 +137,7 @@ def test_surface_dft_bit_exact(decimate):
                 for slot in range(6):
                     got, ref = s.farfield_array(fid, face, slot), o.farfield_array(ofid, face, slot)
                     assert got.shape == ref.shape, (mode, face, slot)
-                    assert np.array_equal(got.view(np.float64), ref.view(np.float64)), (mode, face, slot)
+                    assert_bits_equal(got, ref, err_msg=f"{mode} face {face} slot {slot}")
 
 
 @pytest.mark.gpu

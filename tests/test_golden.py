@@ -8,6 +8,8 @@ import json
 from pathlib import Path
 
 import numpy as np
+
+from bits import assert_bits_equal
 import pytest
 
 from cases import ALL
@@ -31,7 +33,7 @@ def test_oracle_reproduces_golden(name):
     traces, fields = _load()
     pb = ALL[name]()
     o = oracle.Oracle(pb)
-    np.testing.assert_array_equal(o.step(fields[name]["steps"]), traces[name])
+    assert_bits_equal(o.step(fields[name]["steps"]), traces[name])
     assert [_sha(o.field(c)) for c in range(6)] == fields[name]["fields"]
 
 
@@ -43,5 +45,5 @@ def test_gpu_reproduces_golden(name):
     pb = ALL[name]()
     with Solver(pb) as s:
         s.step(fields[name]["steps"])
-        np.testing.assert_array_equal(s.probes(), traces[name])
+        assert_bits_equal(s.probes(), traces[name])
         assert [_sha(s.field(c)) for c in range(6)] == fields[name]["fields"]

@@ -6,6 +6,8 @@ drop-ins, fused half steps, graph-replayed steps) must agree bit for bit;
 the FMA library must stay within 1e-5 relative L2 of the exact one on every
 probe trace that FP32 arithmetic resolves (see the FMA test)."""
 import numpy as np
+
+from bits import assert_bits_equal
 import pytest
 
 from cases import ALL
@@ -40,9 +42,9 @@ def test_bit_exact_against_oracle(name, family):
     with Solver(pb, kernel_family=family) as s:
         gtr = s.run()
         assert gtr.shape == otr.shape
-        np.testing.assert_array_equal(gtr, otr)
+        assert_bits_equal(gtr, otr)
         for c in range(6):
-            np.testing.assert_array_equal(s.field(c), o.field(c), err_msg=f"component {c}")
+            assert_bits_equal(s.field(c), o.field(c), err_msg=f"component {c}")
         assert s.check_finite()
 
 
@@ -56,9 +58,9 @@ def test_stepping_forms_agree(name):
             s.step(steps, mode=mode)
             out[mode] = (s.probes(), [s.field(c) for c in range(6)])
     for mode in ("fused", "graph"):
-        np.testing.assert_array_equal(out[mode][0], out["routines"][0])
+        assert_bits_equal(out[mode][0], out["routines"][0])
         for c in range(6):
-            np.testing.assert_array_equal(out[mode][1][c], out["routines"][1][c])
+            assert_bits_equal(out[mode][1][c], out["routines"][1][c])
 
 
 def _node_scale(pb, tr):
@@ -128,4 +130,4 @@ def test_probe_ring_wraps_and_drains():
     o, otr = _run_oracle(pb, 100)
     with Solver(pb, probe_capacity=16) as s:
         s.step(100)
-        np.testing.assert_array_equal(s.probes(), otr)
+        assert_bits_equal(s.probes(), otr)

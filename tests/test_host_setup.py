@@ -6,6 +6,8 @@ import ctypes as C
 from pathlib import Path
 
 import numpy as np
+
+from bits import assert_bits_equal
 import pytest
 
 from cases import ALL
@@ -48,7 +50,7 @@ def test_host_plan_matches_oracle_setup(name):
         hg = [np.empty(n1, np.float32) for _ in range(4)]
         lib.sgpu_host_get_g(h, *[x.ctypes.data_as(_lib.c_float_p) for x in hg])
         for a, b in zip(hg, o.g_tables()):
-            np.testing.assert_array_equal(a, b)
+            assert_bits_equal(a, b)
         for w in range(18):
             lo, hi = C.c_int(), C.c_int()
             lib.sgpu_host_get_metric(h, w, None, C.byref(lo), C.byref(hi))
@@ -56,7 +58,7 @@ def test_host_plan_matches_oracle_setup(name):
             lib.sgpu_host_get_metric(h, w, arr.ctypes.data_as(_lib.c_float_p), None, None)
             olo, oarr = o.metric(w)
             assert olo == lo.value
-            np.testing.assert_array_equal(arr, oarr)
+            assert_bits_equal(arr, oarr)
         # calc_murconstants per Mur face
         for f in range(6):
             oc = o.mur_cab1(f)
@@ -64,12 +66,12 @@ def test_host_plan_matches_oracle_setup(name):
             rc = lib.sgpu_host_get_mur_cab1(h, f, hc.ctypes.data_as(_lib.c_float_p))
             assert (rc == 0) == (oc is not None)
             if oc is not None:
-                np.testing.assert_array_equal(hc, oc)
+                assert_bits_equal(hc, oc)
         for c in range(6):
             xi, xe, yi, ye, zi, ze = a6[c].tuple()
             m = np.empty((ze - zi + 1, ye - yi + 1, xe - xi + 1), np.int16)
             lib.sgpu_host_get_media(h, c, m.ctypes.data_as(C.POINTER(C.c_int16)))
-            np.testing.assert_array_equal(m, o.media(c).transpose(2, 1, 0))
+            assert_bits_equal(m, o.media(c).transpose(2, 1, 0))
     finally:
         lib.sgpu_destroy(h)
 
@@ -125,11 +127,11 @@ def test_reference_mur_case_plan_matches_oracle():
         for f in range(6):
             hc = np.empty(n1, np.float32)
             assert lib.sgpu_host_get_mur_cab1(h, f, hc.ctypes.data_as(_lib.c_float_p)) == 0
-            np.testing.assert_array_equal(hc, o.mur_cab1(f))
+            assert_bits_equal(hc, o.mur_cab1(f))
         for c in range(6):
             xi, xe, yi, ye, zi, ze = o.alloc[c]
             m = np.empty((ze - zi + 1, ye - yi + 1, xe - xi + 1), np.int16)
             lib.sgpu_host_get_media(h, c, m.ctypes.data_as(C.POINTER(C.c_int16)))
-            np.testing.assert_array_equal(m, o.media(c).transpose(2, 1, 0))
+            assert_bits_equal(m, o.media(c).transpose(2, 1, 0))
     finally:
         lib.sgpu_destroy(h)

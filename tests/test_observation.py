@@ -6,6 +6,8 @@ its own field history and check the host helpers (frequency list, file
 records); GPU tests compare the library's device accumulators and frames
 with the oracle on the same cases."""
 import numpy as np
+
+from bits import assert_bits_equal
 import pytest
 
 from cases import disp, mdisp, small
@@ -62,7 +64,7 @@ def test_oracle_dft_matches_numpy(magnetic):
 
 def test_frequency_list():
     lin = observation.frequency_list(1e9, 2e9, 2.5e8)
-    np.testing.assert_array_equal(lin, np.float32(1e9) + np.arange(5, dtype=np.float32) * np.float32(2.5e8))
+    assert_bits_equal(lin, np.float32(1e9) + np.arange(5, dtype=np.float32) * np.float32(2.5e8))
     assert observation.frequency_list(1e9, 1e9, 0).tolist() == [np.float32(1e9)]
     lg = observation.frequency_list(1e6, 1e9, 1e8, logarithmic=True)
     assert len(lg) == int(np.float32(1e9 - 1e6) / np.float32(1e8)) + 1
@@ -81,8 +83,8 @@ def test_freq_probe_file_records(tmp_path):
     assert len(recs[0]) == 24 and len(recs[1]) == 8 and len(recs[2]) == 4 and len(recs[3]) == 4 * 16
     ijk0, shape, at, fr, v = observation.read_freq_probe(p)
     assert ijk0 == (3, 1, 5) and shape == (4, 3, 2) and at == 1.25e-9
-    np.testing.assert_array_equal(fr, np.float32([1e9, 2e9]))
-    np.testing.assert_array_equal(v, vals)
+    assert_bits_equal(fr, np.float32([1e9, 2e9]))
+    assert_bits_equal(v, vals)
 
 
 @pytest.mark.gpu
@@ -104,7 +106,7 @@ def test_freq_probe_bit_exact(case, magnetic, box, stride):
             pid = s.add_freq_probe(magnetic, box, stride, FREQS)
             s.step(steps, mode=mode)
             got = s.freq_probe(pid, len(FREQS))
-        np.testing.assert_array_equal(got, ref, err_msg=mode)
+        assert_bits_equal(got, ref, err_msg=mode)
     with Solver(pb, variant="fast") as s:
         pid = s.add_freq_probe(magnetic, box, stride, FREQS)
         s.step(steps)
@@ -136,13 +138,13 @@ def test_movie_frames_equal_fields():
         first, fr = s.movie_frames(pid)
         assert first == n_first and len(fr) == 3
         for q in range(3):
-            np.testing.assert_array_equal(fr[q], ref[n_first + q * every])
+            assert_bits_equal(fr[q], ref[n_first + q * every])
         s.step(steps - 20)
         first, fr = s.movie_frames(pid)  # 4 more frames were written; the ring kept the last 3
         kept = sorted(ref)[-3:]
         assert first == kept[0] and len(fr) == 3
         for q, n in enumerate(kept):
-            np.testing.assert_array_equal(fr[q], ref[n])
+            assert_bits_equal(fr[q], ref[n])
 
 
 @pytest.mark.gpu

@@ -5,6 +5,8 @@ import tempfile
 from pathlib import Path
 
 import numpy as np
+
+from bits import assert_bits_equal
 import pytest
 
 import oracle
@@ -28,7 +30,7 @@ def _stream(n=8, seed=7):
 
 def test_poisson_arrivals_are_seeded_and_increasing():
     a, b = poisson_arrivals(100, 5.0, 3), poisson_arrivals(100, 5.0, 3)
-    np.testing.assert_array_equal(a, b)
+    assert_bits_equal(a, b)
     assert np.all(np.diff(a) > 0)
     assert 10.0 < a[-1] < 40.0
 
@@ -44,7 +46,7 @@ def test_served_results_equal_solo_runs():
     assert st.completed == len(reqs) and st.peak_resident >= 2
     for r in reqs:
         want = oracle.Oracle(r.problem).step(r.nsteps + 1)
-        np.testing.assert_array_equal(r.traces, want, err_msg=f"request {r.rid}")
+        assert_bits_equal(r.traces, want, err_msg=f"request {r.rid}")
     s = st.summary()
     assert s["p50_s"] <= s["p99_s"]
 
@@ -56,4 +58,4 @@ def test_plain_baseline_equals_solo_runs():
     assert st.completed == 3
     for r in reqs:
         want = oracle.Oracle(r.problem).step(r.nsteps + 1)
-        np.testing.assert_array_equal(r.traces, want)
+        assert_bits_equal(r.traces, want)

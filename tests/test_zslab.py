@@ -8,6 +8,8 @@ import os
 import socket
 
 import numpy as np
+
+from bits import assert_bits_equal
 import pytest
 
 from cases import disp, mdisp, mixed, mur, small
@@ -104,9 +106,9 @@ def test_zslabs_bit_exact(name, nslabs):
         ref = [s.field(c) for c in range(6)]
     with zslab.ZSlabs(pb, nslabs) as z:
         z.step(steps)
-        np.testing.assert_array_equal(z.probes(), ref_tr)
+        assert_bits_equal(z.probes(), ref_tr)
         for c in range(6):
-            np.testing.assert_array_equal(z.field(c), ref[c], err_msg=f"component {c}")
+            assert_bits_equal(z.field(c), ref[c], err_msg=f"component {c}")
 
 
 @pytest.mark.gpu
