@@ -15,8 +15,9 @@ Under torchrun (N > 1) every rank runs an independent replica on its own GPU
 value is the sum of the replicas' cell updates over that time.
 
 --impl reference times the reference algorithm's CPU implementation (the
-C++ restatement in oracle/, OpenMP over all host cores) on a bounded sample of
-the same workload; the Fortran reference itself cannot be built here.
+C++ restatement in oracle/, OpenMP over all host cores) on the same workload
+(its set-up untimed, a bounded number of whole steps timed); the Fortran
+reference itself cannot be built here.
 """
 from __future__ import annotations
 
@@ -48,7 +49,7 @@ CONFIGS = {
     "served": (None, {}, "Poisson stream (seed 7): edges log-U[48,256], CPML 10, 0-2 pole-residue blocks, soft dipole, "
                          "4-32 probes, steps U{500..4000} x steps_scale"),
 }
-CPU_SAMPLE_N = 160  # the reference arm and cpu_baseline run this scaled sample
+CPU_STEPS = 3  # whole steps of the CPU baseline on the benchmarked case (about 0.5 s each on 16 cores)
 
 
 def env_rank():
@@ -67,6 +68,8 @@ def make_case(config: str, n: int | None, steps_needed: int):
     path = getattr(casegen, gen)(d, **kw)
     pb = read_case(path)
     pb.nsteps = max(pb.nsteps, steps_needed)
+    if n is not None:
+        label = f"{label}; scaled to {n} cells per axis"
     return pb, label
 
 
@@ -84,9 +87,19 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                          "-lms", "100"], stdout=self.out, stderr=subprocess.DEVNULL)
+                                          "-lms", "50"], stdout=self.out, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+        # nvidia-smi takes a moment to start: wait for its first sample so the
+        # (short) timed region that follows is sampled
+        t0 = time.perf_counter()
+        while self.proc and time.perf_counter() - t0 < 5.0:
+            try:
+                if Path(self.out.name).read_text().strip():
+                    break
+            except Exception:
+                pass
+            time.sleep(0.02)
         return self
 
     def __exit__(self, *exc):
@@ -130,38 +143,66 @@ def ncu_traffic(kernel: str):
         return None
 
 
-def cpu_oracle_rate(steps: int, threads: int | None = None, budget_s: float = 20.0):
-    """Gcell-upd/s of the oracle on a bounded sample (scaled dispersive case)."""
+def cpu_model() -> str:
+    try:
+        for ln in Path("/proc/cpuinfo").read_text().splitlines():
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
+def cpu_oracle(pb, steps: int, warmup: int = 0, budget_s: float = 120.0, single_thread_step: bool = True,
+               keep_fields: bool = False):
+    """The oracle (the reference algorithm restated in C++, OpenMP over all
+    host cores) on the benchmarked case itself: set-up untimed, `warmup`
+    untimed steps, then up to `steps` whole steps timed (fewer if they exceed
+    budget_s), then one more step on a single thread.  Returns a dict with
+    the rates, the sample description and (keep_fields) the six fields after
+    the timed steps."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle
-    pb, _ = make_case("dispersive_large", CPU_SAMPLE_N, steps + 2)
-    threads = threads or os.cpu_count() or 1
+    threads = os.cpu_count() or 1
     o = oracle.Oracle(pb, threads=threads)
-    o.step(1)  # warm-up step
-    t0 = time.perf_counter()
-    done = 0
-    while done < steps:
-        o.step(1)
-        done += 1
-        if time.perf_counter() - t0 > budget_s:
-            break
-    dt = time.perf_counter() - t0
-    rate = pb.swept_cells * done / dt / 1e9
-    o.close()
-    sample = f"dispersive case scaled to {CPU_SAMPLE_N}^3 (+CPML: {pb.swept_cells} swept cells), {done} steps, FP32 oracle"
-    return rate, threads, sample
+    try:
+        if warmup:
+            o.step(warmup)
+        t0 = time.perf_counter()
+        done = 0
+        while done < steps:
+            o.step(1)
+            done += 1
+            if time.perf_counter() - t0 > budget_s:
+                break
+        t_all = time.perf_counter() - t0
+        fields = [o.field(c) for c in range(6)] if keep_fields else None
+        rate1 = None
+        if single_thread_step:
+            o.set_threads(1)
+            t1 = time.perf_counter()
+            o.step(1)
+            rate1 = pb.swept_cells / (time.perf_counter() - t1) / 1e9
+    finally:
+        o.close()
+    return {"rate": pb.swept_cells * done / t_all / 1e9, "threads": threads, "steps": done, "warmup": warmup,
+            "rate_1thread": rate1, "cpu_model": cpu_model(), "fields": fields,
+            "sample": f"the benchmarked case itself ({pb.swept_cells} swept cells), {done} whole steps after "
+                      f"{warmup} untimed, set-up untimed, FP32 oracle (-O2, no FMA contraction), OpenMP"}
 
 
 def run_reference(args):
     rank, _, world = env_rank()
     if rank != 0:
         return
-    warm = max(0, args.warmup)
-    rate, cores, sample = cpu_oracle_rate(max(1, args.steps), budget_s=max(30.0, 5.0 * args.steps))
+    pb, label = make_case(args.config, args.n, args.steps + args.warmup + 8)
+    r = cpu_oracle(pb, max(1, args.steps), warmup=min(max(0, args.warmup), 2), budget_s=150.0)
+    rate = r["rate"]
     line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": "Gcell-upd/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": warm, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": CONFIGS["dispersive_large"][2], "sample_n": CPU_SAMPLE_N},
-            "cpu_baseline": {"value": rate, "unit": "Gcell-upd/s", "cores": cores, "kind": "port", "sample": sample},
+            "steps": r["steps"], "warmup": r["warmup"], "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": label, "swept_cells": pb.swept_cells},
+            "cpu_baseline": {"value": rate, "unit": "Gcell-upd/s", "cores": r["threads"], "kind": "port",
+                             "sample": r["sample"], "cpu_model": r["cpu_model"], "value_1thread": r["rate_1thread"]},
             "e2e": {"value": rate, "unit": "Gcell-upd/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -204,7 +245,13 @@ def run_ours(args):
         return float(t.item())
 
     # ---- device-resident throughput ------------------------------------
-    s = Solver(pb, probe_capacity=max(1024, K + W + 8), kernel_family=args.family)
+    s = Solver(pb, probe_capacity=max(1024, K + W + CPU_STEPS + 8), kernel_family=args.family)
+    # the first CPU_STEPS steps are kept for the parity check against the
+    # oracle's run of the same steps (rank 0, not timed)
+    check_fields = None
+    if not args.quick and rank == 0:
+        s.step(CPU_STEPS)
+        check_fields = [s.field(c) for c in range(6)]
     s.step(W)
     s.synchronize()
     ms = C.c_float()
@@ -226,8 +273,10 @@ def run_ours(args):
     if rc:
         raise SystemExit(f"sgpu_profile_steps failed: {lib.sgpu_last_error(s.handle).decode()}")
     s.n += K
+    moved6 = (C.c_double * 6)()
+    lib.sgpu_algorithmic_bytes(s.handle, moved6)
     bytes6 = (C.c_double * 6)()
-    lib.sgpu_algorithmic_bytes(s.handle, bytes6)
+    lib.sgpu_compulsory_bytes(s.handle, bytes6)
     names = ["efield_curl_cpml", "edispersive_ade", "sources_e", "hfield_curl_cpml", "sources_h", "probes"]
     fe, fh = ("k_tma_efield", "k_tma_hfield") if args.family == 1 else ("k_efield", "k_hfield")
     kern = [fe, "k_ade", "k_sources", fh, "k_sources", "k_probes"]
@@ -235,6 +284,7 @@ def run_ours(args):
     dom = int(np.argmax(avg_ms))
     peak, peak_kind = measured_hbm_peak()
     achieved = bytes6[dom] / (avg_ms[dom] * 1e-3) / 1e9 if avg_ms[dom] > 0 else None
+    achieved_moved = moved6[dom] / (avg_ms[dom] * 1e-3) / 1e9 if avg_ms[dom] > 0 else None
     finite = s.check_finite()
     s.close()
 
@@ -247,6 +297,8 @@ def run_ours(args):
             dist.destroy_process_group()
         return
     step_bytes = sum(bytes6[q] for q in range(6))
+    step_moved = sum(moved6[q] for q in range(6))
+    step_s = t_ms / K * 1e-3
     line = {"metric": METRIC, "value": value, "unit": "Gcell-upd/s", "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": t_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
@@ -256,18 +308,32 @@ def run_ours(args):
                               "inputs fit in L2 (fields %.0f MB); no flush between steps" % (cells * 24 / 1e6)),
                        "build": "-fmad=false (bit-exact)",
                        "field_kernels": "TMA-pipelined" if args.family == 1 else "register-marching"},
-            "hbm_frac_step": (step_bytes / (t_ms / K * 1e-3) / 1e9) / peak,
+            "step_roofline": {"bytes": step_bytes, "achieved": step_bytes / step_s / 1e9,
+                              "frac": step_bytes / step_s / 1e9 / peak, "moved_bytes": step_moved,
+                              "frac_moved": step_moved / step_s / 1e9 / peak,
+                              "bytes_definition": "compulsory (sgpu_compulsory_bytes): 60 B per cell + 8 B per psi "
+                                                  "point + (8 + 32 x stored poles) B per pole-residue node; moved "
+                                                  "(sgpu_algorithmic_bytes): what the kernels' design reads and writes"},
             "roofline": {"bound": "hbm", "kernel": kern[dom], "phase": names[dom], "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                          "traffic": ncu_traffic(kern[dom]), "algorithmic_bytes": bytes6[dom],
-                         "avg_ms": avg_ms[dom],
-                         "phases_ms": dict(zip(names, avg_ms)), "phases_bytes": dict(zip(names, list(bytes6)))},
+                         "achieved_moved": achieved_moved, "frac_moved": (achieved_moved / peak) if achieved_moved else None,
+                         "moved_bytes": moved6[dom], "avg_ms": avg_ms[dom],
+                         "phases_ms": dict(zip(names, avg_ms)), "phases_bytes": dict(zip(names, list(bytes6))),
+                         "phases_moved_bytes": dict(zip(names, list(moved6)))},
             "clocks": clk.summary(), "gpu_launches": launches, "finite": finite, "e2e": e2e}
     try:
         if args.quick:
             raise RuntimeError("skipped (--quick)")
-        rate, cores, sample = cpu_oracle_rate(3, budget_s=20.0)
-        line["cpu_baseline"] = {"value": rate, "unit": "Gcell-upd/s", "cores": cores, "kind": "port", "sample": sample}
+        r = cpu_oracle(pb, CPU_STEPS, budget_s=60.0, keep_fields=check_fields is not None)
+        line["cpu_baseline"] = {"value": r["rate"], "unit": "Gcell-upd/s", "cores": r["threads"], "kind": "port",
+                                "sample": r["sample"], "cpu_model": r["cpu_model"], "value_1thread": r["rate_1thread"]}
+        if check_fields is not None and r["fields"] is not None and r["steps"] == CPU_STEPS:
+            same = all(a.shape == b.shape and np.array_equal(a.view(np.uint32), b.view(np.uint32))
+                       for a, b in zip(check_fields, r["fields"]))
+            line["parity"] = {"steps": CPU_STEPS, "fields_bit_equal_to_oracle": bool(same),
+                              "what": "all six fields after the first steps of this run, bit patterns, against the "
+                                      "oracle's run of the same steps (tests/test_parity_full.py covers more steps)"}
     except Exception as ex:  # the baseline is reported, not the target
         line["cpu_baseline"] = {"value": None, "unit": "Gcell-upd/s", "cores": os.cpu_count(), "kind": "port",
                                 "sample": f"failed: {ex}"}
@@ -282,6 +348,7 @@ def run_e2e(pb, K, lib, family):
     from semba_fdtd_b200 import Solver
     t0 = time.perf_counter()
     s = Solver(pb, probe_capacity=max(1024, K + 8), kernel_family=family)
+    t_setup = time.perf_counter()
     h2d = 0
     for c in range(6):
         xi, xe, yi, ye, zi, ze = s.alloc[c]
@@ -297,15 +364,21 @@ def run_e2e(pb, K, lib, family):
         if rc:
             raise SystemExit("upload failed")
         h2d += n * 4
+    t_h2d = time.perf_counter()
     s.step(K)
+    s.synchronize()
+    t_steps = time.perf_counter()
     tr = s.probes()
     d2h = tr.nbytes
     for c in range(6):
         d2h += s.field(c).nbytes
-    t = time.perf_counter() - t0
+    t_end = time.perf_counter()
+    t = t_end - t0
     s.close()
     return {"value": pb.swept_cells * K / t / 1e9, "unit": "Gcell-upd/s", "h2d_bytes_per_step": h2d / K,
             "d2h_bytes_per_step": d2h / K, "seconds": t,
+            "breakdown_s": {"setup_and_media_upload": t_setup - t0, "field_upload": t_h2d - t_setup,
+                            "steps": t_steps - t_h2d, "download": t_end - t_steps},
             "includes": "host set-up, media + initial-field upload, K graph steps, probe and final-field download"}
 
 

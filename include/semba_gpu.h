@@ -177,6 +177,8 @@ sgpu_status sgpu_init_borders(sgpu_ctx* ctx, const sgpu_border_desc* d);
 
 /* crea_timevector (timestepping.F90:3230-3240): tiempo(n0 .. n0+count-1). */
 sgpu_status sgpu_set_time(sgpu_ctx* ctx, int n0, int count, const double* tiempo);
+/* tiempo(n0 .. n0+count-1) of the time vector set last (for output files). */
+sgpu_status sgpu_get_time(const sgpu_ctx* ctx, int n0, int count, double* tiempo);
 
 /* Point probes (observation.F90:2633-2668): comp_ijk holds 4 ints per
  * probe (component, i, j, k).  Values are recorded after every whole step
@@ -290,6 +292,14 @@ sgpu_status sgpu_profile_steps(sgpu_ctx* ctx, int n0, int count, float* ms6);
  * compulsory field/media/psi/ADE-state traffic, without neighbour re-reads
  * or coefficient tables. */
 sgpu_status sgpu_algorithmic_bytes(const sgpu_ctx* ctx, double* bytes6);
+/* The compulsory bytes of the same phases: every field node read and written
+ * once a step with its int16 medium (10 B), every CPML psi point read and
+ * written (8 B), every pole-residue node's previous field and stored
+ * currents read and written (8 B + 32 B per stored pole); the other field's
+ * reads in a half step, neighbour re-reads, node lists and a separate ADE
+ * pass's field re-read are not counted (60 B per cell and step over the six
+ * components, the bound of a kernel that touches each value once). */
+sgpu_status sgpu_compulsory_bytes(const sgpu_ctx* ctx, double* bytes6);
 /* Select the CUDA device this library's runtime uses on the calling thread
  * (call before sgpu_create / sgpu_host_create). */
 sgpu_status sgpu_select_device(int device);
@@ -439,6 +449,13 @@ sgpu_status sgpu_copy_zplane(sgpu_ctx* dst, sgpu_ctx* src, int comp, int z);
 
 /* eps0 and mu0 of the set-up (real(4)), as flush_and_save_resume takes them. */
 sgpu_status sgpu_host_get_constants(const sgpu_ctx* ctx, float* eps0, float* mu0);
+/* The incident-field column of a point-probe file: Incid as
+ * FlushObservationFiles calls it (observation.F90:3826-3875, planewaves.F90:
+ * 778-853), the sum over every plane wave of fpw(comp) * evolucion at the
+ * PhysCoor of component comp at node (i, j, k), at each of the nt real(4)
+ * times t (tiempo(n) for E, tiempo(n) + dt/2 for H); zeros without plane
+ * waves.  Host only; the run's plane-wave switch is not touched. */
+sgpu_status sgpu_host_incident(const sgpu_ctx* ctx, int comp, int i, int j, int k, int nt, const float* t, float* out);
 
 /* Restart files (resuming.F90:213-496).  sgpu_store_resume writes the
  * records flush_and_save_resume writes, in its order: StoreFields (one

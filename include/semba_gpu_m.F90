@@ -269,6 +269,12 @@ module semba_gpu_m
          integer(c_int), value :: n0, count
          type(c_ptr), value :: tiempo        ! c_loc(sgg%tiempo(n0))
       end function sgpu_set_time
+      integer(c_int) function sgpu_get_time(ctx, n0, count, tiempo) bind(C, name="sgpu_get_time")
+         import :: c_int, c_ptr
+         type(c_ptr), value :: ctx
+         integer(c_int), value :: n0, count
+         type(c_ptr), value :: tiempo        ! real(c_double) :: tiempo(count)
+      end function sgpu_get_time
 
       ! ---- observation -----------------------------------------------------
       integer(c_int) function sgpu_set_probes(ctx, nprobes, comp_ijk, capacity_steps) bind(C, name="sgpu_set_probes")
@@ -441,6 +447,11 @@ module semba_gpu_m
          type(c_ptr), value :: ctx
          real(c_double), intent(out) :: bytes6(6)
       end function sgpu_algorithmic_bytes
+      integer(c_int) function sgpu_compulsory_bytes(ctx, bytes6) bind(C, name="sgpu_compulsory_bytes")
+         import :: c_int, c_ptr, c_double
+         type(c_ptr), value :: ctx
+         real(c_double), intent(out) :: bytes6(6)
+      end function sgpu_compulsory_bytes
       integer(c_int) function sgpu_select_device(device) bind(C, name="sgpu_select_device")
          import :: c_int
          integer(c_int), value :: device
@@ -536,6 +547,13 @@ module semba_gpu_m
          type(c_ptr), value :: ctx
          real(c_float), intent(out) :: eps0, mu0
       end function sgpu_host_get_constants
+      integer(c_int) function sgpu_host_incident(ctx, comp, i, j, k, nt, t, out) bind(C, name="sgpu_host_incident")
+         import :: c_int, c_ptr
+         type(c_ptr), value :: ctx
+         integer(c_int), value :: comp, i, j, k, nt
+         type(c_ptr), value :: t             ! real(c_float) :: t(nt)
+         type(c_ptr), value :: out           ! real(c_float) :: out(nt)
+      end function sgpu_host_incident
 
       ! ---- restart files (resuming.F90:213-496) ------------------------------
       integer(c_int) function sgpu_store_resume(ctx, path, last_step, eps0, mu0) bind(C, name="sgpu_store_resume")

@@ -2104,6 +2104,8 @@ int orc_load_resume(void* hv, const char* path, int* last_step) {
     return rc;
 }
 
+void orc_set_threads(void* hv, int nthreads) { ((Handle*)hv)->nthreads = nthreads; }
+
 int orc_run(void* hv, int n0, int n1, float* out) {
     Handle* h = (Handle*)hv;
 #ifdef _OPENMP
@@ -2247,6 +2249,34 @@ long orc_check_div_dt(double dt, long n, unsigned long long seed) {
         if (q != a / dt) ++bad;
     }
     return bad;
+}
+
+// Incid with calledfromobservation (observation.F90:3826-3875 ->
+// planewaves.F90:778-853): the sum over every plane wave of
+// fpw(comp) * evolucion at the node's PhysCoor, with a dummy switch.
+int orc_incident(void* hv, int comp, int i, int j, int k, int nt, const float* t, float* out) {
+    Handle* h = (Handle*)hv;
+    if (h->fp64 || comp < 0 || comp > 5) return 1;
+    Sim<float>& s = *h->sf;
+    const int ijk[3] = {i, j, k};
+    for (int a = 0; a < 3; ++a)
+        if (!s.pws.empty() && (ijk[a] < s.phys_lo[comp][a] || ijk[a] - s.phys_lo[comp][a] >= (int)s.phys[comp][a].size()))
+            return 1;
+    for (int q = 0; q < nt; ++q) {
+        float ehi = 0.0f;
+        for (const PlaneWave<float>& pw : s.pws) {
+            const float xf = s.physc(comp, 0, i), yf = s.physc(comp, 1, j), zf = s.physc(comp, 2, k);
+            const float d = (xf * pw.px + yf * pw.py + zf * pw.pz) - pw.d0;
+            float ev = 0.0f;
+            const long long nprev = (long long)((t[q] - d / s.cluz) / pw.deltaevol);
+            if (nprev + 1 <= pw.numus && nprev > 0)
+                ev = (pw.evol[nprev + 1] - pw.evol[nprev]) / pw.deltaevol * ((t[q] - d / s.cluz) - (float)nprev * pw.deltaevol) +
+                     pw.evol[nprev];
+            ehi = ehi + pw.fpw[comp] * ev;
+        }
+        out[q] = ehi;
+    }
+    return 0;
 }
 
 int orc_get_mur_cab1(void* hv, int face, float* out) {

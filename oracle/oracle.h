@@ -173,6 +173,11 @@ double orc_get_time(void* h, int n);
  * left, right, down, up), num_media+1 values; returns 1 when the face has no
  * Mur condition. */
 int orc_get_mur_cab1(void* h, int face, float* out);
+/* Incid as the observation flush calls it: the incident field of component
+ * comp at node (i, j, k) summed over the plane waves, at nt real(4) times. */
+/* OpenMP threads of the following orc_run calls. */
+void orc_set_threads(void* h, int nthreads);
+int orc_incident(void* h, int comp, int i, int j, int k, int nt, const float* t, float* out);
 /* Checks the library's quotient by dt, RN(q + (a - dt*q)*y) with y = RN(1/dt)
  * and q = RN(a*y) (two FMAs), against IEEE division a/dt for n operands
  * drawn from `seed` over the whole finite exponent range that does not

@@ -112,6 +112,10 @@ def load():
         lib.orc_read_farfield.restype = C.c_int
         lib.orc_farfield_transform.argtypes = [vp, C.c_int, fp, fp, C.c_int, C.POINTER(C.c_double), C.c_int, ip]
         lib.orc_farfield_transform.restype = C.c_int
+        lib.orc_incident.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, fp, fp]
+        lib.orc_incident.restype = C.c_int
+        lib.orc_set_threads.argtypes = [vp, C.c_int]
+        lib.orc_set_threads.restype = None
         _lib = lib
     return _lib
 
@@ -256,6 +260,19 @@ class Oracle:
 
     def time(self, n: int) -> float:
         return self.lib.orc_get_time(self._h, n)
+
+    def set_threads(self, n: int) -> None:
+        """OpenMP threads of the following steps."""
+        self.lib.orc_set_threads(self._h, int(n))
+
+    def incident(self, comp: int, i: int, j: int, k: int, t) -> np.ndarray:
+        """Incid as the observation flush calls it, at the real(4) times t."""
+        tt = np.ascontiguousarray(t, np.float32)
+        out = np.empty(len(tt), np.float32)
+        fp = C.POINTER(C.c_float)
+        if self.lib.orc_incident(self._h, comp, i, j, k, len(tt), tt.ctypes.data_as(fp), out.ctypes.data_as(fp)):
+            raise ValueError("incident field: FP32 oracle and a node inside PhysCoor needed")
+        return out
 
     def store_resume(self, path) -> None:
         """Restart file of the state after the last step run (n = self.n - 1)."""

@@ -134,6 +134,8 @@ def _declare(lib: C.CDLL) -> None:
         "sgpu_copy_zplane": ([vp, vp, C.c_int, C.c_int], C.c_int),
         "sgpu_load_resume": ([vp, C.c_char_p, c_int_p], C.c_int),
         "sgpu_host_get_constants": ([vp, c_float_p, c_float_p], C.c_int),
+        "sgpu_get_time": ([vp, C.c_int, C.c_int, C.POINTER(C.c_double)], C.c_int),
+        "sgpu_host_incident": ([vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, c_float_p, c_float_p], C.c_int),
         "sgpu_add_movie_probe": ([vp, C.POINTER(MovieProbeDesc), c_int_p], C.c_int),
         "sgpu_volume_probe_shape": ([vp, C.c_int, c_int_p, c_int_p, c_int_p, c_int_p], C.c_int),
         "sgpu_read_freq_probe": ([vp, C.c_int, C.POINTER(C.c_double)], C.c_int),
@@ -152,6 +154,7 @@ def _declare(lib: C.CDLL) -> None:
         "sgpu_profile_steps": ([vp, C.c_int, C.c_int, c_float_p], C.c_int),
         "sgpu_kernels_per_step": ([vp, c_int_p], C.c_int),
         "sgpu_algorithmic_bytes": ([vp, c_double_p], C.c_int),
+        "sgpu_compulsory_bytes": ([vp, c_double_p], C.c_int),
         "sgpu_select_device": ([C.c_int], C.c_int),
         "sgpu_set_kernel_family": ([vp, C.c_int], C.c_int),
         "sgpu_scan_nonfinite_noalloc": ([vp, C.c_uint64, vp, C.POINTER(C.c_uint64), C.POINTER(C.c_int64)], C.c_int),

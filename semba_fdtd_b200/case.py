@@ -107,8 +107,14 @@ class Problem:
     nodals: list = field(default_factory=list)
     probes: np.ndarray = field(default_factory=lambda: np.zeros((0, 4), np.int32))
     probe_names: list = field(default_factory=list)
+    # per probe row: (output request name, initialTime, finalTime,
+    # samplingPeriod) of its probe, the times real(4) as smbjson reads them
+    probe_requests: list = field(default_factory=list)
     origin: tuple = (0.0, 0.0, 0.0)
     name: str = "case"
+    # the case file's name without ".json" (nEntradaRoot): output files are
+    # named <root>_<request>_...
+    root: str = "case.fdtd"
     boundary: str = "pml"
     # per face (back, front, left, right, down, up): "pml", "pec", "pmc",
     # "periodic" or "mur"; only "pml" faces carry layers
@@ -362,17 +368,28 @@ def read_case(path: str | Path, search: tuple = ()) -> Problem:
                                          wave=read_waveform(wave_path(s["magnitudeFile"]))))
         else:
             raise ValueError(f"source type {s['type']!r} is outside this path")
-    probes, names = [], []
+    probes, names, requests = [], [], []
     for p in js.get("probes", []):
         if p["type"] != "point":
             continue
         base_c = 0 if p.get("field", "electric") == "electric" else 3
+        # readProbe / getDomain (smbjson.F90:686-730, :1310-1350): the name is
+        # the output request, "_log_" appended for a logarithmic frequency
+        # spacing; the time window defaults to 0 (save every step)
+        dom = p.get("domain", {})
+        req = str(p.get("name", " ")).strip()
+        if dom.get("frequencySpacing", "linear") == "logarithmic":
+            req += "_log_"
+        window = tuple(float(np.float32(dom.get(k, 0.0))) for k in ("initialTime", "finalTime", "samplingPeriod"))
         for eid in p["elementIds"]:
             pos = coords[elems[eid]["coordinateIds"][0]]
             for d in p.get("directions", ["x", "y", "z"]):
                 c = base_c + "xyz".index(d)
                 probes.append([c, int(pos[0]), int(pos[1]), int(pos[2])])
                 names.append(f"{p.get('name', 'probe')}_{'EH'[c // 3]}{d}_{pos[0]}_{pos[1]}_{pos[2]}")
+                requests.append((req,) + window)
     pb.probes = np.asarray(probes, np.int32).reshape(-1, 4)
     pb.probe_names = names
+    pb.probe_requests = requests
+    pb.root = path.name[:-5] if path.name.endswith(".json") else path.name
     return pb

@@ -1235,6 +1235,42 @@ sgpu_status sgpu_host_get_constants(const sgpu_ctx* c, float* eps0, float* mu0) 
     return SGPU_OK;
 }
 
+// Incid as FlushObservationFiles calls it for the incident column of a point
+// probe file (observation.F90:3826-3875 -> planewaves.F90:778-853 with
+// calledfromobservation): EhI = 0, then EhI = EhI + fpw(w, comp) * evolucion
+// over every plane wave w, at the node's PhysCoor of component comp; a dummy
+// flag takes still_planewave_time's place, so the run's switch is untouched.
+sgpu_status sgpu_host_incident(const sgpu_ctx* c, int comp, int i, int j, int k, int nt, const float* t, float* out) {
+    if (!c || !c->host || comp < 0 || comp > 5 || nt < 0 || (nt > 0 && (!t || !out))) return SGPU_ERR_ARG;
+    const HostState* h = (const HostState*)c->host;
+    if (h->pw.empty()) {
+        for (int q = 0; q < nt; ++q) out[q] = 0.0f;
+        return SGPU_OK;
+    }
+    const int ijk[3] = {i, j, k};
+    float xyz[3];
+    for (int a = 0; a < 3; ++a) {
+        const int r = ijk[a] - h->phys_lo[comp][a];
+        if (r < 0 || r >= (int)h->phys[comp][a].size())
+            return sgpu::set_error(const_cast<sgpu_ctx*>(c), SGPU_ERR_ARG, "node outside the PhysCoor range");
+        xyz[a] = h->phys[comp][a][r];
+    }
+    for (int q = 0; q < nt; ++q) {
+        float ehi = 0.0f;
+        for (const sgpu_planewave_desc& d : h->pw) {
+            const float dd = (xyz[0] * d.px + xyz[1] * d.py + xyz[2] * d.pz) - d.d0;
+            float ev = 0.0f;
+            const long long nprev = (long long)((t[q] - dd / d.cluz) / d.deltaevol);
+            if (nprev + 1 <= d.numus && nprev > 0)
+                ev = (d.evol[nprev + 1] - d.evol[nprev]) / d.deltaevol * ((t[q] - dd / d.cluz) - (float)nprev * d.deltaevol) +
+                     d.evol[nprev];
+            ehi = ehi + d.fpw[comp] * ev;
+        }
+        out[q] = ehi;
+    }
+    return SGPU_OK;
+}
+
 // InitFarField (farfield.F90:118-1158) for the descriptor of
 // sgpu_add_farfield.  SINPMLSweep is the SINPML range of one layout.
 sgpu_status sgpu_host_add_farfield(sgpu_ctx* c, const sgpu_farfield_spec* s, int* id) {

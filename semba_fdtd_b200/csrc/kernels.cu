@@ -1353,6 +1353,14 @@ sgpu_status sgpu_set_time(sgpu_ctx* c, int n0, int count, const double* t) {
     return SGPU_OK;
 }
 
+sgpu_status sgpu_get_time(const sgpu_ctx* c, int n0, int count, double* t) {
+    if (!c || count < 0 || (count > 0 && !t)) return SGPU_ERR_ARG;
+    if (n0 < c->t_n0 || (long long)n0 + count > (long long)c->t_n0 + (long long)c->h_tiempo.size())
+        return set_error(const_cast<sgpu_ctx*>(c), SGPU_ERR_ARG, "steps outside the time vector");
+    for (int q = 0; q < count; ++q) t[q] = c->h_tiempo[n0 - c->t_n0 + q];
+    return SGPU_OK;
+}
+
 sgpu_status sgpu_set_probes(sgpu_ctx* c, int np, const int* cijk, int cap) {
     if (!c || np < 0 || (np > 0 && (!cijk || cap <= 0))) return set_error(c, SGPU_ERR_ARG, "bad probe set");
     free_list(c, c->probe_allocs);
@@ -1803,6 +1811,39 @@ sgpu_status sgpu_algorithmic_bytes(const sgpu_ctx* c, double* b6) {
     // and both Past_ values (26 B)
     b6[4] = 8.0 * (double)c->border.cl_cells + 26.0 * (double)c->border.mur_cells +
             (c->mdisp_on ? mnodes * (21.0 + 32.0 * c->mdisp.nu_max) : 0.0);
+    b6[5] = 8.0 * c->probes.n;
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_compulsory_bytes(const sgpu_ctx* c, double* b6) {
+    if (!c || !b6) return SGPU_ERR_ARG;
+    auto cells = [](const sgpu_lim& l) { return (double)(l.xe - l.xi + 1) * (l.ye - l.yi + 1) * (l.ze - l.zi + 1); };
+    auto psi_points = [&](int c0) {
+        double n = 0;
+        for (int f = c0; f < c0 + 3; ++f)
+            for (int w = 0; w < 2; ++w)
+                for (int sd = 0; sd < 2; ++sd) {
+                    const Slab& sl = c->cpml.s[f][w][sd];
+                    if (sl.psi) n += (double)(sl.xhi - sl.xlo + 1) * (sl.yhi - sl.ylo + 1) * (sl.zhi - sl.zlo + 1);
+                }
+        return n;
+    };
+    // Each field node is read and written once a step with its int16 medium
+    // (10 B), each psi point read and written (8 B), each pole-residue node's
+    // previous field read and written (8 B) and each stored current read and
+    // written (32 B); the other component's reads, neighbour re-reads, node
+    // lists and the field re-read of a separate ADE pass are not counted.
+    double e = 0, h = 0, nodes = 0, mnodes = 0;
+    for (int f = 0; f < 3; ++f) e += cells(c->sweep[f]) * 10.0;
+    for (int f = 3; f < 6; ++f) h += cells(c->sweep[f]) * 10.0;
+    for (int comp = 0; comp < 3; ++comp) nodes += (double)c->disp.n[comp];
+    for (int comp = 0; comp < 3; ++comp) mnodes += (double)c->mdisp.n[comp];
+    b6[0] = e + 8.0 * psi_points(0);
+    b6[1] = c->disp_on ? nodes * (8.0 + 32.0 * c->disp.nu_max) : 0.0;
+    b6[2] = 0;
+    b6[3] = h + 8.0 * psi_points(3);
+    b6[4] = 8.0 * (double)c->border.cl_cells + 26.0 * (double)c->border.mur_cells +
+            (c->mdisp_on ? mnodes * (8.0 + 32.0 * c->mdisp.nu_max) : 0.0);
     b6[5] = 8.0 * c->probes.n;
     return SGPU_OK;
 }

@@ -1,5 +1,11 @@
-"""Volume-probe helpers that mirror observation.F90's host side.
+"""Probe output files that mirror observation.F90's host side.
 
+* ``write_point_probes`` -- the text file of every point probe
+  (FlushObservationFiles, observation.F90:3763-3874; names and header,
+  :600-731 and :941-945): one line per saved step with the time, the value
+  and, when the problem has plane waves, the incident field there, in the
+  format '(e27.17e3,11(e19.9e3))' (fdetypes.F90:229);
+* ``fortran_e`` -- the Ew.dEe edit descriptor as gfortran writes it;
 * ``frequency_list`` -- the frequencies of a frequency-domain probe
   (observation.F90:505-536), in real(4) arithmetic as the reference lists
   them;
@@ -8,16 +14,146 @@
   sequential records, each framed by its byte length as a 4-byte integer
   before and after (gfortran's default record markers).
 
-The accumulation itself runs on the device (``Solver.add_freq_probe``).
+The sampling and accumulation run on the device (``Solver.probes``,
+``Solver.add_freq_probe``).
 """
 from __future__ import annotations
 
+import math
 import struct
 from pathlib import Path
 
 import numpy as np
 
-__all__ = ["frequency_list", "write_freq_probe", "read_freq_probe", "fortran_records"]
+__all__ = ["frequency_list", "write_freq_probe", "read_freq_probe", "fortran_records", "fortran_e",
+           "probe_header", "point_probe_paths", "point_probe_rows", "write_point_probes"]
+
+_TINY32 = float(np.finfo(np.float32).tiny)
+_PREFIX = ("Ex_", "Ey_", "Ez_", "Hx_", "Hy_", "Hz_")  # prefix() of observation.F90:4225-4245
+
+
+def fortran_e(x: float, w: int, d: int, e: int = 3) -> str:
+    """``x`` under the Fortran edit descriptor Ew.dEe as gfortran writes it:
+    right-justified in w characters, an optional minus sign (also for -0.0),
+    "0." and d digits of the correctly rounded decimal significand, then "E",
+    the exponent's sign and e digits."""
+    x = float(x)
+    if math.isnan(x):
+        body = "NaN"
+    elif math.isinf(x):
+        body = "Infinity" if x > 0 else "-Infinity"
+    else:
+        neg = math.copysign(1.0, x) < 0
+        a = abs(x)
+        if a == 0.0:
+            digits, ex = "0" * d, 0
+        else:
+            mant, ex10 = f"{a:.{d - 1}e}".split("e")
+            digits, ex = mant.replace(".", ""), int(ex10) + 1
+        body = ("-" if neg else "") + "0." + digits + "E" + ("-" if ex < 0 else "+") + f"{abs(ex):0{e}d}"
+    if len(body) > w:
+        return "*" * w
+    return body.rjust(w)
+
+
+def probe_header(name: str, suffix: str) -> str:
+    """The first line of a probe file (observation.F90:944-945):
+    trim(adjustl(' t' // 14 blanks // name // 7 blanks // suffix)); the
+    suffix of E and H probes is 'incid' with plane waves, else blank."""
+    return (" t" + " " * 14 + name.strip() + " " * 7 + suffix.strip()).strip()
+
+
+def point_probe_paths(problem) -> list:
+    """File name of every point probe row of `problem` (InitObservation,
+    observation.F90:600-731): <root>_<request>_<prefix><i>_<j>_<k>.dat with
+    the prefix of the component (Ex_ .. Hz_); a name already taken by an
+    earlier item gets "_duplicate_<unit>.dat" appended once per earlier
+    match (checkduplicatenames, :2090-2106; units count from 1001)."""
+    paths = []
+    for q, (c, i, j, k) in enumerate(np.asarray(problem.probes).tolist()):
+        req = problem.probe_requests[q][0] if problem.probe_requests else "probe"
+        p = f"{problem.root}_{req}_{_PREFIX[c]}{i}_{j}_{k}.dat"
+        p1 = p
+        for prev in paths:
+            if prev == p1:
+                p = f"{p}_duplicate_{1001 + q}.dat"
+        paths.append(p)
+    return paths
+
+
+def point_probe_rows(problem, q: int, tiempo, dt: float, first_n: int, last_n: int, final_step: int):
+    """Steps n (first_n <= n <= last_n) that probe row q writes, with the
+    time column and the real(4) time of its incident field.
+
+    The window of FlushObservationFiles (observation.F90:3801-3818) after
+    InitObservation's clipping (:268-290): a probe whose finalTime or
+    samplingPeriod is below real(4) TINY saves every step; otherwise it
+    saves the steps with mod(n, max(1, int(samplingPeriod/dt))) = 0 whose
+    time at (tiempo(n), or tiempo(n) + dt/2 for H) lies in [initialTime,
+    finalTime + dt/2], finalTime clipped to tiempo(final_step + 2).  The
+    time column is at for E and at - dt/2 for H."""
+    c = int(problem.probes[q][0])
+    _, t0, t1, ts = problem.probe_requests[q] if problem.probe_requests else ("", 0.0, 0.0, 0.0)
+    f32 = np.float32
+    saveall = f32(t1) < _TINY32 or f32(ts) < _TINY32
+    if saveall:
+        trancos, init, final = 1, f32(0.0), f32(tiempo[final_step + 2])
+    else:
+        trancos = max(1, int(float(f32(ts)) / dt))
+        init = f32(max(0.0, float(f32(t0))))
+        final = f32(min(float(tiempo[final_step + 2]), float(f32(t1))))
+        if final < init:
+            final = init
+    half = dt / 2.0
+    steps, tcol, tinc = [], [], []
+    for n in range(first_n, last_n + 1):
+        if n % trancos:
+            continue
+        at = float(tiempo[n]) + half if c >= 3 else float(tiempo[n])
+        if saveall or (at >= float(init) and at <= float(final) + half):
+            steps.append(n)
+            tcol.append(at - half if c >= 3 else at)
+            tinc.append(at)
+    return steps, np.asarray(tcol, np.float64), np.asarray(tinc, np.float64).astype(np.float32)
+
+
+def write_point_probes(outdir, problem, traces, tiempo, dt: float, first_n: int = 0, final_step: int | None = None,
+                       incident=None) -> list:
+    """Write the point-probe files of a run (FlushObservationFiles,
+    observation.F90:3763-3874, for the steps first_n .. first_n + rows - 1).
+
+    traces: [rows, probes] float32 as ``Solver.probes`` returns them (row r
+    is step first_n + r); tiempo: the FP64 time vector indexed by step
+    (``Solver.time_vector()``), at least to final_step + 2; final_step: the
+    run's last step (default the last row's); incident(comp, i, j, k, t32)
+    gives the incident-field column (``Solver.incident``) and is required
+    when the problem has plane waves.  Each file starts with the header
+    line "t              <name>       incid" ("incid" only with plane
+    waves) and holds one line per saved step.  Returns the paths."""
+    outdir = Path(outdir)
+    outdir.mkdir(parents=True, exist_ok=True)
+    tr = np.asarray(traces, np.float32)
+    last_n = first_n + tr.shape[0] - 1
+    final_step = last_n if final_step is None else final_step
+    with_incid = len(problem.planewaves) >= 1
+    if with_incid and incident is None:
+        raise ValueError("the problem has plane waves: pass incident=Solver.incident (or the oracle's)")
+    out = []
+    for q, name in enumerate(point_probe_paths(problem)):
+        c, i, j, k = (int(v) for v in problem.probes[q])
+        steps, tcol, tinc = point_probe_rows(problem, q, tiempo, dt, first_n, last_n, final_step)
+        vals = tr[np.asarray(steps, np.int64) - first_n, q] if steps else np.zeros(0, np.float32)
+        inc = incident(c, i, j, k, tinc) if with_incid and steps else None
+        lines = [probe_header(name, "incid" if with_incid else "")]
+        for r in range(len(steps)):
+            ln = fortran_e(tcol[r], 27, 17) + fortran_e(vals[r], 19, 9)
+            if with_incid:
+                ln += fortran_e(inc[r], 19, 9)
+            lines.append(ln)
+        path = outdir / name
+        path.write_text("\n".join(lines) + "\n")
+        out.append(path)
+    return out
 
 
 def frequency_list(initial: float, final: float, step: float, logarithmic: bool = False) -> np.ndarray:

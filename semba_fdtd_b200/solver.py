@@ -328,6 +328,23 @@ class Solver:
         rc = self.lib.sgpu_host_get_mur_cab1(self._h, int(face), out.ctypes.data_as(_lib.c_float_p))
         return None if rc else out
 
+    def time_vector(self, n0: int = 0, count: int | None = None) -> np.ndarray:
+        """tiempo(n0 .. n0+count-1), FP64, as the library holds it."""
+        count = self.max_steps + 3 - n0 if count is None else count
+        out = np.empty(count, np.float64)
+        self._check(self.lib.sgpu_get_time(self._h, n0, count, out.ctypes.data_as(C.POINTER(C.c_double))),
+                    "sgpu_get_time")
+        return out
+
+    def incident(self, comp: int, i: int, j: int, k: int, t) -> np.ndarray:
+        """The incident-field column of a point-probe file at node (i, j, k)
+        of component comp, at the real(4) times t (sgpu_host_incident)."""
+        tt = np.ascontiguousarray(t, np.float32)
+        out = np.empty(len(tt), np.float32)
+        self._check(self.lib.sgpu_host_incident(self._h, comp, i, j, k, len(tt), tt.ctypes.data_as(_lib.c_float_p),
+                                                out.ctypes.data_as(_lib.c_float_p)), "sgpu_host_incident")
+        return out
+
     def check_finite(self) -> bool:
         rc = self.lib.sgpu_check_finite(self._h)
         if rc == 5:

@@ -201,13 +201,13 @@ def test_fp32_tracks_fp64():
         assert np.linalg.norm(a[:, q] - b[:, q]) / np.linalg.norm(b[:, q]) < 1e-5
 
 
-REF = Path("/root/reference")
+# the reference's own case, copied by tests/golden/make_reference_fixtures.py
+REF_CASE = Path(__file__).resolve().parent / "golden" / "ref" / "planewave.fdtd.json"
 
 
-@pytest.mark.skipif(not (REF / "testData/cases/planewave.fdtd.json").exists(), reason="reference tree absent")
 def test_reader_matches_reference_parser_fixture():
     """Expected values of test/smbjson/test_read_planewave.F90:24-96."""
-    pb = read_case(REF / "testData/cases/planewave.fdtd.json", search=(REF / "testData/excitations",))
+    pb = read_case(REF_CASE)
     assert pb.dt == pytest.approx(10e-12) and pb.nsteps == 2000
     assert (pb.nx, pb.ny, pb.nz) == (10, 10, 10)
     for d in (pb.desx, pb.desy, pb.desz):
