@@ -311,10 +311,12 @@ sgpu_status sgpu_kernels_per_step(const sgpu_ctx* ctx, int* n);
  * the check (a host whose device memory belongs to its own pool allocator, a
  * service loop that forbids allocation after start-up, a watchdog checking a
  * buffer it does not own).  Counts the NaN/Inf values among the n floats at
- * the device pointer `data` (memory of the calling thread's current device)
- * and returns the count and the index of the first one (-1 when none) in
- * host memory.  `stream` is a cudaStream_t passed as a pointer (NULL: the
- * legacy default stream); the call waits for that stream.
+ * the device pointer `data` and returns the count and the index of the first
+ * one (-1 when none) in host memory.  The scan runs on the device that holds
+ * `data`: the library's runtime switches to it for the call and back, so the
+ * caller's own device selection does not matter.  `stream` is a cudaStream_t
+ * of that device passed as a pointer (NULL: its legacy default stream); the
+ * call waits for that stream.
  *   - n may be at most 268,435,456 (4096 x 65536); larger n returns
  *     SGPU_ERR_SIZE without touching the data.
  *   - Scratch is a file-scope __device__ array of 512 KiB that every device

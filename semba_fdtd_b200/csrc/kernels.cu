@@ -1958,16 +1958,26 @@ extern "C" sgpu_status sgpu_scan_nonfinite_noalloc(const float* data, uint64_t n
     if (n > kScanMaxElems) return SGPU_ERR_SIZE;
     *count = 0;
     *first_index = -1;
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kScanMaxDevices) return SGPU_ERR_CUDA;
     if (n == 0) return SGPU_OK;
     cudaPointerAttributes attr{};
     if (cudaPointerGetAttributes(&attr, data) != cudaSuccess) {
         cudaGetLastError();
         return SGPU_ERR_ARG;
     }
-    if ((attr.type != cudaMemoryTypeDevice && attr.type != cudaMemoryTypeManaged) || attr.device != dev)
-        return SGPU_ERR_ARG;  // not device memory of the calling thread's current device
+    if (attr.type != cudaMemoryTypeDevice && attr.type != cudaMemoryTypeManaged) return SGPU_ERR_ARG;
+    // The scan runs on the device that holds the data, whichever device the
+    // caller's own runtime has selected: this library links the CUDA runtime
+    // statically, so its current device is its own; it switches to the
+    // data's device for the call and back before returning.
+    const int dev = attr.device;
+    if (dev < 0 || dev >= kScanMaxDevices) return SGPU_ERR_ARG;
+    int prev = -1;
+    if (cudaGetDevice(&prev) != cudaSuccess) return SGPU_ERR_CUDA;
+    struct Restore {
+        int d;
+        ~Restore() { if (d >= 0) cudaSetDevice(d); }
+    } restore{prev != dev ? prev : -1};
+    if (prev != dev && cudaSetDevice(dev) != cudaSuccess) return SGPU_ERR_CUDA;
     unsigned long long* scratch = nullptr;
     {
         // once per device, with that device current: the device address of
