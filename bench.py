@@ -249,7 +249,7 @@ def run_ours(args):
     # the first CPU_STEPS steps are kept for the parity check against the
     # oracle's run of the same steps (rank 0, not timed)
     check_fields = None
-    if not args.quick and rank == 0:
+    if not args.quick and not args.skip_cpu and rank == 0:
         s.step(CPU_STEPS)
         check_fields = [s.field(c) for c in range(6)]
     s.step(W)
@@ -323,8 +323,8 @@ def run_ours(args):
                          "phases_moved_bytes": dict(zip(names, list(moved6)))},
             "clocks": clk.summary(), "gpu_launches": launches, "finite": finite, "e2e": e2e}
     try:
-        if args.quick:
-            raise RuntimeError("skipped (--quick)")
+        if args.quick or args.skip_cpu:
+            raise RuntimeError("skipped (--quick / --skip-cpu)")
         r = cpu_oracle(pb, CPU_STEPS, budget_s=60.0, keep_fields=check_fields is not None)
         line["cpu_baseline"] = {"value": r["rate"], "unit": "Gcell-upd/s", "cores": r["threads"], "kind": "port",
                                 "sample": r["sample"], "cpu_model": r["cpu_model"], "value_1thread": r["rate_1thread"]}
@@ -343,27 +343,33 @@ def run_ours(args):
 
 
 def run_e2e(pb, K, lib, family):
-    """Host problem -> device (set-up, media and initial fields from host
-    buffers) -> K steps -> probe traces and final fields back to host."""
-    from semba_fdtd_b200 import Solver
+    """Host problem -> device (set-up, media from the problem description,
+    initial fields from pinned host buffers) -> K steps -> probe traces and
+    final fields back into pinned host buffers."""
+    from semba_fdtd_b200 import Solver, _lib
+    # the caller's host buffers: the initial fields (zeros, a fresh start)
+    # and the final fields, in pinned memory allocated before timing
+    desc, keep = pb.to_desc()
+    plan = C.c_void_p()
+    if lib.sgpu_host_plan(C.byref(desc), 1, C.byref(plan)):
+        raise SystemExit("sgpu_host_plan failed")
+    a6, s6, q6 = (_lib.Lim * 6)(), (_lib.Lim * 6)(), (_lib.Lim * 6)()
+    lib.sgpu_host_info(plan, C.byref(C.c_double()), C.byref(C.c_int()), a6, s6, q6)
+    lib.sgpu_destroy(plan)
+    shapes = [(a.ze - a.zi + 1, a.ye - a.yi + 1, a.xe - a.xi + 1) for a in a6]
+    init = [_lib.pinned_empty(sh, np.float32) for sh in shapes]
+    final = [_lib.pinned_empty(sh, np.float32) for sh in shapes]
+    for a in init + final:
+        a.fill(0.0)
     t0 = time.perf_counter()
     s = Solver(pb, probe_capacity=max(1024, K + 8), kernel_family=family)
     t_setup = time.perf_counter()
     h2d = 0
     for c in range(6):
-        xi, xe, yi, ye, zi, ze = s.alloc[c]
-        n = (xe - xi + 1) * (ye - yi + 1) * (ze - zi + 1)
-        h2d += n * 2  # media matrices uploaded by sgpu_host_create
-    zeros = None
+        h2d += int(np.prod(shapes[c])) * 2  # media matrices uploaded by sgpu_host_create
     for c in range(6):
-        xi, xe, yi, ye, zi, ze = s.alloc[c]
-        n = (xe - xi + 1) * (ye - yi + 1) * (ze - zi + 1)
-        if zeros is None or zeros.size < n:
-            zeros = np.zeros(n, np.float32)
-        rc = lib.sgpu_upload_field(s.handle, c, zeros.ctypes.data_as(C.POINTER(C.c_float)))
-        if rc:
-            raise SystemExit("upload failed")
-        h2d += n * 4
+        s.upload_field(c, init[c])
+        h2d += init[c].nbytes
     t_h2d = time.perf_counter()
     s.step(K)
     s.synchronize()
@@ -371,7 +377,8 @@ def run_e2e(pb, K, lib, family):
     tr = s.probes()
     d2h = tr.nbytes
     for c in range(6):
-        d2h += s.field(c).nbytes
+        s.field(c, out=final[c])
+        d2h += final[c].nbytes
     t_end = time.perf_counter()
     t = t_end - t0
     s.close()
@@ -379,7 +386,8 @@ def run_e2e(pb, K, lib, family):
             "d2h_bytes_per_step": d2h / K, "seconds": t,
             "breakdown_s": {"setup_and_media_upload": t_setup - t0, "field_upload": t_h2d - t_setup,
                             "steps": t_steps - t_h2d, "download": t_end - t_steps},
-            "includes": "host set-up, media + initial-field upload, K graph steps, probe and final-field download"}
+            "includes": "host set-up, media + initial-field upload (fields from pinned host memory), K graph steps, "
+                        "probe and final-field download (into pinned host memory)"}
 
 
 def _stream_batched(n_inst: int, seed: int = 6):
@@ -523,6 +531,7 @@ def main():
     ap.add_argument("--family", type=int, default=1, choices=[0, 1],
                     help="field kernels: 1 TMA-pipelined (default), 0 register-marching")
     ap.add_argument("--quick", action="store_true", help="skip the end-to-end and CPU-baseline legs (profiling runs)")
+    ap.add_argument("--skip-cpu", action="store_true", help="skip the CPU-baseline leg and its parity check")
     ap.add_argument("--instances", type=int, default=64, help="batched: instances in the stream")
     ap.add_argument("--skip-plain", action="store_true", help="batched: leave out the one-at-a-time arm (profiling)")
     ap.add_argument("--batch-order", default="stream", choices=["longest", "stream"],

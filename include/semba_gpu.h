@@ -88,9 +88,15 @@ sgpu_status sgpu_synchronize(sgpu_ctx* ctx);
 /* Media matrices sggMiEx..sggMiHz (int16, -DCompileWithInt2), column-major
  * over alloc[comp]. */
 sgpu_status sgpu_upload_media(sgpu_ctx* ctx, int comp, const int16_t* mi);
-/* Field arrays Ex..Hz, column-major over alloc[comp]. */
+/* Field arrays Ex..Hz, column-major over alloc[comp].  Host arrays the
+ * driver has pinned (sgpu_pinned_alloc, cudaHostAlloc, cudaHostRegister) are
+ * copied directly by the copy engine; others go through the library's
+ * pinned staging buffers. */
 sgpu_status sgpu_upload_field(sgpu_ctx* ctx, int comp, const float* f);
 sgpu_status sgpu_download_field(sgpu_ctx* ctx, int comp, float* f);
+/* Page-locked host memory for such arrays (cudaHostAlloc, portable). */
+sgpu_status sgpu_pinned_alloc(uint64_t bytes, void** out);
+sgpu_status sgpu_pinned_free(void* p);
 
 /* InitCPMLBorders (borderscpml.F90:90-473): the PMLc boxes of the six slab
  * regions per component and the coefficient vectors of calc_cpmlconstants.

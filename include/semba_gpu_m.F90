@@ -231,6 +231,15 @@ module semba_gpu_m
          integer(c_int), value :: comp
          type(c_ptr), value :: f
       end function sgpu_download_field
+      integer(c_int) function sgpu_pinned_alloc(bytes, out) bind(C, name="sgpu_pinned_alloc")
+         import :: c_int, c_ptr, c_int64_t
+         integer(c_int64_t), value :: bytes
+         type(c_ptr), intent(out) :: out     ! c_f_pointer it onto the field array
+      end function sgpu_pinned_alloc
+      integer(c_int) function sgpu_pinned_free(p) bind(C, name="sgpu_pinned_free")
+         import :: c_int, c_ptr
+         type(c_ptr), value :: p
+      end function sgpu_pinned_free
 
       ! ---- set-up of the per-step routines ---------------------------------
       integer(c_int) function sgpu_init_cpml(ctx, d) bind(C, name="sgpu_init_cpml")

@@ -124,6 +124,8 @@ def _declare(lib: C.CDLL) -> None:
         "sgpu_upload_media": ([vp, C.c_int, C.POINTER(C.c_int16)], C.c_int),
         "sgpu_upload_field": ([vp, C.c_int, c_float_p], C.c_int),
         "sgpu_download_field": ([vp, C.c_int, c_float_p], C.c_int),
+        "sgpu_pinned_alloc": ([C.c_uint64, C.POINTER(vp)], C.c_int),
+        "sgpu_pinned_free": ([vp], C.c_int),
         "sgpu_set_time": ([vp, C.c_int, C.c_int, c_double_p], C.c_int),
         "sgpu_set_probes": ([vp, C.c_int, c_int_p, C.c_int], C.c_int),
         "sgpu_read_probes": ([vp, c_float_p, C.c_int, c_int_p, c_int_p], C.c_int),
@@ -202,6 +204,26 @@ def _declare(lib: C.CDLL) -> None:
         f = getattr(lib, name)
         f.argtypes = [vp, C.c_int]
         f.restype = C.c_int
+
+
+def pinned_empty(shape, dtype, variant: str = "exact"):
+    """A numpy array in page-locked host memory (sgpu_pinned_alloc): field
+    uploads and downloads through it go straight to the copy engine.  The
+    memory is freed when the array (and every view of it) is gone."""
+    import weakref
+
+    import numpy as np
+    lib = load(variant)
+    dt = np.dtype(dtype)
+    n = int(np.prod(shape)) * dt.itemsize
+    p = C.c_void_p()
+    rc = lib.sgpu_pinned_alloc(max(n, 1), C.byref(p))
+    if rc:
+        raise SembaGpuError(f"sgpu_pinned_alloc failed ({ERRORS.get(rc, rc)})")
+    buf = (C.c_char * max(n, 1)).from_address(p.value)
+    arr = np.frombuffer(buf, dtype=dt, count=int(np.prod(shape))).reshape(shape)
+    weakref.finalize(buf, lib.sgpu_pinned_free, C.c_void_p(p.value))
+    return arr
 
 
 def exported_symbols(header: Path | None = None) -> list[str]:

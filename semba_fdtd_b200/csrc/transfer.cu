@@ -115,8 +115,30 @@ void host_parallel(long long n, const std::function<void(long long, long long)>&
     for (std::thread& t : th) t.join();
 }
 
+// Host memory the driver has pinned (cudaHostAlloc, cudaHostRegister): the
+// copy engine reaches it directly, so one pitched copy of the whole box
+// replaces the staging.
+bool is_pinned(const void* host) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, host) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+cudaError_t box_direct(void* dev, void* host, size_t es, long long ax, long long ay, long long az, int pitch, long long rows,
+                       cudaStream_t st, bool to_device) {
+    const Chunk all{0, az, 0, ay};
+    const cudaMemcpy3DParms p = pitched(dev, pitch, rows, host, es, ax, all, to_device);
+    const cudaError_t e = cudaMemcpy3DAsync(&p, st);
+    const cudaError_t w = cudaStreamSynchronize(st);
+    return e != cudaSuccess ? e : w;
+}
+
 cudaError_t box_to_device(void* dev, const void* host, size_t es, long long ax, long long ay, long long az, int pitch,
                           long long rows, cudaStream_t st) {
+    if (is_pinned(host)) return box_direct(dev, const_cast<void*>(host), es, ax, ay, az, pitch, rows, st, true);
     Staging& s = staging();
     std::lock_guard<std::mutex> lock(s.mu);
     cudaError_t e = staging_ready(s);
@@ -143,6 +165,7 @@ cudaError_t box_to_device(void* dev, const void* host, size_t es, long long ax, 
 
 cudaError_t box_to_host(void* host, const void* dev, size_t es, long long ax, long long ay, long long az, int pitch,
                         long long rows, cudaStream_t st) {
+    if (is_pinned(host)) return box_direct(const_cast<void*>(dev), host, es, ax, ay, az, pitch, rows, st, false);
     Staging& s = staging();
     std::lock_guard<std::mutex> lock(s.mu);
     cudaError_t e = staging_ready(s);
@@ -173,3 +196,27 @@ cudaError_t box_to_host(void* host, const void* dev, size_t es, long long ax, lo
 }
 
 }  // namespace sgpu
+
+extern "C" {
+
+sgpu_status sgpu_pinned_alloc(uint64_t bytes, void** out) {
+    if (!out) return SGPU_ERR_ARG;
+    *out = nullptr;
+    if (bytes == 0) return SGPU_OK;
+    if (cudaHostAlloc(out, (size_t)bytes, cudaHostAllocPortable) != cudaSuccess) {
+        cudaGetLastError();
+        *out = nullptr;
+        return SGPU_ERR_OOM;
+    }
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_pinned_free(void* p) {
+    if (p && cudaFreeHost(p) != cudaSuccess) {
+        cudaGetLastError();
+        return SGPU_ERR_CUDA;
+    }
+    return SGPU_OK;
+}
+
+}  // extern "C"

@@ -294,13 +294,34 @@ class Solver:
         self._check(self.lib.sgpu_set_kernel_family(self._h, int(family)), "sgpu_set_kernel_family")
 
     # -- data --------------------------------------------------------------
-    def field(self, comp: int) -> np.ndarray:
-        """Field component (0..5) over its Alloc range, Fortran order, as a
-        3-D array indexed [i, j, k] relative to the Alloc lower corner."""
+    def field_shape(self, comp: int) -> tuple:
+        """(nz, ny, nx) of component comp's Alloc box: the C-order shape of
+        the buffers ``field(out=...)`` and ``upload_field`` take."""
         xi, xe, yi, ye, zi, ze = self.alloc[comp]
-        out = np.empty((ze - zi + 1, ye - yi + 1, xe - xi + 1), np.float32)
+        return (ze - zi + 1, ye - yi + 1, xe - xi + 1)
+
+    def field(self, comp: int, out: np.ndarray | None = None) -> np.ndarray:
+        """Field component (0..5) over its Alloc range, Fortran order, as a
+        3-D array indexed [i, j, k] relative to the Alloc lower corner.  `out`
+        (float32, C-contiguous, shape field_shape(comp)) receives the values;
+        a pinned one (``_lib.pinned_empty``) is filled by the copy engine
+        directly."""
+        shape = self.field_shape(comp)
+        if out is None:
+            out = np.empty(shape, np.float32)
+        elif out.shape != shape or out.dtype != np.float32 or not out.flags.c_contiguous:
+            raise ValueError(f"out must be C-contiguous float32 of shape {shape}")
         self._check(self.lib.sgpu_download_field(self._h, comp, out.ctypes.data_as(_lib.c_float_p)), "download")
         return out.transpose(2, 1, 0)
+
+    def upload_field(self, comp: int, values: np.ndarray) -> None:
+        """Set component comp from a C-contiguous float32 array of shape
+        field_shape(comp) ([k][j][i]); pinned arrays go straight to the copy
+        engine."""
+        shape = self.field_shape(comp)
+        if values.shape != shape or values.dtype != np.float32 or not values.flags.c_contiguous:
+            raise ValueError(f"values must be C-contiguous float32 of shape {shape}")
+        self._check(self.lib.sgpu_upload_field(self._h, comp, values.ctypes.data_as(_lib.c_float_p)), "upload")
 
     def media(self, comp: int) -> np.ndarray:
         xi, xe, yi, ye, zi, ze = self.alloc[comp]
