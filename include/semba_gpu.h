@@ -282,6 +282,15 @@ sgpu_status sgpu_advance_steps(sgpu_ctx* ctx, int n0, int count);
  * plain loads.  Both give identical results. */
 sgpu_status sgpu_set_kernel_family(sgpu_ctx* ctx, int family);
 
+/* Bound, in SM clock cycles, of every wait inside the TMA-pipelined kernels
+ * (a consumer waiting for a plane, the producer waiting for a free stage);
+ * default 4e9 (about 2 s).  When a wait runs out the kernel records the
+ * place in an error word, stops, waits (with the default bound) for the
+ * loads it has in flight and exits; the next sgpu_synchronize returns
+ * SGPU_ERR_TIMEOUT and the fields are then undefined.  A failure-detection
+ * test shortens it to make the wait expire without a fault. */
+sgpu_status sgpu_set_wait_cycles(sgpu_ctx* ctx, int64_t cycles);
+
 /* Scans the six field components for NaN/Inf on the device; returns
  * SGPU_ERR_NONFINITE if any is found (the host-side counterpart of the
  * reference's energy/NaN stop, errorreport.F90:1433-1460). */
@@ -530,6 +539,9 @@ sgpu_status sgpu_batch_footprint(const sgpu_ctx* plan, uint64_t* bytes, uint64_t
  * kernels (each instance's tensor maps in global memory), 0 the
  * register-marching kernels.  Both give identical results. */
 sgpu_status sgpu_batch_set_kernel_family(sgpu_batch* b, int family);
+/* The wait bound of sgpu_set_wait_cycles for the batch's pipelined kernels;
+ * sgpu_batch_synchronize reports an expiry as SGPU_ERR_TIMEOUT. */
+sgpu_status sgpu_batch_set_wait_cycles(sgpu_batch* b, int64_t cycles);
 /* Launch shape: z-chunk length (1..64) of the field work items for the three
  * size classes (Alloc z extent <= 80, <= 160, larger) and persistent CTAs per SM.
  * Either may be NULL / 0 to keep the current value. */

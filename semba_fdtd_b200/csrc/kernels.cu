@@ -152,10 +152,11 @@ __device__ __forceinline__ const float* tma_tables(unsigned char* smem, const fl
 }
 
 __global__ void __launch_bounds__(kTmaThreads, 3)
-    k_tma_efield(KGrid g, KCpml cp, const __grid_constant__ TMaps tm, int y0, int z0, int z1, int zchunk, int* err) {
+    k_tma_efield(KGrid g, KCpml cp, const __grid_constant__ TMaps tm, int y0, int z0, int z1, int zchunk, int* err,
+                 long long wait) {
     extern __shared__ __align__(128) unsigned char smem[];
     const float* tab = tma_tables(smem, g.g1, g.g2, g.nmed1);
-    const TmaCta t = tma_cta_setup(smem, y0, z0, z1, zchunk);
+    const TmaCta t = tma_cta_setup(smem, y0, z0, z1, zchunk, wait);
     bool cpml_block = false;
     if (cp.on)
         for (int f = 0; f < 3; ++f)
@@ -179,10 +180,11 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
 }
 
 __global__ void __launch_bounds__(kTmaThreads, 3)
-    k_tma_hfield(KGrid g, KCpml cp, const __grid_constant__ TMaps tm, int y0, int z0, int z1, int zchunk, int* err) {
+    k_tma_hfield(KGrid g, KCpml cp, const __grid_constant__ TMaps tm, int y0, int z0, int z1, int zchunk, int* err,
+                 long long wait) {
     extern __shared__ __align__(128) unsigned char smem[];
     const float* tab = tma_tables(smem, g.gm1, g.gm2, g.nmed1);
-    const TmaCta t = tma_cta_setup(smem, y0, z0, z1, zchunk);
+    const TmaCta t = tma_cta_setup(smem, y0, z0, z1, zchunk, wait);
     bool cpml_block = false;
     if (cp.on)
         for (int f = 3; f < 6; ++f)
@@ -381,9 +383,11 @@ sgpu_status launch_tma(sgpu_ctx* c, bool hside) {
     const int n1 = c->num_media + 1;
     const size_t smem = kTmaSmem + (n1 <= kShTable ? 2 * n1 * sizeof(float) : 0);
     if (hside)
-        k_tma_hfield<<<grid, kTmaThreads, smem, c->stream>>>(kgrid(c), c->cpml, c->tmh, L.y0, L.z0, L.z1, chunk, c->d_err);
+        k_tma_hfield<<<grid, kTmaThreads, smem, c->stream>>>(kgrid(c), c->cpml, c->tmh, L.y0, L.z0, L.z1, chunk, c->d_err,
+                                                             c->wait_cycles);
     else
-        k_tma_efield<<<grid, kTmaThreads, smem, c->stream>>>(kgrid(c), c->cpml, c->tme, L.y0, L.z0, L.z1, chunk, c->d_err);
+        k_tma_efield<<<grid, kTmaThreads, smem, c->stream>>>(kgrid(c), c->cpml, c->tme, L.y0, L.z0, L.z1, chunk, c->d_err,
+                                                             c->wait_cycles);
     return check_launch(c, hside ? "k_tma_hfield" : "k_tma_efield");
 }
 
@@ -788,6 +792,16 @@ sgpu_status sgpu_synchronize(sgpu_ctx* c) {
             CUDA_TRY(c, cudaMemset(c->d_err, 0, sizeof(int)));
             return set_error(c, SGPU_ERR_TIMEOUT, "a bounded wait in a pipelined kernel expired (code " + std::to_string(e) + ")");
         }
+    }
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_set_wait_cycles(sgpu_ctx* c, int64_t cycles) {
+    if (!c || cycles < 0) return set_error(c, SGPU_ERR_ARG, "bad wait budget");
+    c->wait_cycles = cycles;
+    if (c->graph) {  // captured launches carry the old budget
+        cudaGraphExecDestroy(c->graph);
+        c->graph = nullptr;
     }
     return SGPU_OK;
 }

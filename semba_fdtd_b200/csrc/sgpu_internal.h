@@ -296,6 +296,7 @@ struct sgpu_ctx {
     bool tma_ready = false;
     int family = 1;  // 1: TMA-pipelined fused kernels when available, 0: register-marching kernels
     int* d_err = nullptr;
+    long long wait_cycles = 4000000000LL;  // bound of a pipeline wait (clock cycles, ~2 s)
     // a z-slab sub-domain (sgpu_host_create_zslab): sources are kept only on
     // the planes this context sweeps
     bool zslab = false;

@@ -91,11 +91,12 @@ __device__ __forceinline__ bool mbar_try(unsigned a, unsigned parity) {
         : "memory");
     return done != 0;
 }
-// Bounded wait; false (and an error code in *err) when the budget runs out.
-__device__ __forceinline__ bool mbar_wait(unsigned a, unsigned parity, int* err, int code) {
+// Bounded wait; false (and an error code in *err) when `budget` clock
+// cycles run out.
+__device__ __forceinline__ bool mbar_wait(unsigned a, unsigned parity, int* err, int code, long long budget) {
     const long long t0 = clock64();
     while (!mbar_try(a, parity)) {
-        if (clock64() - t0 > kWaitCycles) {
+        if (clock64() - t0 > budget) {
             atomicExch(err, code);
             return false;
         }
@@ -121,11 +122,15 @@ struct TmaCta {
     unsigned full0, empty0;  // shared addresses of the barrier arrays
     int ib, jb, kb, ke;
     int warp, lane;
+    long long wait;  // budget of a pipeline wait (consumers and the producer's
+                     // wait for a free stage); the final drain keeps kWaitCycles
 };
 
-__device__ __forceinline__ TmaCta tma_cta_setup(unsigned char* smem, int y0, int z0, int z1, int zchunk) {
+__device__ __forceinline__ TmaCta tma_cta_setup(unsigned char* smem, int y0, int z0, int z1, int zchunk,
+                                                long long wait) {
     TmaCta t;
     t.ring = smem;
+    t.wait = wait;
     unsigned long long* bars = (unsigned long long*)(smem + kStages * kStageBytes);
     t.full0 = smem_u32(bars);
     t.empty0 = smem_u32(bars + kStages);
@@ -201,7 +206,7 @@ __device__ __forceinline__ int tma_issue(const TmaCta& t, const CUtensorMap* map
     for (int p = p0; p <= p1; ++p) {
         const unsigned G = G0 + (unsigned)(p - p0), s = G % kStages, u = G / kStages;
         const PlaneWords w = tb->w[p - p0];
-        if (u >= 1 && !mbar_wait(t.empty0 + 8 * s, (u - 1) & 1, err, hside ? 13 : 11)) return p - p0;
+        if (u >= 1 && !mbar_wait(t.empty0 + 8 * s, (u - 1) & 1, err, hside ? 13 : 11, t.wait)) return p - p0;
         const unsigned bar = t.full0 + 8 * s;
         unsigned char* st = t.ring + s * kStageBytes;
         const bool part = p == edge;
@@ -261,7 +266,7 @@ __device__ __forceinline__ int tma_issue_warp(const TmaCta& t, const CUtensorMap
         const PlaneWords w = tb->w[p - p0];
         int ok = 1;
         if (q == 0) {
-            if (u >= 1 && !mbar_wait(t.empty0 + 8 * s, (u - 1) & 1, err, hside ? 13 : 11)) {
+            if (u >= 1 && !mbar_wait(t.empty0 + 8 * s, (u - 1) & 1, err, hside ? 13 : 11, t.wait)) {
                 ok = 0;
             } else {
                 if (!part) *(PlaneWords*)(st + kOffW) = w;
@@ -304,13 +309,14 @@ __device__ __forceinline__ float cpml_corr(const Slab (&s)[2], unsigned live2, i
 // (bounded) for the last loads of the `issued` planes numbered 0..issued-1.
 __device__ __forceinline__ void tma_drain(const TmaCta& t, unsigned issued, int* err, int code) {
     const unsigned first = issued > (unsigned)kStages ? issued - kStages : 0;
-    for (unsigned G = first; G < issued; ++G) mbar_wait(t.full0 + 8 * (G % kStages), (G / kStages) & 1, err, code);
+    for (unsigned G = first; G < issued; ++G)
+        mbar_wait(t.full0 + 8 * (G % kStages), (G / kStages) & 1, err, code, kWaitCycles);
 }
 
 // Every lane waits on the barrier (each needs the acquire); the warp then
 // agrees on the outcome so all lanes leave together on a timeout.
-__device__ __forceinline__ bool warp_wait(unsigned bar, unsigned parity, int* err, int code) {
-    const bool ok = mbar_wait(bar, parity, err, code);
+__device__ __forceinline__ bool warp_wait(unsigned bar, unsigned parity, int* err, int code, long long budget) {
+    const bool ok = mbar_wait(bar, parity, err, code, budget);
     return __all_sync(0xffffffffu, ok);
 }
 
@@ -339,8 +345,8 @@ __device__ __forceinline__ bool e_consume(const TmaCta& t, unsigned G0, const KG
     for (int k = t.kb; k <= t.ke; ++k) {
         const unsigned Gk = G0 + 1 + (unsigned)(k - t.kb), Gp = Gk - 1;
         const unsigned s = Gk % kStages, sp = Gp % kStages;
-        if (k == t.kb && !warp_wait(t.full0 + 8 * sp, (Gp / kStages) & 1, err, 2)) return false;
-        if (!warp_wait(t.full0 + 8 * s, (Gk / kStages) & 1, err, 1)) return false;
+        if (k == t.kb && !warp_wait(t.full0 + 8 * sp, (Gp / kStages) & 1, err, 2, t.wait)) return false;
+        if (!warp_wait(t.full0 + 8 * s, (Gk / kStages) & 1, err, 1, t.wait)) return false;
         const unsigned char* st = t.ring + s * kStageBytes;
         // slabs holding cell (i, j, k): the column's slabs that hold plane k;
         // the plane's Idzh and z-indexed P_b / P_c come with the plane
@@ -421,8 +427,8 @@ __device__ __forceinline__ bool h_consume(const TmaCta& t, unsigned G0, const KG
     for (int k = t.kb; k <= t.ke; ++k) {
         const unsigned Gk = G0 + (unsigned)(k - t.kb), Gn = Gk + 1;
         const unsigned s = Gk % kStages, sn = Gn % kStages;
-        if (!warp_wait(t.full0 + 8 * s, (Gk / kStages) & 1, err, 3)) return false;
-        if (!warp_wait(t.full0 + 8 * sn, (Gn / kStages) & 1, err, 4)) return false;
+        if (!warp_wait(t.full0 + 8 * s, (Gk / kStages) & 1, err, 3, t.wait)) return false;
+        if (!warp_wait(t.full0 + 8 * sn, (Gn / kStages) & 1, err, 4, t.wait)) return false;
         const unsigned char* st = t.ring + s * kStageBytes;
         // slabs holding cell (i, j, k), the plane's Idze and P_b / P_c pair
         const PlaneWords pw = *(const PlaneWords*)(st + kOffW);

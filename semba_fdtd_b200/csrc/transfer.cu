@@ -3,12 +3,19 @@
 // The device keeps each component in the padded box of sgpu_internal.h (rows
 // of `pitch` elements, `rows` rows per plane); callers hand over the compact
 // column-major Alloc box (ax x ay x az).  A copy goes in chunks of whole
-// planes (or of rows, when one plane exceeds a chunk) through two pinned
-// staging buffers shared by the process: host threads move one chunk between
-// the caller's array and a staging buffer -- a plain contiguous copy, since a
-// chunk of the compact box is contiguous -- while the copy engine moves the
-// other between the staging buffer and the padded device array with a pitched
-// 3D copy, which does the re-layout.
+// planes (or of rows, when one plane exceeds a chunk).
+//
+// Host to device: the copy engine moves a chunk from pinned host memory with
+// one linear copy into a device staging buffer, and a device-to-device
+// pitched copy then lays it out in the padded array.  (A pitched copy
+// straight from host memory moves rows of a few KB one by one and ran at 16
+// GB/s on B200 against 55 GB/s for the linear one.)  The pinned memory is
+// the caller's array itself when the driver has pinned it, else one of two
+// pinned staging buffers that host threads fill while the engine drains the
+// other.  Device to host: a pitched copy into the caller's pinned array, or
+// into the staging buffers that host threads empty into the caller's array.
+// The staging buffers (2 x 32 MB pinned host memory, 32 MB on each device
+// used) are shared by the process and kept for its life.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -25,9 +32,12 @@ namespace {
 
 constexpr size_t kStageBytes = 32u << 20;
 
+constexpr int kStageDevices = 64;
+
 struct Staging {
     std::mutex mu;
     void* buf[2] = {nullptr, nullptr};
+    void* dev[kStageDevices] = {};  // device staging buffer of each device
 };
 
 Staging& staging() {
@@ -44,6 +54,20 @@ cudaError_t staging_ready(Staging& s) {
                 return e;
             }
         }
+    return cudaSuccess;
+}
+
+// The current device's staging buffer (allocated on first use).
+cudaError_t device_stage(Staging& s, void** out) {
+    int d = 0;
+    cudaError_t e = cudaGetDevice(&d);
+    if (e != cudaSuccess) return e;
+    if (d < 0 || d >= kStageDevices) return cudaErrorInvalidDevice;
+    if (!s.dev[d] && (e = cudaMalloc(&s.dev[d], kStageBytes)) != cudaSuccess) {
+        s.dev[d] = nullptr;
+        return e;
+    }
+    *out = s.dev[d];
     return cudaSuccess;
 }
 
@@ -67,8 +91,10 @@ std::vector<Chunk> chunks(size_t es, long long ax, long long ay, long long az) {
     return v;
 }
 
+// The chunk in a compact buffer (at `stage`, on the host or the device) to
+// or from its place in the padded device array.
 cudaMemcpy3DParms pitched(void* dev, int pitch, long long rows, void* stage, size_t es, long long ax, const Chunk& q,
-                          bool to_device) {
+                          bool to_device, cudaMemcpyKind kind = cudaMemcpyDefault) {
     cudaMemcpy3DParms p{};
     const cudaPitchedPtr d = make_cudaPitchedPtr(dev, (size_t)pitch * es, (size_t)pitch * es, (size_t)rows);
     const cudaPitchedPtr h = make_cudaPitchedPtr(stage, (size_t)ax * es, (size_t)ax * es, (size_t)q.nj);
@@ -85,7 +111,19 @@ cudaMemcpy3DParms pitched(void* dev, int pitch, long long rows, void* stage, siz
         p.kind = cudaMemcpyDeviceToHost;
     }
     p.extent = make_cudaExtent((size_t)ax * es, (size_t)q.nj, (size_t)q.nk);
+    if (kind != cudaMemcpyDefault) p.kind = kind;
     return p;
+}
+
+// One chunk from pinned host memory to its place in the device array: a
+// linear copy into the device staging buffer, then the pitched device copy.
+cudaError_t chunk_to_device(void* dev, const void* pinned, void* dstage, size_t es, long long ax, int pitch, long long rows,
+                            const Chunk& c, cudaStream_t st) {
+    const size_t n = (size_t)c.nk * c.nj * ax * es;
+    cudaError_t e = cudaMemcpyAsync(dstage, pinned, n, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return e;
+    const cudaMemcpy3DParms p = pitched(dev, pitch, rows, dstage, es, ax, c, true, cudaMemcpyDeviceToDevice);
+    return cudaMemcpy3DAsync(&p, st);
 }
 
 void copy_bytes(void* dst, const void* src, size_t n) {
@@ -116,8 +154,8 @@ void host_parallel(long long n, const std::function<void(long long, long long)>&
 }
 
 // Host memory the driver has pinned (cudaHostAlloc, cudaHostRegister): the
-// copy engine reaches it directly, so one pitched copy of the whole box
-// replaces the staging.
+// copy engine reaches it directly, so the library's host staging buffers
+// are not needed.
 bool is_pinned(const void* host) {
     cudaPointerAttributes a{};
     if (cudaPointerGetAttributes(&a, host) != cudaSuccess) {
@@ -127,22 +165,22 @@ bool is_pinned(const void* host) {
     return a.type == cudaMemoryTypeHost;
 }
 
-cudaError_t box_direct(void* dev, void* host, size_t es, long long ax, long long ay, long long az, int pitch, long long rows,
-                       cudaStream_t st, bool to_device) {
-    const Chunk all{0, az, 0, ay};
-    const cudaMemcpy3DParms p = pitched(dev, pitch, rows, host, es, ax, all, to_device);
-    const cudaError_t e = cudaMemcpy3DAsync(&p, st);
-    const cudaError_t w = cudaStreamSynchronize(st);
-    return e != cudaSuccess ? e : w;
-}
-
 cudaError_t box_to_device(void* dev, const void* host, size_t es, long long ax, long long ay, long long az, int pitch,
                           long long rows, cudaStream_t st) {
-    if (is_pinned(host)) return box_direct(dev, const_cast<void*>(host), es, ax, ay, az, pitch, rows, st, true);
     Staging& s = staging();
     std::lock_guard<std::mutex> lock(s.mu);
-    cudaError_t e = staging_ready(s);
+    void* dstage = nullptr;
+    cudaError_t e = device_stage(s, &dstage);
     if (e != cudaSuccess) return e;
+    if (is_pinned(host)) {
+        for (const Chunk& c : chunks(es, ax, ay, az)) {
+            const size_t off = ((size_t)c.k0 * ay + c.j0) * ax * es;
+            if ((e = chunk_to_device(dev, (const char*)host + off, dstage, es, ax, pitch, rows, c, st)) != cudaSuccess) break;
+        }
+        const cudaError_t w = cudaStreamSynchronize(st);
+        return e != cudaSuccess ? e : w;
+    }
+    if ((e = staging_ready(s)) != cudaSuccess) return e;
     cudaEvent_t done[2] = {nullptr, nullptr};
     for (cudaEvent_t& d : done)
         if ((e = cudaEventCreateWithFlags(&d, cudaEventDisableTiming)) != cudaSuccess) break;
@@ -153,8 +191,7 @@ cudaError_t box_to_device(void* dev, const void* host, size_t es, long long ax, 
         const Chunk& c = cs[q];
         const size_t off = ((size_t)c.k0 * ay + c.j0) * ax * es, n = (size_t)c.nk * c.nj * ax * es;
         copy_bytes(s.buf[b], (const char*)host + off, n);
-        const cudaMemcpy3DParms p = pitched(dev, pitch, rows, s.buf[b], es, ax, c, true);
-        if ((e = cudaMemcpy3DAsync(&p, st)) != cudaSuccess) break;
+        if ((e = chunk_to_device(dev, s.buf[b], dstage, es, ax, pitch, rows, c, st)) != cudaSuccess) break;
         e = cudaEventRecord(done[b], st);
     }
     const cudaError_t w = cudaStreamSynchronize(st);  // the staging buffers are free again
@@ -165,7 +202,12 @@ cudaError_t box_to_device(void* dev, const void* host, size_t es, long long ax, 
 
 cudaError_t box_to_host(void* host, const void* dev, size_t es, long long ax, long long ay, long long az, int pitch,
                         long long rows, cudaStream_t st) {
-    if (is_pinned(host)) return box_direct(const_cast<void*>(dev), host, es, ax, ay, az, pitch, rows, st, false);
+    if (is_pinned(host)) {
+        const cudaMemcpy3DParms p = pitched(const_cast<void*>(dev), pitch, rows, host, es, ax, Chunk{0, az, 0, ay}, false);
+        const cudaError_t e = cudaMemcpy3DAsync(&p, st);
+        const cudaError_t w = cudaStreamSynchronize(st);
+        return e != cudaSuccess ? e : w;
+    }
     Staging& s = staging();
     std::lock_guard<std::mutex> lock(s.mu);
     cudaError_t e = staging_ready(s);
