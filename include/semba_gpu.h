@@ -290,6 +290,11 @@ sgpu_status sgpu_set_kernel_family(sgpu_ctx* ctx, int family);
  * SGPU_ERR_TIMEOUT and the fields are then undefined.  A failure-detection
  * test shortens it to make the wait expire without a fault. */
 sgpu_status sgpu_set_wait_cycles(sgpu_ctx* ctx, int64_t cycles);
+/* Failure drill (off by default): while on, the producer warps of the
+ * pipelined field kernels issue no loads, so every consumer wait runs out
+ * after the wait bound and the next synchronize returns SGPU_ERR_TIMEOUT;
+ * nothing is left in flight.  For tests of the timeout path. */
+sgpu_status sgpu_set_wait_drill(sgpu_ctx* ctx, int on);
 
 /* Scans the six field components for NaN/Inf on the device; returns
  * SGPU_ERR_NONFINITE if any is found (the host-side counterpart of the
@@ -542,6 +547,8 @@ sgpu_status sgpu_batch_set_kernel_family(sgpu_batch* b, int family);
 /* The wait bound of sgpu_set_wait_cycles for the batch's pipelined kernels;
  * sgpu_batch_synchronize reports an expiry as SGPU_ERR_TIMEOUT. */
 sgpu_status sgpu_batch_set_wait_cycles(sgpu_batch* b, int64_t cycles);
+/* The failure drill of sgpu_set_wait_drill for the batch's kernels. */
+sgpu_status sgpu_batch_set_wait_drill(sgpu_batch* b, int on);
 /* Launch shape: z-chunk length (1..64) of the field work items for the three
  * size classes (Alloc z extent <= 80, <= 160, larger) and persistent CTAs per SM.
  * Either may be NULL / 0 to keep the current value. */

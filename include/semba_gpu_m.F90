@@ -440,6 +440,11 @@ module semba_gpu_m
          type(c_ptr), value :: ctx
          integer(c_int64_t), value :: cycles
       end function sgpu_set_wait_cycles
+      integer(c_int) function sgpu_set_wait_drill(ctx, on) bind(C, name="sgpu_set_wait_drill")
+         import :: c_int, c_ptr
+         type(c_ptr), value :: ctx
+         integer(c_int), value :: on
+      end function sgpu_set_wait_drill
       integer(c_int) function sgpu_check_finite(ctx) bind(C, name="sgpu_check_finite")
          import :: c_int, c_ptr
          type(c_ptr), value :: ctx
@@ -668,6 +673,11 @@ module semba_gpu_m
          type(c_ptr), value :: b
          integer(c_int64_t), value :: cycles
       end function sgpu_batch_set_wait_cycles
+      integer(c_int) function sgpu_batch_set_wait_drill(b, on) bind(C, name="sgpu_batch_set_wait_drill")
+         import :: c_int, c_ptr
+         type(c_ptr), value :: b
+         integer(c_int), value :: on
+      end function sgpu_batch_set_wait_drill
       integer(c_int) function sgpu_batch_set_tuning(b, chunk3, ctas_per_sm) bind(C, name="sgpu_batch_set_tuning")
          import :: c_int, c_ptr
          type(c_ptr), value :: b

@@ -22,7 +22,7 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 OUT = HERE / "_build"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["kernels.cu", "batch.cu", "host_setup.cpp", "transfer.cu", "resume.cu", "farfield.cu"]
+SOURCES = ["kernels.cu", "batch.cu", "host_setup.cpp", "transfer.cu", "resume.cu", "farfield.cu", "paint.cu"]
 LIBS = {"libsemba_gpu.so": ["-fmad=false"], "libsemba_gpu_fast.so": ["-fmad=true"]}
 
 

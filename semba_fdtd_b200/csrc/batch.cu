@@ -217,7 +217,7 @@ __device__ __forceinline__ void tensormap_acquire(const CUtensorMap* m) {
 template <int SIDE>
 __global__ void __launch_bounds__(kTmaThreads, 3)
     k_batch_tma_field(const InstDesc* __restrict__ descs, const TMaps* __restrict__ maps, const FieldItem* __restrict__ items,
-                      const int* counts, const int* G, int* err, long long wait) {
+                      const int* counts, const int* G, int* err, long long wait, int drill) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ WarpView views[kConsumerWarps];
     __shared__ ProdTable tb;
@@ -242,6 +242,7 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
         const int np = w.ke - w.kb + 2;  // the item's planes, edge plane included
         const int c0 = SIDE == 0 ? 0 : 3;
         if (producer) {
+            if (drill) return;  // a failure drill: no plane arrives, every consumer wait runs out
             // CPML items stage their psi tiles through the ring when the tile's
             // slabs fit the kPsiSlots slots (the consumers derive the same mask)
             const int p0 = SIDE == 0 ? w.kb - 1 : w.kb, p1 = SIDE == 0 ? w.ke : w.ke + 1;
@@ -415,6 +416,7 @@ struct sgpu_batch {
     TMaps* d_maps = nullptr;  // [slot][E side, H side]
     int* d_err = nullptr;     // bounded-wait error word of the TMA kernels
     long long wait_cycles = 4000000000LL;  // bound of a pipeline wait (clock cycles, ~2 s)
+    int wait_drill = 0;                    // failure drill: producers issue no loads
     int* d_counts = nullptr;
     int* d_G = nullptr;
     FieldItem* d_field[2] = {};
@@ -441,6 +443,7 @@ struct sgpu_batch {
     int graph_nu = 0, graph_ctas = 0;
     bool graph_tma = false, graph_border[2] = {}, graph_mnode = false;
     long long graph_wait = -1;
+    int graph_drill = -1;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // instances are set up on their own stream, so host set-up and uploads
     // overlap the steps already queued; the batch stream waits on setup_done
@@ -649,7 +652,7 @@ sgpu_status enqueue_step(sgpu_batch* b, cudaEvent_t* marks = nullptr) {
     };
     if (tma)
         k_batch_tma_field<0><<<tgrid, kTmaThreads, kTmaSmem, b->stream>>>(b->d_desc, b->d_maps, b->d_field[0], b->d_counts,
-                                                                          b->d_G, b->d_err, b->wait_cycles);
+                                                                          b->d_G, b->d_err, b->wait_cycles, b->wait_drill);
     else
         k_batch_field<0><<<grid, blk, 0, b->stream>>>(b->d_desc, b->d_field[0], b->d_counts, b->d_G);
     mark(0);
@@ -659,7 +662,7 @@ sgpu_status enqueue_step(sgpu_batch* b, cudaEvent_t* marks = nullptr) {
     mark(2);
     if (tma)
         k_batch_tma_field<1><<<tgrid, kTmaThreads, kTmaSmem, b->stream>>>(b->d_desc, b->d_maps, b->d_field[1], b->d_counts,
-                                                                          b->d_G, b->d_err, b->wait_cycles);
+                                                                          b->d_G, b->d_err, b->wait_cycles, b->wait_drill);
     else
         k_batch_field<1><<<grid, blk, 0, b->stream>>>(b->d_desc, b->d_field[1], b->d_counts, b->d_G);
     mark(3);
@@ -680,7 +683,7 @@ sgpu_status enqueue_step(sgpu_batch* b, cudaEvent_t* marks = nullptr) {
 sgpu_status ensure_graph(sgpu_batch* b) {
     if (b->graph && b->graph_nu == b->nu_max && b->graph_ctas == b->ctas_per_sm && b->graph_tma == use_tma(b) &&
         b->graph_border[0] == b->any_border[0] && b->graph_border[1] == b->any_border[1] &&
-        b->graph_mnode == b->any_mnode && b->graph_wait == b->wait_cycles)
+        b->graph_mnode == b->any_mnode && b->graph_wait == b->wait_cycles && b->graph_drill == b->wait_drill)
         return SGPU_OK;
     if (b->graph) {
         cudaGraphExecDestroy(b->graph);
@@ -709,6 +712,7 @@ sgpu_status ensure_graph(sgpu_batch* b) {
     b->graph_border[1] = b->any_border[1];
     b->graph_mnode = b->any_mnode;
     b->graph_wait = b->wait_cycles;
+    b->graph_drill = b->wait_drill;
     return SGPU_OK;
 }
 
@@ -888,6 +892,12 @@ sgpu_status sgpu_batch_synchronize(sgpu_batch* b) {
 sgpu_status sgpu_batch_set_wait_cycles(sgpu_batch* b, int64_t cycles) {
     if (!b || cycles < 0) return SGPU_ERR_ARG;
     b->wait_cycles = cycles;
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_batch_set_wait_drill(sgpu_batch* b, int on) {
+    if (!b) return SGPU_ERR_ARG;
+    b->wait_drill = on ? 1 : 0;
     return SGPU_OK;
 }
 

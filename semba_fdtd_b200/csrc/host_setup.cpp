@@ -128,6 +128,14 @@ struct HostState {
     std::vector<int> probes;
     int probe_cap = 1024;
     int max_steps = 0;
+    // media matrices built on the device (sgpu_host_create): the regions to
+    // paint, in painting order, instead of host matrices
+    bool device_media = false;
+    struct PaintRegion {
+        int idx, prio;
+        std::vector<Box> boxes;
+    };
+    std::vector<PaintRegion> paint_regions;
 };
 
 void free_host(void* p) { delete (HostState*)p; }
@@ -206,49 +214,114 @@ void timestep(HostState& h, const sgpu_problem* p) {
     h.dt = dt;
 }
 
-// CreateVolumeMM (healer.F90:66-243): E nodes on the voxel edges take the
-// medium when its priority is higher, H nodes on the faces when it is not
-// lower.
-void paint(HostState& h, const Box& pt, int idx) {
+// The cells CreateVolumeMM (healer.F90:66-243) paints for cell box pt, per
+// component: from the box's lower corner (clipped to the H Alloc ranges) to
+// its upper corner, one further on the axes along which the component sits
+// on voxel edges or faces (clipped likewise).  Empty boxes have hi < lo.
+void paint_ranges(const HostState& h, const Box& pt, Box out[6]) {
     const Box bb{h.alloc[HX].x0, h.alloc[HX].x1, h.alloc[HY].y0, h.alloc[HY].y1, h.alloc[HZ].z0, h.alloc[HZ].z1};
     const int x0 = std::max(pt.x0, bb.x0), y0 = std::max(pt.y0, bb.y0), z0 = std::max(pt.z0, bb.z0);
     const int x1 = std::min(pt.x1, bb.x1 - 1), y1 = std::min(pt.y1, bb.y1 - 1), z1 = std::min(pt.z1, bb.z1 - 1);
     const int X1 = std::min(pt.x1 + 1, bb.x1), Y1 = std::min(pt.y1 + 1, bb.y1), Z1 = std::min(pt.z1 + 1, bb.z1);
-    const int pr = h.med[idx].prio;
     // per component: upper bounds along x, y, z (edge components reach +1)
     const int up[6][3] = {{x1, Y1, Z1}, {X1, y1, Z1}, {X1, Y1, z1}, {X1, y1, z1}, {x1, Y1, z1}, {x1, y1, Z1}};
+    for (int f = 0; f < 6; ++f) out[f] = Box{x0, up[f][0], y0, up[f][1], z0, up[f][2]};
+}
+
+// CreateVolumeMM (healer.F90:66-243): E nodes on the voxel edges take the
+// medium when its priority is higher, H nodes on the faces when it is not
+// lower.
+void paint(HostState& h, const Box& pt, int idx) {
+    Box rg[6];
+    paint_ranges(h, pt, rg);
+    const int pr = h.med[idx].prio;
     for (int f = 0; f < 6; ++f) {
         MediaMat& m = h.mm[f];
         const bool electric = f < 3;
-        const int nk = up[f][2] - z0 + 1;
-        if (nk <= 0 || up[f][1] < y0 || up[f][0] < x0) continue;
-        sgpu::host_parallel(nk, [&, f](long long a, long long e) {
+        const int x0 = rg[f].x0, y0 = rg[f].y0, z0 = rg[f].z0;
+        const int up[3] = {rg[f].x1, rg[f].y1, rg[f].z1};
+        const int nk = up[2] - z0 + 1;
+        if (nk <= 0 || up[1] < y0 || up[0] < x0) continue;
+        sgpu::host_parallel(nk, [&](long long a, long long e) {
             for (int k = z0 + (int)a; k < z0 + (int)e; ++k)
-                for (int j = y0; j <= up[f][1]; ++j)
-                    for (int i = x0; i <= up[f][0]; ++i) {
+                for (int j = y0; j <= up[1]; ++j)
+                    for (int i = x0; i <= up[0]; ++i) {
                         int16_t& cell = m.at(i, j, k);
                         const int cur = h.med[cell].prio;
                         if (electric ? pr > cur : pr >= cur) cell = (int16_t)idx;
                     }
-        }, plane_grain(h.mm[0].size(), up[f][0] - x0 + 1, up[f][1] - y0 + 1));
+        }, plane_grain(h.mm[0].size(), up[0] - x0 + 1, up[1] - y0 + 1));
+    }
+}
+
+// healer.F90:44-50, as [comp][axis] for the lower (in) and upper (on) side
+const int kInLo[6][3] = {{0, 1, 1}, {1, 0, 1}, {1, 1, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+const int kOnHi[6][3] = {{-1, 0, 0}, {0, -1, 0}, {0, 0, -1}, {0, -1, -1}, {-1, 0, -1}, {-1, -1, 0}};
+
+// The boxes of CreatePMLmatrix: the outer (H Alloc) box, the inner box
+// inside the PML, and per component the reach its extrusion covers.
+struct PmlGeom {
+    Box outer, inner, reach[6];
+};
+PmlGeom pml_geom(const HostState& h) {
+    PmlGeom g;
+    g.outer = Box{h.alloc[HX].x0, h.alloc[HX].x1, h.alloc[HY].y0, h.alloc[HY].y1, h.alloc[HZ].z0, h.alloc[HZ].z1};
+    const Box& outer = g.outer;
+    g.inner = Box{std::max(outer.x0, h.sinpml[HX].x0), std::min(outer.x1, h.sinpml[HX].x1),
+                  std::max(outer.y0, h.sinpml[HY].y0), std::min(outer.y1, h.sinpml[HY].y1),
+                  std::max(outer.z0, h.sinpml[HZ].z0), std::min(outer.z1, h.sinpml[HZ].z1)};
+    for (int f = 0; f < 6; ++f)
+        g.reach[f] = Box{std::max(outer.x0, h.full[HX].x0), std::min(outer.x1 + kOnHi[f][0], h.full[HX].x1),
+                         std::max(outer.y0, h.full[HY].y0), std::min(outer.y1 + kOnHi[f][1], h.full[HY].y1),
+                         std::max(outer.z0, h.full[HZ].z0), std::min(outer.z1 + kOnHi[f][2], h.full[HZ].z1)};
+    return g;
+}
+
+// Media copies for the PML (the renumbering of CreatePMLmatrix): the media
+// whose negated entries the shell holds, ordered by first appearance in the
+// sweep (components in order, then k, j, i), become media num_media+1, ...;
+// copy_of maps a medium to its copy.  first[v] < 0: v does not appear.
+void pml_copies(HostState& h, const std::vector<long long>& first, std::vector<int>& copy_of) {
+    std::vector<int> order;
+    for (int v = 1; v <= h.num_media; ++v)
+        if (first[v] >= 0) order.push_back(v);
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return first[a] < first[b]; });
+    copy_of.assign(h.num_media + 1, 0);
+    int next = h.num_media;
+    h.med.resize(h.num_media + 1 + order.size());
+    for (int v : order) {
+        copy_of[v] = ++next;
+        h.med[next] = h.med[v];
+    }
+    h.num_media = next;
+}
+
+// PEC borders (healer.F90:1442-1617): medium 0 on the boundary plane of the
+// E components tangential to a PEC face and the H component normal to it;
+// fn(component, plane box) for each.
+template <class Fn> void pec_planes(const HostState& h, const PmlGeom& g, Fn&& fn) {
+    for (int f = 0; f < 6; ++f) {
+        const bool elec = f < 3;
+        const int own = f % 3;
+        for (int a = 0; a < 3; ++a)
+            for (int sd = 0; sd < 2; ++sd) {
+                if (h.kind[a][sd] != 1 || (elec ? a == own : a != own)) continue;
+                const Box& r = g.reach[f];
+                int lo[3] = {r.x0, r.y0, r.z0}, hi[3] = {r.x1, r.y1, r.z1};
+                lo[a] = hi[a] = sd == 0 ? lo[a] : hi[a];
+                fn(f, Box{lo[0], hi[0], lo[1], hi[1], lo[2], hi[2]});
+            }
     }
 }
 
 // CreatePMLmatrix (healer.F90:961-1420): media reaching the PML interface
 // are extruded across the PML and renumbered as new copies.
 void pml_media(HostState& h) {
-    // healer.F90:44-50, as [comp][axis] for the lower (in) and upper (on) side
-    const int in_lo[6][3] = {{0, 1, 1}, {1, 0, 1}, {1, 1, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
-    const int on_hi[6][3] = {{-1, 0, 0}, {0, -1, 0}, {0, 0, -1}, {0, -1, -1}, {-1, 0, -1}, {-1, -1, 0}};
-    const Box outer{h.alloc[HX].x0, h.alloc[HX].x1, h.alloc[HY].y0, h.alloc[HY].y1, h.alloc[HZ].z0, h.alloc[HZ].z1};
-    const Box inner{std::max(outer.x0, h.sinpml[HX].x0), std::min(outer.x1, h.sinpml[HX].x1),
-                    std::max(outer.y0, h.sinpml[HY].y0), std::min(outer.y1, h.sinpml[HY].y1),
-                    std::max(outer.z0, h.sinpml[HZ].z0), std::min(outer.z1, h.sinpml[HZ].z1)};
-    Box reach[6];
-    for (int f = 0; f < 6; ++f)
-        reach[f] = Box{std::max(outer.x0, h.full[HX].x0), std::min(outer.x1 + on_hi[f][0], h.full[HX].x1),
-                       std::max(outer.y0, h.full[HY].y0), std::min(outer.y1 + on_hi[f][1], h.full[HY].y1),
-                       std::max(outer.z0, h.full[HZ].z0), std::min(outer.z1 + on_hi[f][2], h.full[HZ].z1)};
+    const int (&in_lo)[6][3] = kInLo;
+    const PmlGeom geom = pml_geom(h);
+    const Box& outer = geom.outer;
+    const Box& inner = geom.inner;
+    const Box* reach = geom.reach;
     auto neg = [](int16_t v) { return (int16_t)(-std::abs((int)v)); };
     // the three extrusions in order; within each, planes are independent
     for (int f = 0; f < 6; ++f) {
@@ -335,17 +408,11 @@ void pml_media(HostState& h) {
         std::lock_guard<std::mutex> g(mu);
         for (size_t v = 0; v < mine.size(); ++v) first[v] = std::min(first[v], mine[v]);
     }, plane_grain(h.mm[0].size(), row_cells, 1));
-    std::vector<int> order;
+    std::vector<long long> firsts(h.num_media + 1, -1);
     for (int v = 1; v <= h.num_media; ++v)
-        if (first[v] != kNone) order.push_back(v);
-    std::sort(order.begin(), order.end(), [&](int a, int b) { return first[a] < first[b]; });
-    std::vector<int> copy_of(h.num_media + 1, 0);
-    int next = h.num_media;
-    h.med.resize(h.num_media + 1 + order.size());
-    for (int v : order) {
-        copy_of[v] = ++next;
-        h.med[next] = h.med[v];
-    }
+        if (first[v] != kNone) firsts[v] = first[v];
+    std::vector<int> copy_of;
+    pml_copies(h, firsts, copy_of);
     sgpu::host_parallel((long long)tasks.size(), [&](long long a, long long e) {
         for (long long q = a; q < e; ++q)
             shell_row_spans(tasks[q], [&](int16_t* row, int, int i0, int i1, int) {
@@ -353,24 +420,12 @@ void pml_media(HostState& h) {
                     if (row[i] < 0) row[i] = (int16_t)copy_of[-row[i]];
             });
     }, plane_grain(h.mm[0].size(), row_cells, 1));
-    h.num_media = next;
-    // PEC borders (healer.F90:1442-1617): medium 0 on the boundary plane of
-    // the E components tangential to the face and the H component normal to it
-    for (int f = 0; f < 6; ++f) {
-        const bool elec = f < 3;
-        const int own = f % 3;
-        for (int a = 0; a < 3; ++a)
-            for (int sd = 0; sd < 2; ++sd) {
-                if (h.kind[a][sd] != 1 || (elec ? a == own : a != own)) continue;
-                const Box& r = reach[f];
-                int lo[3] = {r.x0, r.y0, r.z0}, hi[3] = {r.x1, r.y1, r.z1};
-                lo[a] = hi[a] = sd == 0 ? lo[a] : hi[a];
-                MediaMat& m = h.mm[f];
-                for (int k = lo[2]; k <= hi[2]; ++k)
-                    for (int j = lo[1]; j <= hi[1]; ++j)
-                        for (int i = lo[0]; i <= hi[0]; ++i) m.at(i, j, k) = 0;
-            }
-    }
+    pec_planes(h, geom, [&](int f, const Box& b) {
+        MediaMat& m = h.mm[f];
+        for (int k = b.z0; k <= b.z1; ++k)
+            for (int j = b.y0; j <= b.y1; ++j)
+                for (int i = b.x0; i <= b.x1; ++i) m.at(i, j, k) = 0;
+    });
 }
 
 // Media table and matrices of read_geomData (preprocess_geom.F90:421-760,
@@ -387,12 +442,22 @@ void media(HostState& h, const sgpu_problem* p) {
     h.med[1].mur = kMu0 / h.mu0;
     h.med[2].inert = true;  // conformal placeholder
     h.med[3].inert = true;  // split placeholder
-    for (int f = 0; f < 6; ++f) h.mm[f].init(h.alloc[f]);
+    if (!h.device_media)
+        for (int f = 0; f < 6; ++f) h.mm[f].init(h.alloc[f]);
     auto regions_of = [&](int kind, auto&& fn) {
         for (int r = 0; r < p->nregions; ++r)
             if (p->regions[r].kind == kind) fn(r, p->regions[r]);
     };
     auto paint_all = [&](const sgpu_region& g, int idx) {
+        if (h.device_media) {
+            HostState::PaintRegion pr{idx, h.med[idx].prio, {}};
+            for (int b = 0; b < g.nboxes; ++b) {
+                const int* q = g.boxes + 6 * b;
+                pr.boxes.push_back(Box{q[0], q[1], q[2], q[3], q[4], q[5]});
+            }
+            h.paint_regions.push_back(std::move(pr));
+            return;
+        }
         for (int b = 0; b < g.nboxes; ++b) {
             const int* q = g.boxes + 6 * b;
             paint(h, Box{q[0], q[1], q[2], q[3], q[4], q[5]}, idx);
@@ -425,7 +490,7 @@ void media(HostState& h, const sgpu_problem* p) {
         paint_all(g, ++n);
     });
     h.num_media = n;
-    pml_media(h);
+    if (!h.device_media) pml_media(h);
 }
 
 // calc_G1G2Gm1Gm2 (calc_constants.F90:36-148), branches reachable here.
@@ -812,7 +877,7 @@ void nodal(HostState& h, const sgpu_problem* p) {
                 }
 }
 
-HostState* make_plan(const sgpu_problem* p, int max_steps, sgpu_status* rc) {
+HostState* make_plan(const sgpu_problem* p, int max_steps, sgpu_status* rc, bool device_media = false) {
     *rc = SGPU_OK;
     if (!p || p->nx < 2 || p->ny < 2 || p->nz < 2 || !p->desx || !p->desy || !p->desz || max_steps < 0) {
         *rc = SGPU_ERR_ARG;
@@ -833,6 +898,7 @@ HostState* make_plan(const sgpu_problem* p, int max_steps, sgpu_status* rc) {
         }
     HostState* h = new (std::nothrow) HostState();
     if (!h) { *rc = SGPU_ERR_OOM; return nullptr; }
+    h->device_media = device_media;
     try {
         limits(*h, p);
         timestep(*h, p);
@@ -896,7 +962,79 @@ struct ZWindow {
     int z0 = 0, z1 = 0;
 };
 
-sgpu_status realize(HostState* h, sgpu::Arena* arena, cudaStream_t stream, sgpu_ctx** out, ZWindow zw = ZWindow()) {
+// The media matrices of `h` built on the context's device arrays (regions
+// painted in order, the PML extrusion, the copies of the media the PML
+// needs, the PEC borders), then the tables that depend on the final media
+// list (G1..GM2, CAB1, the ADE coefficients, the PEC flags) recomputed and
+// handed to the context.
+sgpu_status build_media_on_device(HostState* h, const sgpu_problem* p, sgpu_ctx* c) {
+    struct Guard {
+        sgpu::DevicePainter* p;
+        ~Guard() { sgpu::painter_delete(p); }
+    } g{sgpu::painter_new(c)};
+    sgpu::DevicePainter* dp = g.p;
+    std::vector<int> prio(h->num_media + 1);
+    for (int m = 0; m <= h->num_media; ++m) prio[m] = h->med[m].prio;
+    sgpu_status s = sgpu::painter_start(dp, prio);
+    if (s) return s;
+    for (const HostState::PaintRegion& r : h->paint_regions) {
+        std::vector<int> items;
+        for (const Box& b : r.boxes) {
+            Box rg[6];
+            paint_ranges(*h, b, rg);
+            for (int f = 0; f < 6; ++f)
+                if (rg[f].x1 >= rg[f].x0 && rg[f].y1 >= rg[f].y0 && rg[f].z1 >= rg[f].z0)
+                    items.insert(items.end(), {f, rg[f].x0, rg[f].x1, rg[f].y0, rg[f].y1, rg[f].z0, rg[f].z1});
+        }
+        if ((s = sgpu::painter_paint(dp, items, r.idx, r.prio))) return s;
+    }
+    // CreatePMLmatrix: extrusion along x, y, z per component
+    const PmlGeom geom = pml_geom(*h);
+    const Box& in = geom.inner;
+    int r6[6][6], in6[6][6];
+    std::vector<long long> task0(6);
+    long long tasks = 0;
+    for (int f = 0; f < 6; ++f) {
+        const Box& r = geom.reach[f];
+        const int v[6] = {r.x0, r.x1, r.y0, r.y1, r.z0, r.z1};
+        const int w[6] = {in.x0, in.x1 + kInLo[f][0] - 1, in.y0, in.y1 + kInLo[f][1] - 1, in.z0, in.z1 + kInLo[f][2] - 1};
+        std::copy(v, v + 6, r6[f]);
+        std::copy(w, w + 6, in6[f]);
+        task0[f] = tasks;
+        tasks += std::max(0, r.z1 - r.z0 + 1);
+        const int lo[3] = {in.x0, in.y0, in.z0};
+        for (int a = 0; a < 3; ++a)
+            if ((s = sgpu::painter_extrude(dp, f, r6[f], a, lo[a], w[2 * a + 1] + 1, lo[a], w[2 * a + 1]))) return s;
+    }
+    const long long nyo = geom.outer.y1 - geom.outer.y0 + 1, nxo = geom.outer.x1 - geom.outer.x0 + 1;
+    std::vector<long long> first;
+    if ((s = sgpu::painter_first(dp, task0, r6, in6, nyo, nxo, h->num_media + 1, first))) return s;
+    std::vector<int> copy_of;
+    const int before = h->num_media;
+    pml_copies(*h, first, copy_of);
+    if (h->num_media > 32767) return sgpu::set_error(c, SGPU_ERR_UNSUPPORTED, "more than 32767 media");
+    std::vector<int16_t> copy16(before + 1);
+    for (int v = 0; v <= before; ++v) copy16[v] = (int16_t)copy_of[v];
+    if ((s = sgpu::painter_relabel(dp, r6, in6, copy16))) return s;
+    pec_planes(*h, geom, [&](int f, const Box& b) {
+        const int b6[6] = {b.x0, b.x1, b.y0, b.y1, b.z0, b.z1};
+        if (!s) s = sgpu::painter_zero(dp, f, b6);
+    });
+    if (s || (s = sgpu::painter_finish(dp))) return s;
+    // the tables over the final media list
+    coefficients(*h);
+    mur_constants(*h);
+    h->didx.clear(); h->dnp.clear(); h->dK.clear(); h->dB.clear(); h->dG.clear();
+    h->mdidx.clear(); h->mdnp.clear(); h->mdK.clear(); h->mdB.clear(); h->mdG.clear();
+    pole_residue(*h, p, false, h->didx, h->dnp, h->dK, h->dB, h->dG);
+    pole_residue(*h, p, true, h->mdidx, h->mdnp, h->mdK, h->mdB, h->mdG);
+    h->pec.resize(h->num_media + 1);
+    for (int m = 0; m <= h->num_media; ++m) h->pec[m] = h->med[m].pec ? 1 : 0;
+    return sgpu::set_media_tables(c, h->num_media, h->g1.data(), h->g2.data(), h->gm1.data(), h->gm2.data(), h->pec.data());
+}
+
+sgpu_status realize(HostState* h, sgpu::Arena* arena, cudaStream_t stream, sgpu_ctx** out, ZWindow zw = ZWindow(),
+                    const sgpu_problem* p = nullptr) {
     Box A[6], W[6];
     for (int f = 0; f < 6; ++f) {
         A[f] = h->alloc[f];
@@ -934,10 +1072,15 @@ sgpu_status realize(HostState* h, sgpu::Arena* arena, cudaStream_t stream, sgpu_
     c->host = h;
     c->host_free = free_host;
     c->zslab = zw.on;
-    for (int f = 0; f < 6; ++f) {
-        const size_t off = (size_t)(A[f].z0 - h->alloc[f].z0) * h->mm[f].nx * h->mm[f].ny;
-        if ((s = sgpu::upload_media(c, f, h->mm[f].data() + off, false))) return s;  // built here: in range
-        h->mm[f].release();  // released once on the device
+    if (h->device_media) {
+        if (!p || zw.on) return sgpu::set_error(c, SGPU_ERR_STATE, "device media need the whole problem");
+        if ((s = build_media_on_device(h, p, c))) return s;
+    } else {
+        for (int f = 0; f < 6; ++f) {
+            const size_t off = (size_t)(A[f].z0 - h->alloc[f].z0) * h->mm[f].nx * h->mm[f].ny;
+            if ((s = sgpu::upload_media(c, f, h->mm[f].data() + off, false))) return s;  // built here: in range
+            h->mm[f].release();  // released once on the device
+        }
     }
     sgpu_cpml_desc cd = h->cd;
     if (zw.on) {
@@ -1024,9 +1167,10 @@ sgpu_status sgpu_host_create(const sgpu_problem* p, int max_steps, sgpu_ctx** ou
     if (!out) return SGPU_ERR_ARG;
     *out = nullptr;
     sgpu_status rc;
-    HostState* h = make_plan(p, max_steps, &rc);
+    // a problem set up alone builds its media matrices on the device
+    HostState* h = make_plan(p, max_steps, &rc, true);
     if (!h) return rc;
-    return realize(h, nullptr, nullptr, out);
+    return realize(h, nullptr, nullptr, out, ZWindow(), p);
 }
 
 sgpu_status sgpu_host_create_zslab(const sgpu_problem* p, int max_steps, int z0, int z1, sgpu_ctx** out) {

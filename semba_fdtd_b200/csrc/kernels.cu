@@ -153,7 +153,7 @@ __device__ __forceinline__ const float* tma_tables(unsigned char* smem, const fl
 
 __global__ void __launch_bounds__(kTmaThreads, 3)
     k_tma_efield(KGrid g, KCpml cp, const __grid_constant__ TMaps tm, int y0, int z0, int z1, int zchunk, int* err,
-                 long long wait) {
+                 long long wait, int drill) {
     extern __shared__ __align__(128) unsigned char smem[];
     const float* tab = tma_tables(smem, g.g1, g.g2, g.nmed1);
     const TmaCta t = tma_cta_setup(smem, y0, z0, z1, zchunk, wait);
@@ -166,6 +166,7 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
     const unsigned tmask = cpml_block ? cpml_tile_mask(cp, 0, t.ib, t.ib + kTX - 1, t.jb, t.jb + kTY - 1) : 0u;
     const unsigned smask = cpml_block ? staged_mask(cp, 0, t.ib, t.jb) : 0u;
     if (t.warp == kConsumerWarps) {
+        if (drill) return;  // a failure drill: no plane arrives, every consumer wait runs out
         __shared__ ProdTable tb;
         prod_prepare(&tb, t, t.kb - 1, t.ke, t.kb - 1, false, g, cp, tmask);
         if (t.lane == 0) tma_drain(t, (unsigned)tma_issue(t, tm.m, 0, t.kb - 1, t.ke, t.kb - 1, false, err, &tb, smask), err, 12);
@@ -181,7 +182,7 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
 
 __global__ void __launch_bounds__(kTmaThreads, 3)
     k_tma_hfield(KGrid g, KCpml cp, const __grid_constant__ TMaps tm, int y0, int z0, int z1, int zchunk, int* err,
-                 long long wait) {
+                 long long wait, int drill) {
     extern __shared__ __align__(128) unsigned char smem[];
     const float* tab = tma_tables(smem, g.gm1, g.gm2, g.nmed1);
     const TmaCta t = tma_cta_setup(smem, y0, z0, z1, zchunk, wait);
@@ -194,6 +195,7 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
     const unsigned tmask = cpml_block ? cpml_tile_mask(cp, 3, t.ib, t.ib + kTX - 1, t.jb, t.jb + kTY - 1) : 0u;
     const unsigned smask = cpml_block ? staged_mask(cp, 3, t.ib, t.jb) : 0u;
     if (t.warp == kConsumerWarps) {
+        if (drill) return;  // a failure drill: no plane arrives, every consumer wait runs out
         __shared__ ProdTable tb;
         prod_prepare(&tb, t, t.kb, t.ke + 1, t.ke + 1, true, g, cp, tmask);
         if (t.lane == 0) tma_drain(t, (unsigned)tma_issue(t, tm.m, 0, t.kb, t.ke + 1, t.ke + 1, true, err, &tb, smask), err, 14);
@@ -384,10 +386,10 @@ sgpu_status launch_tma(sgpu_ctx* c, bool hside) {
     const size_t smem = kTmaSmem + (n1 <= kShTable ? 2 * n1 * sizeof(float) : 0);
     if (hside)
         k_tma_hfield<<<grid, kTmaThreads, smem, c->stream>>>(kgrid(c), c->cpml, c->tmh, L.y0, L.z0, L.z1, chunk, c->d_err,
-                                                             c->wait_cycles);
+                                                             c->wait_cycles, c->wait_drill);
     else
         k_tma_efield<<<grid, kTmaThreads, smem, c->stream>>>(kgrid(c), c->cpml, c->tme, L.y0, L.z0, L.z1, chunk, c->d_err,
-                                                             c->wait_cycles);
+                                                             c->wait_cycles, c->wait_drill);
     return check_launch(c, hside ? "k_tma_hfield" : "k_tma_efield");
 }
 
@@ -806,6 +808,16 @@ sgpu_status sgpu_set_wait_cycles(sgpu_ctx* c, int64_t cycles) {
     return SGPU_OK;
 }
 
+sgpu_status sgpu_set_wait_drill(sgpu_ctx* c, int on) {
+    if (!c) return SGPU_ERR_ARG;
+    c->wait_drill = on ? 1 : 0;
+    if (c->graph) {
+        cudaGraphExecDestroy(c->graph);
+        c->graph = nullptr;
+    }
+    return SGPU_OK;
+}
+
 sgpu_status sgpu_set_kernel_family(sgpu_ctx* c, int family) {
     if (!c || family < 0 || family > 1) return SGPU_ERR_ARG;
     if (family == 1 && !c->tma_ready) return set_error(c, SGPU_ERR_UNSUPPORTED, "TMA tensor maps unavailable");
@@ -820,6 +832,28 @@ sgpu_status sgpu_set_kernel_family(sgpu_ctx* c, int family) {
 sgpu_status sgpu_upload_media(sgpu_ctx* c, int comp, const int16_t* mi) { return sgpu::upload_media(c, comp, mi, true); }
 
 }  // extern "C"
+
+sgpu_status sgpu::set_media_tables(sgpu_ctx* c, int num_media, const float* g1, const float* g2, const float* gm1,
+                                   const float* gm2, const uint8_t* is_pec) {
+    if (!c || num_media < 0 || !g1 || !g2 || !gm1 || !gm2 || !is_pec) return set_error(c, SGPU_ERR_ARG, "bad media tables");
+    const int n1 = num_media + 1;
+    float** dv[4] = {&c->g1, &c->g2, &c->gm1, &c->gm2};
+    const float* src[4] = {g1, g2, gm1, gm2};
+    std::vector<float>* hv[4] = {&c->h_g1, &c->h_g2, &c->h_gm1, &c->h_gm2};
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    for (int q = 0; q < 4; ++q) {
+        dev_free(c, *dv[q]);
+        *dv[q] = nullptr;
+        sgpu_status s = dalloc(c, dv[q], n1);
+        if (s) return s;
+        if ((s = h2d(c, *dv[q], src[q], n1))) return s;
+        hv[q]->assign(src[q], src[q] + n1);
+    }
+    c->h_pec.assign(is_pec, is_pec + n1);
+    c->num_media = num_media;
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return SGPU_OK;
+}
 
 sgpu_status sgpu::upload_media(sgpu_ctx* c, int comp, const int16_t* mi, bool check) {
     if (!c || !mi || comp < 0 || comp > 5) return set_error(c, SGPU_ERR_ARG, "bad media upload");

@@ -297,6 +297,7 @@ struct sgpu_ctx {
     int family = 1;  // 1: TMA-pipelined fused kernels when available, 0: register-marching kernels
     int* d_err = nullptr;
     long long wait_cycles = 4000000000LL;  // bound of a pipeline wait (clock cycles, ~2 s)
+    int wait_drill = 0;                    // failure drill: producers issue no loads
     // a z-slab sub-domain (sgpu_host_create_zslab): sources are kept only on
     // the planes this context sweeps
     bool zslab = false;
@@ -334,6 +335,25 @@ cudaError_t box_to_device(void* dev, const void* host, size_t es, long long ax, 
                           long long rows, cudaStream_t st);
 cudaError_t box_to_host(void* host, const void* dev, size_t es, long long ax, long long ay, long long az, int pitch,
                         long long rows, cudaStream_t st);
+// Replace the context's medium count and coefficient tables (before the
+// first launch): the level-2 host learns the final count only after the
+// media matrices are built on the device.
+sgpu_status set_media_tables(sgpu_ctx* c, int num_media, const float* g1, const float* g2, const float* gm1,
+                             const float* gm2, const uint8_t* is_pec);
+// Media matrices built on the device (paint.cu); coordinates absolute,
+// boxes inclusive as {x0, x1, y0, y1, z0, z1}.
+struct DevicePainter;
+DevicePainter* painter_new(sgpu_ctx* c);
+void painter_delete(DevicePainter* p);
+sgpu_status painter_start(DevicePainter* p, const std::vector<int>& prio);
+sgpu_status painter_paint(DevicePainter* p, const std::vector<int>& items7, int idx, int pr);
+sgpu_status painter_extrude(DevicePainter* p, int f, const int* r6, int axis, int lo_end, int hi_beg, int lo_src,
+                            int hi_src);
+sgpu_status painter_first(DevicePainter* p, const std::vector<long long>& task0, const int (*r6)[6], const int (*in6)[6],
+                          long long nyo, long long nxo, int nmed1, std::vector<long long>& first);
+sgpu_status painter_relabel(DevicePainter* p, const int (*r6)[6], const int (*in6)[6], const std::vector<int16_t>& copy_of);
+sgpu_status painter_zero(DevicePainter* p, int f, const int* b6);
+sgpu_status painter_finish(DevicePainter* p);
 // fn(lo, hi) over [0, n) split across up to 8 host threads, each taking at
 // least `grain` units.
 void host_parallel(long long n, const std::function<void(long long, long long)>& fn, long long grain = 2048);

@@ -4,11 +4,12 @@ Every wait inside the TMA-pipelined field kernels (a consumer warp waiting
 for a plane, the producer waiting for a free ring stage) is bounded; when a
 bound runs out the kernel records where in an error word, stops, waits with
 the default bound for the loads it still has in flight, and exits, and the
-next synchronize reports SGPU_ERR_TIMEOUT.  Here the bound is set to zero
-cycles (sgpu_set_wait_cycles), so the first wait for a plane that has not
-landed expires: no wait is endless, nothing faults, and the error path runs.
-The loads in flight always complete (they read the context's own arrays),
-so the final drain ends by itself."""
+next synchronize reports SGPU_ERR_TIMEOUT.  The failure drill
+(sgpu_set_wait_drill) makes the producer warps issue no loads, so no plane
+ever arrives -- a flag nothing sets -- and with a short bound
+(sgpu_set_wait_cycles, 2e5 cycles, about 0.1 ms) every consumer wait runs
+out: no wait is endless, nothing is in flight, nothing faults, and the error
+path runs."""
 import tempfile
 from pathlib import Path
 
@@ -25,22 +26,28 @@ import oracle
 pytestmark = pytest.mark.gpu
 
 SGPU_ERR_TIMEOUT = 6
+SHORT = 200_000  # clock cycles, about 0.1 ms
 
 
 def test_expired_wait_reports_timeout_then_a_fresh_context_runs():
     pb = small()
     with Solver(pb, kernel_family=1) as s:
         lib = s.lib
-        assert lib.sgpu_set_wait_cycles(s.handle, 0) == 0
+        assert lib.sgpu_set_wait_cycles(s.handle, SHORT) == 0
+        assert lib.sgpu_set_wait_drill(s.handle, 1) == 0
         assert lib.sgpu_advance_e(s.handle, 0) == 0
         rc = lib.sgpu_synchronize(s.handle)
         assert rc == SGPU_ERR_TIMEOUT, rc
         assert "bounded wait" in lib.sgpu_last_error(s.handle).decode()
         # the error word is cleared once reported
         assert lib.sgpu_synchronize(s.handle) == 0
-        # the default bound back: the context launches again without error
+        # the H side too, through the graph-replayed steps
+        assert lib.sgpu_advance_steps(s.handle, 1, 2) == 0
+        assert lib.sgpu_synchronize(s.handle) == SGPU_ERR_TIMEOUT
+        # drill off, default bound: the context launches again without error
+        assert lib.sgpu_set_wait_drill(s.handle, 0) == 0
         assert lib.sgpu_set_wait_cycles(s.handle, 4_000_000_000) == 0
-        assert lib.sgpu_advance_h(s.handle, 0) == 0
+        assert lib.sgpu_advance_h(s.handle, 3) == 0
         assert lib.sgpu_synchronize(s.handle) == 0
     # a fresh context is unaffected and still equals the oracle
     o = oracle.Oracle(pb)
@@ -60,7 +67,8 @@ def test_expired_wait_in_the_batch_reports_timeout():
     with Batch(256 << 20, 4, kernel_family=1) as b:
         for pb in pbs:
             b.add(pb)
-        assert b.lib.sgpu_batch_set_wait_cycles(b._h, 0) == 0
+        assert b.lib.sgpu_batch_set_wait_cycles(b._h, SHORT) == 0
+        assert b.lib.sgpu_batch_set_wait_drill(b._h, 1) == 0
         b.advance(1)
         rc = b.lib.sgpu_batch_synchronize(b._h)
         assert rc == SGPU_ERR_TIMEOUT, rc

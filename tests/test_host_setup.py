@@ -135,3 +135,46 @@ def test_reference_mur_case_plan_matches_oracle():
             assert_bits_equal(m, o.media(c).transpose(2, 1, 0))
     finally:
         lib.sgpu_destroy(h)
+
+
+def _device_case(name):
+    from semba_fdtd_b200 import read_case
+    if name == "reference":
+        return read_case(REF_CASE)
+    return ALL[name]()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(ALL) + ["reference"])
+def test_device_built_media_equal_host_plan(name):
+    """sgpu_host_create builds the media matrices on the device (region
+    painting, PML extrusion and copies, PEC borders); they, the media count,
+    the coefficient tables and CAB1 equal the host plan's bit for bit."""
+    from semba_fdtd_b200 import Solver
+    pb = _device_case(name)
+    lib, h = _plan(pb)
+    try:
+        with Solver(pb) as s:
+            dt, nm = C.c_double(), C.c_int()
+            a6, s6, q6 = (_lib.Lim * 6)(), (_lib.Lim * 6)(), (_lib.Lim * 6)()
+            assert lib.sgpu_host_info(h, C.byref(dt), C.byref(nm), a6, s6, q6) == 0
+            assert s.num_media == nm.value
+            n1 = nm.value + 1
+            hg = [np.empty(n1, np.float32) for _ in range(4)]
+            lib.sgpu_host_get_g(h, *[x.ctypes.data_as(_lib.c_float_p) for x in hg])
+            for a, b in zip(s.g_tables(), hg):
+                assert_bits_equal(a, b)
+            for f in range(6):
+                hc = np.empty(n1, np.float32)
+                rc = lib.sgpu_host_get_mur_cab1(h, f, hc.ctypes.data_as(_lib.c_float_p))
+                dc = s.mur_cab1(f)
+                assert (rc == 0) == (dc is not None)
+                if dc is not None:
+                    assert_bits_equal(dc, hc)
+            for c in range(6):
+                xi, xe, yi, ye, zi, ze = a6[c].tuple()
+                m = np.empty((ze - zi + 1, ye - yi + 1, xe - xi + 1), np.int16)
+                lib.sgpu_host_get_media(h, c, m.ctypes.data_as(C.POINTER(C.c_int16)))
+                assert_bits_equal(s.media(c), m.transpose(2, 1, 0), err_msg=f"component {c}")
+    finally:
+        lib.sgpu_destroy(h)
