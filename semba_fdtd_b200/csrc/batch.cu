@@ -333,11 +333,12 @@ __global__ void __launch_bounds__(kPhaseThreads)
         const InstDesc& D = descs[w.slot];
         bool on;
         const int n = inst_step(D, G, &on);
-        if (!on) continue;
+        if (!on) continue;  // the same for the whole block: the item is one instance's
+        const bool pw_on = pw_switch_block(D.src[side], n, D.tiempo, 0, D.dt, side);
         const long long r = w.q0 + threadIdx.x;
         if (r < w.q1)
             source_row(D.g, D.src[side], n, D.tiempo, 0, D.dt, side,
-                       (1 << kSrcPlaneWave) | (1 << kSrcNodalSoft) | (1 << kSrcNodalHard), (int)r);
+                       (1 << kSrcPlaneWave) | (1 << kSrcNodalSoft) | (1 << kSrcNodalHard), (int)r, pw_on);
     }
 }
 
@@ -856,7 +857,7 @@ sgpu_status sgpu_batch_add(sgpu_batch* b, const sgpu_problem* p, sgpu_ctx* plan,
     S.size_class = size_class_of(c);
     InstDesc D = make_desc(S, true);
     BTRY(b, cudaMemcpyAsync(b->d_desc + sl, &D, sizeof(InstDesc), cudaMemcpyHostToDevice, b->stream));
-    b->has_maps[sl] = c->tma_ready ? 1 : 0;
+    b->has_maps[sl] = tma_usable(c) ? 1 : 0;
     TMaps m2[2] = {c->tme, c->tmh};
     if (c->tma_ready) BTRY(b, cudaMemcpyAsync(b->d_maps + 2 * sl, m2, sizeof(m2), cudaMemcpyHostToDevice, b->stream));
     b->dirty = true;

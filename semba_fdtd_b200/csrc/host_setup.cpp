@@ -1204,7 +1204,7 @@ sgpu_status sgpu_host_footprint(const sgpu_ctx* c, uint64_t* bytes) {
         nza = std::max<long long>(nza, h->alloc[f].z1 - h->alloc[0].z0 + 1);
     }
     const long long vol = (nxa + 31) / 32 * 32 * nya * nza;
-    uint64_t b = (uint64_t)vol * 6 * (sizeof(float) + sizeof(int16_t));
+    uint64_t b = (uint64_t)vol * 6 * (sizeof(float) + sizeof(int16_t) + sizeof(uint8_t));
     // psi slabs
     for (int f = 0; f < 6; ++f)
         for (int reg = 0; reg < 6; ++reg) b += psi_floats(*h, h->cd.pmlc[f][reg]) * 4;
@@ -1258,6 +1258,7 @@ sgpu_status sgpu_batch_footprint(const sgpu_ctx* c, uint64_t* bytes, uint64_t* l
     for (int f = 0; f < 6; ++f) {
         buf((uint64_t)vol * 4);  // field
         buf((uint64_t)vol * 2);  // media
+        buf((uint64_t)vol * 1);  // one-byte media copy
     }
     const uint64_t n1 = (uint64_t)h->num_media + 1;
     for (int q = 0; q < 4; ++q) buf(n1 * 4);  // G1 G2 GM1 GM2

@@ -221,7 +221,9 @@ __global__ void __launch_bounds__(256, 6) k_ade(KGrid g, KDisp d, int comp) {
 // touched node applies that node's contributions in the reference order.
 __global__ void k_sources(KGrid g, KSrc s, StepRef sr, const double* tiempo, int t_n0, double dt, int hside, int mask) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r < s.nrows) source_row(g, s, step_of(sr), tiempo, t_n0, dt, hside, mask, r);
+    const int n = step_of(sr);
+    const bool pw_on = (mask & (1 << kSrcPlaneWave)) ? pw_switch_block(s, n, tiempo, t_n0, dt, hside) : false;
+    if (r < s.nrows) source_row(g, s, n, tiempo, t_n0, dt, hside, mask, r, pw_on);
 }
 
 // UpdateObservation point probes (observation.F90:2633-2668).
@@ -275,6 +277,11 @@ __global__ void k_mur_h(KGrid g, KBorder b) { mur_cell(g, b, blockIdx.x * (long 
 __global__ void k_fill_i16(int16_t* p, long long n, int v) {
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
         p[q] = (int16_t)v;
+}
+// The one-byte copy of a media matrix (indices below 256).
+__global__ void k_narrow_media(const int16_t* M, uint8_t* M8, long long n) {
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        M8[q] = (uint8_t)M[q];
 }
 __global__ void k_set_step(int* d, int v) { *d = v; }
 __global__ void k_add_step(int* d, int v) { *d += v; }
@@ -413,15 +420,15 @@ EncodeTiled encoder() {
 }
 
 // A 3-D tiled map over one padded array with a (bx, by, 1) box.
-bool encode_map(const sgpu_ctx* c, CUtensorMap* m, void* base, bool int16, int bx, int by) {
+bool encode_map(const sgpu_ctx* c, CUtensorMap* m, void* base, bool bytes, int bx, int by) {
     EncodeTiled fn = encoder();
     if (!fn) return false;
-    const cuuint64_t esz = int16 ? 2 : 4;
+    const cuuint64_t esz = bytes ? 1 : 4;
     const cuuint64_t dims[3] = {(cuuint64_t)c->pitch, (cuuint64_t)c->nya, (cuuint64_t)c->nza};
     const cuuint64_t strides[2] = {(cuuint64_t)c->pitch * esz, (cuuint64_t)c->plane * esz};
     const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
     const cuuint32_t es[3] = {1, 1, 1};
-    return fn(m, int16 ? CU_TENSOR_MAP_DATA_TYPE_UINT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, es,
+    return fn(m, bytes ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, es,
               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
@@ -451,9 +458,9 @@ bool build_tensor_maps(sgpu_ctx* c) {
     ok = ok && encode_map(c, &c->tmh.m[2], c->F[2], false, kHaloW, kTY + 1);
     for (int q = 0; q < 3; ++q) {
         ok = ok && encode_map(c, &c->tme.m[3 + q], c->F[q], false, kTX, kTY);
-        ok = ok && encode_map(c, &c->tme.m[6 + q], c->M[q], true, kTX, kTY);
+        ok = ok && encode_map(c, &c->tme.m[6 + q], c->M8[q], true, kTX, kTY);
         ok = ok && encode_map(c, &c->tmh.m[3 + q], c->F[3 + q], false, kTX, kTY);
-        ok = ok && encode_map(c, &c->tmh.m[6 + q], c->M[3 + q], true, kTX, kTY);
+        ok = ok && encode_map(c, &c->tmh.m[6 + q], c->M8[3 + q], true, kTX, kTY);
     }
     return ok;
 }
@@ -570,12 +577,12 @@ sgpu_status launch_borders_h(sgpu_ctx* c) {
 }
 
 sgpu_status field_e(sgpu_ctx* c) {
-    if (c->family == 1 && c->tma_ready) return launch_tma(c, false);
+    if (c->family == 1 && tma_usable(c)) return launch_tma(c, false);
     return c->cpml.on ? launch_e<kBulk | kCpml | kAll>(c) : launch_e<kBulk | kAll>(c);
 }
 
 sgpu_status field_h(sgpu_ctx* c) {
-    if (c->family == 1 && c->tma_ready) return launch_tma(c, true);
+    if (c->family == 1 && tma_usable(c)) return launch_tma(c, true);
     return c->cpml.on ? launch_h<kBulk | kCpml | kAll>(c) : launch_h<kBulk | kAll>(c);
 }
 
@@ -701,7 +708,9 @@ sgpu_status sgpu::create_in(const sgpu_grid_desc* d, Arena* arena, cudaStream_t 
     for (int f = 0; f < 6; ++f) {
         if ((s = dalloc(c, &c->F[f], c->vol))) return fail(s);
         if ((s = dalloc(c, &c->M[f], c->vol))) return fail(s);
+        if ((s = dalloc(c, &c->M8[f], c->vol))) return fail(s);
         CUDA_TRY(c, cudaMemsetAsync(c->F[f], 0, c->vol * sizeof(float), c->stream));
+        CUDA_TRY(c, cudaMemsetAsync(c->M8[f], 1, c->vol, c->stream));
         // padding cells keep medium 1 (vacuum), as the reference initialises
         // every media matrix before assigning regions
     }
@@ -765,6 +774,7 @@ void sgpu_destroy(sgpu_ctx* c) {
     for (int f = 0; f < 6; ++f) {
         dev_free(c, c->F[f]);
         dev_free(c, c->M[f]);
+        dev_free(c, c->M8[f]);
     }
     dev_free(c, c->g1); dev_free(c, c->g2); dev_free(c, c->gm1); dev_free(c, c->gm2);
     dev_free(c, c->idxe); dev_free(c, c->idye); dev_free(c, c->idze);
@@ -880,8 +890,17 @@ sgpu_status sgpu::upload_media(sgpu_ctx* c, int comp, const int16_t* mi, bool ch
     CUDA_TRY(c, box_to_device(c->M[comp], mi, sizeof(int16_t), ax, ay, az, c->pitch, c->plane / c->pitch, c->stream));
     c->media_loaded[comp] = true;
     c->src_dirty = true;
+    return narrow_media(c, comp);
+}
+
+sgpu_status sgpu::narrow_media(sgpu_ctx* c, int comp) {
+    k_narrow_media<<<(unsigned)std::min<long long>((c->vol + 255) / 256, 148 * 16), 256, 0, c->stream>>>(c->M[comp], c->M8[comp],
+                                                                                                      c->vol);
+    CUDA_TRY(c, cudaGetLastError());
     return SGPU_OK;
 }
+
+bool sgpu::tma_usable(const sgpu_ctx* c) { return c->tma_ready && c->num_media < 256; }
 
 extern "C" {
 
@@ -2060,7 +2079,7 @@ extern "C" {
 
 sgpu_status sgpu_device_bytes(const sgpu_ctx* c, uint64_t* bytes) {
     if (!c || !bytes) return SGPU_ERR_ARG;
-    uint64_t b = (uint64_t)c->vol * 6 * (sizeof(float) + sizeof(int16_t));
+    uint64_t b = (uint64_t)c->vol * 6 * (sizeof(float) + sizeof(int16_t) + sizeof(uint8_t));
     for (int f = 0; f < 6; ++f)
         for (int w = 0; w < 2; ++w)
             for (int s = 0; s < 2; ++s) {

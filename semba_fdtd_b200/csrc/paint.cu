@@ -280,6 +280,10 @@ sgpu_status painter_relabel(DevicePainter* p, const int (*r6)[6], const int (*in
 }
 sgpu_status painter_zero(DevicePainter* p, int f, const int* b6) { return p->zero(f, b6); }
 sgpu_status painter_finish(DevicePainter* p) {
+    for (int f = 0; f < 6; ++f) {
+        const sgpu_status s = narrow_media(p->c, f);
+        if (s) return s;
+    }
     PAINT_TRY(p->c, cudaStreamSynchronize(p->c->stream));
     for (int f = 0; f < 6; ++f) p->c->media_loaded[f] = true;
     p->c->src_dirty = true;

@@ -229,6 +229,9 @@ struct sgpu_ctx {
     // device buffers
     float* F[6] = {};
     int16_t* M[6] = {};
+    // the media matrices again as one byte a cell, the copy the TMA-pipelined
+    // field kernels stream (they run only while num_media < 256)
+    uint8_t* M8[6] = {};
     float *g1 = nullptr, *g2 = nullptr, *gm1 = nullptr, *gm2 = nullptr;
     float *idxe = nullptr, *idye = nullptr, *idze = nullptr, *idxh = nullptr, *idyh = nullptr, *idzh = nullptr;
     std::vector<float> h_g1, h_g2, h_gm1, h_gm2;
@@ -335,6 +338,11 @@ cudaError_t box_to_device(void* dev, const void* host, size_t es, long long ax, 
                           long long rows, cudaStream_t st);
 cudaError_t box_to_host(void* host, const void* dev, size_t es, long long ax, long long ay, long long az, int pitch,
                         long long rows, cudaStream_t st);
+// Refresh the one-byte copy of media matrix comp (after it changed).
+sgpu_status narrow_media(sgpu_ctx* c, int comp);
+// Whether the TMA-pipelined field kernels can run (tensor maps built and
+// every medium index fits the one-byte media copy).
+bool tma_usable(const sgpu_ctx* c);
 // Replace the context's medium count and coefficient tables (before the
 // first launch): the level-2 host learns the final count only after the
 // media matrices are built on the device.

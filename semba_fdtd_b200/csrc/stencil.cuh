@@ -505,26 +505,34 @@ __device__ __forceinline__ bool pw_switch_up(const KSrc& s, int n, const double*
     return true;
 }
 
+// The switch for a whole block of source rows of one half step: thread 0
+// evaluates it, every thread of the block returns it (all must call).
+__device__ __forceinline__ bool pw_switch_block(const KSrc& s, int n, const double* tiempo, int t_n0, double dt, int hside) {
+    __shared__ int on;
+    __syncthreads();  // the previous call's value has been read
+    if (threadIdx.x == 0) on = pw_switch_up(s, n, tiempo, t_n0, dt, hside) ? 1 : 0;
+    __syncthreads();
+    return on != 0;
+}
+
 // AdvancePlaneWaveE/H (planewaves.F90:878-1475) with Incid/evolucion
 // (:778-853) and AdvanceNodalE/H (nodalsources.F90:310-777): source row r
 // (one touched node) applies that node's contributions in the reference
-// order; plane-wave contributions only while the global switch is up.
+// order; plane-wave contributions only while the global switch (pw_on) is up.
 __device__ __forceinline__ void source_row(const KGrid& g, const KSrc& s, int n, const double* tiempo, int t_n0, double dt,
-                                           int hside, int mask, int r) {
+                                           int hside, int mask, int r, bool pw_on) {
     const double tn = tiempo[n - t_n0];
     const float t = hside ? (float)(tn + (double)0.5f * dt) : (float)tn;
     const float G21 = hside ? g.gm2[1] : g.g2[1];
     float* F = g.F[s.row_comp[r]];
     const int node = s.row_node[r];
     float v = F[node];
-    int pw_on = -1;  // the switch, evaluated at the row's first plane-wave entry
     for (int p = s.row_ptr[r]; p < s.row_ptr[r + 1]; ++p) {
         const SrcEntry en = s.e[p];
         if (!((1 << en.type) & mask)) continue;
         const SrcTable tb = s.tab[en.table];
         const float* ev0 = s.samples + tb.offset;
         if (en.type == kSrcPlaneWave) {
-            if (pw_on < 0) pw_on = pw_switch_up(s, n, tiempo, t_n0, dt, hside) ? 1 : 0;
             if (!pw_on) continue;
             float ev = 0.0f;
             const long long nprev = (long long)((t - en.a) / tb.delta);

@@ -4,8 +4,9 @@
 //
 // Each CTA owns a 32 x 8 tile of (i, j) columns and marches a z chunk.  One
 // producer warp streams every plane the tile needs -- the H (or E) tiles with
-// their one-cell halos, the tile's own E (or H) values and the three int16
-// media tiles -- into a 4-stage shared-memory ring with cp.async.bulk.tensor
+// their one-cell halos, the tile's own E (or H) values and the three media
+// tiles (one byte a cell, a copy of the int16 matrices kept while the media
+// number under 256) -- into a 4-stage shared-memory ring with cp.async.bulk.tensor
 // loads that complete on mbarriers; eight consumer warps update one cell per
 // thread from shared memory and store the result with plain coalesced stores.
 // The x origin of a haloed tile is rounded down to a 16-byte boundary (4
@@ -34,7 +35,7 @@ constexpr int kBoxA = kTX * (kTY + 1) * 4;      // 32 x 9 floats
 constexpr int kBoxB = kHaloW * kTY * 4;         // 36 x 8 floats
 constexpr int kBoxC = kHaloW * (kTY + 1) * 4;   // 36 x 9 floats
 constexpr int kBoxF = kTX * kTY * 4;            // 32 x 8 floats
-constexpr int kBoxM = kTX * kTY * 2;            // 32 x 8 int16
+constexpr int kBoxM = kTX * kTY;                // 32 x 8 one-byte media indices
 constexpr int kBoxP = kTX * kTY * 4;            // 32 x 8 floats of one psi slab
 constexpr int kPsiSlots = 6;                    // psi tiles staged per plane
 __host__ __device__ constexpr int align128(int b) { return (b + 127) / 128 * 128; }
@@ -53,8 +54,8 @@ constexpr unsigned kTxFull = kBoxA + kBoxB + kBoxC + 3 * kBoxF + 3 * kBoxM;
 constexpr unsigned kTxEdge = kBoxA + kBoxB;  // the extra plane: two arrays only
 
 // TMaps holds the tensor maps in the order the kernels use them:
-//   E kernel: Hx(32x9) Hy(36x8) Hz(36x9) Ex Ey Ez (32x8) Mx My Mz (32x8 int16)
-//   H kernel: Ex(32x9) Ey(36x8) Ez(36x9) Hx Hy Hz (32x8) Mx My Mz (32x8 int16)
+//   E kernel: Hx(32x9) Hy(36x8) Hz(36x9) Ex Ey Ez (32x8) Mx My Mz (32x8 one-byte media)
+//   H kernel: Ex(32x9) Ey(36x8) Ez(36x9) Hx Hy Hz (32x8) Mx My Mz (32x8 one-byte media)
 // then the psi slabs of the side (32x8), map 9+n for slab bit n of the
 // CPML masks (cp.s[c0 + n/4][(n/2)%2][n%2]).
 //
@@ -360,9 +361,9 @@ __device__ __forceinline__ bool e_consume(const TmaCta& t, unsigned G0, const KG
         const float* HXp = (const float*)(pv + kOffA);
         const float* HYp = (const float*)(pv + kOffB);
         const float* EF = (const float*)(st + kOffF);
-        const int16_t* MF = (const int16_t*)(st + kOffM);
+        const uint8_t* MF = (const uint8_t*)(st + kOffM);
         const float* PS = (const float*)(st + kOffP);
-        constexpr int fs = align128(kBoxF) / 4, ms = align128(kBoxM) / 2;
+        constexpr int fs = align128(kBoxF) / 4, ms = align128(kBoxM);
         const float hx = HX[(w + 1) * kTX + l], hx_jm = HX[w * kTX + l], hx_km = HXp[(w + 1) * kTX + l];
         const float hy = HY[w * kHaloW + l + 4], hy_im = HY[w * kHaloW + l + 3], hy_km = HYp[w * kHaloW + l + 4];
         const float hz = HZ[(w + 1) * kHaloW + l + 4], hz_jm = HZ[w * kHaloW + l + 4], hz_im = HZ[(w + 1) * kHaloW + l + 3];
@@ -441,9 +442,9 @@ __device__ __forceinline__ bool h_consume(const TmaCta& t, unsigned G0, const KG
         const float* EXn = (const float*)(nx + kOffA);
         const float* EYn = (const float*)(nx + kOffB);
         const float* HF = (const float*)(st + kOffF);
-        const int16_t* MF = (const int16_t*)(st + kOffM);
+        const uint8_t* MF = (const uint8_t*)(st + kOffM);
         const float* PS = (const float*)(st + kOffP);
-        constexpr int fs = align128(kBoxF) / 4, ms = align128(kBoxM) / 2;
+        constexpr int fs = align128(kBoxF) / 4, ms = align128(kBoxM);
         const float ex = EX[w * kTX + l], ex_jp = EX[(w + 1) * kTX + l], ex_kp = EXn[w * kTX + l];
         const float ey = EY[w * kHaloW + l], ey_ip = EY[w * kHaloW + l + 1], ey_kp = EYn[w * kHaloW + l];
         const float ez = EZ[w * kHaloW + l], ez_ip = EZ[w * kHaloW + l + 1], ez_jp = EZ[(w + 1) * kHaloW + l];
