@@ -323,6 +323,11 @@ sgpu_status sgpu_compulsory_bytes(const sgpu_ctx* ctx, double* bytes6);
 /* Select the CUDA device this library's runtime uses on the calling thread
  * (call before sgpu_create / sgpu_host_create). */
 sgpu_status sgpu_select_device(int device);
+/* Device memory of contexts outside a batch comes from the current device's
+ * default memory pool (stream-ordered), which keeps freed memory for the
+ * next context; this hands the kept memory back to the driver (waits for the
+ * device).  sgpu_batch_create does it before allocating its arena. */
+sgpu_status sgpu_trim_device_memory(void);
 /* Kernel launches issued per whole step (graph replays add one per chunk). */
 sgpu_status sgpu_kernels_per_step(const sgpu_ctx* ctx, int* n);
 

@@ -471,6 +471,9 @@ module semba_gpu_m
          type(c_ptr), value :: ctx
          real(c_double), intent(out) :: bytes6(6)
       end function sgpu_compulsory_bytes
+      integer(c_int) function sgpu_trim_device_memory() bind(C, name="sgpu_trim_device_memory")
+         import :: c_int
+      end function sgpu_trim_device_memory
       integer(c_int) function sgpu_select_device(device) bind(C, name="sgpu_select_device")
          import :: c_int
          integer(c_int), value :: device

@@ -184,6 +184,7 @@ def _declare(lib: C.CDLL) -> None:
         "sgpu_batch_set_kernel_family": ([vp, C.c_int], C.c_int),
         "sgpu_batch_set_wait_cycles": ([vp, C.c_int64], C.c_int),
         "sgpu_set_wait_cycles": ([vp, C.c_int64], C.c_int),
+        "sgpu_trim_device_memory": ([], C.c_int),
         "sgpu_set_wait_drill": ([vp, C.c_int], C.c_int),
         "sgpu_batch_set_wait_drill": ([vp, C.c_int], C.c_int),
         "sgpu_batch_set_tuning": ([vp, c_int_p, C.c_int], C.c_int),

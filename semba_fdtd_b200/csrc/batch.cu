@@ -764,6 +764,8 @@ sgpu_status sgpu_batch_create(uint64_t arena_bytes, int max_instances, sgpu_batc
     BTRY(b, cudaStreamCreateWithFlags(&b->setup, cudaStreamNonBlocking));
     BTRY(b, cudaEventCreateWithFlags(&b->setup_done, cudaEventDisableTiming));
     void* base = nullptr;
+    // memory the solo contexts' pool keeps is handed back first
+    sgpu_trim_device_memory();
     if (cudaMalloc(&base, arena_bytes) != cudaSuccess) {
         cudaGetLastError();
         return berr(b, SGPU_ERR_OOM, "arena of " + std::to_string(arena_bytes) + " bytes could not be allocated");

@@ -608,20 +608,46 @@ sgpu_status whole_step(sgpu_ctx* c, StepRef sr) {
     return launch_probes(c, sr);
 }
 
+// A context outside a batch takes its device memory from the device's
+// default memory pool, stream-ordered on its own stream, and the pool is
+// told to keep what is freed: a problem set up after another one (a sweep,
+// solves served one at a time) reuses memory already mapped instead of the
+// driver unmapping and mapping gigabytes again (measured at 536^3: 0.8 s to
+// set up and 0.4 s to tear down the second problem with plain cudaMalloc /
+// cudaFree).  sgpu_trim_device_memory hands the kept memory back.
+void keep_pool_memory(int device) {
+    static std::mutex mu;
+    static bool done[64] = {};
+    std::lock_guard<std::mutex> lock(mu);
+    if (device < 0 || device >= 64 || done[device]) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
+    done[device] = true;
+}
+
 void* dev_malloc(sgpu_ctx* c, size_t bytes) {
     if (c->arena) return arena_alloc(c->arena, bytes);
+    keep_pool_memory(c->device);
     void* p = nullptr;
-    if (cudaMalloc(&p, bytes) != cudaSuccess) {
-        cudaGetLastError();
-        return nullptr;
-    }
-    return p;
+    if (cudaMallocAsync(&p, bytes, c->stream) == cudaSuccess) return p;
+    cudaGetLastError();
+    // memory the pool keeps may be what is missing: hand it back and retry
+    cudaMemPool_t pool;
+    if (cudaStreamSynchronize(c->stream) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, c->device) == cudaSuccess &&
+        cudaMemPoolTrimTo(pool, 0) == cudaSuccess && cudaMallocAsync(&p, bytes, c->stream) == cudaSuccess)
+        return p;
+    cudaGetLastError();
+    return nullptr;
 }
 
 void dev_free(sgpu_ctx* c, void* p) {
     if (!p) return;
     if (c->arena) arena_free(c->arena, p);
-    else cudaFree(p);
+    else cudaFreeAsync(p, c->stream);
 }
 
 template <class T> sgpu_status dalloc(sgpu_ctx* c, T** p, size_t n, std::vector<void*>* track = nullptr) {
@@ -1912,6 +1938,17 @@ sgpu_status sgpu_compulsory_bytes(const sgpu_ctx* c, double* b6) {
     b6[4] = 8.0 * (double)c->border.cl_cells + 26.0 * (double)c->border.mur_cells +
             (c->mdisp_on ? mnodes * (8.0 + 32.0 * c->mdisp.nu_max) : 0.0);
     b6[5] = 8.0 * c->probes.n;
+    return SGPU_OK;
+}
+
+sgpu_status sgpu_trim_device_memory(void) {
+    int device = 0;
+    cudaMemPool_t pool;
+    if (cudaGetDevice(&device) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess ||
+        cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess || cudaMemPoolTrimTo(pool, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return SGPU_ERR_CUDA;
+    }
     return SGPU_OK;
 }
 

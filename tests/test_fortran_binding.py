@@ -21,7 +21,7 @@ def _c_source():
 def c_functions():
     out = {}
     for m in re.finditer(r"(sgpu_status|void|const char\*)\s+(sgpu_\w+)\s*\(([^)]*)\)\s*;", _c_source()):
-        args = [a.strip() for a in m.group(3).split(",") if a.strip()]
+        args = [a.strip() for a in m.group(3).split(",") if a.strip() and a.strip() != "void"]
         out[m.group(2)] = (m.group(1), args)
     return out
 
