@@ -1884,13 +1884,14 @@ sgpu_status sgpu_algorithmic_bytes(const sgpu_ctx* c, double* b6) {
         return b;
     };
     // E (H) half step: every swept node of the three updated components is
-    // read and written once (8 B) with its int16 medium (2 B), and each node
-    // of the three other components is read once (4 B); psi points are read
-    // and written (8 B).  Neighbour re-reads and coefficient tables are not
-    // counted.
+    // read and written once (8 B) with its medium (1 B from the one-byte copy
+    // the TMA-pipelined kernels read, else 2 B), and each node of the three
+    // other components is read once (4 B); psi points are read and written
+    // (8 B).  Neighbour re-reads and coefficient tables are not counted.
+    const double node = (c->family == 1 && tma_usable(c)) ? 9.0 : 10.0;
     double e = 0, h = 0;
-    for (int f = 0; f < 3; ++f) e += cells(c->sweep[f]) * 10.0 + cells(c->sweep[f + 3]) * 4.0;
-    for (int f = 3; f < 6; ++f) h += cells(c->sweep[f]) * 10.0 + cells(c->sweep[f - 3]) * 4.0;
+    for (int f = 0; f < 3; ++f) e += cells(c->sweep[f]) * node + cells(c->sweep[f + 3]) * 4.0;
+    for (int f = 3; f < 6; ++f) h += cells(c->sweep[f]) * node + cells(c->sweep[f - 3]) * 4.0;
     b6[0] = e + psi_bytes(0);
     // ADE node: index 4 + medium slot 1 + E 8 + previous E 8 + 32 per state slot
     double nodes = 0, mnodes = 0;
