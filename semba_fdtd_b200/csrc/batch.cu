@@ -204,9 +204,12 @@ __global__ void __launch_bounds__(kBX * kBY, 4)
 }
 
 // The same half steps through the TMA ring (tma_fields.cuh) as one
-// persistent kernel: each CTA walks its work items in order and the ring's
-// running plane number carries on from item to item, so the producer warp
-// fetches the next item's planes while the consumers finish the current one.
+// persistent kernel: each CTA's producer warp takes the next work item from a
+// counter shared by the launch (so CTAs that draw cheap items take more of
+// them and all finish together) and the ring's running plane number carries
+// on from item to item, so the producer fetches the next item's planes while
+// the consumers finish the current one; each plane names its item, which is
+// how the consumer warps follow.
 // Each instance's tensor maps live in global memory (written by the host
 // before the launch) and are acquired through the tensormap proxy before
 // their first use in the CTA.
@@ -217,7 +220,7 @@ __device__ __forceinline__ void tensormap_acquire(const CUtensorMap* m) {
 template <int SIDE>
 __global__ void __launch_bounds__(kTmaThreads, 3)
     k_batch_tma_field(const InstDesc* __restrict__ descs, const TMaps* __restrict__ maps, const FieldItem* __restrict__ items,
-                      const int* counts, const int* G, int* err, long long wait, int drill) {
+                      const int* counts, const int* G, int* err, long long wait, int drill, int* next) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ WarpView views[kConsumerWarps];
     __shared__ ProdTable tb;
@@ -229,20 +232,24 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
     int fenced = -1;     // the instance whose tensor maps the producer has acquired
     bool facq = false;   // ... and whether this lane has acquired its own map
     int viewed = -1;  // ... whose view the consumer warp holds
-    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
-        const FieldItem w = items[it];
-        const InstDesc& D = descs[w.slot];
-        bool on;
-        inst_step(D, G, &on);
-        if (!on) continue;
-        t.ib = w.ib;
-        t.jb = w.jb;
-        t.kb = w.kb;
-        t.ke = w.ke;
-        const int np = w.ke - w.kb + 2;  // the item's planes, edge plane included
-        const int c0 = SIDE == 0 ? 0 : 3;
-        if (producer) {
-            if (drill) return;  // a failure drill: no plane arrives, every consumer wait runs out
+    const int c0 = SIDE == 0 ? 0 : 3;
+    if (producer) {
+        if (drill) return;  // a failure drill: no plane arrives, every consumer wait runs out
+        for (;;) {
+            int it = 0;
+            if (t.lane == 0) it = atomicAdd(next, 1);
+            it = __shfl_sync(0xffffffffu, it, 0);
+            if (it >= n_items) break;
+            const FieldItem w = items[it];
+            const InstDesc& D = descs[w.slot];
+            bool on;
+            inst_step(D, G, &on);
+            if (!on) continue;
+            t.ib = w.ib;
+            t.jb = w.jb;
+            t.kb = w.kb;
+            t.ke = w.ke;
+            const int np = w.ke - w.kb + 2;  // the item's planes, edge plane included
             // CPML items stage their psi tiles through the ring when the tile's
             // slabs fit the kPsiSlots slots (the consumers derive the same mask)
             const int p0 = SIDE == 0 ? w.kb - 1 : w.kb, p1 = SIDE == 0 ? w.ke : w.ke + 1;
@@ -262,36 +269,54 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
                 tensormap_acquire(&m[t.lane]);
                 facq = true;
             }
-            const int got = tma_issue_warp(t, m, gp, p0, p1, edge, SIDE != 0, err, &tb, smask);
+            const int got = tma_issue_warp(t, m, gp, p0, p1, edge, SIDE != 0, err, &tb, smask, it);
             if (got < np) {
                 if (t.lane == 0) tma_drain(t, gp + (unsigned)got, err, 15);
                 return;
             }
-        } else {
-            if (w.slot != viewed) {
-                stage_view(&views[t.warp], D, true, t.lane, SIDE);
-                viewed = w.slot;
-            }
-            const WarpView& V = views[t.warp];
-            const KGrid& g = V.g;
-            const unsigned smask = w.cp ? staged_mask(V.cp, c0, w.ib, w.jb) : 0u;
-            const bool local = g.nmed1 <= kWarpTab;
-            const float* t1 = local ? V.tab : SIDE == 0 ? g.g1 : g.gm1;
-            const float* t2 = local ? V.tab + kWarpTab : SIDE == 0 ? g.g2 : g.gm2;
-            bool ok;
-            if (SIDE == 0)
-                ok = smask  ? e_consume<2>(t, gp, g, V.cp, t1, t2, err, true, rows[t.warp])
-                     : w.cp ? e_consume<1>(t, gp, g, V.cp, t1, t2, err, true, rows[t.warp])
-                            : e_consume<0>(t, gp, g, V.cp, t1, t2, err, true, rows[t.warp]);
-            else
-                ok = smask  ? h_consume<2>(t, gp, g, V.cp, t1, t2, err, true, rows[t.warp])
-                     : w.cp ? h_consume<1>(t, gp, g, V.cp, t1, t2, err, true, rows[t.warp])
-                            : h_consume<0>(t, gp, g, V.cp, t1, t2, err, true, rows[t.warp]);
-            if (!ok) return;
+            gp += (unsigned)np;
         }
+        if (t.lane == 0) {
+            const bool ended = tma_publish_end(t, gp, err);
+            tma_drain(t, gp + (ended ? 1u : 0u), err, 15);
+        }
+        return;
+    }
+    for (;;) {
+        // the item of the next plane (item -1: no more)
+        const unsigned s = gp % kStages;
+        if (!warp_wait(t.full0 + 8 * s, (gp / kStages) & 1, err, 5, t.wait)) return;
+        const int it = *(const volatile int*)(t.ring + s * kStageBytes + kOffItem);
+        if (it < 0) return;
+        const FieldItem w = items[it];
+        const InstDesc& D = descs[w.slot];
+        t.ib = w.ib;
+        t.jb = w.jb;
+        t.kb = w.kb;
+        t.ke = w.ke;
+        const int np = w.ke - w.kb + 2;
+        if (w.slot != viewed) {
+            stage_view(&views[t.warp], D, true, t.lane, SIDE);
+            viewed = w.slot;
+        }
+        const WarpView& V = views[t.warp];
+        const KGrid& g = V.g;
+        const unsigned smask = w.cp ? staged_mask(V.cp, c0, w.ib, w.jb) : 0u;
+        const bool local = g.nmed1 <= kWarpTab;
+        const float* t1 = local ? V.tab : SIDE == 0 ? g.g1 : g.gm1;
+        const float* t2 = local ? V.tab + kWarpTab : SIDE == 0 ? g.g2 : g.gm2;
+        bool ok;
+        if (SIDE == 0)
+            ok = smask  ? e_consume<2>(t, gp, g, V.cp, t1, t2, err, true, rows[t.warp])
+                 : w.cp ? e_consume<1>(t, gp, g, V.cp, t1, t2, err, true, rows[t.warp])
+                        : e_consume<0>(t, gp, g, V.cp, t1, t2, err, true, rows[t.warp]);
+        else
+            ok = smask  ? h_consume<2>(t, gp, g, V.cp, t1, t2, err, true, rows[t.warp])
+                 : w.cp ? h_consume<1>(t, gp, g, V.cp, t1, t2, err, true, rows[t.warp])
+                        : h_consume<0>(t, gp, g, V.cp, t1, t2, err, true, rows[t.warp]);
+        if (!ok) return;
         gp += (unsigned)np;
     }
-    if (producer && t.lane == 0) tma_drain(t, gp, err, 15);
 }
 
 // AdvanceEDispersiveE (MAG false) or AdvanceMdispersiveH (MAG true) over
@@ -416,6 +441,7 @@ struct sgpu_batch {
     InstDesc* d_desc = nullptr;
     TMaps* d_maps = nullptr;  // [slot][E side, H side]
     int* d_err = nullptr;     // bounded-wait error word of the TMA kernels
+    int* d_next = nullptr;    // next work item of the E and H field launches
     long long wait_cycles = 4000000000LL;  // bound of a pipeline wait (clock cycles, ~2 s)
     int wait_drill = 0;                    // failure drill: producers issue no loads
     int* d_counts = nullptr;
@@ -651,9 +677,12 @@ sgpu_status enqueue_step(sgpu_batch* b, cudaEvent_t* marks = nullptr) {
     auto mark = [&](int q) {
         if (marks) cudaEventRecord(marks[q], b->stream);
     };
-    if (tma)
+    if (tma) {
+        cudaMemsetAsync(b->d_next, 0, 2 * sizeof(int), b->stream);  // the launches' item counters
         k_batch_tma_field<0><<<tgrid, kTmaThreads, kTmaSmem, b->stream>>>(b->d_desc, b->d_maps, b->d_field[0], b->d_counts,
-                                                                          b->d_G, b->d_err, b->wait_cycles, b->wait_drill);
+                                                                          b->d_G, b->d_err, b->wait_cycles, b->wait_drill,
+                                                                          b->d_next);
+    }
     else
         k_batch_field<0><<<grid, blk, 0, b->stream>>>(b->d_desc, b->d_field[0], b->d_counts, b->d_G);
     mark(0);
@@ -663,7 +692,8 @@ sgpu_status enqueue_step(sgpu_batch* b, cudaEvent_t* marks = nullptr) {
     mark(2);
     if (tma)
         k_batch_tma_field<1><<<tgrid, kTmaThreads, kTmaSmem, b->stream>>>(b->d_desc, b->d_maps, b->d_field[1], b->d_counts,
-                                                                          b->d_G, b->d_err, b->wait_cycles, b->wait_drill);
+                                                                          b->d_G, b->d_err, b->wait_cycles, b->wait_drill,
+                                                                          b->d_next + 1);
     else
         k_batch_field<1><<<grid, blk, 0, b->stream>>>(b->d_desc, b->d_field[1], b->d_counts, b->d_G);
     mark(3);
@@ -779,6 +809,7 @@ sgpu_status sgpu_batch_create(uint64_t arena_bytes, int max_instances, sgpu_batc
     BTRY(b, cudaMalloc((void**)&b->d_desc, sizeof(InstDesc) * max_instances));
     BTRY(b, cudaMalloc((void**)&b->d_maps, sizeof(TMaps) * 2 * max_instances));
     BTRY(b, cudaMalloc((void**)&b->d_err, sizeof(int)));
+    BTRY(b, cudaMalloc((void**)&b->d_next, 2 * sizeof(int)));
     BTRY(b, cudaMalloc((void**)&b->d_counts, sizeof(int) * kNumCounts));
     BTRY(b, cudaMalloc((void**)&b->d_G, sizeof(int)));
     BTRY(b, cudaMemsetAsync(b->d_err, 0, sizeof(int), b->stream));
@@ -806,6 +837,7 @@ void sgpu_batch_destroy(sgpu_batch* b) {
     cudaFree(b->d_desc);
     cudaFree(b->d_maps);
     cudaFree(b->d_err);
+    cudaFree(b->d_next);
     cudaFree(b->d_counts);
     cudaFree(b->d_G);
     for (int s = 0; s < 2; ++s) {

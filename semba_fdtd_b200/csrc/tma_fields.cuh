@@ -240,8 +240,13 @@ __device__ __forceinline__ int tma_issue(const TmaCta& t, const CUtensorMap* map
 // staged slab.  A lane is the only issuer of its map, so a tensor map that
 // lane acquired through the tensormap proxy needs no other thread's fence.
 // All lanes return the number of planes issued.
+// Every plane also carries, in the word after its PlaneWords, the work item
+// it belongs to (`item`; -1 marks the end of a CTA's items), which is how the
+// consumers of a dynamically scheduled persistent kernel learn their item.
+constexpr int kOffItem = kOffW + (int)sizeof(PlaneWords);
 __device__ __forceinline__ int tma_issue_warp(const TmaCta& t, const CUtensorMap* maps, unsigned G0, int p0, int p1,
-                                              int edge, bool hside, int* err, const ProdTable* tb, unsigned smask) {
+                                              int edge, bool hside, int* err, const ProdTable* tb, unsigned smask,
+                                              int item) {
     const int q = t.lane;
     const int xh = hside ? t.ib : t.ib - 4, ya = hside ? t.jb : t.jb - 1;
     // this lane's box: shared-memory offset and x, y origin (psi: per plane below)
@@ -271,6 +276,7 @@ __device__ __forceinline__ int tma_issue_warp(const TmaCta& t, const CUtensorMap
                 ok = 0;
             } else {
                 if (!part) *(PlaneWords*)(st + kOffW) = w;
+                *(int*)(st + kOffItem) = item;
                 mbar_expect_tx(bar, (part ? kTxEdge : kTxFull) + (unsigned)__popc(w.live & smask) * (unsigned)kBoxP);
             }
         }
@@ -284,6 +290,17 @@ __device__ __forceinline__ int tma_issue_warp(const TmaCta& t, const CUtensorMap
         }
     }
     return p1 - p0 + 1;
+}
+
+// The end of a CTA's items (producer lane 0): plane G carries item -1 and no
+// loads; its full barrier completes on the plain arrive.  False when the wait
+// for the free stage ran out.
+__device__ __forceinline__ bool tma_publish_end(const TmaCta& t, unsigned G, int* err) {
+    const unsigned s = G % kStages, u = G / kStages;
+    if (u >= 1 && !mbar_wait(t.empty0 + 8 * s, (u - 1) & 1, err, 16, t.wait)) return false;
+    *(int*)(t.ring + s * kStageBytes + kOffItem) = -1;
+    mbar_arrive(t.full0 + 8 * s);
+    return true;
 }
 
 // The slab mask whose psi tiles a CPML tile stages (0: psi from global
