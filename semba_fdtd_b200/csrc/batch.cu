@@ -149,7 +149,7 @@ constexpr int kWarpTab = 32;  // media per coefficient table held in a warp's vi
 struct WarpView {
     KGrid g;
     KCpml cp;
-    float tab[2 * kWarpTab];  // the side's two coefficient tables, when nmed1 <= kWarpTab
+    float2 tab[kWarpTab];  // the side's coefficient pairs, when nmed1 <= kWarpTab
 };
 template <class T> __device__ __forceinline__ void warp_copy(T* dst, const T* src, int lane) {
     static_assert(sizeof(T) % 4 == 0, "word copy");
@@ -164,10 +164,8 @@ __device__ __forceinline__ const WarpView& stage_view(WarpView* slot, const Inst
     __syncwarp();  // the warp is done with the previous item's view
     warp_copy(&slot->g, &D.g, lane);
     if (cpml) warp_copy(&slot->cp, &D.cp, lane);
-    if (side >= 0 && lane < D.g.nmed1 && D.g.nmed1 <= kWarpTab) {
-        slot->tab[lane] = (side ? D.g.gm1 : D.g.g1)[lane];
-        slot->tab[kWarpTab + lane] = (side ? D.g.gm2 : D.g.g2)[lane];
-    }
+    if (side >= 0 && lane < D.g.nmed1 && D.g.nmed1 <= kWarpTab)
+        slot->tab[lane] = make_float2((side ? D.g.gm1 : D.g.g1)[lane], (side ? D.g.gm2 : D.g.g2)[lane]);
     __syncwarp();
     return *slot;
 }
@@ -215,6 +213,19 @@ __global__ void __launch_bounds__(kBX * kBY, 4)
 // their first use in the CTA.
 __device__ __forceinline__ void tensormap_acquire(const CUtensorMap* m) {
     asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"((unsigned long long)m) : "memory");
+}
+
+// One work item of a consumer warp: the staged-psi, global-psi or bulk form.
+template <int SIDE, class TAB>
+__device__ __forceinline__ bool consume(const TmaCta& t, unsigned gp, const KGrid& g, const KCpml& cp, const TAB tab, int* err,
+                                        PsiRow* rows, unsigned smask, bool cpml) {
+    if (SIDE == 0)
+        return smask ? e_consume<2>(t, gp, g, cp, tab, err, true, rows)
+               : cpml ? e_consume<1>(t, gp, g, cp, tab, err, true, rows)
+                      : e_consume<0>(t, gp, g, cp, tab, err, true, rows);
+    return smask ? h_consume<2>(t, gp, g, cp, tab, err, true, rows)
+           : cpml ? h_consume<1>(t, gp, g, cp, tab, err, true, rows)
+                  : h_consume<0>(t, gp, g, cp, tab, err, true, rows);
 }
 
 template <int SIDE>
@@ -302,18 +313,12 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
         const WarpView& V = views[t.warp];
         const KGrid& g = V.g;
         const unsigned smask = w.cp ? staged_mask(V.cp, c0, w.ib, w.jb) : 0u;
-        const bool local = g.nmed1 <= kWarpTab;
-        const float* t1 = local ? V.tab : SIDE == 0 ? g.g1 : g.gm1;
-        const float* t2 = local ? V.tab + kWarpTab : SIDE == 0 ? g.g2 : g.gm2;
         bool ok;
-        if (SIDE == 0)
-            ok = smask  ? e_consume<2>(t, gp, g, V.cp, t1, t2, err, true, rows[t.warp])
-                 : w.cp ? e_consume<1>(t, gp, g, V.cp, t1, t2, err, true, rows[t.warp])
-                        : e_consume<0>(t, gp, g, V.cp, t1, t2, err, true, rows[t.warp]);
+        if (g.nmed1 <= kWarpTab)
+            ok = consume<SIDE>(t, gp, g, V.cp, TabPairs{V.tab}, err, rows[t.warp], smask, w.cp != 0);
         else
-            ok = smask  ? h_consume<2>(t, gp, g, V.cp, t1, t2, err, true, rows[t.warp])
-                 : w.cp ? h_consume<1>(t, gp, g, V.cp, t1, t2, err, true, rows[t.warp])
-                        : h_consume<0>(t, gp, g, V.cp, t1, t2, err, true, rows[t.warp]);
+            ok = consume<SIDE>(t, gp, g, V.cp, TabSplit{SIDE == 0 ? g.g1 : g.gm1, SIDE == 0 ? g.g2 : g.gm2}, err,
+                               rows[t.warp], smask, w.cp != 0);
         if (!ok) return;
         gp += (unsigned)np;
     }
@@ -338,12 +343,12 @@ __global__ void __launch_bounds__(kPhaseThreads)
             const long long q2 = q + blockDim.x;
             const bool two = q2 < w.q1;
             AdeNode<NU> a, b;
-            ade_load<NU>(r, q, a);
-            if (two) ade_load<NU>(r, q2, b);
-            ade_update<NU, MAG>(r, a);
-            if (two) ade_update<NU, MAG>(r, b);
-            ade_store<NU>(r, q, a);
-            if (two) ade_store<NU>(r, q2, b);
+            ade_load<NU, false>(r, q, a);
+            if (two) ade_load<NU, false>(r, q2, b);
+            ade_update<NU, MAG, false>(r, a);
+            if (two) ade_update<NU, MAG, false>(r, b);
+            ade_store<NU, false>(r, q, a);
+            if (two) ade_store<NU, false>(r, q2, b);
         }
     }
 }

@@ -1231,6 +1231,7 @@ sgpu_status sgpu_host_footprint(const sgpu_ctx* c, uint64_t* bytes) {
         }
         if (!have) nodes = (uint64_t)vol * 3;  // upper bound once the host copy is released
         b += nodes * (4 + 1 + 4 + 16 * (uint64_t)nu);
+        b += (nodes / 32 + 6) * 16;  // run descriptors of the node groups (one per 32 nodes and component, plus one)
     }
     mur_buffers(*h, [&](uint64_t n) { b += n; });
     b += (uint64_t)h->probes.size() / 4 * h->probe_cap * 4;
@@ -1299,6 +1300,7 @@ sgpu_status sgpu_batch_footprint(const sgpu_ctx* c, uint64_t* bytes, uint64_t* l
             buf(nodes * 1);
             buf(nodes * 4);
             buf(nodes * 16 * (uint64_t)std::max(1, nu));
+            if (nodes) buf(((nodes + 31) / 32 + 1) * 16);  // run descriptors of the node groups
             buf(rows * 8);
             buf(rows * 4);
         }

@@ -139,23 +139,20 @@ __global__ void __launch_bounds__(kBX * kBY, 4) k_hfield(KGrid g, KCpml cp, int 
 // Same per-cell arithmetic as efield_column / hfield_column, from shared
 // memory instead of global loads.
 
-__device__ __forceinline__ const float* tma_tables(unsigned char* smem, const float* a, const float* b, int nmed1) {
-    float* tab = (float*)(smem + kTmaSmem);
-    if (nmed1 <= kShTable) {
-        for (int q = threadIdx.x; q < nmed1; q += blockDim.x) {
-            tab[q] = a[q];
-            tab[nmed1 + q] = b[q];
-        }
-        return tab;
-    }
-    return nullptr;
+// The side's coefficient pairs (G1, G2) or (GM1, GM2) in shared memory after
+// the ring; the TMA kernels run only with fewer than 256 media, so the table
+// always fits (the launch sizes the shared memory for it).
+__device__ __forceinline__ TabPairs tma_tables(unsigned char* smem, const float* a, const float* b, int nmed1) {
+    float2* tab = (float2*)(smem + kTmaSmem);
+    for (int q = threadIdx.x; q < nmed1; q += blockDim.x) tab[q] = make_float2(a[q], b[q]);
+    return TabPairs{tab};
 }
 
 __global__ void __launch_bounds__(kTmaThreads, 3)
     k_tma_efield(KGrid g, KCpml cp, const __grid_constant__ TMaps tm, int y0, int z0, int z1, int zchunk, int* err,
                  long long wait, int drill) {
     extern __shared__ __align__(128) unsigned char smem[];
-    const float* tab = tma_tables(smem, g.g1, g.g2, g.nmed1);
+    const TabPairs tab = tma_tables(smem, g.g1, g.g2, g.nmed1);
     const TmaCta t = tma_cta_setup(smem, y0, z0, z1, zchunk, wait);
     bool cpml_block = false;
     if (cp.on)
@@ -172,19 +169,17 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
         if (t.lane == 0) tma_drain(t, (unsigned)tma_issue(t, tm.m, 0, t.kb - 1, t.ke, t.kb - 1, false, err, &tb, smask), err, 12);
         return;
     }
-    const float* t1 = tab ? tab : g.g1;
-    const float* t2 = tab ? tab + g.nmed1 : g.g2;
     __shared__ PsiRow rows[kConsumerWarps][12];
-    if (smask) e_consume<2>(t, 0, g, cp, t1, t2, err, false, rows[t.warp]);
-    else if (cpml_block) e_consume<1>(t, 0, g, cp, t1, t2, err, false, rows[t.warp]);
-    else e_consume<0>(t, 0, g, cp, t1, t2, err, false, rows[t.warp]);
+    if (smask) e_consume<2>(t, 0, g, cp, tab, err, false, rows[t.warp]);
+    else if (cpml_block) e_consume<1>(t, 0, g, cp, tab, err, false, rows[t.warp]);
+    else e_consume<0>(t, 0, g, cp, tab, err, false, rows[t.warp]);
 }
 
 __global__ void __launch_bounds__(kTmaThreads, 3)
     k_tma_hfield(KGrid g, KCpml cp, const __grid_constant__ TMaps tm, int y0, int z0, int z1, int zchunk, int* err,
                  long long wait, int drill) {
     extern __shared__ __align__(128) unsigned char smem[];
-    const float* tab = tma_tables(smem, g.gm1, g.gm2, g.nmed1);
+    const TabPairs tab = tma_tables(smem, g.gm1, g.gm2, g.nmed1);
     const TmaCta t = tma_cta_setup(smem, y0, z0, z1, zchunk, wait);
     bool cpml_block = false;
     if (cp.on)
@@ -201,18 +196,16 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
         if (t.lane == 0) tma_drain(t, (unsigned)tma_issue(t, tm.m, 0, t.kb, t.ke + 1, t.ke + 1, true, err, &tb, smask), err, 14);
         return;
     }
-    const float* t1 = tab ? tab : g.gm1;
-    const float* t2 = tab ? tab + g.nmed1 : g.gm2;
     __shared__ PsiRow rows[kConsumerWarps][12];
-    if (smask) h_consume<2>(t, 0, g, cp, t1, t2, err, false, rows[t.warp]);
-    else if (cpml_block) h_consume<1>(t, 0, g, cp, t1, t2, err, false, rows[t.warp]);
-    else h_consume<0>(t, 0, g, cp, t1, t2, err, false, rows[t.warp]);
+    if (smask) h_consume<2>(t, 0, g, cp, tab, err, false, rows[t.warp]);
+    else if (cpml_block) h_consume<1>(t, 0, g, cp, tab, err, false, rows[t.warp]);
+    else h_consume<0>(t, 0, g, cp, tab, err, false, rows[t.warp]);
 }
 
-template <int NU, bool MAG>
+template <int NU, bool MAG, bool UNI>
 __global__ void __launch_bounds__(256, 6) k_ade(KGrid g, KDisp d, int comp) {
     const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (q < d.n[comp]) ade_node<NU, MAG>(ade_refs<MAG>(g, d, comp), q);
+    if (q < d.n[comp]) ade_node<NU, MAG, UNI>(ade_refs<MAG>(g, d, comp), q);
 }
 
 
@@ -316,6 +309,31 @@ __global__ void k_fill_disp(const int16_t* M, const int16_t* slot, int pitch, lo
     }
 }
 
+// The run descriptors of the node groups (32 consecutive nodes each): a run
+// is a stretch of nodes on consecutive cells with one medium slot.  Groups of
+// more than two runs get z = -1 and are counted in *irregular.
+__global__ void k_fill_grp(const int* node, const uint8_t* med, long long n, int4* grp, unsigned long long* irregular) {
+    const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long q0 = g * 32;
+    if (q0 >= n) return;
+    const int cnt = (int)min(32LL, n - q0);
+    int runs = 1, lane1 = 32;
+    for (int l = 1; l < cnt; ++l)
+        if (node[q0 + l] != node[q0 + l - 1] + 1 || med[q0 + l] != med[q0 + l - 1]) {
+            if (++runs == 2) lane1 = l;
+        }
+    int4 d;
+    if (runs > 2) {
+        d = make_int4(0, 0, -1, 0);
+        atomicAdd(irregular, 1ULL);
+    } else {
+        const int l1 = lane1 < cnt ? lane1 : cnt - 1;
+        d = make_int4(node[q0], node[q0 + l1] - lane1, lane1, (int)med[q0] | ((int)med[q0 + l1] << 8));
+        if (lane1 >= 32) d.y = d.x;  // one run: the second never applies
+    }
+    grp[g] = d;
+}
+
 __global__ void k_nonfinite(const float* a, long long n, unsigned int* flag) {
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
         if (!isfinite(a[q])) {
@@ -390,7 +408,7 @@ sgpu_status launch_tma(sgpu_ctx* c, bool hside) {
     chunk = std::min(chunk, nz);
     dim3 grid(bx, by, (nz + chunk - 1) / chunk);
     const int n1 = c->num_media + 1;
-    const size_t smem = kTmaSmem + (n1 <= kShTable ? 2 * n1 * sizeof(float) : 0);
+    const size_t smem = kTmaSmem + n1 * sizeof(float2);  // n1 <= 256: tma_usable
     if (hside)
         k_tma_hfield<<<grid, kTmaThreads, smem, c->stream>>>(kgrid(c), c->cpml, c->tmh, L.y0, L.z0, L.z1, chunk, c->d_err,
                                                              c->wait_cycles, c->wait_drill);
@@ -474,7 +492,9 @@ bool ready(sgpu_ctx* c) {
 sgpu_status build_sources(sgpu_ctx* c);
 
 template <int NU, bool MAG> void ade_launch(sgpu_ctx* c, int comp, unsigned blocks) {
-    k_ade<NU, MAG><<<blocks, 256, 0, c->stream>>>(kgrid(c), MAG ? c->mdisp : c->disp, comp);
+    const KDisp& d = MAG ? c->mdisp : c->disp;
+    if (d.uniform) k_ade<NU, MAG, true><<<blocks, 256, 0, c->stream>>>(kgrid(c), d, comp);
+    else k_ade<NU, MAG, false><<<blocks, 256, 0, c->stream>>>(kgrid(c), d, comp);
 }
 
 template <bool MAG> sgpu_status launch_ade_side(sgpu_ctx* c) {
@@ -1159,6 +1179,8 @@ sgpu_status init_ade(sgpu_ctx* c, const sgpu_edisp_desc* d, bool mag) {
     k.media = dmedia;
     k.slot_of_medium = dslot;
     k.nu_max = nu_max;
+    k.uniform = 1;
+    for (const DispMedium& dm : media) k.uniform &= dm.nu == nu_max;
     k.dt = c->dt;
     k.inv_dt = 1.0 / c->dt;
     for (int comp = 0; comp < 3; ++comp) {
@@ -1197,10 +1219,25 @@ sgpu_status init_ade(sgpu_ctx* c, const sgpu_edisp_desc* d, bool mag) {
         k_fill_disp<<<(unsigned)((rows + 255) / 256), 256, 0, c->stream>>>(c->M[c0 + comp], dslot, c->pitch, c->plane, x0, x1, y0,
                                                                            y1, z0, z1, doffs, node, med);
         if ((s = check_launch(c, "k_fill_disp"))) { dev_free(c, doffs); return s; }
+        // the run descriptors; one more int4 holds the irregular-group count
+        const long long ngrp = (tot + 31) / 32;
+        int4* grp;
+        if ((s = dalloc(c, &grp, (size_t)ngrp + 1, &allocs))) {
+            dev_free(c, doffs);
+            return s;
+        }
+        CUDA_TRY(c, cudaMemsetAsync(grp + ngrp, 0, sizeof(int4), c->stream));
+        k_fill_grp<<<(unsigned)((ngrp + 255) / 256), 256, 0, c->stream>>>(node, med, tot, grp,
+                                                                         (unsigned long long*)(grp + ngrp));
+        if ((s = check_launch(c, "k_fill_grp"))) { dev_free(c, doffs); return s; }
+        unsigned long long irr = 0;
+        CUDA_TRY(c, cudaMemcpyAsync(&irr, grp + ngrp, sizeof(irr), cudaMemcpyDeviceToHost, c->stream));
         CUDA_TRY(c, cudaMemsetAsync(prev, 0, tot * sizeof(float), c->stream));
         CUDA_TRY(c, cudaMemsetAsync(J, 0, (size_t)tot * std::max(1, nu_max) * sizeof(double2), c->stream));
         CUDA_TRY(c, cudaStreamSynchronize(c->stream));
         dev_free(c, doffs);
+        c->disp_irregular[mag ? 1 : 0][comp] = (long long)irr;
+        k.grp[comp] = grp;
         k.node[comp] = node;
         k.med[comp] = med;
         k.prev[comp] = prev;
@@ -1893,18 +1930,25 @@ sgpu_status sgpu_algorithmic_bytes(const sgpu_ctx* c, double* b6) {
     for (int f = 0; f < 3; ++f) e += cells(c->sweep[f]) * node + cells(c->sweep[f + 3]) * 4.0;
     for (int f = 3; f < 6; ++f) h += cells(c->sweep[f]) * node + cells(c->sweep[f - 3]) * 4.0;
     b6[0] = e + psi_bytes(0);
-    // ADE node: index 4 + medium slot 1 + E 8 + previous E 8 + 32 per state slot
-    double nodes = 0, mnodes = 0;
-    for (int comp = 0; comp < 3; ++comp) nodes += (double)c->disp.n[comp];
-    for (int comp = 0; comp < 3; ++comp) mnodes += (double)c->mdisp.n[comp];
-    b6[1] = c->disp_on ? nodes * (21.0 + 32.0 * c->disp.nu_max) : 0.0;
+    // ADE node: E 8 + previous E 8 + 32 per state slot, its share of the
+    // group's run descriptor (16 B per 32 nodes) and, in groups of more than
+    // two runs, index 4 + medium slot 1
+    auto ade_bytes = [&](const KDisp& d, int side) {
+        double b = 0;
+        for (int comp = 0; comp < 3; ++comp) {
+            const double n = (double)d.n[comp], irr = 32.0 * (double)c->disp_irregular[side][comp];
+            b += n * (16.0 + 32.0 * d.nu_max) + 16.0 * std::ceil(n / 32.0) + 5.0 * std::min(n, irr);
+        }
+        return b;
+    };
+    b6[1] = c->disp_on ? ade_bytes(c->disp, 0) : 0.0;
     b6[2] = 0;
     b6[3] = h + psi_bytes(3);
     // H sources (not counted) and borders: a clone cell reads and writes 4 B
     // each; a Mur cell reads H, its medium and both Past_ values and writes H
     // and both Past_ values (26 B)
     b6[4] = 8.0 * (double)c->border.cl_cells + 26.0 * (double)c->border.mur_cells +
-            (c->mdisp_on ? mnodes * (21.0 + 32.0 * c->mdisp.nu_max) : 0.0);
+            (c->mdisp_on ? ade_bytes(c->mdisp, 1) : 0.0);
     b6[5] = 8.0 * c->probes.n;
     return SGPU_OK;
 }

@@ -69,9 +69,16 @@ struct KDisp {
     float* prev[3];
     double2* J[3];                // [unique slot][node]
     long long n[3];
+    // per 32 consecutive nodes (a warp's worth): the group's nodes as at
+    // most two runs of consecutive cells of one medium each -- x: cell of
+    // lane 0's run start minus 0, y: cell of the second run's start minus its
+    // first lane, z: that first lane (32: one run; negative: more than two
+    // runs, read node[] and med[]), w: slot of run 0 | slot of run 1 << 8
+    const int4* grp[3];
     const DispMedium* media;
     const int16_t* slot_of_medium;  // media index -> slot (-1 none)
     int nu_max;
+    int uniform;  // every medium has nu_max state slots
     double dt;
     double inv_dt;  // RN(1/dt), for the corrected quotient by dt
 };
@@ -246,6 +253,7 @@ struct sgpu_ctx {
     sgpu::KDisp disp{}, mdisp{};
     std::vector<sgpu::DispMedium> h_disp_media[2];  // host copies of the media tables [electric, magnetic]
     std::vector<void*> disp_allocs, mdisp_allocs;
+    long long disp_irregular[2][3] = {};  // node groups of more than two runs [electric, magnetic][component]
     // borders (PMC / periodic clones, Mur)
     sgpu::KBorder border{};
     std::vector<void*> border_allocs;

@@ -383,6 +383,7 @@ __device__ __forceinline__ double div_dt(double a, double dt, double inv_dt) {
 struct AdeRefs {
     const int* node;
     const uint8_t* med;
+    const int4* grp;
     float* prev;
     double2* J;
     long long n;
@@ -391,12 +392,33 @@ struct AdeRefs {
     double dt, inv_dt;
 };
 template <bool MAG> __device__ __forceinline__ AdeRefs ade_refs(const KGrid& g, const KDisp& d, int comp) {
-    return AdeRefs{d.node[comp], d.med[comp], d.prev[comp], d.J[comp], d.n[comp], d.media, g.F[MAG ? 3 + comp : comp],
-                   d.dt, d.inv_dt};
+    return AdeRefs{d.node[comp], d.med[comp], d.grp[comp], d.prev[comp], d.J[comp], d.n[comp], d.media,
+                   g.F[MAG ? 3 + comp : comp], d.dt, d.inv_dt};
+}
+
+// Node q's cell and medium slot.  Nodes are numbered in cell order, so the 32
+// nodes of a group usually form one or two runs of consecutive cells of one
+// medium each; the group's descriptor then gives both (one 16-byte load the
+// warp shares), and only groups of more than two runs read the per-node
+// index and slot arrays.
+__device__ __forceinline__ void ade_where(const AdeRefs& d, long long q, int& idx, int& slot) {
+    if (d.grp) {
+        const int4 gd = __ldg(d.grp + (q >> 5));
+        if (gd.z >= 0) {
+            const int lane = (int)(q & 31);
+            const bool second = lane >= gd.z;
+            idx = (second ? gd.y : gd.x) + lane;
+            slot = second ? (gd.w >> 8) & 255 : gd.w & 255;
+            return;
+        }
+    }
+    idx = d.node[q];
+    slot = d.med[q];
 }
 
 // The node's update in three parts (loads, arithmetic, stores), so a thread
-// can issue the loads of several nodes before any store.
+// can issue the loads of several nodes before any store.  With UNI (every
+// medium has NU state slots) the state loads depend on nothing but q.
 template <int NU> struct AdeNode {
     int idx;
     const DispMedium* md;
@@ -404,21 +426,29 @@ template <int NU> struct AdeNode {
     double2 st[NU];
 };
 
-template <int NU>
+template <int NU, bool UNI>
 __device__ __forceinline__ void ade_load(const AdeRefs& d, long long q, AdeNode<NU>& a) {
-    a.idx = d.node[q];
-    a.md = d.media + d.med[q];
-    const int nu = a.md->nu;
+    if (UNI) {
 #pragma unroll
-    for (int u = 0; u < NU; ++u) a.st[u] = u < nu ? d.J[u * d.n + q] : make_double2(0.0, 0.0);
+        for (int u = 0; u < NU; ++u) a.st[u] = d.J[u * d.n + q];
+        a.prev = d.prev[q];
+    }
+    int slot;
+    ade_where(d, q, a.idx, slot);
+    a.md = d.media + slot;
+    if (!UNI) {
+        const int nu = a.md->nu;
+#pragma unroll
+        for (int u = 0; u < NU; ++u) a.st[u] = u < nu ? d.J[u * d.n + q] : make_double2(0.0, 0.0);
+        a.prev = d.prev[q];
+    }
     a.e = d.F[a.idx];
-    a.prev = d.prev[q];
 }
 
-template <int NU, bool MAG>
+template <int NU, bool MAG, bool UNI>
 __device__ __forceinline__ void ade_update(const AdeRefs& d, AdeNode<NU>& a) {
     const DispMedium* __restrict__ md = a.md;
-    const int nu = md->nu;
+    const int nu = UNI ? NU : md->nu;
     float e = a.e;
     for (int p = 0; p < md->np; ++p) {
         const int up = md->map[p];
@@ -454,9 +484,9 @@ __device__ __forceinline__ void ade_update(const AdeRefs& d, AdeNode<NU>& a) {
     a.e = e;
 }
 
-template <int NU>
+template <int NU, bool UNI>
 __device__ __forceinline__ void ade_store(const AdeRefs& d, long long q, const AdeNode<NU>& a) {
-    const int nu = a.md->nu;
+    const int nu = UNI ? NU : a.md->nu;
 #pragma unroll
     for (int u = 0; u < NU; ++u)
         if (u < nu) d.J[u * d.n + q] = a.st[u];
@@ -464,12 +494,12 @@ __device__ __forceinline__ void ade_store(const AdeRefs& d, long long q, const A
     d.F[a.idx] = a.e;
 }
 
-template <int NU, bool MAG>
+template <int NU, bool MAG, bool UNI>
 __device__ __forceinline__ void ade_node(const AdeRefs& d, long long q) {
     AdeNode<NU> a;
-    ade_load<NU>(d, q, a);
-    ade_update<NU, MAG>(d, a);
-    ade_store<NU>(d, q, a);
+    ade_load<NU, UNI>(d, q, a);
+    ade_update<NU, MAG, UNI>(d, a);
+    ade_store<NU, UNI>(d, q, a);
 }
 
 __device__ __forceinline__ int step_of(const StepRef& s) { return (s.dev_n ? *s.dev_n : 0) + s.n; }

@@ -332,8 +332,10 @@ __device__ __forceinline__ void tma_drain(const TmaCta& t, unsigned issued, int*
 }
 
 // Every lane waits on the barrier (each needs the acquire); the warp then
-// agrees on the outcome so all lanes leave together on a timeout.
+// agrees on the outcome so all lanes leave together on a timeout.  The usual
+// case, a plane that has already landed, takes one test and one vote.
 __device__ __forceinline__ bool warp_wait(unsigned bar, unsigned parity, int* err, int code, long long budget) {
+    if (__all_sync(0xffffffffu, mbar_try(bar, parity))) return true;
     const bool ok = mbar_wait(bar, parity, err, code, budget);
     return __all_sync(0xffffffffu, ok);
 }
@@ -343,14 +345,28 @@ __device__ __forceinline__ void warp_release(const TmaCta& t, unsigned G) {
     if (t.lane == 0) mbar_arrive(t.empty0 + 8 * (G % kStages));
 }
 
+// The coefficient pair (G1, G2) -- or (GM1, GM2) -- of a medium: from a
+// shared-memory table of pairs, or from the two global tables.
+struct TabPairs {
+    const float2* t;
+    __device__ __forceinline__ float2 operator()(int m) const { return t[m]; }
+};
+struct TabSplit {
+    const float* a;
+    const float* b;
+    __device__ __forceinline__ float2 operator()(int m) const { return make_float2(a[m], b[m]); }
+};
+
 // Consumers of the E side: Advance_Ex/Ey/Ez + AdvanceelectricCPML from the
 // ring, the same per-cell arithmetic as efield_column.  The item's planes are
-// G0 (k = kb-1, edge) and G0+1+(k-kb).  Plane k-1 is released once plane k is
-// done; with `release_last` the item's last plane is released too (a
-// persistent CTA goes on to another item).  False on a timeout.
-template <int CP>
-__device__ __forceinline__ bool e_consume(const TmaCta& t, unsigned G0, const KGrid& g, const KCpml& cp, const float* t1,
-                                          const float* t2, int* err, bool release_last, PsiRow* rows) {
+// G0 (k = kb-1, edge) and G0+1+(k-kb).  Hx and Hy of plane k-1 are carried
+// in registers (the edge plane's, then the previous iteration's), so a plane
+// is released as soon as it is done and the edge plane right after its two
+// values are read; with `release_last` the item's last plane is released too
+// (a persistent CTA goes on to another item).  False on a timeout.
+template <int CP, class TAB>
+__device__ __forceinline__ bool e_consume(const TmaCta& t, unsigned G0, const KGrid& g, const KCpml& cp, const TAB tab,
+                                          int* err, bool release_last, PsiRow* rows) {
     const int w = t.warp, l = t.lane;
     const int i = t.ib + l, j = t.jb + w;
     const int nya = (int)(g.plane / g.pitch);
@@ -360,10 +376,19 @@ __device__ __forceinline__ bool e_consume(const TmaCta& t, unsigned G0, const KG
     const unsigned tmask = CP ? cpml_tile_mask(cp, 0, t.ib, t.ib + kTX - 1, t.jb, t.jb + kTY - 1) : 0u;
     const CpmlCol cc = CP ? cpml_col(cp, 0, tmask, i, j, t.kb, t.ke) : CpmlCol{};
     if (CP == 2) psi_rows_fill(rows, cp, 0, tmask, kPsiSlotFloats, t.ib, j, l);
-    for (int k = t.kb; k <= t.ke; ++k) {
-        const unsigned Gk = G0 + 1 + (unsigned)(k - t.kb), Gp = Gk - 1;
-        const unsigned s = Gk % kStages, sp = Gp % kStages;
-        if (k == t.kb && !warp_wait(t.full0 + 8 * sp, (Gp / kStages) & 1, err, 2, t.wait)) return false;
+    float hx_km, hy_km;
+    {
+        const unsigned sp = G0 % kStages;
+        if (!warp_wait(t.full0 + 8 * sp, (G0 / kStages) & 1, err, 2, t.wait)) return false;
+        const unsigned char* pv = t.ring + sp * kStageBytes;
+        hx_km = ((const float*)(pv + kOffA))[(w + 1) * kTX + l];
+        hy_km = ((const float*)(pv + kOffB))[w * kHaloW + l + 4];
+        warp_release(t, G0);
+    }
+    long long c = i + pitch * j + plane * t.kb;
+    for (int k = t.kb; k <= t.ke; ++k, c += plane) {
+        const unsigned Gk = G0 + 1 + (unsigned)(k - t.kb);
+        const unsigned s = Gk % kStages;
         if (!warp_wait(t.full0 + 8 * s, (Gk / kStages) & 1, err, 1, t.wait)) return false;
         const unsigned char* st = t.ring + s * kStageBytes;
         // slabs holding cell (i, j, k): the column's slabs that hold plane k;
@@ -371,68 +396,67 @@ __device__ __forceinline__ bool e_consume(const TmaCta& t, unsigned G0, const KG
         const PlaneWords pw = *(const PlaneWords*)(st + kOffW);
         const unsigned pm = CP ? (cc.col & pw.live) : 0u;
         const float bz = pw.bz, cz = pw.cz;
-        const unsigned char* pv = t.ring + sp * kStageBytes;
         const float* HX = (const float*)(st + kOffA);
         const float* HY = (const float*)(st + kOffB);
         const float* HZ = (const float*)(st + kOffC);
-        const float* HXp = (const float*)(pv + kOffA);
-        const float* HYp = (const float*)(pv + kOffB);
         const float* EF = (const float*)(st + kOffF);
         const uint8_t* MF = (const uint8_t*)(st + kOffM);
         const float* PS = (const float*)(st + kOffP);
         constexpr int fs = align128(kBoxF) / 4, ms = align128(kBoxM);
-        const float hx = HX[(w + 1) * kTX + l], hx_jm = HX[w * kTX + l], hx_km = HXp[(w + 1) * kTX + l];
-        const float hy = HY[w * kHaloW + l + 4], hy_im = HY[w * kHaloW + l + 3], hy_km = HYp[w * kHaloW + l + 4];
+        const float hx = HX[(w + 1) * kTX + l], hx_jm = HX[w * kTX + l];
+        const float hy = HY[w * kHaloW + l + 4], hy_im = HY[w * kHaloW + l + 3];
         const float hz = HZ[(w + 1) * kHaloW + l + 4], hz_jm = HZ[w * kHaloW + l + 4], hz_im = HZ[(w + 1) * kHaloW + l + 3];
         const float idzh = pw.idz;
-        const long long c = i + pitch * j + plane * k;
         const int o = w * kTX + l;
         bool st_ = true;
         if (vx && k >= g.sw[0][4] && k <= g.sw[0][5]) {
             float e = EF[o];
-            const int m = MF[o];
+            const float2 tt = tab(MF[o]);
             const float dy = hz - hz_jm, dz = hy - hy_km;
-            e = t1[m] * e + t2[m] * (dy * idyh - dz * idzh);
+            e = tt.x * e + tt.y * (dy * idyh - dz * idzh);
             if (CP && pm) {
-                e = cpml_corr<CP, true>(cp.s[0][0], pm & 3, 0, PS, o, rows, i, j, k, cc.by, cc.cy, dy, t2[m], e, st_);
-                e = cpml_corr<CP, false>(cp.s[0][1], (pm >> 2) & 3, 2, PS, o, rows, i, j, k, bz, cz, dz, t2[m], e, st_);
+                e = cpml_corr<CP, true>(cp.s[0][0], pm & 3, 0, PS, o, rows, i, j, k, cc.by, cc.cy, dy, tt.y, e, st_);
+                e = cpml_corr<CP, false>(cp.s[0][1], (pm >> 2) & 3, 2, PS, o, rows, i, j, k, bz, cz, dz, tt.y, e, st_);
             }
             g.F[0][c] = e;
         }
         if (vy && k >= g.sw[1][4] && k <= g.sw[1][5]) {
             float e = EF[fs + o];
-            const int m = MF[ms + o];
+            const float2 tt = tab(MF[ms + o]);
             const float dz = hx - hx_km, dx = hz - hz_im;
-            e = t1[m] * e + t2[m] * (dz * idzh - dx * idxh);
+            e = tt.x * e + tt.y * (dz * idzh - dx * idxh);
             if (CP && pm) {
-                e = cpml_corr<CP, true>(cp.s[1][0], (pm >> 4) & 3, 4, PS, o, rows, i, j, k, bz, cz, dz, t2[m], e, st_);
-                e = cpml_corr<CP, false>(cp.s[1][1], (pm >> 6) & 3, 6, PS, o, rows, i, j, k, cc.bx, cc.cx, dx, t2[m], e, st_);
+                e = cpml_corr<CP, true>(cp.s[1][0], (pm >> 4) & 3, 4, PS, o, rows, i, j, k, bz, cz, dz, tt.y, e, st_);
+                e = cpml_corr<CP, false>(cp.s[1][1], (pm >> 6) & 3, 6, PS, o, rows, i, j, k, cc.bx, cc.cx, dx, tt.y, e, st_);
             }
             g.F[1][c] = e;
         }
         if (vz && k >= g.sw[2][4] && k <= g.sw[2][5]) {
             float e = EF[2 * fs + o];
-            const int m = MF[2 * ms + o];
+            const float2 tt = tab(MF[2 * ms + o]);
             const float dx = hy - hy_im, dy = hx - hx_jm;
-            e = t1[m] * e + t2[m] * (dx * idxh - dy * idyh);
+            e = tt.x * e + tt.y * (dx * idxh - dy * idyh);
             if (CP && pm) {
-                e = cpml_corr<CP, false>(cp.s[2][0], (pm >> 8) & 3, 8, PS, o, rows, i, j, k, cc.by, cc.cy, dy, t2[m], e, st_);
-                e = cpml_corr<CP, true>(cp.s[2][1], (pm >> 10) & 3, 10, PS, o, rows, i, j, k, cc.bx, cc.cx, dx, t2[m], e, st_);
+                e = cpml_corr<CP, false>(cp.s[2][0], (pm >> 8) & 3, 8, PS, o, rows, i, j, k, cc.by, cc.cy, dy, tt.y, e, st_);
+                e = cpml_corr<CP, true>(cp.s[2][1], (pm >> 10) & 3, 10, PS, o, rows, i, j, k, cc.bx, cc.cx, dx, tt.y, e, st_);
             }
             g.F[2][c] = e;
         }
-        warp_release(t, Gp);  // plane k-1 is no longer needed
+        hx_km = hx;
+        hy_km = hy;
+        if (k < t.ke || release_last) warp_release(t, Gk);  // plane k is no longer needed
     }
-    if (release_last) warp_release(t, G0 + 1 + (unsigned)(t.ke - t.kb));
     return true;
 }
 
 // Consumers of the H side: Advance_Hx/Hy/Hz + AdvanceMagneticCPML from the
 // ring (hfield_column's arithmetic).  The item's planes are G0+(k-kb) for
-// k = kb..ke+1 (ke+1 the edge); plane k is released once it is done.
-template <int CP>
-__device__ __forceinline__ bool h_consume(const TmaCta& t, unsigned G0, const KGrid& g, const KCpml& cp, const float* t1,
-                                          const float* t2, int* err, bool release_last, PsiRow* rows) {
+// k = kb..ke+1 (ke+1 the edge); plane k is released once it is done.  Ex and
+// Ey of plane k are carried from the previous iteration (they were its k+1
+// values), and plane k itself was waited for there.
+template <int CP, class TAB>
+__device__ __forceinline__ bool h_consume(const TmaCta& t, unsigned G0, const KGrid& g, const KCpml& cp, const TAB tab,
+                                          int* err, bool release_last, PsiRow* rows) {
     const int w = t.warp, l = t.lane;
     const int i = t.ib + l, j = t.jb + w;
     const int nya = (int)(g.plane / g.pitch);
@@ -442,10 +466,18 @@ __device__ __forceinline__ bool h_consume(const TmaCta& t, unsigned G0, const KG
     const unsigned tmask = CP ? cpml_tile_mask(cp, 3, t.ib, t.ib + kTX - 1, t.jb, t.jb + kTY - 1) : 0u;
     const CpmlCol cc = CP ? cpml_col(cp, 3, tmask, i, j, t.kb, t.ke) : CpmlCol{};
     if (CP == 2) psi_rows_fill(rows, cp, 3, tmask, kPsiSlotFloats, t.ib, j, l);
-    for (int k = t.kb; k <= t.ke; ++k) {
+    float ex, ey;
+    {
+        const unsigned s0 = G0 % kStages;
+        if (!warp_wait(t.full0 + 8 * s0, (G0 / kStages) & 1, err, 3, t.wait)) return false;
+        const unsigned char* st = t.ring + s0 * kStageBytes;
+        ex = ((const float*)(st + kOffA))[w * kTX + l];
+        ey = ((const float*)(st + kOffB))[w * kHaloW + l];
+    }
+    long long c = i + pitch * j + plane * t.kb;
+    for (int k = t.kb; k <= t.ke; ++k, c += plane) {
         const unsigned Gk = G0 + (unsigned)(k - t.kb), Gn = Gk + 1;
         const unsigned s = Gk % kStages, sn = Gn % kStages;
-        if (!warp_wait(t.full0 + 8 * s, (Gk / kStages) & 1, err, 3, t.wait)) return false;
         if (!warp_wait(t.full0 + 8 * sn, (Gn / kStages) & 1, err, 4, t.wait)) return false;
         const unsigned char* st = t.ring + s * kStageBytes;
         // slabs holding cell (i, j, k), the plane's Idze and P_b / P_c pair
@@ -456,52 +488,51 @@ __device__ __forceinline__ bool h_consume(const TmaCta& t, unsigned G0, const KG
         const float* EX = (const float*)(st + kOffA);
         const float* EY = (const float*)(st + kOffB);
         const float* EZ = (const float*)(st + kOffC);
-        const float* EXn = (const float*)(nx + kOffA);
-        const float* EYn = (const float*)(nx + kOffB);
         const float* HF = (const float*)(st + kOffF);
         const uint8_t* MF = (const uint8_t*)(st + kOffM);
         const float* PS = (const float*)(st + kOffP);
         constexpr int fs = align128(kBoxF) / 4, ms = align128(kBoxM);
-        const float ex = EX[w * kTX + l], ex_jp = EX[(w + 1) * kTX + l], ex_kp = EXn[w * kTX + l];
-        const float ey = EY[w * kHaloW + l], ey_ip = EY[w * kHaloW + l + 1], ey_kp = EYn[w * kHaloW + l];
+        const float ex_jp = EX[(w + 1) * kTX + l], ex_kp = ((const float*)(nx + kOffA))[w * kTX + l];
+        const float ey_ip = EY[w * kHaloW + l + 1], ey_kp = ((const float*)(nx + kOffB))[w * kHaloW + l];
         const float ez = EZ[w * kHaloW + l], ez_ip = EZ[w * kHaloW + l + 1], ez_jp = EZ[(w + 1) * kHaloW + l];
         const float idze = pw.idz;
-        const long long c = i + pitch * j + plane * k;
         const int o = w * kTX + l;
         bool st_ = true;
         if (vx && k >= g.sw[3][4] && k <= g.sw[3][5]) {
             float h = HF[o];
-            const int m = MF[o];
+            const float2 tt = tab(MF[o]);
             const float dz = ey_kp - ey, dy = ez_jp - ez;
-            h = t1[m] * h + t2[m] * (dz * idze - dy * idye);
+            h = tt.x * h + tt.y * (dz * idze - dy * idye);
             if (CP && pm) {
-                h = cpml_corr<CP, false>(cp.s[3][0], pm & 3, 0, PS, o, rows, i, j, k, cc.by, cc.cy, dy, t2[m], h, st_);
-                h = cpml_corr<CP, true>(cp.s[3][1], (pm >> 2) & 3, 2, PS, o, rows, i, j, k, bz, cz, dz, t2[m], h, st_);
+                h = cpml_corr<CP, false>(cp.s[3][0], pm & 3, 0, PS, o, rows, i, j, k, cc.by, cc.cy, dy, tt.y, h, st_);
+                h = cpml_corr<CP, true>(cp.s[3][1], (pm >> 2) & 3, 2, PS, o, rows, i, j, k, bz, cz, dz, tt.y, h, st_);
             }
             g.F[3][c] = h;
         }
         if (vy && k >= g.sw[4][4] && k <= g.sw[4][5]) {
             float h = HF[fs + o];
-            const int m = MF[ms + o];
+            const float2 tt = tab(MF[ms + o]);
             const float dx = ez_ip - ez, dz = ex_kp - ex;
-            h = t1[m] * h + t2[m] * (dx * idxe - dz * idze);
+            h = tt.x * h + tt.y * (dx * idxe - dz * idze);
             if (CP && pm) {
-                h = cpml_corr<CP, false>(cp.s[4][0], (pm >> 4) & 3, 4, PS, o, rows, i, j, k, bz, cz, dz, t2[m], h, st_);
-                h = cpml_corr<CP, true>(cp.s[4][1], (pm >> 6) & 3, 6, PS, o, rows, i, j, k, cc.bx, cc.cx, dx, t2[m], h, st_);
+                h = cpml_corr<CP, false>(cp.s[4][0], (pm >> 4) & 3, 4, PS, o, rows, i, j, k, bz, cz, dz, tt.y, h, st_);
+                h = cpml_corr<CP, true>(cp.s[4][1], (pm >> 6) & 3, 6, PS, o, rows, i, j, k, cc.bx, cc.cx, dx, tt.y, h, st_);
             }
             g.F[4][c] = h;
         }
         if (vz && k >= g.sw[5][4] && k <= g.sw[5][5]) {
             float h = HF[2 * fs + o];
-            const int m = MF[2 * ms + o];
+            const float2 tt = tab(MF[2 * ms + o]);
             const float dy = ex_jp - ex, dx = ey_ip - ey;
-            h = t1[m] * h + t2[m] * (dy * idye - dx * idxe);
+            h = tt.x * h + tt.y * (dy * idye - dx * idxe);
             if (CP && pm) {
-                h = cpml_corr<CP, true>(cp.s[5][0], (pm >> 8) & 3, 8, PS, o, rows, i, j, k, cc.by, cc.cy, dy, t2[m], h, st_);
-                h = cpml_corr<CP, false>(cp.s[5][1], (pm >> 10) & 3, 10, PS, o, rows, i, j, k, cc.bx, cc.cx, dx, t2[m], h, st_);
+                h = cpml_corr<CP, true>(cp.s[5][0], (pm >> 8) & 3, 8, PS, o, rows, i, j, k, cc.by, cc.cy, dy, tt.y, h, st_);
+                h = cpml_corr<CP, false>(cp.s[5][1], (pm >> 10) & 3, 10, PS, o, rows, i, j, k, cc.bx, cc.cx, dx, tt.y, h, st_);
             }
             g.F[5][c] = h;
         }
+        ex = ex_kp;
+        ey = ey_kp;
         warp_release(t, Gk);  // plane k is no longer needed
     }
     if (release_last) warp_release(t, G0 + 1 + (unsigned)(t.ke - t.kb));
