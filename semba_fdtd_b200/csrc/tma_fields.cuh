@@ -191,8 +191,10 @@ __device__ __forceinline__ void prod_prepare(ProdTable* tb, const TmaCta& t, int
 }
 
 // Producer (lane 0 of the producer warp): planes p0 .. p1 of one work item
-// into the ring; the item's first plane has the running plane number G0 (a
-// plane lands in stage G % kStages; its n-th use of that stage is phase n).
+// into the ring, upwards on the E side and downwards on the H side, so that
+// either side's edge plane comes first; the item's first plane has the
+// running plane number G0 (a plane lands in stage G % kStages; its n-th use
+// of that stage is phase n).
 // `edge` is the plane that carries only the first two arrays (the E side's
 // k-1 plane, the H side's k+1 plane).  Tile origins: E side Hx (ib, jb-1),
 // Hy (ib-4, jb), Hz (ib-4, jb-1), own fields and media (ib, jb); H side all
@@ -204,10 +206,11 @@ __device__ __forceinline__ void prod_prepare(ProdTable* tb, const TmaCta& t, int
 // and psi coordinates come from the table prod_prepare filled.
 __device__ __forceinline__ int tma_issue(const TmaCta& t, const CUtensorMap* maps, unsigned G0, int p0, int p1, int edge,
                                          bool hside, int* err, const ProdTable* tb, unsigned smask) {
-    for (int p = p0; p <= p1; ++p) {
-        const unsigned G = G0 + (unsigned)(p - p0), s = G % kStages, u = G / kStages;
+    for (int n = 0; n <= p1 - p0; ++n) {
+        const int p = hside ? p1 - n : p0 + n;  // the H side marches down
+        const unsigned G = G0 + (unsigned)n, s = G % kStages, u = G / kStages;
         const PlaneWords w = tb->w[p - p0];
-        if (u >= 1 && !mbar_wait(t.empty0 + 8 * s, (u - 1) & 1, err, hside ? 13 : 11, t.wait)) return p - p0;
+        if (u >= 1 && !mbar_wait(t.empty0 + 8 * s, (u - 1) & 1, err, hside ? 13 : 11, t.wait)) return n;
         const unsigned bar = t.full0 + 8 * s;
         unsigned char* st = t.ring + s * kStageBytes;
         const bool part = p == edge;
@@ -223,11 +226,11 @@ __device__ __forceinline__ int tma_issue(const TmaCta& t, const CUtensorMap* map
             for (int q = 0; q < 3; ++q) tma_load3(smem_u32(st + kOffM + q * align128(kBoxM)), &maps[6 + q], t.ib, t.jb, p, bar);
         }
         while (live) {
-            const int n = __ffs(live) - 1;
+            const int b = __ffs(live) - 1;
             live &= live - 1u;
-            const int4 c = tb->psi[n];
-            const int slot = psi_slot(smask, n);
-            tma_load3(smem_u32(st + kOffP + slot * align128(kBoxP)), &maps[kPsiMap0 + n], c.x, c.y, p - c.z, bar);
+            const int4 c = tb->psi[b];
+            const int slot = psi_slot(smask, b);
+            tma_load3(smem_u32(st + kOffP + slot * align128(kBoxP)), &maps[kPsiMap0 + b], c.x, c.y, p - c.z, bar);
         }
     }
     return p1 - p0 + 1;
@@ -264,8 +267,9 @@ __device__ __forceinline__ int tma_issue_warp(const TmaCta& t, const CUtensorMap
         pc = tb->psi[n];
         poff = kOffP + psi_slot(smask, n) * align128(kBoxP);
     }
-    for (int p = p0; p <= p1; ++p) {
-        const unsigned G = G0 + (unsigned)(p - p0), s = G % kStages, u = G / kStages;
+    for (int m = 0; m <= p1 - p0; ++m) {
+        const int p = hside ? p1 - m : p0 + m;  // the H side marches down
+        const unsigned G = G0 + (unsigned)m, s = G % kStages, u = G / kStages;
         const unsigned bar = t.full0 + 8 * s;
         unsigned char* st = t.ring + s * kStageBytes;
         const bool part = p == edge;
@@ -281,7 +285,7 @@ __device__ __forceinline__ int tma_issue_warp(const TmaCta& t, const CUtensorMap
             }
         }
         ok = __shfl_sync(0xffffffffu, ok, 0);
-        if (!ok) return p - p0;
+        if (!ok) return m;
         __syncwarp();  // the stage is free and armed before any lane writes into it
         if (q < kPsiMap0) {
             if (q < 2 || !part) tma_load3(smem_u32(st + off), &maps[q], bx, by, p, bar);
@@ -450,10 +454,11 @@ __device__ __forceinline__ bool e_consume(const TmaCta& t, unsigned G0, const KG
 }
 
 // Consumers of the H side: Advance_Hx/Hy/Hz + AdvanceMagneticCPML from the
-// ring (hfield_column's arithmetic).  The item's planes are G0+(k-kb) for
-// k = kb..ke+1 (ke+1 the edge); plane k is released once it is done.  Ex and
-// Ey of plane k are carried from the previous iteration (they were its k+1
-// values), and plane k itself was waited for there.
+// ring (hfield_column's arithmetic), marching down: the item's planes are G0
+// (k = ke+1, edge) and G0+1+(ke-k).  Ex and Ey of plane k+1 are carried in
+// registers (the edge plane's, then the previous iteration's), so a plane is
+// released as soon as it is done and the edge plane right after its two
+// values are read; with `release_last` the item's last plane is released too.
 template <int CP, class TAB>
 __device__ __forceinline__ bool h_consume(const TmaCta& t, unsigned G0, const KGrid& g, const KCpml& cp, const TAB tab,
                                           int* err, bool release_last, PsiRow* rows) {
@@ -466,25 +471,25 @@ __device__ __forceinline__ bool h_consume(const TmaCta& t, unsigned G0, const KG
     const unsigned tmask = CP ? cpml_tile_mask(cp, 3, t.ib, t.ib + kTX - 1, t.jb, t.jb + kTY - 1) : 0u;
     const CpmlCol cc = CP ? cpml_col(cp, 3, tmask, i, j, t.kb, t.ke) : CpmlCol{};
     if (CP == 2) psi_rows_fill(rows, cp, 3, tmask, kPsiSlotFloats, t.ib, j, l);
-    float ex, ey;
+    float ex_kp, ey_kp;
     {
         const unsigned s0 = G0 % kStages;
-        if (!warp_wait(t.full0 + 8 * s0, (G0 / kStages) & 1, err, 3, t.wait)) return false;
-        const unsigned char* st = t.ring + s0 * kStageBytes;
-        ex = ((const float*)(st + kOffA))[w * kTX + l];
-        ey = ((const float*)(st + kOffB))[w * kHaloW + l];
+        if (!warp_wait(t.full0 + 8 * s0, (G0 / kStages) & 1, err, 4, t.wait)) return false;
+        const unsigned char* nx = t.ring + s0 * kStageBytes;
+        ex_kp = ((const float*)(nx + kOffA))[w * kTX + l];
+        ey_kp = ((const float*)(nx + kOffB))[w * kHaloW + l];
+        warp_release(t, G0);
     }
-    long long c = i + pitch * j + plane * t.kb;
-    for (int k = t.kb; k <= t.ke; ++k, c += plane) {
-        const unsigned Gk = G0 + (unsigned)(k - t.kb), Gn = Gk + 1;
-        const unsigned s = Gk % kStages, sn = Gn % kStages;
-        if (!warp_wait(t.full0 + 8 * sn, (Gn / kStages) & 1, err, 4, t.wait)) return false;
+    long long c = i + pitch * j + plane * t.ke;
+    for (int k = t.ke; k >= t.kb; --k, c -= plane) {
+        const unsigned Gk = G0 + 1 + (unsigned)(t.ke - k);
+        const unsigned s = Gk % kStages;
+        if (!warp_wait(t.full0 + 8 * s, (Gk / kStages) & 1, err, 3, t.wait)) return false;
         const unsigned char* st = t.ring + s * kStageBytes;
         // slabs holding cell (i, j, k), the plane's Idze and P_b / P_c pair
         const PlaneWords pw = *(const PlaneWords*)(st + kOffW);
         const unsigned pm = CP ? (cc.col & pw.live) : 0u;
         const float bz = pw.bz, cz = pw.cz;
-        const unsigned char* nx = t.ring + sn * kStageBytes;
         const float* EX = (const float*)(st + kOffA);
         const float* EY = (const float*)(st + kOffB);
         const float* EZ = (const float*)(st + kOffC);
@@ -492,8 +497,8 @@ __device__ __forceinline__ bool h_consume(const TmaCta& t, unsigned G0, const KG
         const uint8_t* MF = (const uint8_t*)(st + kOffM);
         const float* PS = (const float*)(st + kOffP);
         constexpr int fs = align128(kBoxF) / 4, ms = align128(kBoxM);
-        const float ex_jp = EX[(w + 1) * kTX + l], ex_kp = ((const float*)(nx + kOffA))[w * kTX + l];
-        const float ey_ip = EY[w * kHaloW + l + 1], ey_kp = ((const float*)(nx + kOffB))[w * kHaloW + l];
+        const float ex = EX[w * kTX + l], ex_jp = EX[(w + 1) * kTX + l];
+        const float ey = EY[w * kHaloW + l], ey_ip = EY[w * kHaloW + l + 1];
         const float ez = EZ[w * kHaloW + l], ez_ip = EZ[w * kHaloW + l + 1], ez_jp = EZ[(w + 1) * kHaloW + l];
         const float idze = pw.idz;
         const int o = w * kTX + l;
@@ -531,11 +536,10 @@ __device__ __forceinline__ bool h_consume(const TmaCta& t, unsigned G0, const KG
             }
             g.F[5][c] = h;
         }
-        ex = ex_kp;
-        ey = ey_kp;
-        warp_release(t, Gk);  // plane k is no longer needed
+        ex_kp = ex;
+        ey_kp = ey;
+        if (k > t.kb || release_last) warp_release(t, Gk);  // plane k is no longer needed
     }
-    if (release_last) warp_release(t, G0 + 1 + (unsigned)(t.ke - t.kb));
     return true;
 }
 
