@@ -365,6 +365,7 @@ __global__ void __launch_bounds__(kPhaseThreads)
         const int n = inst_step(D, G, &on);
         if (!on) continue;  // the same for the whole block: the item is one instance's
         const bool pw_on = pw_switch_block(D.src[side], n, D.tiempo, 0, D.dt, side);
+        if (D.src[side].pw_only && !pw_on) continue;  // nothing applies once the switch is down
         const long long r = w.q0 + threadIdx.x;
         if (r < w.q1)
             source_row(D.g, D.src[side], n, D.tiempo, 0, D.dt, side,

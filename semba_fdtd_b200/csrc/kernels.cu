@@ -202,8 +202,10 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
     else h_consume<0>(t, 0, g, cp, tab, err, false, rows[t.warp]);
 }
 
+// One node a thread, 128-thread blocks, 12 blocks an SM (40 registers).
+constexpr int kAdeBlock = 128;
 template <int NU, bool MAG, bool UNI>
-__global__ void __launch_bounds__(256, 6) k_ade(KGrid g, KDisp d, int comp) {
+__global__ void __launch_bounds__(kAdeBlock, 12) k_ade(KGrid g, KDisp d, int comp) {
     const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (q < d.n[comp]) ade_node<NU, MAG, UNI>(ade_refs<MAG>(g, d, comp), q);
 }
@@ -216,6 +218,9 @@ __global__ void k_sources(KGrid g, KSrc s, StepRef sr, const double* tiempo, int
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = step_of(sr);
     const bool pw_on = (mask & (1 << kSrcPlaneWave)) ? pw_switch_block(s, n, tiempo, t_n0, dt, hside) : false;
+    // with the switch down a row of plane-wave contributions alone changes
+    // nothing: the reference calls no plane-wave routine then
+    if (s.pw_only && !pw_on) return;
     if (r < s.nrows) source_row(g, s, n, tiempo, t_n0, dt, hside, mask, r, pw_on);
 }
 
@@ -392,7 +397,12 @@ template <int MODE> sgpu_status launch_h(sgpu_ctx* c) {
     return check_launch(c, "k_hfield");
 }
 
-constexpr int kTmaChunk = 32;
+// planes per CTA of the TMA field kernels (halved on small grids until the
+// grid has four CTAs per SM)
+#ifndef SGPU_TMA_CHUNK
+#define SGPU_TMA_CHUNK 64
+#endif
+constexpr int kTmaChunk = SGPU_TMA_CHUNK;
 
 sgpu_status launch_tma(sgpu_ctx* c, bool hside) {
     Launch L = plan(c, hside ? 3 : 0, hside ? 5 : 2);
@@ -493,8 +503,8 @@ sgpu_status build_sources(sgpu_ctx* c);
 
 template <int NU, bool MAG> void ade_launch(sgpu_ctx* c, int comp, unsigned blocks) {
     const KDisp& d = MAG ? c->mdisp : c->disp;
-    if (d.uniform) k_ade<NU, MAG, true><<<blocks, 256, 0, c->stream>>>(kgrid(c), d, comp);
-    else k_ade<NU, MAG, false><<<blocks, 256, 0, c->stream>>>(kgrid(c), d, comp);
+    if (d.uniform && d.nu_max == NU) k_ade<NU, MAG, true><<<blocks, kAdeBlock, 0, c->stream>>>(kgrid(c), d, comp);
+    else k_ade<NU, MAG, false><<<blocks, kAdeBlock, 0, c->stream>>>(kgrid(c), d, comp);
 }
 
 template <bool MAG> sgpu_status launch_ade_side(sgpu_ctx* c) {
@@ -503,7 +513,7 @@ template <bool MAG> sgpu_status launch_ade_side(sgpu_ctx* c) {
     for (int comp = 0; comp < 3; ++comp) {
         long long n = d.n[comp];
         if (n == 0) continue;
-        const unsigned blocks = (unsigned)((n + 255) / 256);
+        const unsigned blocks = (unsigned)((n + kAdeBlock - 1) / kAdeBlock);
         switch (d.nu_max) {
             case 1: ade_launch<1, MAG>(c, comp, blocks); break;
             case 2: ade_launch<2, MAG>(c, comp, blocks); break;
@@ -1179,7 +1189,7 @@ sgpu_status init_ade(sgpu_ctx* c, const sgpu_edisp_desc* d, bool mag) {
     k.media = dmedia;
     k.slot_of_medium = dslot;
     k.nu_max = nu_max;
-    k.uniform = 1;
+    k.uniform = nu_max >= 1;
     for (const DispMedium& dm : media) k.uniform &= dm.nu == nu_max;
     k.dt = c->dt;
     k.inv_dt = 1.0 / c->dt;
@@ -1340,6 +1350,8 @@ sgpu_status build_sources(sgpu_ctx* c) {
         k.samples = dsm;
         k.ntab = (int)tabs.size();
         k.h_first = c->h_first;
+        k.pw_only = 1;
+        for (const SrcEntry& en : ent) k.pw_only &= en.type == kSrcPlaneWave;
     }
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     c->src_dirty = false;

@@ -195,7 +195,7 @@ sgpu_status dispersive(sgpu_ctx* c, Records& r, bool mag) {
                 if (med[comp][q] != m) continue;
                 RREC(&prev[comp][q], sizeof(float));
                 for (int p = 0; p < dm.np; ++p) {
-                    double2& slot = J[comp][(size_t)dm.map[p] * n + q];
+                    double2& slot = J[comp][q * (size_t)std::max(1, k.nu_max) + dm.map[p]];
                     double v[2] = {slot.x, first[p] ? slot.y : -slot.y};
                     RREC(v, sizeof(v));
                     if (!r.write && first[p]) slot = make_double2(v[0], v[1]);

@@ -67,7 +67,7 @@ struct KDisp {
     const int* node[3];           // linear local index per node
     const uint8_t* med[3];        // dispersive-medium slot per node
     float* prev[3];
-    double2* J[3];                // [unique slot][node]
+    double2* J[3];                // [node][unique slot], nu_max slots a node
     long long n[3];
     // per 32 consecutive nodes (a warp's worth): the group's nodes as at
     // most two runs of consecutive cells of one medium each -- x: cell of
@@ -113,6 +113,7 @@ struct KSrc {
     const float* samples;
     int ntab;
     int h_first;           // first half step 2n + side run since the start (or a resume)
+    int pw_only;           // every contribution is a plane wave's: rows change nothing once the switch is down
 };
 
 // Borders of the H field outside the swept box (local coordinates).

@@ -385,15 +385,16 @@ struct AdeRefs {
     const uint8_t* med;
     const int4* grp;
     float* prev;
-    double2* J;
+    double2* J;  // [node][state slot], ju slots a node
     long long n;
+    int ju;
     const DispMedium* media;
     float* F;
     double dt, inv_dt;
 };
 template <bool MAG> __device__ __forceinline__ AdeRefs ade_refs(const KGrid& g, const KDisp& d, int comp) {
-    return AdeRefs{d.node[comp], d.med[comp], d.grp[comp], d.prev[comp], d.J[comp], d.n[comp], d.media,
-                   g.F[MAG ? 3 + comp : comp], d.dt, d.inv_dt};
+    return AdeRefs{d.node[comp], d.med[comp], d.grp[comp], d.prev[comp], d.J[comp], d.n[comp], max(1, d.nu_max),
+                   d.media, g.F[MAG ? 3 + comp : comp], d.dt, d.inv_dt};
 }
 
 // Node q's cell and medium slot.  Nodes are numbered in cell order, so the 32
@@ -430,7 +431,7 @@ template <int NU, bool UNI>
 __device__ __forceinline__ void ade_load(const AdeRefs& d, long long q, AdeNode<NU>& a) {
     if (UNI) {
 #pragma unroll
-        for (int u = 0; u < NU; ++u) a.st[u] = d.J[u * d.n + q];
+        for (int u = 0; u < NU; ++u) a.st[u] = d.J[q * d.ju + u];
         a.prev = d.prev[q];
     }
     int slot;
@@ -439,7 +440,7 @@ __device__ __forceinline__ void ade_load(const AdeRefs& d, long long q, AdeNode<
     if (!UNI) {
         const int nu = a.md->nu;
 #pragma unroll
-        for (int u = 0; u < NU; ++u) a.st[u] = u < nu ? d.J[u * d.n + q] : make_double2(0.0, 0.0);
+        for (int u = 0; u < NU; ++u) a.st[u] = u < nu ? d.J[q * d.ju + u] : make_double2(0.0, 0.0);
         a.prev = d.prev[q];
     }
     a.e = d.F[a.idx];
@@ -489,7 +490,7 @@ __device__ __forceinline__ void ade_store(const AdeRefs& d, long long q, const A
     const int nu = UNI ? NU : a.md->nu;
 #pragma unroll
     for (int u = 0; u < NU; ++u)
-        if (u < nu) d.J[u * d.n + q] = a.st[u];
+        if (u < nu) d.J[q * d.ju + u] = a.st[u];
     d.prev[q] = a.e;
     d.F[a.idx] = a.e;
 }
