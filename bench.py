@@ -443,13 +443,17 @@ def run_batched(args):
         marks["plan"] = time.perf_counter() - t0
         arena = int(sum(p.footprint for p in plans) * 1.05) + (64 << 20)
         with Batch(arena, len(pbs) + 1, kernel_family=args.batch_family) as b:
-            # in stream order (or longest solves first, which measured slower:
-            # the tuner then sees only the largest grids), a first group tuned
-            # on, then 32-step chunks queued between the remaining set-ups: an
-            # instance is set up on its own stream while the queued steps of
-            # the others run
+            # most steps first (or in stream order, or most work first, which
+            # measured slower: the tuner then sees only the largest grids), a
+            # first group tuned on, then 32-step chunks queued between the
+            # remaining set-ups: an instance is set up on its own stream while
+            # the queued steps of the others run
             if args.batch_order == "longest":
                 plans = sorted(plans, key=lambda p: -(p.nsteps + 1) * p.problem.swept_cells)
+            elif args.batch_order == "steps":
+                # most steps first: the solves that set the length of the run
+                # start first (a stable sort, stream order among equals)
+                plans = sorted(plans, key=lambda p: -p.nsteps)
             first = 8
             slots = [b.add(p) for p in plans[:first]]
             chunks, ctas = b.autotune(2)
@@ -532,7 +536,7 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true", help="skip the CPU-baseline leg and its parity check")
     ap.add_argument("--instances", type=int, default=64, help="batched: instances in the stream")
     ap.add_argument("--skip-plain", action="store_true", help="batched: leave out the one-at-a-time arm (profiling)")
-    ap.add_argument("--batch-order", default="stream", choices=["longest", "stream"],
+    ap.add_argument("--batch-order", default="steps", choices=["longest", "steps", "stream"],
                     help="batched: order in which the instances join the batch")
     ap.add_argument("--batch-advance-every", type=int, default=4,
                     help="batched: a 32-step chunk is queued after this many instance set-ups")

@@ -554,14 +554,15 @@ sgpu_status sgpu_batch_set_kernel_family(sgpu_batch* b, int family);
 sgpu_status sgpu_batch_set_wait_cycles(sgpu_batch* b, int64_t cycles);
 /* The failure drill of sgpu_set_wait_drill for the batch's kernels. */
 sgpu_status sgpu_batch_set_wait_drill(sgpu_batch* b, int on);
-/* Launch shape: z-chunk length (1..64) of the field work items for the three
+/* Launch shape: z-chunk length (1..1024) of the field work items for the three
  * size classes (Alloc z extent <= 80, <= 160, larger) and persistent CTAs per SM.
  * Either may be NULL / 0 to keep the current value. */
 sgpu_status sgpu_batch_set_tuning(sgpu_batch* b, const int* chunk3, int ctas_per_sm);
 sgpu_status sgpu_batch_get_tuning(const sgpu_batch* b, int* chunk3, int* ctas_per_sm);
 /* Online autotuner: times steps_per_trial real steps of the live instances
- * per candidate (CTAs per SM in 2,3,4,6, then z chunk 4..64 per size class
- * present) and keeps the fastest.  The trials advance the instances. */
+ * per candidate (CTAs per SM in 2,3,4,6, then z chunk 128..8 per size class
+ * present, a shorter chunk kept only when 3 % faster) and keeps the fastest.
+ * The trials advance the instances. */
 sgpu_status sgpu_batch_autotune(sgpu_batch* b, int steps_per_trial, int* chunk3, int* ctas_per_sm);
 /* Device time of each phase summed over nsteps real steps launched one by
  * one: E field + CPML, ADE, E sources, H field + CPML, H sources and

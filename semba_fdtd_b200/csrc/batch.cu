@@ -234,7 +234,7 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
                       const int* counts, const int* G, int* err, long long wait, int drill, int* next) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ WarpView views[kConsumerWarps];
-    __shared__ ProdTable tb;
+    __shared__ ProdWindow tb;
     __shared__ PsiRow rows[kConsumerWarps][12];
     TmaCta t = tma_cta_setup(smem, 0, 0, 0, 1, wait);
     const int n_items = counts[SIDE == 0 ? kCntE : kCntH];
@@ -267,7 +267,8 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
             const int edge = SIDE == 0 ? w.kb - 1 : w.ke + 1;
             const unsigned tmask = w.cp ? cpml_tile_mask(D.cp, c0, w.ib, w.ib + kTX - 1, w.jb, w.jb + kTY - 1) : 0u;
             const unsigned smask = w.cp ? staged_mask(D.cp, c0, w.ib, w.jb) : 0u;
-            prod_prepare(&tb, t, p0, p1, edge, SIDE != 0, D.g, D.cp, tmask);
+            prod_psi(&tb, t, SIDE != 0, D.cp, tmask);
+            const PlaneSource src{&D.g, &D.cp, tmask};
             const CUtensorMap* m = maps[2 * w.slot + SIDE].m;
             // each lane acquires the one map it issues through (lane q: map q),
             // once per instance, when this item loads through it
@@ -280,7 +281,7 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
                 tensormap_acquire(&m[t.lane]);
                 facq = true;
             }
-            const int got = tma_issue_warp(t, m, gp, p0, p1, edge, SIDE != 0, err, &tb, smask, it);
+            const int got = tma_issue_warp(t, m, gp, p0, p1, edge, SIDE != 0, err, &tb, src, smask, it);
             if (got < np) {
                 if (t.lane == 0) tma_drain(t, gp + (unsigned)got, err, 15);
                 return;
@@ -469,7 +470,7 @@ struct sgpu_batch {
     int G = 0;                 // host mirror of the device step counter
     int nu_max = 1;
     // launch shape
-    int chunk[kNumClasses] = {16, 16, 32};
+    int chunk[kNumClasses] = {32, 64, 64};
     int ctas_per_sm = 4;
     // graph of kGraphSteps steps
     cudaGraphExec_t graph = nullptr;
@@ -1007,7 +1008,7 @@ sgpu_status sgpu_batch_set_tuning(sgpu_batch* b, const int* chunk3, int ctas_per
     if (!b) return SGPU_ERR_ARG;
     if (chunk3)
         for (int q = 0; q < kNumClasses; ++q) {
-            if (chunk3[q] < 1 || chunk3[q] > kMaxItemPlanes - 8) return berr(b, SGPU_ERR_ARG, "z chunk out of range (1..64)");
+            if (chunk3[q] < 1 || chunk3[q] > 1024) return berr(b, SGPU_ERR_ARG, "z chunk out of range (1..1024)");
             if (b->chunk[q] != chunk3[q]) b->dirty = true;
             b->chunk[q] = chunk3[q];
         }
@@ -1062,14 +1063,16 @@ sgpu_status sgpu_batch_autotune(sgpu_batch* b, int steps_per_trial, int* chunk3,
     b->ctas_per_sm = best_ctas;
     for (int cl = 0; cl < kNumClasses; ++cl) {
         if (!present[cl]) continue;
+        // longest chunks first; a shorter one must win by 3 % (fewer items
+        // cost less set-up, and a short trial is noisy)
         int best_chunk = b->chunk[cl];
         float best_ms = -1;
-        for (int ch : {4, 8, 16, 32, 64}) {
+        for (int ch : {128, 64, 32, 16, 8}) {
             if (b->chunk[cl] != ch) b->dirty = true;
             b->chunk[cl] = ch;
             float ms = 0;
             if ((s = trial(&ms))) return s;
-            if (best_ms < 0 || ms < best_ms) {
+            if (best_ms < 0 || ms < 0.97f * best_ms) {
                 best_ms = ms;
                 best_chunk = ch;
             }

@@ -190,6 +190,51 @@ __device__ __forceinline__ void prod_prepare(ProdTable* tb, const TmaCta& t, int
     __syncwarp();
 }
 
+// The persistent producer's table holds the plane words of a window of 32
+// planes of the item (refilled by the warp as the issue loop reaches it), so
+// an item may have any number of planes, and the psi coordinates.
+struct ProdWindow {
+    PlaneWords w[32];
+    int4 psi[12];
+};
+struct PlaneSource {  // what the window refill reads
+    const KGrid* g;
+    const KCpml* cp;
+    unsigned tmask;
+};
+// Producer warp, all lanes: the words of the planes m0 .. m0+31 of the
+// item's issue order (p = p0 + m upwards, p1 - m downwards on the H side).
+__device__ __forceinline__ void prod_window(ProdWindow* tb, const TmaCta& t, int m0, int p0, int p1, int edge, bool hside,
+                                            const PlaneSource& src) {
+    const int c0 = hside ? 3 : 0;
+    const KGrid& g = *src.g;
+    const KCpml& cp = *src.cp;
+    const int m = m0 + t.lane;
+    __syncwarp();  // every lane has read the previous window
+    if (m <= p1 - p0) {
+        const int p = hside ? p1 - m : p0 + m;
+        PlaneWords w{0u, 0.0f, 0.0f, 0.0f};
+        if (p != edge) {
+            w.live = src.tmask ? cpml_plane_mask(cp, c0, src.tmask, p) : 0u;
+            w.idz = (hside ? g.idze : g.idzh)[p];
+            if (w.live & kCpmlZ) {
+                w.bz = (hside ? cp.pbm[2] : cp.pbe[2])[p];
+                w.cz = (hside ? cp.pcm[2] : cp.pce[2])[p];
+            }
+        }
+        tb->w[t.lane] = w;
+    }
+    __syncwarp();
+}
+__device__ __forceinline__ void prod_psi(ProdWindow* tb, const TmaCta& t, bool hside, const KCpml& cp, unsigned tmask) {
+    const int c0 = hside ? 3 : 0;
+    if (t.lane < 12 && ((tmask >> t.lane) & 1u)) {
+        const Slab& sl = cp.s[c0 + (t.lane >> 2)][(t.lane >> 1) & 1][t.lane & 1];
+        tb->psi[t.lane] = make_int4(t.ib - sl.xb, t.jb - sl.ylo, sl.zlo, 0);
+    }
+    __syncwarp();
+}
+
 // Producer (lane 0 of the producer warp): planes p0 .. p1 of one work item
 // into the ring, upwards on the E side and downwards on the H side, so that
 // either side's edge plane comes first; the item's first plane has the
@@ -248,8 +293,8 @@ __device__ __forceinline__ int tma_issue(const TmaCta& t, const CUtensorMap* map
 // consumers of a dynamically scheduled persistent kernel learn their item.
 constexpr int kOffItem = kOffW + (int)sizeof(PlaneWords);
 __device__ __forceinline__ int tma_issue_warp(const TmaCta& t, const CUtensorMap* maps, unsigned G0, int p0, int p1,
-                                              int edge, bool hside, int* err, const ProdTable* tb, unsigned smask,
-                                              int item) {
+                                              int edge, bool hside, int* err, ProdWindow* tb, const PlaneSource& src,
+                                              unsigned smask, int item) {
     const int q = t.lane;
     const int xh = hside ? t.ib : t.ib - 4, ya = hside ? t.jb : t.jb - 1;
     // this lane's box: shared-memory offset and x, y origin (psi: per plane below)
@@ -273,7 +318,8 @@ __device__ __forceinline__ int tma_issue_warp(const TmaCta& t, const CUtensorMap
         const unsigned bar = t.full0 + 8 * s;
         unsigned char* st = t.ring + s * kStageBytes;
         const bool part = p == edge;
-        const PlaneWords w = tb->w[p - p0];
+        if ((m & 31) == 0) prod_window(tb, t, m, p0, p1, edge, hside, src);
+        const PlaneWords w = tb->w[m & 31];
         int ok = 1;
         if (q == 0) {
             if (u >= 1 && !mbar_wait(t.empty0 + 8 * s, (u - 1) & 1, err, hside ? 13 : 11, t.wait)) {
@@ -377,6 +423,12 @@ __device__ __forceinline__ bool e_consume(const TmaCta& t, unsigned G0, const KG
     const bool vx = col_in(g.sw[0], i, j), vy = col_in(g.sw[1], i, j), vz = col_in(g.sw[2], i, j);
     const float idyh = g.idyh[min(j, nya - 1)], idxh = g.idxh[i];
     const long long pitch = g.pitch, plane = g.plane;
+    // the grid view may sit in shared memory (the batched kernel): what the
+    // plane loop needs is read into registers once
+    float* const F0 = g.F[0];
+    float* const F1 = g.F[1];
+    float* const F2 = g.F[2];
+    const int kx0 = g.sw[0][4], kx1 = g.sw[0][5], ky0 = g.sw[1][4], ky1 = g.sw[1][5], kz0 = g.sw[2][4], kz1 = g.sw[2][5];
     const unsigned tmask = CP ? cpml_tile_mask(cp, 0, t.ib, t.ib + kTX - 1, t.jb, t.jb + kTY - 1) : 0u;
     const CpmlCol cc = CP ? cpml_col(cp, 0, tmask, i, j, t.kb, t.ke) : CpmlCol{};
     if (CP == 2) psi_rows_fill(rows, cp, 0, tmask, kPsiSlotFloats, t.ib, j, l);
@@ -413,7 +465,7 @@ __device__ __forceinline__ bool e_consume(const TmaCta& t, unsigned G0, const KG
         const float idzh = pw.idz;
         const int o = w * kTX + l;
         bool st_ = true;
-        if (vx && k >= g.sw[0][4] && k <= g.sw[0][5]) {
+        if (vx && k >= kx0 && k <= kx1) {
             float e = EF[o];
             const float2 tt = tab(MF[o]);
             const float dy = hz - hz_jm, dz = hy - hy_km;
@@ -422,9 +474,9 @@ __device__ __forceinline__ bool e_consume(const TmaCta& t, unsigned G0, const KG
                 e = cpml_corr<CP, true>(cp.s[0][0], pm & 3, 0, PS, o, rows, i, j, k, cc.by, cc.cy, dy, tt.y, e, st_);
                 e = cpml_corr<CP, false>(cp.s[0][1], (pm >> 2) & 3, 2, PS, o, rows, i, j, k, bz, cz, dz, tt.y, e, st_);
             }
-            g.F[0][c] = e;
+            F0[c] = e;
         }
-        if (vy && k >= g.sw[1][4] && k <= g.sw[1][5]) {
+        if (vy && k >= ky0 && k <= ky1) {
             float e = EF[fs + o];
             const float2 tt = tab(MF[ms + o]);
             const float dz = hx - hx_km, dx = hz - hz_im;
@@ -433,9 +485,9 @@ __device__ __forceinline__ bool e_consume(const TmaCta& t, unsigned G0, const KG
                 e = cpml_corr<CP, true>(cp.s[1][0], (pm >> 4) & 3, 4, PS, o, rows, i, j, k, bz, cz, dz, tt.y, e, st_);
                 e = cpml_corr<CP, false>(cp.s[1][1], (pm >> 6) & 3, 6, PS, o, rows, i, j, k, cc.bx, cc.cx, dx, tt.y, e, st_);
             }
-            g.F[1][c] = e;
+            F1[c] = e;
         }
-        if (vz && k >= g.sw[2][4] && k <= g.sw[2][5]) {
+        if (vz && k >= kz0 && k <= kz1) {
             float e = EF[2 * fs + o];
             const float2 tt = tab(MF[2 * ms + o]);
             const float dx = hy - hy_im, dy = hx - hx_jm;
@@ -444,7 +496,7 @@ __device__ __forceinline__ bool e_consume(const TmaCta& t, unsigned G0, const KG
                 e = cpml_corr<CP, false>(cp.s[2][0], (pm >> 8) & 3, 8, PS, o, rows, i, j, k, cc.by, cc.cy, dy, tt.y, e, st_);
                 e = cpml_corr<CP, true>(cp.s[2][1], (pm >> 10) & 3, 10, PS, o, rows, i, j, k, cc.bx, cc.cx, dx, tt.y, e, st_);
             }
-            g.F[2][c] = e;
+            F2[c] = e;
         }
         hx_km = hx;
         hy_km = hy;
@@ -468,6 +520,10 @@ __device__ __forceinline__ bool h_consume(const TmaCta& t, unsigned G0, const KG
     const bool vx = col_in(g.sw[3], i, j), vy = col_in(g.sw[4], i, j), vz = col_in(g.sw[5], i, j);
     const float idye = g.idye[min(j, nya - 1)], idxe = g.idxe[i];
     const long long pitch = g.pitch, plane = g.plane;
+    float* const F3 = g.F[3];
+    float* const F4 = g.F[4];
+    float* const F5 = g.F[5];
+    const int kx0 = g.sw[3][4], kx1 = g.sw[3][5], ky0 = g.sw[4][4], ky1 = g.sw[4][5], kz0 = g.sw[5][4], kz1 = g.sw[5][5];
     const unsigned tmask = CP ? cpml_tile_mask(cp, 3, t.ib, t.ib + kTX - 1, t.jb, t.jb + kTY - 1) : 0u;
     const CpmlCol cc = CP ? cpml_col(cp, 3, tmask, i, j, t.kb, t.ke) : CpmlCol{};
     if (CP == 2) psi_rows_fill(rows, cp, 3, tmask, kPsiSlotFloats, t.ib, j, l);
@@ -503,7 +559,7 @@ __device__ __forceinline__ bool h_consume(const TmaCta& t, unsigned G0, const KG
         const float idze = pw.idz;
         const int o = w * kTX + l;
         bool st_ = true;
-        if (vx && k >= g.sw[3][4] && k <= g.sw[3][5]) {
+        if (vx && k >= kx0 && k <= kx1) {
             float h = HF[o];
             const float2 tt = tab(MF[o]);
             const float dz = ey_kp - ey, dy = ez_jp - ez;
@@ -512,9 +568,9 @@ __device__ __forceinline__ bool h_consume(const TmaCta& t, unsigned G0, const KG
                 h = cpml_corr<CP, false>(cp.s[3][0], pm & 3, 0, PS, o, rows, i, j, k, cc.by, cc.cy, dy, tt.y, h, st_);
                 h = cpml_corr<CP, true>(cp.s[3][1], (pm >> 2) & 3, 2, PS, o, rows, i, j, k, bz, cz, dz, tt.y, h, st_);
             }
-            g.F[3][c] = h;
+            F3[c] = h;
         }
-        if (vy && k >= g.sw[4][4] && k <= g.sw[4][5]) {
+        if (vy && k >= ky0 && k <= ky1) {
             float h = HF[fs + o];
             const float2 tt = tab(MF[ms + o]);
             const float dx = ez_ip - ez, dz = ex_kp - ex;
@@ -523,9 +579,9 @@ __device__ __forceinline__ bool h_consume(const TmaCta& t, unsigned G0, const KG
                 h = cpml_corr<CP, false>(cp.s[4][0], (pm >> 4) & 3, 4, PS, o, rows, i, j, k, bz, cz, dz, tt.y, h, st_);
                 h = cpml_corr<CP, true>(cp.s[4][1], (pm >> 6) & 3, 6, PS, o, rows, i, j, k, cc.bx, cc.cx, dx, tt.y, h, st_);
             }
-            g.F[4][c] = h;
+            F4[c] = h;
         }
-        if (vz && k >= g.sw[5][4] && k <= g.sw[5][5]) {
+        if (vz && k >= kz0 && k <= kz1) {
             float h = HF[2 * fs + o];
             const float2 tt = tab(MF[2 * ms + o]);
             const float dy = ex_jp - ex, dx = ey_ip - ey;
@@ -534,7 +590,7 @@ __device__ __forceinline__ bool h_consume(const TmaCta& t, unsigned G0, const KG
                 h = cpml_corr<CP, true>(cp.s[5][0], (pm >> 8) & 3, 8, PS, o, rows, i, j, k, cc.by, cc.cy, dy, tt.y, h, st_);
                 h = cpml_corr<CP, false>(cp.s[5][1], (pm >> 10) & 3, 10, PS, o, rows, i, j, k, cc.bx, cc.cx, dx, tt.y, h, st_);
             }
-            g.F[5][c] = h;
+            F5[c] = h;
         }
         ex_kp = ex;
         ey_kp = ey;

@@ -87,7 +87,7 @@ def test_autotuned_shapes_keep_results():
     with Batch(1 << 30, 16) as b:
         slots = [b.add(pb) for pb in pbs]
         chunks, ctas = b.autotune(2)
-        assert all(c in (4, 8, 16, 32, 64) for c in chunks) and ctas in (2, 3, 4, 6)
+        assert all(c in (8, 16, 32, 64, 128) for c in chunks) and ctas in (2, 3, 4, 6)
         b.run_all()
         _check(b, slots, pbs)
 
