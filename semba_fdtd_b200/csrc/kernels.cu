@@ -139,6 +139,11 @@ __global__ void __launch_bounds__(kBX * kBY, 4) k_hfield(KGrid g, KCpml cp, int 
 // Same per-cell arithmetic as efield_column / hfield_column, from shared
 // memory instead of global loads.
 
+#ifndef SGPU_TMA_MINB
+#define SGPU_TMA_MINB 4
+#endif
+constexpr int kTmaMinBlocks = SGPU_TMA_MINB;  // CTAs an SM holds of the plain TMA field kernels
+
 // The side's coefficient pairs (G1, G2) or (GM1, GM2) in shared memory after
 // the ring; the TMA kernels run only with fewer than 256 media, so the table
 // always fits (the launch sizes the shared memory for it).
@@ -148,7 +153,7 @@ __device__ __forceinline__ TabPairs tma_tables(unsigned char* smem, const float*
     return TabPairs{tab};
 }
 
-__global__ void __launch_bounds__(kTmaThreads, 3)
+__global__ void __launch_bounds__(kTmaThreads, kTmaMinBlocks)
     k_tma_efield(KGrid g, KCpml cp, const __grid_constant__ TMaps tm, int y0, int z0, int z1, int zchunk, int* err,
                  long long wait, int drill) {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -175,7 +180,7 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
     else e_consume<0>(t, 0, g, cp, tab, err, false, rows[t.warp]);
 }
 
-__global__ void __launch_bounds__(kTmaThreads, 3)
+__global__ void __launch_bounds__(kTmaThreads, kTmaMinBlocks)
     k_tma_hfield(KGrid g, KCpml cp, const __grid_constant__ TMaps tm, int y0, int z0, int z1, int zchunk, int* err,
                  long long wait, int drill) {
     extern __shared__ __align__(128) unsigned char smem[];

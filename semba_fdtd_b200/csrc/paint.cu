@@ -108,18 +108,27 @@ __device__ __forceinline__ bool in_shell(int i, int j, int k, const PBox& in) {
 }
 
 // Smallest sweep key of every negative entry of the shell of r (outside `in`).
+// The key grows with q (nxo, nyo cover the box), so within a warp the lowest
+// lane holding a value has that value's smallest key: one lane per distinct
+// value records it, and only when it beats what is already there (the shell
+// is mostly one or two values, which would otherwise serialise on a handful
+// of addresses).
 __global__ void k_first(const int16_t* m, Local L, PBox r, PBox in, long long task0, long long nyo, long long nxo,
                         unsigned long long* first) {
     const long long n = box_cells(r);
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
         int i, j, k;
         box_cell(r, q, i, j, k);
-        if (!in_shell(i, j, k, in)) continue;
-        const int v = m[L.at(i, j, k)];
-        if (v >= 0) continue;
+        const int v = in_shell(i, j, k, in) ? (int)m[L.at(i, j, k)] : 0;
         const unsigned long long key =
             (unsigned long long)(((task0 + (k - r.z0)) * nyo + (j - r.y0)) * nxo + (i - r.x0));
-        atomicMin(first + (-v), key);
+        const unsigned act = __activemask();
+        const unsigned want = __ballot_sync(act, v < 0);
+        if (v < 0) {
+            const unsigned grp = __match_any_sync(want, v);
+            if ((int)(threadIdx.x & 31) == __ffs(grp) - 1 && key < *(volatile unsigned long long*)(first + (-v)))
+                atomicMin(first + (-v), key);
+        }
     }
 }
 

@@ -6,7 +6,7 @@
 // producer warp streams every plane the tile needs -- the H (or E) tiles with
 // their one-cell halos, the tile's own E (or H) values and the three media
 // tiles (one byte a cell, a copy of the int16 matrices kept while the media
-// number under 256) -- into a 4-stage shared-memory ring with cp.async.bulk.tensor
+// number under 256) -- into a 3-stage shared-memory ring with cp.async.bulk.tensor
 // loads that complete on mbarriers; eight consumer warps update one cell per
 // thread from shared memory and store the result with plain coalesced stores.
 // The x origin of a haloed tile is rounded down to a 16-byte boundary (4
@@ -24,7 +24,13 @@ namespace sgpu {
 using namespace sgpu::dev;
 
 constexpr int kTX = 32, kTY = 8;          // tile (threads per row, rows)
-constexpr int kStages = 4;                // shared-memory ring depth
+#ifndef SGPU_TMA_STAGES
+#define SGPU_TMA_STAGES 3
+#endif
+#ifndef SGPU_PSI_SLOTS
+#define SGPU_PSI_SLOTS 6
+#endif
+constexpr int kStages = SGPU_TMA_STAGES;  // shared-memory ring depth
 constexpr int kConsumerWarps = kTY;       // one warp per tile row
 constexpr int kTmaThreads = (kConsumerWarps + 1) * 32;
 constexpr int kHaloW = kTX + 4;           // haloed row width (x rounded to 16 B)
@@ -37,7 +43,7 @@ constexpr int kBoxC = kHaloW * (kTY + 1) * 4;   // 36 x 9 floats
 constexpr int kBoxF = kTX * kTY * 4;            // 32 x 8 floats
 constexpr int kBoxM = kTX * kTY;                // 32 x 8 one-byte media indices
 constexpr int kBoxP = kTX * kTY * 4;            // 32 x 8 floats of one psi slab
-constexpr int kPsiSlots = 6;                    // psi tiles staged per plane
+constexpr int kPsiSlots = SGPU_PSI_SLOTS;       // psi tiles staged per plane
 __host__ __device__ constexpr int align128(int b) { return (b + 127) / 128 * 128; }
 constexpr int kOffA = 0;
 constexpr int kOffB = kOffA + align128(kBoxA);
