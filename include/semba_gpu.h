@@ -84,6 +84,11 @@ sgpu_status sgpu_create(const sgpu_grid_desc* grid, sgpu_ctx** out);
 void sgpu_destroy(sgpu_ctx* ctx);
 const char* sgpu_last_error(const sgpu_ctx* ctx);
 sgpu_status sgpu_synchronize(sgpu_ctx* ctx);
+/* The CUDA stream (a cudaStream_t, passed as a pointer) on which the context
+ * issues every launch and copy: a caller orders its own device work against
+ * the context's on it (a z-slab halo message, say) without a host wait.
+ * No reference counterpart (the reference's routines are synchronous). */
+sgpu_status sgpu_get_stream(const sgpu_ctx* ctx, void** stream);
 
 /* Media matrices sggMiEx..sggMiHz (int16, -DCompileWithInt2), column-major
  * over alloc[comp]. */

@@ -213,6 +213,11 @@ module semba_gpu_m
          import :: c_int, c_ptr
          type(c_ptr), value :: ctx
       end function sgpu_synchronize
+      integer(c_int) function sgpu_get_stream(ctx, stream) bind(C, name="sgpu_get_stream")
+         import :: c_int, c_ptr
+         type(c_ptr), value :: ctx
+         type(c_ptr), intent(out) :: stream  ! the context's cudaStream_t
+      end function sgpu_get_stream
       integer(c_int) function sgpu_upload_media(ctx, comp, mi) bind(C, name="sgpu_upload_media")
          import :: c_int, c_ptr
          type(c_ptr), value :: ctx

@@ -121,6 +121,7 @@ def _declare(lib: C.CDLL) -> None:
         "sgpu_destroy": ([vp], None),
         "sgpu_last_error": ([vp], C.c_char_p),
         "sgpu_synchronize": ([vp], C.c_int),
+        "sgpu_get_stream": ([vp, C.POINTER(vp)], C.c_int),
         "sgpu_upload_media": ([vp, C.c_int, C.POINTER(C.c_int16)], C.c_int),
         "sgpu_upload_field": ([vp, C.c_int, c_float_p], C.c_int),
         "sgpu_download_field": ([vp, C.c_int, c_float_p], C.c_int),

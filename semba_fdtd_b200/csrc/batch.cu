@@ -31,6 +31,9 @@
 
 #include "sgpu_internal.h"
 #include "stencil.cuh"
+// The persistent batched field kernels keep a 4-stage ring (3 CTAs an SM,
+// bound by their registers); the plain ones run 3 stages at 4 CTAs an SM.
+#define SGPU_TMA_STAGES 4
 #include "tma_fields.cuh"
 
 using namespace sgpu;
@@ -281,7 +284,8 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
                 tensormap_acquire(&m[t.lane]);
                 facq = true;
             }
-            const int got = tma_issue_warp(t, m, gp, p0, p1, edge, SIDE != 0, err, &tb, src, smask, it);
+            const ItemWords iw{{it, w.slot, w.ib, w.jb, w.kb, w.ke, w.cp}};
+            const int got = tma_issue_warp(t, m, gp, p0, p1, edge, SIDE != 0, err, &tb, src, smask, iw);
             if (got < np) {
                 if (t.lane == 0) tma_drain(t, gp + (unsigned)got, err, 15);
                 return;
@@ -298,9 +302,9 @@ __global__ void __launch_bounds__(kTmaThreads, 3)
         // the item of the next plane (item -1: no more)
         const unsigned s = gp % kStages;
         if (!warp_wait(t.full0 + 8 * s, (gp / kStages) & 1, err, 5, t.wait)) return;
-        const int it = *(const volatile int*)(t.ring + s * kStageBytes + kOffItem);
-        if (it < 0) return;
-        const FieldItem w = items[it];
+        const volatile int* iv = (const volatile int*)(t.ring + s * kStageBytes + kOffItem);
+        if (iv[0] < 0) return;
+        const FieldItem w{iv[1], iv[2], iv[3], iv[4], iv[5], iv[6]};
         const InstDesc& D = descs[w.slot];
         t.ib = w.ib;
         t.jb = w.jb;

@@ -855,6 +855,12 @@ void sgpu_destroy(sgpu_ctx* c) {
     delete c;
 }
 
+sgpu_status sgpu_get_stream(const sgpu_ctx* c, void** stream) {
+    if (!c || !stream) return SGPU_ERR_ARG;
+    *stream = (void*)c->stream;
+    return SGPU_OK;
+}
+
 sgpu_status sgpu_synchronize(sgpu_ctx* c) {
     if (!c) return SGPU_ERR_ARG;
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));

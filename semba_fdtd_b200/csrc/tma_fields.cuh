@@ -294,13 +294,18 @@ __device__ __forceinline__ int tma_issue(const TmaCta& t, const CUtensorMap* map
 // staged slab.  A lane is the only issuer of its map, so a tensor map that
 // lane acquired through the tensormap proxy needs no other thread's fence.
 // All lanes return the number of planes issued.
-// Every plane also carries, in the word after its PlaneWords, the work item
-// it belongs to (`item`; -1 marks the end of a CTA's items), which is how the
-// consumers of a dynamically scheduled persistent kernel learn their item.
+// Every plane also carries, after its PlaneWords, the work item it belongs to
+// (`item`: its index, -1 marking the end of a CTA's items, then six words of
+// the item itself), which is how the consumers of a dynamically scheduled
+// persistent kernel learn their item without a global load.
 constexpr int kOffItem = kOffW + (int)sizeof(PlaneWords);
+struct ItemWords {
+    int v[7];
+};
+static_assert(sizeof(PlaneWords) + sizeof(ItemWords) <= 128, "the plane words fit their stage slot");
 __device__ __forceinline__ int tma_issue_warp(const TmaCta& t, const CUtensorMap* maps, unsigned G0, int p0, int p1,
                                               int edge, bool hside, int* err, ProdWindow* tb, const PlaneSource& src,
-                                              unsigned smask, int item) {
+                                              unsigned smask, const ItemWords& item) {
     const int q = t.lane;
     const int xh = hside ? t.ib : t.ib - 4, ya = hside ? t.jb : t.jb - 1;
     // this lane's box: shared-memory offset and x, y origin (psi: per plane below)
@@ -332,7 +337,7 @@ __device__ __forceinline__ int tma_issue_warp(const TmaCta& t, const CUtensorMap
                 ok = 0;
             } else {
                 if (!part) *(PlaneWords*)(st + kOffW) = w;
-                *(int*)(st + kOffItem) = item;
+                *(ItemWords*)(st + kOffItem) = item;
                 mbar_expect_tx(bar, (part ? kTxEdge : kTxFull) + (unsigned)__popc(w.live & smask) * (unsigned)kBoxP);
             }
         }

@@ -176,9 +176,17 @@ def run_distributed(problem, steps: int, variant: str = "exact", group=None, pla
         s._check(s.lib.sgpu_zplane(s.handle, comp, z, C.byref(ptr), C.byref(nbytes)), "sgpu_zplane")
         return torch.as_tensor(_DeviceArray(ptr.value, nbytes.value // 4), device="cuda")
 
+    # The messages are ordered on the context's own stream, with no host
+    # wait: made current, it is the stream the process group's sends wait on
+    # (the half step that wrote the planes is ahead of them) and the one that
+    # waits for the receives (the next half step comes after them).
+    ctx_stream = None
+    if s is not None:
+        ptr = C.c_void_p()
+        s._check(s.lib.sgpu_get_stream(s.handle, C.byref(ptr)), "sgpu_get_stream")
+        ctx_stream = torch.cuda.ExternalStream(ptr.value) if ptr.value else torch.cuda.default_stream()
+
     def halo(phase):
-        if s is not None:
-            s.synchronize()  # the half step has written the planes
         ops = []
         for ph, src, dst, comps, z in sched:
             if ph != phase:
@@ -188,11 +196,15 @@ def run_distributed(problem, steps: int, variant: str = "exact", group=None, pla
                     ops.append(dist.P2POp(dist.isend, plane_tensor(c, z), dst, group))
                 elif rank == dst:
                     ops.append(dist.P2POp(dist.irecv, plane_tensor(c, z), src, group))
-        if ops:
+        if not ops:
+            return
+        if ctx_stream is None:
             for r in dist.batch_isend_irecv(ops):
                 r.wait()
-        if s is not None and planes is None:
-            torch.cuda.synchronize()  # the received planes are in place before the next half step
+            return
+        with torch.cuda.stream(ctx_stream):
+            for r in dist.batch_isend_irecv(ops):
+                r.wait()  # the context's stream waits for the message, the host does not
 
     lib = s.lib if s is not None else None
     for n in range(steps):
