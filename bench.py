@@ -245,6 +245,7 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.SUM)
         return float(t.item())
 
+    bufs = None if args.quick else e2e_buffers(pb, lib)
     # ---- device-resident throughput ------------------------------------
     s = Solver(pb, probe_capacity=max(1024, K + W + CPU_STEPS + 8), kernel_family=args.family)
     # the first CPU_STEPS steps are kept for the parity check against the
@@ -290,7 +291,7 @@ def run_ours(args):
     s.close()
 
     # ---- end to end through the C ABI with host buffers -----------------
-    e2e = None if args.quick else run_e2e(pb, K, lib, args.family)
+    e2e = None if args.quick else run_e2e(pb, K, lib, args.family, bufs)
 
     value = allsum(cells * K) / (t_ms * 1e-3) / 1e9
     if rank != 0:
@@ -345,13 +346,12 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def run_e2e(pb, K, lib, family):
-    """Host problem -> device (set-up, media from the problem description,
-    initial fields from pinned host buffers) -> K steps -> probe traces and
-    final fields back into pinned host buffers."""
-    from semba_fdtd_b200 import Solver, _lib
-    # the caller's host buffers: the initial fields (zeros, a fresh start)
-    # and the final fields, in pinned memory allocated before timing
+def e2e_buffers(pb, lib):
+    """The caller's host buffers of the end-to-end leg: the initial fields
+    (zeros, a fresh start) and the final fields, in pinned memory.  They are
+    made before any timing (7.4 GB at 536^3 take a few seconds to pin), so
+    the end-to-end leg does not start on a GPU that idled meanwhile."""
+    from semba_fdtd_b200 import _lib
     desc, keep = pb.to_desc()
     plan = C.c_void_p()
     if lib.sgpu_host_plan(C.byref(desc), 1, C.byref(plan)):
@@ -364,6 +364,15 @@ def run_e2e(pb, K, lib, family):
     final = [_lib.pinned_empty(sh, np.float32) for sh in shapes]
     for a in init + final:
         a.fill(0.0)
+    return init, final
+
+
+def run_e2e(pb, K, lib, family, bufs):
+    """Host problem -> device (set-up, media from the problem description,
+    initial fields from pinned host buffers) -> K steps -> probe traces and
+    final fields back into pinned host buffers."""
+    from semba_fdtd_b200 import Solver
+    init, final = bufs
     t0 = time.perf_counter()
     s = Solver(pb, probe_capacity=max(1024, K + 8), kernel_family=family)
     t_setup = time.perf_counter()
@@ -446,11 +455,11 @@ def run_batched(args):
         marks["plan"] = time.perf_counter() - t0
         arena = int(sum(p.footprint for p in plans) * 1.05) + (64 << 20)
         with Batch(arena, len(pbs) + 1, kernel_family=args.batch_family) as b:
-            # most steps first (or in stream order, or most work first, which
-            # measured slower: the tuner then sees only the largest grids), a
-            # first group tuned on, then 32-step chunks queued between the
-            # remaining set-ups: an instance is set up on its own stream while
-            # the queued steps of the others run
+            # most steps first (or in stream order, or most work first), a
+            # first group, then 32-step chunks queued between the remaining
+            # set-ups (an instance is set up on its own stream while the
+            # queued steps of the others run), then the tuner with every
+            # instance live, so its trial steps run at full occupancy
             if args.batch_order == "longest":
                 plans = sorted(plans, key=lambda p: -(p.nsteps + 1) * p.problem.swept_cells)
             elif args.batch_order == "steps":
@@ -459,13 +468,13 @@ def run_batched(args):
                 plans = sorted(plans, key=lambda p: -p.nsteps)
             first = 8
             slots = [b.add(p) for p in plans[:first]]
-            chunks, ctas = b.autotune(2)
-            marks["tune"] = time.perf_counter() - t0
             for q, p in enumerate(plans[first:]):
                 if q % args.batch_advance_every == 0:
                     b.advance(32)
                 slots.append(b.add(p))
             marks["add"] = time.perf_counter() - t0
+            chunks, ctas = b.autotune(2)
+            marks["tune"] = time.perf_counter() - t0
             live = sum(1 for x in slots if not b.done(x))
             phases = b.profile(8)  # real steps, per-phase device time of the live instances
             dev_ms = 0.0
@@ -477,6 +486,7 @@ def run_batched(args):
                 b.probes(x)
             marks["read"] = time.perf_counter() - t0
         t_batch = time.perf_counter() - t0
+        marks["closed"] = t_batch
     line = {"metric": "solves/s", "value": len(pbs) / t_batch, "unit": "solves/s", "n_gpus": 1, "steps": None,
             "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "impl": "batched",

@@ -968,6 +968,7 @@ sgpu_status sgpu::narrow_media(sgpu_ctx* c, int comp) {
 }
 
 bool sgpu::tma_usable(const sgpu_ctx* c) { return c->tma_ready && c->num_media < 256; }
+void sgpu::keep_device_pool(int device) { keep_pool_memory(device); }
 
 extern "C" {
 

@@ -352,6 +352,9 @@ sgpu_status narrow_media(sgpu_ctx* c, int comp);
 // Whether the TMA-pipelined field kernels can run (tensor maps built and
 // every medium index fits the one-byte media copy).
 bool tma_usable(const sgpu_ctx* c);
+// Tell the device's default memory pool to keep freed memory (once per
+// device): the solo contexts and the batch arena allocate from it.
+void keep_device_pool(int device);
 // Replace the context's medium count and coefficient tables (before the
 // first launch): the level-2 host learns the final count only after the
 // media matrices are built on the device.
