@@ -805,11 +805,19 @@ sgpu_status sgpu_batch_create(uint64_t arena_bytes, int max_instances, sgpu_batc
     BTRY(b, cudaStreamCreateWithFlags(&b->setup, cudaStreamNonBlocking));
     BTRY(b, cudaEventCreateWithFlags(&b->setup_done, cudaEventDisableTiming));
     void* base = nullptr;
-    // memory the solo contexts' pool keeps is handed back first
-    sgpu_trim_device_memory();
-    if (cudaMalloc(&base, arena_bytes) != cudaSuccess) {
+    keep_device_pool(b->device);
+    // the arena comes from the device's default memory pool, which keeps the
+    // memory solo contexts (or an earlier batch) freed; only when the pool
+    // cannot serve it is its unused memory handed back and the request
+    // retried.  The pool gets the arena back when the batch is destroyed.
+    if (cudaMallocAsync(&base, arena_bytes, b->stream) != cudaSuccess) {
         cudaGetLastError();
-        return berr(b, SGPU_ERR_OOM, "arena of " + std::to_string(arena_bytes) + " bytes could not be allocated");
+        base = nullptr;
+        sgpu_trim_device_memory();
+        if (cudaMallocAsync(&base, arena_bytes, b->stream) != cudaSuccess) {
+            cudaGetLastError();
+            return berr(b, SGPU_ERR_OOM, "arena of " + std::to_string(arena_bytes) + " bytes could not be allocated");
+        }
     }
     b->arena.base = (char*)base;
     b->arena.cap = arena_bytes / kArenaAlign * kArenaAlign;
@@ -860,7 +868,10 @@ void sgpu_batch_destroy(sgpu_batch* b) {
     cudaFree(b->d_probe);
     cudaFree(b->d_border[0]);
     cudaFree(b->d_border[1]);
-    if (b->arena.base) cudaFree(b->arena.base);
+    if (b->arena.base) {
+        cudaFreeAsync(b->arena.base, b->stream);
+        cudaStreamSynchronize(b->stream);
+    }
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->stream) cudaStreamDestroy(b->stream);
