@@ -202,6 +202,7 @@ __device__ __forceinline__ void prod_prepare(ProdTable* tb, const TmaCta& t, int
 struct ProdWindow {
     PlaneWords w[32];
     int4 psi[12];
+    int2 zr[12];  // z range of each slab of the tile mask (empty for the others)
 };
 struct PlaneSource {  // what the window refill reads
     const KGrid* g;
@@ -210,9 +211,10 @@ struct PlaneSource {  // what the window refill reads
 };
 // Producer warp, all lanes: the words of the planes m0 .. m0+31 of the
 // item's issue order (p = p0 + m upwards, p1 - m downwards on the H side).
+// The slabs' z ranges come from the table prod_psi filled, so a refill reads
+// only the plane's own metric and CPML values from global memory.
 __device__ __forceinline__ void prod_window(ProdWindow* tb, const TmaCta& t, int m0, int p0, int p1, int edge, bool hside,
                                             const PlaneSource& src) {
-    const int c0 = hside ? 3 : 0;
     const KGrid& g = *src.g;
     const KCpml& cp = *src.cp;
     const int m = m0 + t.lane;
@@ -221,9 +223,17 @@ __device__ __forceinline__ void prod_window(ProdWindow* tb, const TmaCta& t, int
         const int p = hside ? p1 - m : p0 + m;
         PlaneWords w{0u, 0.0f, 0.0f, 0.0f};
         if (p != edge) {
-            w.live = src.tmask ? cpml_plane_mask(cp, c0, src.tmask, p) : 0u;
+            unsigned live = 0;
+            if (src.tmask) {
+#pragma unroll
+                for (int n = 0; n < 12; ++n) {
+                    const int2 z = tb->zr[n];
+                    if (p >= z.x && p <= z.y) live |= 1u << n;
+                }
+            }
+            w.live = live;
             w.idz = (hside ? g.idze : g.idzh)[p];
-            if (w.live & kCpmlZ) {
+            if (live & kCpmlZ) {
                 w.bz = (hside ? cp.pbm[2] : cp.pbe[2])[p];
                 w.cz = (hside ? cp.pcm[2] : cp.pce[2])[p];
             }
@@ -232,11 +242,18 @@ __device__ __forceinline__ void prod_window(ProdWindow* tb, const TmaCta& t, int
     }
     __syncwarp();
 }
+// Producer warp, all lanes, once per item: the psi TMA coordinates and the z
+// range of every slab of the tile mask.
 __device__ __forceinline__ void prod_psi(ProdWindow* tb, const TmaCta& t, bool hside, const KCpml& cp, unsigned tmask) {
     const int c0 = hside ? 3 : 0;
-    if (t.lane < 12 && ((tmask >> t.lane) & 1u)) {
-        const Slab& sl = cp.s[c0 + (t.lane >> 2)][(t.lane >> 1) & 1][t.lane & 1];
-        tb->psi[t.lane] = make_int4(t.ib - sl.xb, t.jb - sl.ylo, sl.zlo, 0);
+    if (t.lane < 12) {
+        int2 z = make_int2(1, 0);
+        if ((tmask >> t.lane) & 1u) {
+            const Slab& sl = cp.s[c0 + (t.lane >> 2)][(t.lane >> 1) & 1][t.lane & 1];
+            tb->psi[t.lane] = make_int4(t.ib - sl.xb, t.jb - sl.ylo, sl.zlo, 0);
+            z = make_int2(sl.zlo, sl.zhi);
+        }
+        tb->zr[t.lane] = z;
     }
     __syncwarp();
 }
@@ -294,7 +311,7 @@ __device__ __forceinline__ int tma_issue(const TmaCta& t, const CUtensorMap* map
 // staged slab.  A lane is the only issuer of its map, so a tensor map that
 // lane acquired through the tensormap proxy needs no other thread's fence.
 // All lanes return the number of planes issued.
-// Every plane also carries, after its PlaneWords, the work item it belongs to
+// The first plane of a work item also carries, after its PlaneWords, the item
 // (`item`: its index, -1 marking the end of a CTA's items, then six words of
 // the item itself), which is how the consumers of a dynamically scheduled
 // persistent kernel learn their item without a global load.
@@ -308,8 +325,9 @@ __device__ __forceinline__ int tma_issue_warp(const TmaCta& t, const CUtensorMap
                                               unsigned smask, const ItemWords& item) {
     const int q = t.lane;
     const int xh = hside ? t.ib : t.ib - 4, ya = hside ? t.jb : t.jb - 1;
-    // this lane's box: shared-memory offset and x, y origin (psi: per plane below)
-    int off = 0, bx = t.ib, by = t.jb;
+    // this lane's box: shared-memory offset, x and y origin, and z offset
+    // (psi boxes count planes from their slab's zlo)
+    int off = 0, bx = t.ib, by = t.jb, bz0 = 0;
     if (q == 0) { off = kOffA; by = ya; }
     else if (q == 1) { off = kOffB; bx = xh; }
     else if (q == 2) { off = kOffC; bx = xh; by = ya; }
@@ -317,12 +335,14 @@ __device__ __forceinline__ int tma_issue_warp(const TmaCta& t, const CUtensorMap
     else if (q < 9) off = kOffM + (q - 6) * align128(kBoxM);
     const int n = q - kPsiMap0;
     const bool psi_lane = n >= 0 && n < 12 && ((smask >> n) & 1u);
-    int4 pc = make_int4(0, 0, 0, 0);
-    int poff = 0;
     if (psi_lane) {
-        pc = tb->psi[n];
-        poff = kOffP + psi_slot(smask, n) * align128(kBoxP);
+        const int4 pc = tb->psi[n];
+        off = kOffP + psi_slot(smask, n) * align128(kBoxP);
+        bx = pc.x;
+        by = pc.y;
+        bz0 = pc.z;
     }
+    const CUtensorMap* map = &maps[q < kPsiMap0 + 12 ? q : 0];
     for (int m = 0; m <= p1 - p0; ++m) {
         const int p = hside ? p1 - m : p0 + m;  // the H side marches down
         const unsigned G = G0 + (unsigned)m, s = G % kStages, u = G / kStages;
@@ -337,18 +357,15 @@ __device__ __forceinline__ int tma_issue_warp(const TmaCta& t, const CUtensorMap
                 ok = 0;
             } else {
                 if (!part) *(PlaneWords*)(st + kOffW) = w;
-                *(ItemWords*)(st + kOffItem) = item;
+                if (m == 0) *(ItemWords*)(st + kOffItem) = item;  // the consumers read it at the item's first plane
                 mbar_expect_tx(bar, (part ? kTxEdge : kTxFull) + (unsigned)__popc(w.live & smask) * (unsigned)kBoxP);
             }
         }
         ok = __shfl_sync(0xffffffffu, ok, 0);
         if (!ok) return m;
         __syncwarp();  // the stage is free and armed before any lane writes into it
-        if (q < kPsiMap0) {
-            if (q < 2 || !part) tma_load3(smem_u32(st + off), &maps[q], bx, by, p, bar);
-        } else if (psi_lane && ((w.live >> n) & 1u)) {
-            tma_load3(smem_u32(st + poff), &maps[q], pc.x, pc.y, p - pc.z, bar);
-        }
+        const bool issue = q < kPsiMap0 ? (q < 2 || !part) : (psi_lane && ((w.live >> n) & 1u));
+        if (issue) tma_load3(smem_u32(st + off), map, bx, by, p - bz0, bar);
     }
     return p1 - p0 + 1;
 }
