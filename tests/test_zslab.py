@@ -116,3 +116,33 @@ def test_zslabs_reject_periodic_z():
     from semba_fdtd_b200._lib import SembaGpuError
     with pytest.raises(SembaGpuError):
         zslab.ZSlabs(mixed(), 2)
+
+
+@pytest.mark.gpu
+def test_distributed_single_rank_on_the_context_stream():
+    """run_distributed with one rank: no halo message, but the whole step
+    loop of the distributed form (its messages ordered on the context's own
+    stream, from sgpu_get_stream) runs and equals the plain run bit for bit."""
+    import torch.distributed as dist
+    from semba_fdtd_b200 import Solver
+    pb = CASES[next(iter(CASES))]()
+    steps = 23
+    with Solver(pb) as s:
+        s.step(steps)
+        ref_tr = s.probes()
+        ref = [s.field(c) for c in range(6)]
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1)
+    try:
+        d = zslab.run_distributed(pb, steps)
+        try:
+            d.synchronize()
+            assert_bits_equal(d.probes(), ref_tr)
+            for c in range(6):
+                assert_bits_equal(d.field(c), ref[c])
+        finally:
+            d.close()
+    finally:
+        dist.destroy_process_group()
