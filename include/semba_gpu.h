@@ -328,10 +328,11 @@ sgpu_status sgpu_compulsory_bytes(const sgpu_ctx* ctx, double* bytes6);
 /* Select the CUDA device this library's runtime uses on the calling thread
  * (call before sgpu_create / sgpu_host_create). */
 sgpu_status sgpu_select_device(int device);
-/* Device memory of contexts outside a batch comes from the current device's
- * default memory pool (stream-ordered), which keeps freed memory for the
- * next context; this hands the kept memory back to the driver (waits for the
- * device).  sgpu_batch_create does it before allocating its arena. */
+/* Device memory of contexts outside a batch, and each batch's arena, come
+ * from the current device's default memory pool (stream-ordered), which
+ * keeps freed memory for the next context or batch; this hands the kept
+ * memory back to the driver (waits for the device).  sgpu_batch_create does
+ * it only when the pool cannot serve its arena. */
 sgpu_status sgpu_trim_device_memory(void);
 /* Kernel launches issued per whole step (graph replays add one per chunk). */
 sgpu_status sgpu_kernels_per_step(const sgpu_ctx* ctx, int* n);
@@ -520,8 +521,9 @@ sgpu_status sgpu_load_resume(sgpu_ctx* ctx, const char* path, int* last_step);
  * ------------------------------------------------------------------------ */
 typedef struct sgpu_batch sgpu_batch;
 
-/* One arena of arena_bytes of device memory (one cudaMalloc) on the current
- * device, room for max_instances instances. */
+/* One arena of arena_bytes of device memory (one block from the current
+ * device's default memory pool, given back to it by sgpu_batch_destroy),
+ * room for max_instances instances. */
 sgpu_status sgpu_batch_create(uint64_t arena_bytes, int max_instances, sgpu_batch** out);
 void sgpu_batch_destroy(sgpu_batch* b);
 const char* sgpu_batch_last_error(const sgpu_batch* b);
