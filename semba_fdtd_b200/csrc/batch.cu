@@ -802,7 +802,12 @@ sgpu_status sgpu_batch_create(uint64_t arena_bytes, int max_instances, sgpu_batc
     BTRY(b, cudaGetDevice(&b->device));
     cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, b->device);
     BTRY(b, cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
-    BTRY(b, cudaStreamCreateWithFlags(&b->setup, cudaStreamNonBlocking));
+    // instance set-up runs on a stream of the highest priority: its small
+    // kernels and copies (and the waits between them) go first whenever the
+    // persistent step kernels, which hold every SM, leave the device
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    BTRY(b, cudaStreamCreateWithPriority(&b->setup, cudaStreamNonBlocking, hi));
     BTRY(b, cudaEventCreateWithFlags(&b->setup_done, cudaEventDisableTiming));
     void* base = nullptr;
     keep_device_pool(b->device);
