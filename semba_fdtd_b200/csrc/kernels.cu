@@ -1393,55 +1393,147 @@ sgpu_status sgpu_add_planewave(sgpu_ctx* c, const sgpu_planewave_desc* d) {
                                {{HX, EZ, 0, -1}, {HZ, EX, 0, +1}},
                                {{HX, EY, +1, -1}, {HY, EX, +1, +1}},
                                {{HX, EY, 0, +1}, {HY, EX, 0, -1}}};
-    for (int side = 0; side < 2; ++side) {
+    // The face nodes in the order the reference visits them: side, face, part,
+    // then the two in-face axes.  Each block is one (side, face, part) sheet.
+    struct Blk {
+        int side, axis, fixed;
+        Part P;
+        const int* L;
+        float Id;
+        long long nb, count, ord0, row0;  // nodes a row, nodes, first sequence number, first row
+    };
+    std::vector<Blk> blks;
+    long long nodes = 0, rows = 0;
+    const int org[3] = {c->ox, c->oy, c->oz};
+    const std::vector<float>* idv[2][3] = {{&c->h_idxh, &c->h_idyh, &c->h_idzh}, {&c->h_idxe, &c->h_idye, &c->h_idze}};
+    for (int side = 0; side < 2; ++side)
         for (int face = 0; face < 6; ++face) {
             if (!d->active[face]) continue;
             const int axis = face / 2;  // 0 x (back/front), 1 y (left/right), 2 z (down/up)
             for (int pi = 0; pi < 2; ++pi) {
-                const Part P = side == 0 ? eparts[face][pi] : hparts[face][pi];
-                const int* L = d->lim[face][P.comp];
-                const int fixed = L[0];
+                Blk k;
+                k.side = side;
+                k.axis = axis;
+                k.P = side == 0 ? eparts[face][pi] : hparts[face][pi];
+                k.L = d->lim[face][k.P.comp];
+                k.fixed = k.L[0];
                 // Id of the face: Idxh/Idyh/Idzh (E) or Idxe/Idye/Idze (H) at the fixed index
-                const std::vector<float>* idv[2][3] = {{&c->h_idxh, &c->h_idyh, &c->h_idzh}, {&c->h_idxe, &c->h_idye, &c->h_idze}};
-                const int org[3] = {c->ox, c->oy, c->oz};
-                const float Id = (*idv[side][axis])[fixed - org[axis]];
-                for (int a = L[1]; a <= L[2]; ++a)
-                    for (int b = L[3]; b <= L[4]; ++b) {
-                        int i, j, k;
-                        if (axis == 0) { i = fixed; k = a; j = b; }
-                        else if (axis == 1) { j = fixed; k = a; i = b; }
-                        else { k = fixed; j = a; i = b; }
-                        int si = i, sj = j, sk = k;
-                        if (axis == 0) si += P.off; else if (axis == 1) sj += P.off; else sk += P.off;
-                        // Incid: d = (x*px + y*py + z*pz) - d0 ; the kernel uses d/cluz
-                        const int fl = P.fld;
-                        const int ci[3] = {si, sj, sk};
-                        float xyz[3];
-                        for (int ax = 0; ax < 3; ++ax) {
-                            int q = ci[ax] - d->phys_lo[fl][ax];
-                            if (q < 0 || q >= d->phys_n[fl][ax]) return set_error(c, SGPU_ERR_ARG, "plane-wave node outside PhysCoor");
-                            xyz[ax] = d->phys[fl][ax][q];
-                        }
-                        const float dd = (xyz[0] * d->px + xyz[1] * d->py + xyz[2] * d->pz) - d->d0;
-                        const float a_node = dd / d->cluz;
-                        sgpu_ctx::HostSrcTable& T = c->src_tables[tab];
-                        T.amax[side] = T.has[side] ? std::max(T.amax[side], a_node) : a_node;
-                        T.has[side] = 1;
-                        if (c->zslab && (k < c->sweep[P.comp].zi || k > c->sweep[P.comp].ze)) continue;
-                        sgpu_ctx::HostEntry he;
-                        he.node = lin(c, i, j, k);
-                        he.comp = P.comp;
-                        he.order = c->src_seq++;
-                        he.e.comp = P.comp;
-                        he.e.type = kSrcPlaneWave;
-                        he.e.table = tab;
-                        he.e.a = a_node;
-                        he.e.b = d->fpw[fl];
-                        he.e.c = P.sign > 0 ? Id : -Id;
-                        c->src_host[side].push_back(he);
-                    }
+                k.Id = (*idv[side][axis])[k.fixed - org[axis]];
+                const long long na = std::max(0, k.L[2] - k.L[1] + 1);
+                k.nb = std::max(0, k.L[4] - k.L[3] + 1);
+                k.count = na * k.nb;
+                k.ord0 = nodes;
+                k.row0 = rows;
+                nodes += k.count;
+                rows += na;
+                blks.push_back(k);
             }
         }
+    // One node: its entry and its d/c (Incid: d = (x*px + y*py + z*pz) - d0,
+    // the kernel uses d/cluz); false when the node lies outside PhysCoor.
+    auto node_entry = [&](const Blk& k, int a, int b, sgpu_ctx::HostEntry& he, float& a_node, int& kk) {
+        int i, j, kz;
+        if (k.axis == 0) { i = k.fixed; kz = a; j = b; }
+        else if (k.axis == 1) { j = k.fixed; kz = a; i = b; }
+        else { kz = k.fixed; j = a; i = b; }
+        int si = i, sj = j, sk = kz;
+        if (k.axis == 0) si += k.P.off; else if (k.axis == 1) sj += k.P.off; else sk += k.P.off;
+        const int fl = k.P.fld;
+        const int ci[3] = {si, sj, sk};
+        float xyz[3];
+        for (int ax = 0; ax < 3; ++ax) {
+            const int q = ci[ax] - d->phys_lo[fl][ax];
+            if (q < 0 || q >= d->phys_n[fl][ax]) return false;
+            xyz[ax] = d->phys[fl][ax][q];
+        }
+        const float dd = (xyz[0] * d->px + xyz[1] * d->py + xyz[2] * d->pz) - d->d0;
+        a_node = dd / d->cluz;
+        kk = kz;
+        he.node = lin(c, i, j, kz);
+        he.comp = k.P.comp;
+        he.e.comp = k.P.comp;
+        he.e.type = kSrcPlaneWave;
+        he.e.table = tab;
+        he.e.a = a_node;
+        he.e.b = d->fpw[fl];
+        he.e.c = k.P.sign > 0 ? k.Id : -k.Id;
+        return true;
+    };
+    sgpu_ctx::HostSrcTable& T = c->src_tables[tab];
+    auto take_max = [&](int side, float v) {
+        T.amax[side] = T.has[side] ? std::max(T.amax[side], v) : v;
+        T.has[side] = 1;
+    };
+    if (c->zslab) {
+        // a z slab keeps only its own planes' entries (every node still counts
+        // for the switch-off): one pass in the reference's order
+        for (const Blk& k : blks)
+            for (int a = k.L[1]; a <= k.L[2]; ++a)
+                for (int b = k.L[3]; b <= k.L[4]; ++b) {
+                    sgpu_ctx::HostEntry he;
+                    float an;
+                    int kz;
+                    if (!node_entry(k, a, b, he, an, kz)) return set_error(c, SGPU_ERR_ARG, "plane-wave node outside PhysCoor");
+                    take_max(k.side, an);
+                    if (kz < c->sweep[k.P.comp].zi || kz > c->sweep[k.P.comp].ze) continue;
+                    he.order = c->src_seq++;
+                    c->src_host[k.side].push_back(he);
+                }
+    } else {
+        // every node has an entry: each sheet row is filled by a host thread at
+        // its place in the reference's order (the same sequence numbers as one
+        // pass), and the switch-off's largest d/c is a maximum, exact in any order
+        const int seq0 = c->src_seq;
+        std::vector<sgpu_ctx::HostEntry>& e0 = c->src_host[0];
+        std::vector<sgpu_ctx::HostEntry>& e1 = c->src_host[1];
+        const size_t b0 = e0.size(), b1 = e1.size();
+        long long n0 = 0, n1 = 0;
+        for (const Blk& k : blks) (k.side ? n1 : n0) += k.count;
+        e0.resize(b0 + (size_t)n0);
+        e1.resize(b1 + (size_t)n1);
+        std::vector<long long> base(blks.size());  // first slot of each block in its side's list
+        {
+            long long s0 = 0, s1 = 0;
+            for (size_t q = 0; q < blks.size(); ++q) {
+                long long& sv = blks[q].side ? s1 : s0;
+                base[q] = (long long)(blks[q].side ? b1 : b0) + sv;
+                sv += blks[q].count;
+            }
+        }
+        std::mutex mu;
+        bool bad = false;
+        host_parallel(rows, [&](long long r0, long long r1) {
+            float mx[2] = {0.0f, 0.0f};
+            bool has[2] = {false, false}, oob = false;
+            size_t q = (size_t)(std::upper_bound(blks.begin(), blks.end(), r0,
+                                                 [](long long r, const Blk& k) { return r < k.row0; }) - blks.begin()) - 1;
+            for (long long r = r0; r < r1 && !oob; ++r) {
+                while (q + 1 < blks.size() && r >= blks[q + 1].row0) ++q;
+                const Blk& k = blks[q];
+                const long long ra = r - k.row0;
+                const int a = k.L[1] + (int)ra;
+                std::vector<sgpu_ctx::HostEntry>& ev = k.side ? e1 : e0;
+                for (int b = k.L[3]; b <= k.L[4]; ++b) {
+                    const long long loc = ra * k.nb + (b - k.L[3]);
+                    sgpu_ctx::HostEntry& he = ev[(size_t)(base[q] + loc)];
+                    float an;
+                    int kz;
+                    if (!node_entry(k, a, b, he, an, kz)) {
+                        oob = true;
+                        break;
+                    }
+                    he.order = seq0 + (int)(k.ord0 + loc);
+                    mx[k.side] = has[k.side] ? std::max(mx[k.side], an) : an;
+                    has[k.side] = true;
+                }
+            }
+            std::lock_guard<std::mutex> g(mu);
+            bad = bad || oob;
+            for (int sd = 0; sd < 2; ++sd)
+                if (has[sd]) take_max(sd, mx[sd]);
+        }, 64);
+        if (bad) return set_error(c, SGPU_ERR_ARG, "plane-wave node outside PhysCoor");
+        c->src_seq = seq0 + (int)nodes;
     }
     c->src_dirty = true;
     return SGPU_OK;
