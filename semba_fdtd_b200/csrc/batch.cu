@@ -421,6 +421,7 @@ struct Slot {
     int start = 0;   // batch counter value at the instance's step 0
     int nsteps = 0;  // last step index advanced (steps 0..nsteps)
     int size_class = 0;
+    bool reserved = false;  // an instance is being set up for this slot
 };
 
 bool touches_any(const KCpml& cp, int c0, int x0, int x1, int y0, int y1, int z0, int z1) {
@@ -483,10 +484,11 @@ struct sgpu_batch {
     long long graph_wait = -1;
     int graph_drill = -1;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    // instances are set up on their own stream, so host set-up and uploads
-    // overlap the steps already queued; the batch stream waits on setup_done
-    cudaStream_t setup = nullptr;
-    cudaEvent_t setup_done = nullptr;
+    // Every entry point holds this lock while it reads or changes the slots,
+    // the step counter, the work lists or the graph.  An instance's set-up
+    // runs outside it, on a stream of its own, so several host threads can
+    // set up instances at once while the queued steps of the others run.
+    mutable std::mutex mu;
 };
 
 namespace sgpu {
@@ -802,13 +804,6 @@ sgpu_status sgpu_batch_create(uint64_t arena_bytes, int max_instances, sgpu_batc
     BTRY(b, cudaGetDevice(&b->device));
     cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, b->device);
     BTRY(b, cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
-    // instance set-up runs on a stream of the highest priority: its small
-    // kernels and copies (and the waits between them) go first whenever the
-    // persistent step kernels, which hold every SM, leave the device
-    int lo = 0, hi = 0;
-    cudaDeviceGetStreamPriorityRange(&lo, &hi);
-    BTRY(b, cudaStreamCreateWithPriority(&b->setup, cudaStreamNonBlocking, hi));
-    BTRY(b, cudaEventCreateWithFlags(&b->setup_done, cudaEventDisableTiming));
     void* base = nullptr;
     keep_device_pool(b->device);
     // the arena comes from the device's default memory pool, which keeps the
@@ -853,7 +848,6 @@ sgpu_status sgpu_batch_create(uint64_t arena_bytes, int max_instances, sgpu_batc
 
 void sgpu_batch_destroy(sgpu_batch* b) {
     if (!b) return;
-    if (b->setup) cudaStreamSynchronize(b->setup);
     if (b->stream) cudaStreamSynchronize(b->stream);
     for (Slot& s : b->slots)
         if (s.ctx) sgpu_destroy(s.ctx);
@@ -880,36 +874,73 @@ void sgpu_batch_destroy(sgpu_batch* b) {
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->stream) cudaStreamDestroy(b->stream);
-    if (b->setup) cudaStreamDestroy(b->setup);
-    if (b->setup_done) cudaEventDestroy(b->setup_done);
     delete b;
 }
 
 const char* sgpu_batch_last_error(const sgpu_batch* b) { return b ? b->err.c_str() : "null batch"; }
 
 sgpu_status sgpu_batch_add(sgpu_batch* b, const sgpu_problem* p, sgpu_ctx* plan, int nsteps, int* slot) {
-    if (!b || !slot || (!p && !plan) || nsteps < 0) return berr(b, SGPU_ERR_ARG, "bad sgpu_batch_add arguments");
+    if (!b) return SGPU_ERR_ARG;
+    if (!slot || (!p && !plan) || nsteps < 0) {
+        std::lock_guard<std::mutex> lock(b->mu);
+        return berr(b, SGPU_ERR_ARG, "bad sgpu_batch_add arguments");
+    }
     *slot = -1;
     int sl = -1;
-    for (int q = 0; q < b->max_slots; ++q)
-        if (!b->slots[q].ctx) {
-            sl = q;
-            break;
-        }
-    if (sl < 0) return berr(b, SGPU_ERR_OOM, "no free instance slot");
-    // set-up on the set-up stream: it touches only the new instance's arena
-    // memory, so the steps queued on the batch stream keep running; the
-    // batch stream then waits for it before anything reads the instance
+    {
+        std::lock_guard<std::mutex> lock(b->mu);
+        for (int q = 0; q < b->max_slots; ++q)
+            if (!b->slots[q].ctx && !b->slots[q].reserved) {
+                sl = q;
+                break;
+            }
+        if (sl < 0) return berr(b, SGPU_ERR_OOM, "no free instance slot");
+        b->slots[sl].reserved = true;
+    }
+    // Set-up outside the lock, on a stream of its own of the highest
+    // priority: it touches only the new instance's arena memory (the arena
+    // has its own lock), so the steps queued on the batch stream keep
+    // running and other threads may set up other instances meanwhile; the
+    // batch stream then waits for it before anything reads the instance.
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev = nullptr;
     sgpu_ctx* c = nullptr;
-    sgpu_status s = host_create_in(p, plan, nsteps, &b->arena, b->setup, &c);
+    sgpu_status s = SGPU_OK;
+    std::string msg;
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    if (cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, hi) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        s = SGPU_ERR_CUDA;
+        msg = "the set-up stream could not be created";
+    }
+    if (!s) s = host_create_in(p, plan, nsteps, &b->arena, st, &c);
     if (!s) s = rebuild_sources(c);
+    if (!s && cudaEventRecord(ev, st) != cudaSuccess) {
+        cudaGetLastError();
+        s = SGPU_ERR_CUDA;
+        msg = "the set-up could not be recorded";
+    }
+    if (s && msg.empty()) msg = c ? c->err : "instance set-up failed";
+    auto release = [&]() {
+        if (ev) cudaEventDestroy(ev);
+        if (st) cudaStreamDestroy(st);  // released once its work is done
+    };
+    std::lock_guard<std::mutex> lock(b->mu);
+    b->slots[sl].reserved = false;
+    if (!s && cudaStreamWaitEvent(b->stream, ev, 0) != cudaSuccess) {
+        cudaGetLastError();
+        s = SGPU_ERR_CUDA;
+        msg = "the batch stream could not wait for the set-up";
+    }
     if (s) {
-        b->err = c ? c->err : "instance set-up failed";
+        b->err = msg;
         if (c) sgpu_destroy(c);
+        release();
         return s;
     }
-    BTRY(b, cudaEventRecord(b->setup_done, b->setup));
-    BTRY(b, cudaStreamWaitEvent(b->stream, b->setup_done, 0));
+    release();
     c->stream = b->stream;
     Slot& S = b->slots[sl];
     S.ctx = c;
@@ -927,6 +958,8 @@ sgpu_status sgpu_batch_add(sgpu_batch* b, const sgpu_problem* p, sgpu_ctx* plan,
 }
 
 sgpu_status sgpu_batch_remove(sgpu_batch* b, int slot) {
+    if (!b) return SGPU_ERR_ARG;
+    std::lock_guard<std::mutex> lock(b->mu);
     if (!valid_slot(b, slot)) return berr(b, SGPU_ERR_ARG, "no instance in that slot");
     BTRY(b, cudaStreamSynchronize(b->stream));
     InstDesc off{};
@@ -941,17 +974,23 @@ sgpu_status sgpu_batch_remove(sgpu_batch* b, int slot) {
 }
 
 sgpu_status sgpu_batch_advance(sgpu_batch* b, int nsteps) {
+    if (!b) return SGPU_ERR_ARG;
+    std::lock_guard<std::mutex> lock(b->mu);
     if (!b || nsteps < 0) return SGPU_ERR_ARG;
     return advance(b, nsteps, true);
 }
 
 sgpu_status sgpu_batch_synchronize(sgpu_batch* b) {
     if (!b) return SGPU_ERR_ARG;
+    std::lock_guard<std::mutex> lock(b->mu);
+    if (!b) return SGPU_ERR_ARG;
     BTRY(b, cudaStreamSynchronize(b->stream));
     return check_err(b);
 }
 
 sgpu_status sgpu_batch_set_wait_cycles(sgpu_batch* b, int64_t cycles) {
+    if (!b) return SGPU_ERR_ARG;
+    std::lock_guard<std::mutex> lock(b->mu);
     if (!b || cycles < 0) return SGPU_ERR_ARG;
     b->wait_cycles = cycles;
     return SGPU_OK;
@@ -959,17 +998,23 @@ sgpu_status sgpu_batch_set_wait_cycles(sgpu_batch* b, int64_t cycles) {
 
 sgpu_status sgpu_batch_set_wait_drill(sgpu_batch* b, int on) {
     if (!b) return SGPU_ERR_ARG;
+    std::lock_guard<std::mutex> lock(b->mu);
+    if (!b) return SGPU_ERR_ARG;
     b->wait_drill = on ? 1 : 0;
     return SGPU_OK;
 }
 
 sgpu_status sgpu_batch_set_kernel_family(sgpu_batch* b, int family) {
+    if (!b) return SGPU_ERR_ARG;
+    std::lock_guard<std::mutex> lock(b->mu);
     if (!b || family < 0 || family > 1) return SGPU_ERR_ARG;
     b->family = family;
     return SGPU_OK;
 }
 
 sgpu_status sgpu_batch_elapsed(sgpu_batch* b, int nsteps, float* ms) {
+    if (!b) return SGPU_ERR_ARG;
+    std::lock_guard<std::mutex> lock(b->mu);
     if (!b || !ms || nsteps < 0) return SGPU_ERR_ARG;
     sgpu_status s;
     drop_finished(b);
@@ -984,6 +1029,8 @@ sgpu_status sgpu_batch_elapsed(sgpu_batch* b, int nsteps, float* ms) {
 }
 
 sgpu_status sgpu_batch_slot_info(const sgpu_batch* b, int slot, int* steps_done, int* steps_total, int* nprobes) {
+    if (!b) return SGPU_ERR_ARG;
+    std::lock_guard<std::mutex> lock(b->mu);
     if (!valid_slot(b, slot)) return SGPU_ERR_ARG;
     const Slot& S = b->slots[slot];
     const int done = std::min(std::max(b->G - S.start, 0), S.nsteps + 1);
@@ -994,6 +1041,8 @@ sgpu_status sgpu_batch_slot_info(const sgpu_batch* b, int slot, int* steps_done,
 }
 
 sgpu_status sgpu_batch_read_probes(sgpu_batch* b, int slot, float* out, int max_rows, int* rows) {
+    if (!b) return SGPU_ERR_ARG;
+    std::lock_guard<std::mutex> lock(b->mu);
     if (!valid_slot(b, slot) || !rows) return berr(b, SGPU_ERR_ARG, "bad probe read");
     const Slot& S = b->slots[slot];
     const int done = std::min(std::max(b->G - S.start, 0), S.nsteps + 1);
@@ -1007,6 +1056,8 @@ sgpu_status sgpu_batch_read_probes(sgpu_batch* b, int slot, float* out, int max_
 }
 
 sgpu_status sgpu_batch_instance(sgpu_batch* b, int slot, sgpu_ctx** ctx) {
+    if (!b) return SGPU_ERR_ARG;
+    std::lock_guard<std::mutex> lock(b->mu);
     if (!valid_slot(b, slot) || !ctx) return SGPU_ERR_ARG;
     BTRY(b, cudaStreamSynchronize(b->stream));
     *ctx = b->slots[slot].ctx;
@@ -1026,6 +1077,8 @@ sgpu_status sgpu_batch_memory(sgpu_batch* b, uint64_t* capacity, uint64_t* in_us
 
 sgpu_status sgpu_batch_set_tuning(sgpu_batch* b, const int* chunk3, int ctas_per_sm) {
     if (!b) return SGPU_ERR_ARG;
+    std::lock_guard<std::mutex> lock(b->mu);
+    if (!b) return SGPU_ERR_ARG;
     if (chunk3)
         for (int q = 0; q < kNumClasses; ++q) {
             if (chunk3[q] < 1 || chunk3[q] > 1024) return berr(b, SGPU_ERR_ARG, "z chunk out of range (1..1024)");
@@ -1041,6 +1094,8 @@ sgpu_status sgpu_batch_set_tuning(sgpu_batch* b, const int* chunk3, int ctas_per
 
 sgpu_status sgpu_batch_get_tuning(const sgpu_batch* b, int* chunk3, int* ctas_per_sm) {
     if (!b) return SGPU_ERR_ARG;
+    std::lock_guard<std::mutex> lock(b->mu);
+    if (!b) return SGPU_ERR_ARG;
     if (chunk3)
         for (int q = 0; q < kNumClasses; ++q) chunk3[q] = b->chunk[q];
     if (ctas_per_sm) *ctas_per_sm = b->ctas_per_sm;
@@ -1052,6 +1107,8 @@ sgpu_status sgpu_batch_get_tuning(const sgpu_batch* b, int* chunk3, int* ctas_pe
 // persistent grid size is chosen first, then each size class's z chunk by
 // coordinate descent.
 sgpu_status sgpu_batch_autotune(sgpu_batch* b, int steps_per_trial, int* chunk3, int* ctas_per_sm) {
+    if (!b) return SGPU_ERR_ARG;
+    std::lock_guard<std::mutex> lock(b->mu);
     if (!b || steps_per_trial < 1) return SGPU_ERR_ARG;
     sgpu_status s;
     auto trial = [&](float* ms) -> sgpu_status {
@@ -1110,6 +1167,8 @@ sgpu_status sgpu_batch_autotune(sgpu_batch* b, int steps_per_trial, int* chunk3,
 // (ms6: E field, ADE, E sources, H field, H sources + borders, probes + counter).
 // The steps are real steps of the live instances.
 sgpu_status sgpu_batch_profile_steps(sgpu_batch* b, int nsteps, float* ms6) {
+    if (!b) return SGPU_ERR_ARG;
+    std::lock_guard<std::mutex> lock(b->mu);
     if (!b || !ms6 || nsteps < 0) return SGPU_ERR_ARG;
     sgpu_status s = SGPU_OK;
     drop_finished(b);
@@ -1138,6 +1197,8 @@ sgpu_status sgpu_batch_profile_steps(sgpu_batch* b, int nsteps, float* ms6) {
 }
 
 sgpu_status sgpu_batch_steps(const sgpu_batch* b, int* counter) {
+    if (!b) return SGPU_ERR_ARG;
+    std::lock_guard<std::mutex> lock(b->mu);
     if (!b || !counter) return SGPU_ERR_ARG;
     *counter = b->G;
     return SGPU_OK;

@@ -438,17 +438,18 @@ using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, 
                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
 EncodeTiled encoder() {
-    static EncodeTiled fn = nullptr;
-    static bool tried = false;
-    if (!tried) {
-        tried = true;
+    // looked up once; a function-local static is initialised once even when
+    // several host threads set up contexts at the same time
+    static const EncodeTiled fn = []() -> EncodeTiled {
         void* p = nullptr;
         cudaDriverEntryPointQueryResult q{};
+        EncodeTiled f = nullptr;
         if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
-            fn = (EncodeTiled)p;
+            f = (EncodeTiled)p;
         cudaGetLastError();
-    }
+        return f;
+    }();
     return fn;
 }
 

@@ -61,6 +61,24 @@ def test_batch_equals_solo_runs(family):
         _check(b, slots, pbs)
 
 
+def test_instances_set_up_by_several_threads():
+    """Instances added from four host threads at once, while steps of the
+    first one are queued, give the same bits as their solo runs."""
+    from concurrent.futures import ThreadPoolExecutor
+    pbs = _instances()
+    with Batch(1 << 30, 16) as b:
+        first = b.add(pbs[0])
+        b.advance(11)
+        with ThreadPoolExecutor(4) as pool:
+            futs = [pool.submit(b.add, Plan(pb)) for pb in pbs[1:]]
+            b.advance(5)
+            rest = [f.result() for f in futs]
+        slots = [first] + rest
+        assert len(set(slots)) == len(slots)
+        b.run_all()
+        _check(b, slots, pbs)
+
+
 def test_join_while_running_and_arena_reuse():
     pbs = _instances()
     with Batch(1 << 30, 16) as b:
