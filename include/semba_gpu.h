@@ -530,7 +530,10 @@ const char* sgpu_batch_last_error(const sgpu_batch* b);
 /* Set up a problem inside the arena: from `p`, or from `plan` (a host-only
  * context of sgpu_host_plan, consumed: destroy it afterwards as usual).  The
  * instance runs steps 0..nsteps and keeps every probe row on the device.
- * SGPU_ERR_OOM when the arena has no room (nothing is left allocated). */
+ * SGPU_ERR_OOM when the arena has no room (nothing is left allocated).
+ * Several host threads may add instances to one batch at once (the set-up
+ * of each runs on a stream of its own while the batch's queued steps run);
+ * the other batch entry points take the batch's lock. */
 sgpu_status sgpu_batch_add(sgpu_batch* b, const sgpu_problem* p, sgpu_ctx* plan, int nsteps, int* slot);
 /* Free an instance's arena memory and slot (waits for queued work). */
 sgpu_status sgpu_batch_remove(sgpu_batch* b, int slot);
